@@ -1,0 +1,971 @@
+// api.cu -- the C ABI (include/dba.h): context lifetime, initial conditions,
+// the per-step launch sequence (captured into CUDA graphs), readback,
+// observables and checkpoints.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/dba.h"
+#include "fpmath.h"
+#include "launch.h"
+
+using namespace dba;
+
+namespace {
+
+constexpr int kGraphSteps = 48;   // steps per captured graph (multiple of 6)
+
+struct Alloc {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct dba_ctx {
+    dba_config cfg;
+    int D = 2, B = 4, esz = 8, nch = 1, nstate = 0, nsum = 0;
+    GridP g{};
+    size_t n = 0;
+    int device = 0, sms = 148, grid = 148;
+    cudaStream_t st = nullptr;
+    std::vector<Alloc> allocs;        // every device allocation (checkpointed in order)
+    void* state[4][2] = {};           // ping-pong state fields (dendrite p,T; Model B x,y,z) / KH U in [q][0]
+    void* aux[32] = {};               // Model B mu[3]; KH W[4] Gd[8] Wp[4] Fl[8]
+    uint8_t* par = nullptr;           // [2][nch][nb]
+    uint8_t* wake = nullptr;          // [3][nch][nb]
+    uint8_t* next = nullptr;          // [nch][nb]
+    double* bsum = nullptr;           // [nsum][nb]
+    double* l1 = nullptr;             // [nsum][J]
+    double* avg = nullptr;            // [nsum]
+    unsigned int* ticket = nullptr;
+    int* status = nullptr;
+    unsigned long long* stats = nullptr;   // [4]
+    int* list = nullptr;              // KH active list
+    int* count = nullptr;             // KH list length
+    double* staging = nullptr;        // n doubles
+    double* host_staging = nullptr;   // pinned n doubles
+    long step = 0;
+    double time = 0.0;
+    bool initialized = false;
+    cudaGraphExec_t graphs[6][2] = {};
+    bool use_graphs = true;
+    int last_error = DBA_OK;
+};
+
+namespace {
+
+int cuda_status(cudaError_t e) { return e == cudaSuccess ? DBA_OK : (e == cudaErrorMemoryAllocation ? DBA_ERR_NOMEM : DBA_ERR_CUDA); }
+
+#define DBA_TRY(call)                          \
+    do {                                       \
+        cudaError_t e_ = (call);               \
+        if (e_ != cudaSuccess) return cuda_status(e_); \
+    } while (0)
+
+void* dev_alloc(dba_ctx* c, size_t bytes, int* err)
+{
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        *err = cuda_status(e);
+        return nullptr;
+    }
+    cudaMemset(p, 0, bytes);
+    c->allocs.push_back({p, bytes});
+    return p;
+}
+
+int nfields_of(int model) { return model == DBA_MODEL_DENDRITE ? 2 : (model == DBA_MODEL_MODELB ? 7 : 8); }
+
+GridP make_grid(const dba_config& c, int B)
+{
+    GridP g;
+    g.nx = c.nx; g.ny = c.ny; g.nz = c.nz;
+    g.nbx = c.nx / B; g.nby = c.ny / B; g.nbz = c.nz == 1 ? 1 : c.nz / B;
+    g.nb = g.nbx * g.nby * g.nbz;
+    g.bc = c.bc;
+    return g;
+}
+
+FlagP flags_for(dba_ctx* c, long s)
+{
+    const size_t L = (size_t)c->nch * c->g.nb;
+    FlagP f;
+    f.par_cur = c->par + (s % 2) * L;
+    f.par_nxt = c->par + ((s + 1) % 2) * L;
+    f.wake_cur = c->wake + (s % 3) * L;
+    f.wake_nxt = c->wake + ((s + 1) % 3) * L;
+    f.wake_clr = c->wake + ((s + 2) % 3) * L;
+    f.next = c->next;
+    f.bsum = c->bsum;
+    f.status = c->status;
+    f.stats = c->stats;
+    return f;
+}
+
+// current-buffer parity / next-step wake flags after `step` completed steps
+const uint8_t* cur_par(dba_ctx* c) { return c->par + ((c->step + 1) % 2) * (size_t)c->nch * c->g.nb; }
+const uint8_t* next_wake(dba_ctx* c) { return c->wake + ((c->step + 1) % 3) * (size_t)c->nch * c->g.nb; }
+
+template <typename R>
+DenP<R> den_params(dba_ctx* c)
+{
+    const dba_config& k = c->cfg;
+    DenP<R> P;
+    P.p[0] = (R*)c->state[0][0]; P.p[1] = (R*)c->state[0][1];
+    P.T[0] = (R*)c->state[1][0]; P.T[1] = (R*)c->state[1][1];
+    const double Pi = 3.14159;   // example_Dendritic_growth/kernel.cu:7
+    P.f0 = 1. / (2 * k.dx);
+    P.f1 = 1. / k.dx / k.dx;
+    P.f2 = -k.alpha / Pi;
+    P.f3 = 1. / k.tau;
+    P.dt = k.dt; P.delta = k.delta; P.eps2 = k.epsilon * k.epsilon; P.gamma = k.gamma;
+    P.thr_p = k.metric_p; P.thr_p_hi = 1.0 - k.metric_p; P.thr_T = k.metric_T;
+    return P;
+}
+
+template <typename R>
+MBP<R> mb_params(dba_ctx* c, bool dba_mode)
+{
+    const dba_config& k = c->cfg;
+    MBP<R> P;
+    for (int q = 0; q < 2; ++q) {
+        P.x[q] = (R*)c->state[0][q]; P.y[q] = (R*)c->state[1][q]; P.z[q] = (R*)c->state[2][q];
+    }
+    for (int q = 0; q < 3; ++q) P.mu[q] = (R*)c->aux[q];
+    P.inv_dx2 = 1.0 / (k.dx * k.dx);
+    P.c0x = -1.0 + 1.0 / k.rx; P.c0y = -1.0 + 1.0 / k.ry; P.c0z = -1.0 + 1.0 / k.rz;
+    P.rx = k.rx; P.ry = k.ry; P.rz = k.rz;
+    P.chi_xy = k.chi_xy; P.chi_xz = k.chi_xz; P.chi_yz = k.chi_yz;
+    P.chi_xb = k.chi_xb; P.chi_yb = k.chi_yb; P.chi_zb = k.chi_zb;
+    P.ex = k.eps_x; P.ey = k.eps_y; P.ez = k.eps_z;
+    const double phi = 0.0;   // phi stays 0 in the reference (kernel.cu:231)
+    P.phi_term = k.p_gel * phi * phi / 2.0 / (1.0 - k.z_crit);
+    P.logK_rz = (c->esz == 8 ? dba_log(k.K) : (double)logf((float)k.K)) / k.rz;
+    P.nvx = (double)(k.n * k.vx); P.mvy = (double)(k.m * k.vy); P.dvz = (double)k.vz;
+    P.dtvx = k.dt * k.vx; P.dtvy = k.dt * k.vy; P.dtvz = k.dt * k.vz;
+    P.dn = k.n; P.dm = k.m;
+    P.Mx = k.mob_x; P.My = k.mob_y; P.Mz = k.mob_z; P.k0 = k.k_0;
+    P.thr = k.metric_eps;
+    P.conserved = (k.conserved && dba_mode) ? 1 : 0;
+    return P;
+}
+
+template <typename R>
+KHP<R> kh_params(dba_ctx* c, bool dba_mode)
+{
+    const dba_config& k = c->cfg;
+    KHP<R> P;
+    for (int q = 0; q < 4; ++q) P.U[q] = (R*)c->state[q][0];
+    for (int q = 0; q < 4; ++q) P.W[q] = (R*)c->aux[q];
+    for (int q = 0; q < 8; ++q) P.Gd[q] = (R*)c->aux[4 + q];
+    for (int q = 0; q < 4; ++q) P.Wp[q] = (R*)c->aux[12 + q];
+    for (int q = 0; q < 8; ++q) P.Fl[q] = (R*)c->aux[16 + q];
+    P.dt = k.dt; P.dx = k.dx; P.dy = k.dy; P.vol = k.dx * k.dy; P.gamma = k.kh_gamma; P.thr = k.metric_eps;
+    P.conserved = (k.conserved && dba_mode) ? 1 : 0;
+    P.list = c->list;
+    P.count = c->count;
+    return P;
+}
+
+template <typename R>
+CorrP<R> corr_params(dba_ctx* c, long s)
+{
+    CorrP<R> P;
+    std::memset(&P, 0, sizeof P);
+    P.avg = c->avg;
+    P.B = c->B;
+    P.D = c->D;
+    if (c->cfg.model == DBA_MODEL_MODELB) {
+        for (int q = 0; q < 3; ++q) {
+            P.f[q][0] = (R*)c->state[q][0];
+            P.f[q][1] = (R*)c->state[q][1];
+            P.map[q] = q;
+        }
+        P.nq = 3;
+        P.par = c->par + ((s + 1) % 2) * (size_t)c->nch * c->g.nb;   // after step s
+    } else {
+        for (int q = 0; q < 4; ++q) {
+            P.f[q][0] = (R*)c->state[q][0];
+            P.f[q][1] = (R*)c->state[q][0];
+        }
+        // sums are Mass, Energy, Momx, Momy; fields are Mass, Momx, Momy, Energy
+        P.map[0] = 0; P.map[1] = 3; P.map[2] = 1; P.map[3] = 2;
+        P.nq = 4;
+        P.par = nullptr;
+    }
+    return P;
+}
+
+template <typename R>
+cudaError_t enqueue_step_t(dba_ctx* c, long s, bool dba_mode)
+{
+    FlagP f = flags_for(c, s);
+    cudaError_t e = cudaSuccess;
+    switch (c->cfg.model) {
+    case DBA_MODEL_DENDRITE:
+        return launch_dendrite<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<R>(c));
+    case DBA_MODEL_MODELB: {
+        MBP<R> P = mb_params<R>(c, dba_mode);
+        e = launch_modelb<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P);
+        if (e != cudaSuccess || !P.conserved) return e;
+        break;
+    }
+    case DBA_MODEL_KH: {
+        KHP<R> P = kh_params<R>(c, dba_mode);
+        e = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
+        if (e != cudaSuccess) return e;
+        e = launch_kh<R>(c->B, dba_mode, c->grid, c->st, c->g, f, P);
+        if (e != cudaSuccess || !P.conserved) return e;
+        break;
+    }
+    default:
+        return cudaErrorInvalidValue;
+    }
+    // conserved DBA: global mean change (fixed tree order) and its correction
+    e = launch_reduce(c->st, c->bsum, c->g.nb, c->nsum, c->l1, c->ticket, c->avg, (double)c->n);
+    if (e != cudaSuccess) return e;
+    return launch_correct<R>(c->grid, c->st, c->g, corr_params<R>(c, s));
+}
+
+cudaError_t enqueue_step(dba_ctx* c, long s, bool dba_mode)
+{
+    return c->esz == 8 ? enqueue_step_t<double>(c, s, dba_mode) : enqueue_step_t<float>(c, s, dba_mode);
+}
+
+int validate(const dba_config* k)
+{
+    if (!k) return DBA_ERR_ARG;
+    if (k->model < 0 || k->model > 2) return DBA_ERR_CONFIG;
+    if (k->nx < 1 || k->ny < 1 || k->nz < 1) return DBA_ERR_CONFIG;
+    int B = k->block;
+    if (B < 2) return DBA_ERR_CONFIG;
+    if (k->nx % B || k->ny % B || (k->nz > 1 && k->nz % B)) return DBA_ERR_CONFIG;
+    if (k->nx < 4 || k->ny < 4 || (k->nz > 1 && k->nz < 4)) return DBA_ERR_CONFIG;
+    if (k->model == DBA_MODEL_KH && k->nz != 1) return DBA_ERR_CONFIG;
+    if (k->model != DBA_MODEL_DENDRITE && k->bc != DBA_BC_PERIODIC) return DBA_ERR_CONFIG;
+    if (k->precision != DBA_PREC_F64 && k->precision != DBA_PREC_F32) return DBA_ERR_CONFIG;
+    if (k->dt <= 0 || k->dx <= 0) return DBA_ERR_CONFIG;
+    size_t nb = (size_t)(k->nx / B) * (k->ny / B) * (k->nz == 1 ? 1 : k->nz / B);
+    if (nb > (size_t)1024 * 1024) return DBA_ERR_CONFIG;
+    int D = k->nz == 1 ? 2 : 3;
+    bool ok = k->precision == DBA_PREC_F64 ? shape_supported<double>(k->model, D, B) : shape_supported<float>(k->model, D, B);
+    return ok ? DBA_OK : DBA_ERR_CONFIG;
+}
+
+// ---- host initial conditions (FP64) ----
+void ic_dendrite(const dba_config& k, std::vector<double>& out)
+{
+    size_t n = (size_t)k.nx * k.ny * k.nz;
+    out.assign(2 * n, 0.0);
+    double* p = out.data();
+    double* T = out.data() + n;
+    for (int z = 0; z < k.nz; ++z)
+        for (int y = 0; y < k.ny; ++y)
+            for (int x = 0; x < k.nx; ++x) {
+                size_t i = (size_t)x + (size_t)k.nx * ((size_t)y + (size_t)k.ny * z);
+                if (k.ic == DBA_IC_TANH_SEED) {
+                    double cx = k.ic_corner ? 0.0 : k.nx / 2, cy = k.ic_corner ? 0.0 : k.ny / 2;
+                    double cz = k.ic_corner ? 0.0 : k.nz / 2;
+                    double r = std::sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy) + (k.nz > 1 ? (z - cz) * (z - cz) : 0.0));
+                    p[i] = 0.5 * (1.0 - std::tanh((r - k.ic_radius) / k.ic_width));
+                } else {   // reference cone seed (example_Dendritic_growth/kernel.cu:170-174)
+                    int dx = x - k.nx / 2, dy = y - k.ny / 2, dz = z - k.nz / 2;
+                    double dist = std::sqrt((double)(dx * dx + dy * dy + dz * dz));
+                    p[i] = dist <= 5 ? (1. - 0.2 * dist) : 0;
+                }
+                T[i] = -k.Delta;
+            }
+}
+
+void ic_modelb(const dba_config& k, std::vector<double>& out)
+{
+    // mt19937_64 draws x, y, z interleaved per cell as the reference CPU program
+    // (example_Reactive_ModelB/CPU_version/base_CPU.cpp:540-549), then
+    // Initialize (example_Reactive_ModelB/kernel.cu:209-211)
+    size_t n = (size_t)k.nx * k.ny * k.nz;
+    out.assign(3 * n, 0.0);
+    std::mt19937_64 rng(k.seed);
+    std::uniform_real_distribution<double> u(0.0, 1.0);
+    for (size_t i = 0; i < n; ++i) {
+        double ux = u(rng), uy = u(rng), uz = u(rng);
+        out[i] = k.x0 + k.noise_amp * (ux - 0.5);
+        out[n + i] = k.y0 + k.noise_amp * (uy - 0.5);
+        out[2 * n + i] = k.z0 + k.noise_amp_z * (uz - 0.5);
+    }
+}
+
+void ic_kh(const dba_config& k, std::vector<double>& out)
+{
+    size_t n = (size_t)k.nx * k.ny;
+    out.assign(4 * n, 0.0);
+    double *rho = out.data(), *p = out.data() + n, *vx = out.data() + 2 * n, *vy = out.data() + 3 * n;
+    const int Nx = k.nx, Ny = k.ny;
+    std::mt19937_64 rng(k.seed);
+    std::normal_distribution<double> gauss(0.0, 1.0);
+    for (int Y = 0; Y < Ny; ++Y)
+        for (int X = 0; X < Nx; ++X) {
+            size_t i = (size_t)X + (size_t)Nx * Y;
+            p[i] = 2.5;
+            if (k.ic == DBA_IC_SHARP_BANDS) {
+                double ys = (Y + 0.5) / Ny;
+                bool band = std::fabs(ys - 0.5) < 0.25;
+                rho[i] = band ? 2.0 : 1.0;
+                vx[i] = band ? 0.5 : -0.5;
+                vy[i] = 0.01 * std::sin(4.0 * M_PI * (X + 0.5) / Nx);
+            } else {   // smooth interface (example_Kelvin_Helmholtz/KH_DBA.cu:1102-1125)
+                double rho1 = 1.0, rho2 = 2.0, rho_m = 0.5 * (rho1 - rho2);
+                double vx1 = 0.5, vx2 = -0.5, vx_m = 0.5 * (vx1 - vx2);
+                if (Y >= 0 && Y < Ny / 4) {
+                    rho[i] = rho1 - rho_m * std::exp((1.0 * Y / Ny - 0.25) / 0.025);
+                    vx[i] = vx1 - vx_m * std::exp((1.0 * Y / Ny - 0.25) / 0.025);
+                } else if (Y >= Ny / 4 && Y < Ny / 2) {
+                    rho[i] = rho2 + rho_m * std::exp((-1.0 * Y / Ny + 0.25) / 0.025);
+                    vx[i] = vx2 + vx_m * std::exp((-1.0 * Y / Ny + 0.25) / 0.025);
+                } else if (Y >= Ny / 2 && Y < 3 * Ny / 4) {
+                    rho[i] = rho2 + rho_m * std::exp((1.0 * Y / Ny - 0.75) / 0.025);
+                    vx[i] = vx2 + vx_m * std::exp((1.0 * Y / Ny - 0.75) / 0.025);
+                } else {
+                    rho[i] = rho1 - rho_m * std::exp((-1.0 * Y / Ny + 0.75) / 0.025);
+                    vx[i] = vx1 - vx_m * std::exp((-1.0 * Y / Ny + 0.75) / 0.025);
+                }
+                vy[i] = 0.01 * std::sin(4.0 * M_PI * X / Nx);
+            }
+        }
+    if (k.ic == DBA_IC_SHARP_BANDS)
+        for (size_t i = 0; i < n; ++i) vy[i] += k.noise_amp * gauss(rng);
+}
+
+template <typename R>
+int upload(dba_ctx* c, void* dst, const double* src, size_t n)
+{
+    if (sizeof(R) == 8) return cuda_status(cudaMemcpy(dst, src, n * 8, cudaMemcpyHostToDevice));
+    std::vector<float> tmp(n);
+    for (size_t i = 0; i < n; ++i) tmp[i] = (float)src[i];
+    return cuda_status(cudaMemcpy(dst, tmp.data(), n * 4, cudaMemcpyHostToDevice));
+}
+
+int upload_any(dba_ctx* c, void* dst, const double* src, size_t n)
+{
+    return c->esz == 8 ? upload<double>(c, dst, src, n) : upload<float>(c, dst, src, n);
+}
+
+int gather(dba_ctx* c, const void* b0, const void* b1, const uint8_t* par, size_t start, size_t stride, size_t count,
+           double* host)
+{
+    cudaError_t e = c->esz == 8
+                        ? launch_gather<double>(c->st, c->g, c->B, c->D, (const double*)b0, (const double*)b1, par, start, stride, count, c->staging)
+                        : launch_gather<float>(c->st, c->g, c->B, c->D, (const float*)b0, (const float*)b1, par, start, stride, count, c->staging);
+    if (e != cudaSuccess) return cuda_status(e);
+    e = cudaMemcpyAsync(host, c->staging, count * sizeof(double), cudaMemcpyDeviceToHost, c->st);
+    if (e != cudaSuccess) return cuda_status(e);
+    return cuda_status(cudaStreamSynchronize(c->st));
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* dba_strerror(int s)
+{
+    switch (s) {
+    case DBA_OK: return "ok";
+    case DBA_ERR_CONFIG: return "invalid or unsupported configuration";
+    case DBA_ERR_CUDA: return "CUDA runtime error";
+    case DBA_ERR_NOMEM: return "out of memory";
+    case DBA_ERR_IO: return "file could not be opened or parsed";
+    case DBA_ERR_NONFINITE: return "non-finite value in a state field";
+    case DBA_ERR_TIMEOUT: return "bounded device wait timed out";
+    case DBA_ERR_STATE: return "call out of order";
+    case DBA_ERR_ARG: return "bad argument";
+    default: return "unknown status";
+    }
+}
+
+size_t dba_struct_size(int which)
+{
+    return which == 0 ? sizeof(dba_config) : (which == 1 ? sizeof(dba_obs) : (which == 2 ? sizeof(dba_info) : sizeof(dba_prof)));
+}
+
+int dba_config_default(int model, dba_config* k)
+{
+    if (!k) return DBA_ERR_ARG;
+    std::memset(k, 0, sizeof *k);
+    k->model = model;
+    k->mode = DBA_MODE_DBA;
+    k->precision = DBA_PREC_F64;
+    k->bc = DBA_BC_PERIODIC;
+    k->ic = DBA_IC_REFERENCE;
+    k->seed = 1234ULL;
+    k->noise_amp = 0.05;
+    k->noise_amp_z = 0.001;
+    k->kh_gamma = 5.0 / 3.0;
+    k->ic_radius = 10.0;
+    k->ic_width = 2.0;
+    switch (model) {
+    case DBA_MODEL_DENDRITE:   // example_Dendritic_growth/Input.txt
+        k->nx = k->ny = k->nz = 256;
+        k->t_total = 20000; k->t_freq = 1000; k->dt = 0.00005;
+        k->dx = k->dy = k->dz = 0.02;
+        k->delta = 0.5; k->tau = 0.0003; k->epsilon = 0.01; k->alpha = 0.9; k->gamma = 40.;
+        k->Delta = 0.25; k->metric_p = 0.01; k->metric_T = 1e-5;
+        k->block = 4;
+        break;
+    case DBA_MODEL_MODELB:     // example_Reactive_ModelB/Input.txt
+        k->nx = k->ny = k->nz = 256;
+        k->t_total = 100000; k->t_freq = 5000; k->dt = 0.0005;
+        k->dx = k->dy = k->dz = 1;
+        k->chi_zb = 4;
+        k->vx = 1; k->vy = 1; k->vz = 2; k->rx = 1; k->ry = 1; k->rz = 2; k->n = 1; k->m = 1;
+        k->eps_x = k->eps_y = k->eps_z = 4; k->eps_phi = 0.01;
+        k->mob_x = k->mob_y = k->mob_z = k->mob_phi = 1;
+        k->x0 = 0.2; k->y0 = 0.2; k->z0 = 0.01;
+        k->K = 100; k->z_crit = 0.4; k->p_gel = 1; k->k_0 = 1; k->metric_eps = 1e-6;
+        k->block = 4;
+        break;
+    case DBA_MODEL_KH:         // example_Kelvin_Helmholtz/Input.txt
+        k->nx = k->ny = 512; k->nz = 1;
+        k->t_total = 20000; k->t_freq = 2000; k->dt = 0.0002;
+        k->dx = k->dy = k->dz = 0.002;
+        k->metric_eps = 0;
+        k->block = 8;
+        break;
+    default:
+        return DBA_ERR_CONFIG;
+    }
+    return DBA_OK;
+}
+
+int dba_create(const dba_config* cfg, dba_ctx** out)
+{
+    if (!out) return DBA_ERR_ARG;
+    *out = nullptr;
+    int st = validate(cfg);
+    if (st) return st;
+    dba_ctx* c = new (std::nothrow) dba_ctx();
+    if (!c) return DBA_ERR_NOMEM;
+    c->cfg = *cfg;
+    if (c->cfg.dy == 0) c->cfg.dy = c->cfg.dx;
+    if (c->cfg.dz == 0) c->cfg.dz = c->cfg.dx;
+    c->B = cfg->block;
+    c->D = cfg->nz == 1 ? 2 : 3;
+    c->esz = cfg->precision == DBA_PREC_F64 ? 8 : 4;
+    c->g = make_grid(c->cfg, c->B);
+    c->n = (size_t)cfg->nx * cfg->ny * cfg->nz;
+    c->nch = cfg->model == DBA_MODEL_DENDRITE ? 2 : 1;
+    c->nstate = cfg->model == DBA_MODEL_DENDRITE ? 2 : (cfg->model == DBA_MODEL_MODELB ? 3 : 4);
+    c->nsum = cfg->model == DBA_MODEL_MODELB ? 3 : (cfg->model == DBA_MODEL_KH ? 4 : 0);
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return cuda_status(e);
+    }
+    int err = DBA_OK;
+    const size_t fb = c->n * c->esz;
+    const size_t nb = c->g.nb;
+    if (cfg->model == DBA_MODEL_KH) {
+        for (int q = 0; q < 4 && !err; ++q) c->state[q][0] = dev_alloc(c, fb, &err);
+        for (int q = 0; q < 24 && !err; ++q) c->aux[q] = dev_alloc(c, fb, &err);
+        if (!err) c->list = (int*)dev_alloc(c, nb * sizeof(int), &err);
+        if (!err) c->count = (int*)dev_alloc(c, sizeof(int), &err);
+    } else {
+        for (int q = 0; q < c->nstate && !err; ++q)
+            for (int b = 0; b < 2 && !err; ++b) c->state[q][b] = dev_alloc(c, fb, &err);
+        if (cfg->model == DBA_MODEL_MODELB)
+            for (int q = 0; q < 3 && !err; ++q) c->aux[q] = dev_alloc(c, fb, &err);
+    }
+    if (!err) c->par = (uint8_t*)dev_alloc(c, 2 * c->nch * nb, &err);
+    if (!err) c->wake = (uint8_t*)dev_alloc(c, 3 * c->nch * nb, &err);
+    if (!err) c->next = (uint8_t*)dev_alloc(c, c->nch * nb, &err);
+    if (!err && c->nsum) {
+        c->bsum = (double*)dev_alloc(c, c->nsum * nb * sizeof(double), &err);
+        if (!err) c->l1 = (double*)dev_alloc(c, c->nsum * ((nb + 1023) / 1024) * sizeof(double), &err);
+        if (!err) c->avg = (double*)dev_alloc(c, 4 * sizeof(double), &err);
+        if (!err) c->ticket = (unsigned int*)dev_alloc(c, sizeof(unsigned int), &err);
+    }
+    if (!err) c->status = (int*)dev_alloc(c, sizeof(int), &err);
+    if (!err) c->stats = (unsigned long long*)dev_alloc(c, 4 * sizeof(unsigned long long), &err);
+    if (!err) c->staging = (double*)dev_alloc(c, (c->n > 64 ? c->n : 64) * sizeof(double), &err);
+    if (err) {
+        dba_destroy(c);
+        return err;
+    }
+    c->grid = c->esz == 8 ? step_grid<double>(cfg->model, c->D, c->B, c->sms) : step_grid<float>(cfg->model, c->D, c->B, c->sms);
+    if (c->grid < 1) c->grid = c->sms;
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        dba_destroy(c);
+        return cuda_status(e);
+    }
+    *out = c;
+    return DBA_OK;
+}
+
+void dba_destroy(dba_ctx* c)
+{
+    if (!c) return;
+    if (c->st) cudaStreamSynchronize(c->st);
+    for (auto& row : c->graphs)
+        for (auto& gexec : row)
+            if (gexec) cudaGraphExecDestroy(gexec);
+    for (auto& a : c->allocs) cudaFree(a.p);
+    if (c->host_staging) cudaFreeHost(c->host_staging);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+int dba_init(dba_ctx* c, const double* ic)
+{
+    if (!c) return DBA_ERR_ARG;
+    const dba_config& k = c->cfg;
+    std::vector<double> buf;
+    const double* src = ic;
+    if (!src) {
+        if (k.model == DBA_MODEL_DENDRITE) ic_dendrite(k, buf);
+        else if (k.model == DBA_MODEL_MODELB) ic_modelb(k, buf);
+        else ic_kh(k, buf);
+        src = buf.data();
+    }
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    for (auto& a : c->allocs) DBA_TRY(cudaMemset(a.p, 0, a.bytes));
+    int st = DBA_OK;
+    if (k.model == DBA_MODEL_KH) {
+        // getConserved (example_Kelvin_Helmholtz/KH_DBA.cu:358-367) on the host in FP64
+        const size_t n = c->n;
+        const double *rho = src, *p = src + n, *vx = src + 2 * n, *vy = src + 3 * n;
+        std::vector<double> U(4 * n);
+        const double vol = k.dx * k.dy, gamma = k.kh_gamma;
+        for (size_t i = 0; i < n; ++i) {
+            double r = rho[i], u = vx[i], v = vy[i], pp = p[i];
+            U[i] = r * vol;
+            U[n + i] = r * u * vol;
+            U[2 * n + i] = r * v * vol;
+            U[3 * n + i] = (pp / (gamma - 1.0) + 0.5 * r * (u * u + v * v)) * vol;
+        }
+        for (int q = 0; q < 4 && !st; ++q) st = upload_any(c, c->state[q][0], U.data() + q * n, n);
+        for (int q = 0; q < 4 && !st; ++q) st = upload_any(c, c->aux[q], src + q * n, n);   // initial primitives
+    } else {
+        for (int q = 0; q < c->nstate && !st; ++q) st = upload_any(c, c->state[q][0], src + q * c->n, c->n);
+    }
+    if (st) return st;
+    // step 1 reads wake[1 % 3]: every block starts active (kernel.cu:157-160)
+    DBA_TRY(cudaMemset(c->wake + 1 * (size_t)c->nch * c->g.nb, 1, (size_t)c->nch * c->g.nb));
+    DBA_TRY(cudaDeviceSynchronize());
+    c->step = 0;
+    c->time = 0.0;
+    c->initialized = true;
+    return DBA_OK;
+}
+
+int dba_step(dba_ctx* c, int nsteps, int mode)
+{
+    if (!c) return DBA_ERR_ARG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    if (nsteps < 0 || (mode != 0 && mode != 1)) return DBA_ERR_ARG;
+    const bool dba_mode = mode == DBA_MODE_DBA;
+    while (nsteps > 0) {
+        const int r = (int)((c->step + 1) % 6);
+        if (c->use_graphs && nsteps >= kGraphSteps) {
+            cudaGraphExec_t& ge = c->graphs[r][mode];
+            if (!ge) {
+                cudaGraph_t graph;
+                DBA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+                cudaError_t e = cudaSuccess;
+                for (int q = 0; q < kGraphSteps && e == cudaSuccess; ++q) e = enqueue_step(c, c->step + 1 + q, dba_mode);
+                cudaError_t e2 = cudaStreamEndCapture(c->st, &graph);
+                if (e != cudaSuccess) return cuda_status(e);
+                if (e2 != cudaSuccess) return cuda_status(e2);
+                e = cudaGraphInstantiate(&ge, graph, 0);
+                cudaGraphDestroy(graph);
+                if (e != cudaSuccess) return cuda_status(e);
+            }
+            DBA_TRY(cudaGraphLaunch(ge, c->st));
+            c->step += kGraphSteps;
+            nsteps -= kGraphSteps;
+            c->time += kGraphSteps * c->cfg.dt;
+        } else {
+            DBA_TRY(enqueue_step(c, c->step + 1, dba_mode));
+            c->step += 1;
+            nsteps -= 1;
+            c->time += c->cfg.dt;
+        }
+    }
+    return DBA_OK;
+}
+
+int dba_sync(dba_ctx* c)
+{
+    if (!c) return DBA_ERR_ARG;
+    cudaError_t e = cudaStreamSynchronize(c->st);
+    if (e != cudaSuccess) return cuda_status(e);
+    int s = 0;
+    e = cudaMemcpy(&s, c->status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_status(e);
+    return s;
+}
+
+int dba_read_field(dba_ctx* c, int field, double* host)
+{
+    if (!c || !host) return DBA_ERR_ARG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    const int model = c->cfg.model;
+    if (field < 0 || field >= nfields_of(model)) return DBA_ERR_ARG;
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    if (model == DBA_MODEL_DENDRITE)   // p and T have their own activity channel and buffer parity
+        return gather(c, c->state[field][0], c->state[field][1], cur_par(c) + (size_t)field * c->g.nb, 0, 1, c->n, host);
+    if (model == DBA_MODEL_MODELB) {
+        if (field < 3) return gather(c, c->state[field][0], c->state[field][1], cur_par(c), 0, 1, c->n, host);
+        if (field >= 4) return gather(c, c->aux[field - 4], c->aux[field - 4], nullptr, 0, 1, c->n, host);
+        // b = 1 - x - y - z of the current state (Update, kernel.cu:434)
+        std::vector<double> y(c->n), z(c->n);
+        int st = gather(c, c->state[0][0], c->state[0][1], cur_par(c), 0, 1, c->n, host);
+        if (!st) st = gather(c, c->state[1][0], c->state[1][1], cur_par(c), 0, 1, c->n, y.data());
+        if (!st) st = gather(c, c->state[2][0], c->state[2][1], cur_par(c), 0, 1, c->n, z.data());
+        if (st) return st;
+        for (size_t i = 0; i < c->n; ++i) host[i] = 1.0 - host[i] - y[i] - z[i];
+        return DBA_OK;
+    }
+    // KH
+    if (field < 4) return gather(c, c->state[field][0], c->state[field][0], nullptr, 0, 1, c->n, host);
+    // primitives as the reference's output path computes them: getPrimitive for the
+    // blocks active in the next step (KH_DBA.cu:1518), stale values elsewhere
+    {
+        cudaError_t e = c->esz == 8 ? launch_kh_prim_blocks<double>(c->st, c->g, c->B, kh_params<double>(c, true), next_wake(c))
+                                    : launch_kh_prim_blocks<float>(c->st, c->g, c->B, kh_params<float>(c, true), next_wake(c));
+        if (e != cudaSuccess) return cuda_status(e);
+    }
+    const int w = field - 4;   // rho, p, vx, vy
+    return gather(c, c->aux[w], c->aux[w], nullptr, 0, 1, c->n, host);
+}
+
+int dba_read_flags(dba_ctx* c, int which, int32_t* host)
+{
+    if (!c || !host) return DBA_ERR_ARG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    int ch = which / 2, kind = which % 2;
+    if (which < 0 || ch >= c->nch) return DBA_ERR_ARG;
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    const size_t nb = c->g.nb;
+    std::vector<uint8_t> tmp(nb);
+    const uint8_t* src = kind == 0 ? next_wake(c) + ch * nb : c->next + ch * nb;
+    DBA_TRY(cudaMemcpy(tmp.data(), src, nb, cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < nb; ++i) host[i] = tmp[i] ? 1 : 0;
+    return DBA_OK;
+}
+
+int dba_tip(dba_ctx* c, double* tip)
+{
+    if (!c || !tip) return DBA_ERR_ARG;
+    if (c->cfg.model != DBA_MODEL_DENDRITE) return DBA_ERR_CONFIG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    const dba_config& k = c->cfg;
+    std::vector<double> col(k.ny);
+    size_t start = (size_t)(k.nx / 2) + (size_t)k.nx * (size_t)k.ny * (size_t)(k.nz / 2);
+    int st = gather(c, c->state[0][0], c->state[0][1], cur_par(c), start, (size_t)k.nx, (size_t)k.ny, col.data());
+    if (st) return st;
+    // growth_front (example_Dendritic_growth/kernel.cu:759-773)
+    *tip = NAN;
+    for (int y = k.ny / 2; y < k.ny; ++y)
+        if (col[y] < 0.5) {
+            *tip = (col[y - 1] - 0.5) / (col[y - 1] - col[y]) + y - 1 - k.ny / 2;
+            break;
+        }
+    return DBA_OK;
+}
+
+int dba_observables(dba_ctx* c, dba_obs* o)
+{
+    if (!c || !o) return DBA_ERR_ARG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    std::memset(o, 0, sizeof *o);
+    o->step = c->step;
+    o->time = c->time;
+    o->total_blocks = c->g.nb;
+    o->tip = NAN;
+    o->vy_mode = NAN;
+    std::vector<int32_t> fl(c->g.nb);
+    for (int ch = 0; ch < c->nch; ++ch) {
+        int st = dba_read_flags(c, 2 * ch, fl.data());
+        if (st) return st;
+        int cnt = 0;
+        for (int v : fl) cnt += v;
+        o->active_blocks[ch] = cnt;
+    }
+    unsigned long long stats[4];
+    DBA_TRY(cudaMemcpy(stats, c->stats, sizeof stats, cudaMemcpyDeviceToHost));
+    o->cell_updates = (long)(stats[2] * (unsigned long long)(c->n / c->g.nb));
+    std::vector<double> f(c->n);
+    const dba_config& k = c->cfg;
+    if (k.model == DBA_MODEL_DENDRITE) {
+        int st = dba_tip(c, &o->tip);
+        if (st) return st;
+        for (int q = 0; q < 2; ++q) {
+            st = dba_read_field(c, q, f.data());
+            if (st) return st;
+            double s = 0;
+            for (double v : f) s += v;
+            o->integral[q] = s;
+        }
+    } else if (k.model == DBA_MODEL_MODELB) {
+        for (int q = 0; q < 4; ++q) {   // Integral (example_Reactive_ModelB/kernel.cu:989-1010)
+            int st = dba_read_field(c, q, f.data());
+            if (st) return st;
+            double s = 0;
+            for (double v : f) s += v;
+            o->integral[q] = s;
+        }
+    } else {
+        const int order[4] = {0, 3, 1, 2};   // Mass, Energy, Momx, Momy (Conserved/KH_DBA.cu:1303-1323)
+        for (int q = 0; q < 4; ++q) {
+            int st = dba_read_field(c, order[q], f.data());
+            if (st) return st;
+            double s = 0;
+            for (double v : f) s += v;
+            o->integral[q] = s;
+        }
+        // Calc_Vy_mode (example_Kelvin_Helmholtz/KH_DBA.cu:1291-1327)
+        int st = dba_read_field(c, 7, f.data());
+        if (st) return st;
+        double ss = 0, sc = 0, sd = 0;
+        for (int y = 0; y < k.ny; ++y)
+            for (int x = 0; x < k.nx; ++x) {
+                double xs = (double)x / k.nx, ys = (double)y / k.ny;
+                double d = std::exp(-4.0 * M_PI * std::fabs(ys - (ys < 0.5 ? 0.25 : 0.75)));
+                double v = f[(size_t)x + (size_t)k.nx * y];
+                ss += v * std::sin(4.0 * M_PI * xs) * d;
+                sc += v * std::cos(4.0 * M_PI * xs) * d;
+                sd += d;
+            }
+        o->vy_mode = 2.0 * std::sqrt(ss * ss / (sd * sd) + sc * sc / (sd * sd));
+    }
+    return DBA_OK;
+}
+
+int dba_get_info(dba_ctx* c, dba_info* info)
+{
+    if (!c || !info) return DBA_ERR_ARG;
+    info->nbx = c->g.nbx; info->nby = c->g.nby; info->nbz = c->g.nbz; info->nb = c->g.nb;
+    info->dims = c->D;
+    info->nfields = nfields_of(c->cfg.model);
+    info->nchannels = c->nch;
+    size_t bytes = 0;
+    for (auto& a : c->allocs) bytes += a.bytes;
+    info->device_bytes = bytes;
+    info->step = c->step;
+    info->grid_ctas = c->grid;
+    return DBA_OK;
+}
+
+int dba_get_stream(dba_ctx* c, void** stream)
+{
+    if (!c || !stream) return DBA_ERR_ARG;
+    *stream = (void*)c->st;
+    return DBA_OK;
+}
+
+int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
+{
+    if (!c || !out) return DBA_ERR_ARG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    if (nsteps < 1 || (mode != 0 && mode != 1)) return DBA_ERR_ARG;
+    std::memset(out, 0, sizeof *out);
+    const bool dba_mode = mode == DBA_MODE_DBA;
+    const bool cons = c->nsum && c->cfg.conserved && dba_mode;
+    std::vector<cudaEvent_t> ev((size_t)nsteps * 4 + 2);
+    for (auto& e : ev) DBA_TRY(cudaEventCreate(&e));
+    unsigned long long s0[4], s1[4];
+    DBA_TRY(cudaMemcpyAsync(s0, c->stats, sizeof s0, cudaMemcpyDeviceToHost, c->st));
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    int st = DBA_OK;
+    DBA_TRY(cudaEventRecord(ev[0], c->st));
+    for (int q = 0; q < nsteps && !st; ++q) {
+        const long s = c->step + 1;
+        FlagP f = flags_for(c, s);
+        cudaEvent_t* e = &ev[1 + 4 * (size_t)q];
+        cudaError_t r = cudaEventRecord(e[0], c->st);
+        if (r == cudaSuccess) {
+            if (c->esz == 8) {
+                if (c->cfg.model == DBA_MODEL_DENDRITE) r = launch_dendrite<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<double>(c));
+                else if (c->cfg.model == DBA_MODEL_MODELB) r = launch_modelb<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, mb_params<double>(c, dba_mode));
+                else {
+                    r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
+                    if (r == cudaSuccess) r = launch_kh<double>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_params<double>(c, dba_mode));
+                }
+            } else {
+                if (c->cfg.model == DBA_MODEL_DENDRITE) r = launch_dendrite<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<float>(c));
+                else if (c->cfg.model == DBA_MODEL_MODELB) r = launch_modelb<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, mb_params<float>(c, dba_mode));
+                else {
+                    r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
+                    if (r == cudaSuccess) r = launch_kh<float>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_params<float>(c, dba_mode));
+                }
+            }
+        }
+        if (r == cudaSuccess) r = cudaEventRecord(e[1], c->st);
+        if (r == cudaSuccess && cons) r = launch_reduce(c->st, c->bsum, c->g.nb, c->nsum, c->l1, c->ticket, c->avg, (double)c->n);
+        if (r == cudaSuccess) r = cudaEventRecord(e[2], c->st);
+        if (r == cudaSuccess && cons)
+            r = c->esz == 8 ? launch_correct<double>(c->grid, c->st, c->g, corr_params<double>(c, s))
+                            : launch_correct<float>(c->grid, c->st, c->g, corr_params<float>(c, s));
+        if (r == cudaSuccess) r = cudaEventRecord(e[3], c->st);
+        if (r != cudaSuccess) st = cuda_status(r);
+        c->step += 1;
+        c->time += c->cfg.dt;
+    }
+    cudaEvent_t& last = ev[ev.size() - 1];
+    if (!st) st = cuda_status(cudaEventRecord(last, c->st));
+    if (!st) st = cuda_status(cudaMemcpyAsync(s1, c->stats, sizeof s1, cudaMemcpyDeviceToHost, c->st));
+    if (!st) st = cuda_status(cudaStreamSynchronize(c->st));
+    if (!st) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[0], last);
+        out->step_ms = ms;
+        for (int q = 0; q < nsteps; ++q) {
+            cudaEvent_t* e = &ev[1 + 4 * (size_t)q];
+            cudaEventElapsedTime(&ms, e[0], e[1]);
+            out->stencil_ms += ms;
+            cudaEventElapsedTime(&ms, e[1], e[2]);
+            out->reduce_ms += ms;
+            cudaEventElapsedTime(&ms, e[2], e[3]);
+            out->correct_ms += ms;
+        }
+        out->steps = nsteps;
+        out->active_blocks = (long)(s1[2] - s0[2]);
+        out->active_blocks_ch[0] = (long)(s1[0] - s0[0]);
+        out->active_blocks_ch[1] = (long)(s1[1] - s0[1]);
+        out->ch0_only_blocks = (long)(s1[3] - s0[3]);
+        out->cells_per_block = (long)(c->n / c->g.nb);
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return st;
+}
+
+int dba_state_size(dba_ctx* c, size_t* size)
+{
+    if (!c || !size) return DBA_ERR_ARG;
+    size_t b = sizeof(long) + sizeof(double);
+    for (auto& a : c->allocs)
+        if ((void*)a.p != (void*)c->staging) b += a.bytes;
+    *size = b;
+    return DBA_OK;
+}
+
+int dba_save_state(dba_ctx* c, void* host, size_t size)
+{
+    if (!c || !host) return DBA_ERR_ARG;
+    size_t need = 0;
+    dba_state_size(c, &need);
+    if (size < need) return DBA_ERR_ARG;
+    unsigned char* h = (unsigned char*)host;
+    std::memcpy(h, &c->step, sizeof(long));
+    std::memcpy(h + sizeof(long), &c->time, sizeof(double));
+    size_t off = sizeof(long) + sizeof(double);
+    for (auto& a : c->allocs) {
+        if ((void*)a.p == (void*)c->staging) continue;
+        DBA_TRY(cudaMemcpyAsync(h + off, a.p, a.bytes, cudaMemcpyDeviceToHost, c->st));
+        off += a.bytes;
+    }
+    return cuda_status(cudaStreamSynchronize(c->st));
+}
+
+int dba_load_state(dba_ctx* c, const void* host, size_t size)
+{
+    if (!c || !host) return DBA_ERR_ARG;
+    size_t need = 0;
+    dba_state_size(c, &need);
+    if (size < need) return DBA_ERR_ARG;
+    const unsigned char* h = (const unsigned char*)host;
+    std::memcpy(&c->step, h, sizeof(long));
+    std::memcpy(&c->time, h + sizeof(long), sizeof(double));
+    size_t off = sizeof(long) + sizeof(double);
+    for (auto& a : c->allocs) {
+        if ((void*)a.p == (void*)c->staging) continue;
+        DBA_TRY(cudaMemcpyAsync(a.p, h + off, a.bytes, cudaMemcpyHostToDevice, c->st));
+        off += a.bytes;
+    }
+    c->initialized = true;
+    return DBA_OK;
+}
+
+int dba_get_config(dba_ctx* c, dba_config* cfg)
+{
+    if (!c || !cfg) return DBA_ERR_ARG;
+    *cfg = c->cfg;
+    return DBA_OK;
+}
+
+int dba_checkpoint(dba_ctx* c, const char* path)
+{
+    if (!c || !path) return DBA_ERR_ARG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return DBA_ERR_IO;
+    const char magic[8] = {'D', 'B', 'A', 'C', 'K', 'P', 'T', '1'};
+    bool ok = std::fwrite(magic, 1, 8, f) == 8;
+    ok = ok && std::fwrite(&c->cfg, sizeof c->cfg, 1, f) == 1;
+    ok = ok && std::fwrite(&c->step, sizeof c->step, 1, f) == 1;
+    ok = ok && std::fwrite(&c->time, sizeof c->time, 1, f) == 1;
+    std::vector<unsigned char> tmp;
+    for (auto& a : c->allocs) {
+        if (!ok) break;
+        if ((void*)a.p == (void*)c->staging) continue;
+        tmp.resize(a.bytes);
+        if (cudaMemcpy(tmp.data(), a.p, a.bytes, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            std::fclose(f);
+            return DBA_ERR_CUDA;
+        }
+        ok = std::fwrite(tmp.data(), 1, a.bytes, f) == a.bytes;
+    }
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? DBA_OK : DBA_ERR_IO;
+}
+
+int dba_restore(dba_ctx* c, const char* path)
+{
+    if (!c || !path) return DBA_ERR_ARG;
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return DBA_ERR_IO;
+    char magic[8];
+    dba_config cfg;
+    long step;
+    double time;
+    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "DBACKPT1", 8) == 0;
+    ok = ok && std::fread(&cfg, sizeof cfg, 1, f) == 1;
+    ok = ok && std::fread(&step, sizeof step, 1, f) == 1;
+    ok = ok && std::fread(&time, sizeof time, 1, f) == 1;
+    if (ok && (cfg.model != c->cfg.model || cfg.nx != c->cfg.nx || cfg.ny != c->cfg.ny || cfg.nz != c->cfg.nz ||
+               cfg.block != c->cfg.block || cfg.precision != c->cfg.precision))
+        ok = false;
+    std::vector<unsigned char> tmp;
+    for (auto& a : c->allocs) {
+        if (!ok) break;
+        if ((void*)a.p == (void*)c->staging) continue;
+        tmp.resize(a.bytes);
+        ok = std::fread(tmp.data(), 1, a.bytes, f) == a.bytes;
+        if (ok && cudaMemcpy(a.p, tmp.data(), a.bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
+            std::fclose(f);
+            return DBA_ERR_CUDA;
+        }
+    }
+    std::fclose(f);
+    if (!ok) return DBA_ERR_IO;
+    c->step = step;
+    c->time = time;
+    c->initialized = true;
+    return DBA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+// k_common.cuh -- device-side helpers shared by the step kernels.
+//
+// Work distribution used by every step kernel: CTA c owns blocks c, c+G,
+// c+2G, ... (G = gridDim.x).  Each step it scans its owned blocks' wake flags
+// 256 at a time, turns them into a compact list in shared memory with warp
+// ballots and one shared atomic per warp, and processes the list in batches.
+// The same pass flips the per-block buffer parity of active blocks and clears
+// the flag array that will be reused two steps later, so activation needs no
+// host round trip and no separate compaction kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dba {
+
+constexpr int kThreads = 256;
+
+constexpr __host__ __device__ int ipow(int b, int e) { return e == 0 ? 1 : b * ipow(b, e - 1); }
+
+struct GridP {
+    int nx, ny, nz;        // cells
+    int nbx, nby, nbz, nb; // blocks
+    int bc;                // 0 periodic, 1 zero-flux (clamp)
+};
+
+// Per-step flag pointers.  Arrays are [channel][nb].
+//   par_cur : buffer index (0/1) holding each block's current values
+//   par_nxt : written by the owner: par_cur ^ active
+//   wake_cur: activity of this step; wake_nxt: activity of the next step
+//             (set by wake-up scatter); wake_clr: the array used two steps
+//             later, cleared by the owner this step
+//   next    : the reference's wake_up_*_next (written for active channels)
+//   bsum    : per-block FP64 sums of the conserved change ([nsum][nb])
+struct FlagP {
+    const uint8_t* par_cur;
+    uint8_t* par_nxt;
+    const uint8_t* wake_cur;
+    uint8_t* wake_nxt;
+    uint8_t* wake_clr;
+    uint8_t* next;
+    double* bsum;
+    int* status;
+    unsigned long long* stats;  // [0] ch0 active blocks, [1] ch1, [2] any, [3] ch0 && !ch1
+};
+
+__device__ __forceinline__ int wrapc(int v, int n, int bc)
+{
+    if (v < 0) return bc ? 0 : v + n;
+    if (v >= n) return bc ? n - 1 : v - n;
+    return v;
+}
+
+// block neighbour for the wake-up scatter; -1 when it falls off a zero-flux edge
+__device__ __forceinline__ int block_nb(const GridP& g, int b, int dx, int dy, int dz)
+{
+    int bx = b % g.nbx, by = (b / g.nbx) % g.nby, bz = b / (g.nbx * g.nby);
+    bx += dx; by += dy; bz += dz;
+    if (g.bc) {
+        if (bx < 0 || bx >= g.nbx || by < 0 || by >= g.nby || bz < 0 || bz >= g.nbz) return -1;
+    } else {
+        bx = bx < 0 ? g.nbx - 1 : (bx >= g.nbx ? 0 : bx);
+        by = by < 0 ? g.nby - 1 : (by >= g.nby ? 0 : by);
+        bz = bz < 0 ? g.nbz - 1 : (bz >= g.nbz ? 0 : bz);
+    }
+    return bx + g.nbx * (by + g.nby * bz);
+}
+
+// self + 6 faces (example_Dendritic_growth/kernel.cu:596-628)
+__device__ __forceinline__ void wake_faces(const GridP& g, uint8_t* w, int b)
+{
+    w[b] = 1;
+    const int d[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        int nb = block_nb(g, b, d[k][0], d[k][1], d[k][2]);
+        if (nb >= 0) w[nb] = 1;
+    }
+}
+
+// self + faces + 4 in-plane diagonals (example_Kelvin_Helmholtz/KH_DBA.cu:1026-1039)
+__device__ __forceinline__ void wake_faces_diag(const GridP& g, uint8_t* w, int b)
+{
+    wake_faces(g, w, b);
+    const int d[4][2] = {{-1, -1}, {-1, 1}, {1, -1}, {1, 1}};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int nb = block_nb(g, b, d[k][0], d[k][1], 0);
+        if (nb >= 0) w[nb] = 1;
+    }
+}
+
+__device__ __forceinline__ void raise_status(int* status, int code)
+{
+    atomicCAS(status, 0, code);
+}
+
+// Append (b, meta) to the CTA's compact list when `take`; all threads of the
+// CTA must call it.  One shared atomic per warp.
+__device__ __forceinline__ void list_append(bool take, int b, int meta, int* s_list, int* s_meta, int* s_cnt)
+{
+    unsigned m = __ballot_sync(0xffffffffu, take);
+    if (m == 0) return;
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(s_cnt, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (take) {
+        int pos = base + __popc(m & ((1u << lane) - 1u));
+        s_list[pos] = b;
+        s_meta[pos] = meta;
+    }
+}
+
+__device__ __forceinline__ void count_stats(unsigned long long* stats, int act, bool valid)
+{
+    unsigned m0 = __ballot_sync(0xffffffffu, valid && (act & 1));
+    unsigned m1 = __ballot_sync(0xffffffffu, valid && (act & 2));
+    unsigned m2 = __ballot_sync(0xffffffffu, valid && (act & 3));
+    unsigned m3 = __ballot_sync(0xffffffffu, valid && (act & 1) && !(act & 2));
+    if ((threadIdx.x & 31) == 0 && m2) {
+        atomicAdd(&stats[0], (unsigned long long)__popc(m0));
+        atomicAdd(&stats[1], (unsigned long long)__popc(m1));
+        atomicAdd(&stats[2], (unsigned long long)__popc(m2));
+        atomicAdd(&stats[3], (unsigned long long)__popc(m3));
+    }
+}
+
+// Tree sum of one value per cell of a block, in the fixed order the CPU
+// restatement mirrors: runs of 32 consecutive cells (or the whole block when it
+// has fewer than 32 cells) are reduced with strides 16..1 (shfl_down), then the
+// run sums are reduced with strides R/2..1.  Cell v of block k lives in thread
+// k*V + v (V < kThreads) or thread v % kThreads, pass v / kThreads (V >= kThreads).
+// `val[c]` is this thread's value for pass c.  Writes the block sums to out[k]
+// (thread 0 of each block) via the scratch s_run[kThreads / 32 * CPT].
+template <int V, int CPT>
+__device__ __forceinline__ void block_tree_sums(const double* val, double* s_run, double* out_k, int k_of_thread)
+{
+    const int lane = threadIdx.x & 31;
+    constexpr int SEG = V < 32 ? V : 32;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        double v = val[c];
+#pragma unroll
+        for (int h = SEG / 2; h >= 1; h /= 2) v += __shfl_down_sync(0xffffffffu, v, h, SEG);
+        if (V < 32) {
+            if ((lane % SEG) == 0) out_k[threadIdx.x / V] = v;
+        } else {
+            // run index within the block
+            int cell = (V >= kThreads) ? (threadIdx.x + c * kThreads) : (threadIdx.x % V);
+            int run = cell / 32;
+            int kb = (V >= kThreads) ? 0 : threadIdx.x / V;
+            if (lane == 0) s_run[kb * (V / 32) + run] = v;
+        }
+    }
+    if (V >= 32) {
+        __syncthreads();
+        constexpr int R = V / 32;                    // runs per block
+        constexpr int NB = V >= kThreads ? 1 : kThreads / V;
+        const int warp = threadIdx.x / 32;
+        if (warp < NB) {
+            double v = lane < R ? s_run[warp * R + lane] : 0.0;
+            if (R > 1) {
+#pragma unroll
+                for (int h = (R > 32 ? 16 : R / 2); h >= 1; h /= 2) v += __shfl_down_sync(0xffffffffu, v, h, 32);
+            }
+            if (lane == 0) out_k[warp] = v;
+        }
+        __syncthreads();
+    }
+    (void)k_of_thread;
+}
+
+}  // namespace dba

@@ -1,0 +1,185 @@
+// k_dendrite.cuh -- one fused step of the Kobayashi p/T dendrite model over
+// the active blocks (reference: example_Dendritic_growth/kernel.cu).
+//
+// The reference runs four kernels and a host sync per DBA step:
+//   Evolve_p_wakeup (:322)  p_new for p-active blocks
+//   Evolve_T_wakeup (:411)  T_new = T + dt lapT for T-active blocks, then
+//                           T_new += p_new - p for p-active blocks
+//   Wakeup_Next (:496)      commit p/T of active blocks, per-block tests
+//                           metric_p <= p_new <= 1-metric_p and |T_new-T| >= metric_T
+//   Wakeup_Neighbor (:577)  wake self + 6 face neighbours for the next step
+// Here one kernel does all of it: each active block and its 1-cell halo are
+// staged in shared memory, p and T are advanced (Jacobi: every read sees the
+// start-of-step values, which live in each block's current ping-pong buffer),
+// results go to the block's other buffer (no commit copy), the wake-up tests
+// are block-wide ORs in shared memory and the neighbour wake-up is a scatter
+// into next step's flag array.  A p-active block that is not T-active keeps
+// its T untouched, exactly as the reference, whose T_new is not committed then.
+// Regular mode (DBA=false) uses the reference's mode-0 rounding order for T
+// (T + dt lapT + p_new - p, kernel.cu:289).
+#pragma once
+
+#include "fpmath.h"
+#include "k_common.cuh"
+
+namespace dba {
+
+template <typename R>
+struct DenP {
+    R* p[2];
+    R* T[2];
+    double f0, f1, f2, f3;   // 1/(2dx), 1/dx/dx, -alpha/Pi, 1/tau  (kernel.cu:98-101)
+    double dt, delta, eps2, gamma;
+    double thr_p, thr_p_hi, thr_T;   // metric_p, 1.0 - metric_p, metric_T
+};
+
+template <typename R> __device__ __forceinline__ R atan_r(R v);
+template <> __device__ __forceinline__ double atan_r<double>(double v) { return dba_atan(v); }
+template <> __device__ __forceinline__ float atan_r<float>(float v) { return atanf(v); }
+
+template <typename R, int D, int B, bool DBA>
+__global__ void __launch_bounds__(kThreads) dendrite_step(GridP g, FlagP f, DenP<R> P)
+{
+    constexpr int NT = kThreads;
+    constexpr int V = ipow(B, D);
+    constexpr int E = B + 2;
+    constexpr int TV = ipow(E, D);
+    constexpr int K = V >= NT ? 1 : NT / V;
+    constexpr int CPT = V >= NT ? V / NT : 1;
+    constexpr int SY = E, SZ = (D == 3) ? E * E : 0;
+
+    __shared__ R sp[K * TV];
+    __shared__ R sT[K * TV];
+    __shared__ int s_list[NT], s_lmeta[NT];
+    __shared__ int s_cnt;
+    __shared__ int s_blk[K], s_meta[K], s_np[K], s_nT[K];
+
+    const int tid = threadIdx.x;
+    const int G = gridDim.x;
+    const int nb = g.nb;
+    const R f0 = (R)P.f0, f1 = (R)P.f1, f2 = (R)P.f2, f3 = (R)P.f3;
+    const R dt = (R)P.dt, delta = (R)P.delta, eps2 = (R)P.eps2, gam = (R)P.gamma;
+    const R thr_p = (R)P.thr_p, thr_p_hi = (R)P.thr_p_hi, thr_T = (R)P.thr_T;
+
+    for (long long j0 = 0; blockIdx.x + (long long)G * j0 < nb; j0 += NT) {
+        const long long bl = blockIdx.x + (long long)G * (j0 + tid);
+        const bool valid = bl < nb;
+        const int b = (int)bl;
+        int act = 0, meta = 0;
+        if (valid) {
+            int pp = f.par_cur[b], pT = f.par_cur[nb + b];
+            act = DBA ? ((f.wake_cur[b] ? 1 : 0) | (f.wake_cur[nb + b] ? 2 : 0)) : 3;
+            f.wake_clr[b] = 0;
+            f.wake_clr[nb + b] = 0;
+            if (!DBA) {
+                f.wake_nxt[b] = 1;
+                f.wake_nxt[nb + b] = 1;
+            }
+            f.par_nxt[b] = (uint8_t)(pp ^ (act & 1));
+            f.par_nxt[nb + b] = (uint8_t)(pT ^ ((act >> 1) & 1));
+            meta = act | (pp << 2) | (pT << 3);
+        }
+        count_stats(f.stats, act, valid);
+        if (tid == 0) s_cnt = 0;
+        __syncthreads();
+        list_append(valid && act, b, meta, s_list, s_lmeta, &s_cnt);
+        __syncthreads();
+        const int cnt = s_cnt;
+
+        for (int q0 = 0; q0 < cnt; q0 += K) {
+            if (tid < K) {
+                int q = q0 + tid;
+                s_blk[tid] = q < cnt ? s_list[q] : -1;
+                s_meta[tid] = q < cnt ? s_lmeta[q] : 0;
+                s_np[tid] = 0;
+                s_nT[tid] = 0;
+            }
+            __syncthreads();
+            // stage p and T of each block plus a 1-cell halo (owner's current buffer)
+            for (int i = tid; i < K * TV; i += NT) {
+                const int k = i / TV;
+                const int blk = s_blk[k];
+                if (blk < 0) continue;
+                const int j = i - k * TV;
+                const int lx = j % E, ly = (j / E) % E, lz = (D == 3) ? j / (E * E) : 0;
+                const int bx = blk % g.nbx, by = (blk / g.nbx) % g.nby, bz = blk / (g.nbx * g.nby);
+                const int gx = wrapc(bx * B + lx - 1, g.nx, g.bc);
+                const int gy = wrapc(by * B + ly - 1, g.ny, g.bc);
+                const int gz = (D == 3) ? wrapc(bz * B + lz - 1, g.nz, g.bc) : 0;
+                const int ob = gx / B + g.nbx * (gy / B + g.nby * ((D == 3) ? gz / B : 0));
+                const size_t gi = (size_t)gx + (size_t)g.nx * ((size_t)gy + (size_t)g.ny * gz);
+                sp[i] = P.p[f.par_cur[ob]][gi];
+                sT[i] = P.T[f.par_cur[nb + ob]][gi];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) {
+                const int k = (V >= NT) ? 0 : tid / V;
+                const int v = (V >= NT) ? tid + c * NT : tid - k * V;
+                const int blk = s_blk[k];
+                if (blk < 0) continue;
+                const int m = s_meta[k];
+                const int lx = v % B, ly = (v / B) % B, lz = (D == 3) ? v / (B * B) : 0;
+                const int ti = k * TV + (lx + 1) + SY * (ly + 1) + SZ * (lz + 1);
+                const int bx = blk % g.nbx, by = (blk / g.nbx) % g.nby, bz = blk / (g.nbx * g.nby);
+                const size_t gi = (size_t)(bx * B + lx) +
+                                  (size_t)g.nx * ((size_t)(by * B + ly) + (size_t)g.ny * (size_t)((D == 3) ? bz * B + lz : 0));
+                const R pc = sp[ti], Tc = sT[ti];
+                R pn = pc;
+                if (m & 1) {   // Evolve_p (kernel.cu:220-241)
+                    const R pxp = sp[ti + 1], pxm = sp[ti - 1], pyp = sp[ti + SY], pym = sp[ti - SY];
+                    const R pzp = sp[ti + SZ], pzm = sp[ti - SZ];
+                    const R dpx = (pxp - pxm) * f0;
+                    const R dpy = (pyp - pym) * f0;
+                    const R dpz = (pzp - pzm) * f0;
+                    const R lapP = (pxp + pxm + pyp + pym + pzp + pzm - 6 * pc) * f1;
+                    const R v2 = dpx * dpx + dpy * dpy + dpz * dpz;
+                    R sigma;
+                    if (v2 <= (R)1E-6)
+                        sigma = 1;
+                    else
+                        sigma = 1 - delta * (1 - ((dpx * dpx) * (dpx * dpx) + (dpy * dpy) * (dpy * dpy) +
+                                                  (dpz * dpz) * (dpz * dpz)) / (v2 * v2));
+                    const R mm = f2 * atan_r<R>(gam * sigma * Tc);
+                    const R pchg = f3 * (eps2 * lapP + pc * (1 - pc) * (pc - (R)0.5 + mm));
+                    pn = pc + dt * pchg;
+                    P.p[((m >> 2) & 1) ^ 1][gi] = pn;
+                    if (pn >= thr_p && pn <= thr_p_hi) s_np[k] = 1;
+                    if (!isfinite(pn)) raise_status(f.status, 5);
+                }
+                if (m & 2) {   // Evolve_T (kernel.cu:286-289, :468-489)
+                    const R lapT = (sT[ti + 1] + sT[ti - 1] + sT[ti + SY] + sT[ti - SY] + sT[ti + SZ] + sT[ti - SZ] -
+                                    6 * Tc) * f1;
+                    R Tn;
+                    if (DBA) {
+                        Tn = Tc + dt * lapT;
+                        if (m & 1) Tn = Tn + (pn - pc);
+                    } else {
+                        Tn = Tc + dt * lapT + pn - pc;
+                    }
+                    P.T[((m >> 3) & 1) ^ 1][gi] = Tn;
+                    if (fabs(Tn - Tc) >= thr_T) s_nT[k] = 1;
+                    if (!isfinite(Tn)) raise_status(f.status, 5);
+                }
+            }
+            __syncthreads();
+            if (DBA && tid < K) {
+                const int blk = s_blk[tid];
+                if (blk >= 0) {
+                    const int m = s_meta[tid];
+                    if (m & 1) {
+                        f.next[blk] = (uint8_t)s_np[tid];
+                        if (s_np[tid]) wake_faces(g, f.wake_nxt, blk);
+                    }
+                    if (m & 2) {
+                        f.next[nb + blk] = (uint8_t)s_nT[tid];
+                        if (s_nT[tid]) wake_faces(g, f.wake_nxt + nb, blk);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace dba

@@ -1,0 +1,186 @@
+// k_inst.cuh -- template launchers; included once per precision (k_f64.cu, k_f32.cu).
+#pragma once
+
+#include "launch.h"
+
+namespace dba {
+
+template <typename R>
+static int grid_of(const void* kern, size_t smem, int sms)
+{
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem) != cudaSuccess || occ < 1) occ = 1;
+    return occ * sms;
+}
+
+template <typename R, int D, int B>
+static bool mb_prepare(size_t& smem)
+{
+    smem = MBShape<R, D, B>::smem;
+    if (smem > 200 * 1024) return false;
+    static bool done[2] = {false, false};
+    if (!done[0]) {
+        done[0] = true;
+        cudaFuncSetAttribute(modelb_step<R, D, B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(modelb_step<R, D, B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
+    return true;
+}
+
+#define DBA_DEN_SHAPES(X) X(2, 4) X(2, 8) X(2, 16) X(2, 32) X(3, 4) X(3, 8)
+#define DBA_MB_SHAPES(X) X(2, 4) X(2, 8) X(2, 16) X(2, 32) X(3, 4) X(3, 8)
+#define DBA_KH_SHAPES(X) X(4) X(8) X(16)
+
+template <typename R>
+bool shape_supported(int model, int D, int B)
+{
+#define X2(d, b) if (D == d && B == b) return true;
+#define X1(b) if (D == 2 && B == b) return true;
+    if (model == MODEL_DENDRITE) { DBA_DEN_SHAPES(X2) }
+    if (model == MODEL_MODELB) { DBA_MB_SHAPES(X2) }
+    if (model == MODEL_KH) { DBA_KH_SHAPES(X1) }
+#undef X2
+#undef X1
+    return false;
+}
+
+template <typename R>
+int step_grid(int model, int D, int B, int sms)
+{
+#define XD(d, b) if (D == d && B == b) return grid_of<R>((const void*)dendrite_step<R, d, b, true>, 0, sms);
+#define XM(d, b) if (D == d && B == b) { size_t sm; mb_prepare<R, d, b>(sm); return grid_of<R>((const void*)modelb_step<R, d, b, true>, sm, sms); }
+#define XK(b) if (B == b) return grid_of<R>((const void*)kh_extrap<R, b, true>, 0, sms);
+    if (model == MODEL_DENDRITE) { DBA_DEN_SHAPES(XD) }
+    if (model == MODEL_MODELB) { DBA_MB_SHAPES(XM) }
+    if (model == MODEL_KH) { DBA_KH_SHAPES(XK) }
+#undef XD
+#undef XM
+#undef XK
+    return sms;
+}
+
+template <typename R>
+cudaError_t launch_dendrite(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
+                            const DenP<R>& P)
+{
+#define XD(d, b)                                                                   \
+    if (D == d && B == b) {                                                        \
+        if (dba_mode) dendrite_step<R, d, b, true><<<grid, kThreads, 0, st>>>(g, f, P); \
+        else dendrite_step<R, d, b, false><<<grid, kThreads, 0, st>>>(g, f, P);   \
+        return cudaGetLastError();                                                 \
+    }
+    DBA_DEN_SHAPES(XD)
+#undef XD
+    return cudaErrorInvalidValue;
+}
+
+template <typename R>
+cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
+                          const MBP<R>& P)
+{
+#define XM(d, b)                                                                            \
+    if (D == d && B == b) {                                                                 \
+        size_t sm;                                                                          \
+        if (!mb_prepare<R, d, b>(sm)) return cudaErrorInvalidValue;                         \
+        if (dba_mode) modelb_step<R, d, b, true><<<grid, kThreads, sm, st>>>(g, f, P);      \
+        else modelb_step<R, d, b, false><<<grid, kThreads, sm, st>>>(g, f, P);              \
+        return cudaGetLastError();                                                          \
+    }
+    DBA_MB_SHAPES(XM)
+#undef XM
+    return cudaErrorInvalidValue;
+}
+
+template <typename R>
+cudaError_t launch_kh(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f, const KHP<R>& P)
+{
+    const int sgrid = (g.nb + kThreads - 1) / kThreads < grid ? (g.nb + kThreads - 1) / kThreads : grid;
+#define XK(b)                                                                                   \
+    if (B == b) {                                                                               \
+        if (dba_mode) kh_scan<true><<<sgrid, kThreads, 0, st>>>(g, f, P.list, P.count, P.conserved); \
+        else kh_scan<false><<<sgrid, kThreads, 0, st>>>(g, f, P.list, P.count, P.conserved);    \
+        kh_prim<R, b><<<grid, kThreads, 0, st>>>(g, P);                                         \
+        if (dba_mode) kh_extrap<R, b, true><<<grid, kThreads, 0, st>>>(g, f, P);                \
+        else kh_extrap<R, b, false><<<grid, kThreads, 0, st>>>(g, f, P);                        \
+        kh_flux<R, b><<<grid, kThreads, 0, st>>>(g, P);                                         \
+        kh_apply<R, b><<<grid, kThreads, 0, st>>>(g, f, P);                                     \
+        return cudaGetLastError();                                                              \
+    }
+    DBA_KH_SHAPES(XK)
+#undef XK
+    return cudaErrorInvalidValue;
+}
+
+template <typename R>
+cudaError_t launch_correct(int grid, cudaStream_t st, const GridP& g, const CorrP<R>& P)
+{
+    cons_correct<R><<<grid, kThreads, 0, st>>>(g, P);
+    return cudaGetLastError();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) gather_kernel(GridP g, int B, int D, const R* b0, const R* b1,
+                                                          const uint8_t* par, size_t start, size_t stride, size_t count,
+                                                          double* out)
+{
+    for (size_t k = (size_t)blockIdx.x * kThreads + threadIdx.x; k < count; k += (size_t)gridDim.x * kThreads) {
+        const size_t i = start + k * stride;
+        int buf = 0;
+        if (par) {
+            const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / ((size_t)g.nx * g.ny));
+            buf = par[x / B + g.nbx * (y / B + g.nby * (D == 3 ? z / B : 0))];
+        }
+        out[k] = (double)(buf ? b1[i] : b0[i]);
+    }
+}
+
+template <typename R>
+cudaError_t launch_gather(cudaStream_t st, const GridP& g, int B, int D, const R* b0, const R* b1, const uint8_t* par,
+                          size_t start, size_t stride, size_t count, double* out)
+{
+    size_t blocks = (count + kThreads - 1) / kThreads;
+    int grid = (int)(blocks < 4096 ? (blocks ? blocks : 1) : 4096);
+    gather_kernel<R><<<grid, kThreads, 0, st>>>(g, B, D, b0, b1, par, start, stride, count, out);
+    return cudaGetLastError();
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) kh_prim_blocks(GridP g, int B, KHP<R> P, const uint8_t* only)
+{
+    const size_t n = (size_t)g.nx * g.ny;
+    for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (size_t)gridDim.x * kThreads) {
+        const int x = (int)(i % g.nx), y = (int)(i / g.nx);
+        if (only && !only[x / B + g.nbx * (y / B)]) continue;
+        const R vol = (R)P.vol, gm1 = (R)(P.gamma - 1.0);
+        const R r = P.U[0][i] / vol;
+        const R u = P.U[1][i] / r / vol;
+        const R v = P.U[2][i] / r / vol;
+        const R pp = (P.U[3][i] / vol - (R)0.5 * r * (u * u + v * v)) * gm1;
+        P.W[0][i] = r;
+        P.W[1][i] = pp;
+        P.W[2][i] = u;
+        P.W[3][i] = v;
+    }
+}
+
+template <typename R>
+cudaError_t launch_kh_prim_blocks(cudaStream_t st, const GridP& g, int B, const KHP<R>& P, const uint8_t* only)
+{
+    size_t n = (size_t)g.nx * g.ny;
+    size_t blocks = (n + kThreads - 1) / kThreads;
+    int grid = (int)(blocks < 4096 ? blocks : 4096);
+    kh_prim_blocks<R><<<grid, kThreads, 0, st>>>(g, B, P, only);
+    return cudaGetLastError();
+}
+
+template bool shape_supported<REAL_T>(int, int, int);
+template int step_grid<REAL_T>(int, int, int, int);
+template cudaError_t launch_dendrite<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const DenP<REAL_T>&);
+template cudaError_t launch_modelb<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const MBP<REAL_T>&);
+template cudaError_t launch_kh<REAL_T>(int, bool, int, cudaStream_t, const GridP&, const FlagP&, const KHP<REAL_T>&);
+template cudaError_t launch_correct<REAL_T>(int, cudaStream_t, const GridP&, const CorrP<REAL_T>&);
+template cudaError_t launch_gather<REAL_T>(cudaStream_t, const GridP&, int, int, const REAL_T*, const REAL_T*,
+                                           const uint8_t*, size_t, size_t, size_t, double*);
+template cudaError_t launch_kh_prim_blocks<REAL_T>(cudaStream_t, const GridP&, int, const KHP<REAL_T>&, const uint8_t*);
+
+}  // namespace dba

@@ -1,0 +1,255 @@
+// k_kh.cuh -- the 2-D compressible-Euler Kelvin-Helmholtz step over the active
+// blocks (reference: example_Kelvin_Helmholtz/KH_DBA.cu and Conserved/KH_DBA.cu).
+//
+// The reference's DBA step is four kernels over active blocks that keep full
+// intermediate arrays: getPrimitive_wakeup (:418), extrap_in_time_wakeup
+// (:538, central gradients + half-step states + metric1), calc_flux_wakeup
+// (:747, face extrapolation + Rusanov flux), apply_flux_wakeup (:872, in-place
+// update of the conserved fields), then Wakeup_Next (:926, metric1 >
+// Metric_eps) and Wakeup_Neighbor (:988, faces + diagonals).  Cells next to an
+// inactive block read that block's primitives, gradients, half-step states
+// and fluxes as they were at its last active step.  This engine keeps the same
+// four stages and intermediate arrays so those stale reads are reproduced
+// exactly, runs them over a compacted active-block list built on the device
+// (one warp-aggregated atomic per warp), and folds the wake-up test and the
+// neighbour scatter into the gradient stage.
+#pragma once
+
+#include "k_common.cuh"
+
+namespace dba {
+
+template <typename R>
+struct KHP {
+    R* U[4];          // Mass, Momx, Momy, Energy (updated in place)
+    R* W[4];          // rho, p, vx, vy
+    R* Gd[8];         // rho_dx rho_dy p_dx p_dy vx_dx vx_dy vy_dx vy_dy
+    R* Wp[4];         // rho, p, vx, vy half-step states (prime)
+    R* Fl[8];         // Mass_x Energy_x Momx_x Momy_x Mass_y Energy_y Momx_y Momy_y
+    double dt, dx, dy, vol, gamma, thr;
+    int conserved;
+    int* list;        // compacted active blocks of this step
+    int* count;       // number of entries in list
+};
+
+// --- scan: flag bookkeeping and the compacted active list -----------------
+template <bool DBA>
+__global__ void __launch_bounds__(kThreads) kh_scan(GridP g, FlagP f, int* list, int* count, int conserved)
+{
+    const long long b0 = (long long)blockIdx.x * kThreads + threadIdx.x;
+    for (long long bl = b0; bl - threadIdx.x < g.nb; bl += (long long)gridDim.x * kThreads) {
+        const bool valid = bl < g.nb;
+        const int b = (int)bl;
+        int act = 0;
+        if (valid) {
+            act = DBA ? (f.wake_cur[b] ? 1 : 0) : 1;
+            f.wake_clr[b] = 0;
+            if (!DBA) f.wake_nxt[b] = 1;
+            if (conserved && !act)
+                for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = 0.0;
+        }
+        count_stats(f.stats, act, valid);
+        unsigned m = __ballot_sync(0xffffffffu, valid && act);
+        if (m) {
+            int lane = threadIdx.x & 31, leader = __ffs(m) - 1, base = 0;
+            if (lane == leader) base = atomicAdd(count, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (valid && act) list[base + __popc(m & ((1u << lane) - 1u))] = b;
+        }
+    }
+}
+
+__device__ __forceinline__ void kh_cell(const GridP& g, int B, int blk, int v, int& X, int& Y)
+{
+    const int bx = blk % g.nbx, by = blk / g.nbx;
+    X = bx * B + v % B;
+    Y = by * B + v / B;
+}
+
+// --- stage 1: primitives (KH_DBA.cu:461-475) ------------------------------
+template <typename R, int B>
+__global__ void __launch_bounds__(kThreads) kh_prim(GridP g, KHP<R> P)
+{
+    constexpr int V = B * B;
+    const long long total = (long long)(*P.count) * V;
+    for (long long it = (long long)blockIdx.x * kThreads + threadIdx.x; it < total; it += (long long)gridDim.x * kThreads) {
+        int X, Y;
+        kh_cell(g, B, P.list[it / V], (int)(it % V), X, Y);
+        const size_t i = (size_t)X + (size_t)g.nx * Y;
+        const R vol = (R)P.vol, gm1 = (R)(P.gamma - 1.0);
+        const R r = P.U[0][i] / vol;
+        const R u = P.U[1][i] / r / vol;
+        const R v = P.U[2][i] / r / vol;
+        const R pp = (P.U[3][i] / vol - (R)0.5 * r * (u * u + v * v)) * gm1;
+        P.W[0][i] = r;
+        P.W[1][i] = pp;
+        P.W[2][i] = u;
+        P.W[3][i] = v;
+    }
+}
+
+// --- stage 2: gradients, half-step states, metric, wake-up (:584-617, :926-1044)
+template <typename R, int B, bool DBA>
+__global__ void __launch_bounds__(kThreads) kh_extrap(GridP g, FlagP f, KHP<R> P)
+{
+    constexpr int V = B * B;
+    constexpr int K = kThreads / V;
+    __shared__ int s_nx[K];
+    const long long total = (long long)(*P.count) * V;
+    for (long long c0 = (long long)blockIdx.x * kThreads; c0 < total; c0 += (long long)gridDim.x * kThreads) {
+        if (threadIdx.x < K) s_nx[threadIdx.x] = 0;
+        __syncthreads();
+        const long long it = c0 + threadIdx.x;
+        int blk = -1;
+        if (it < total) {
+            blk = P.list[it / V];
+            int X, Y;
+            kh_cell(g, B, blk, (int)(it % V), X, Y);
+            const int xm = wrapc(X - 1, g.nx, 0), xp = wrapc(X + 1, g.nx, 0);
+            const int ym = wrapc(Y - 1, g.ny, 0), yp = wrapc(Y + 1, g.ny, 0);
+            const size_t i = (size_t)X + (size_t)g.nx * Y;
+            const size_t ixm = (size_t)xm + (size_t)g.nx * Y, ixp = (size_t)xp + (size_t)g.nx * Y;
+            const size_t iym = (size_t)X + (size_t)g.nx * ym, iyp = (size_t)X + (size_t)g.nx * yp;
+            const R dx = (R)P.dx, dy = (R)P.dy, hdt = (R)(0.5 * P.dt), gam = (R)P.gamma;
+            R gr[8];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const R* w = P.W[q == 0 ? 0 : (q == 1 ? 1 : (q == 2 ? 2 : 3))];
+                gr[2 * q] = (w[ixp] - w[ixm]) / (R)2.0 / dx;
+                gr[2 * q + 1] = (w[iyp] - w[iym]) / (R)2.0 / dy;
+            }
+            // gr: rho_dx rho_dy p_dx p_dy vx_dx vx_dy vy_dx vy_dy
+#pragma unroll
+            for (int q = 0; q < 8; ++q) P.Gd[q][i] = gr[q];
+            const R r = P.W[0][i], pp = P.W[1][i], u = P.W[2][i], v = P.W[3][i];
+            P.Wp[0][i] = r - hdt * (u * gr[0] + r * gr[4] + v * gr[1] + r * gr[7]);
+            P.Wp[2][i] = u - hdt * (u * gr[4] + v * gr[5] + ((R)1.0 / r) * gr[2]);
+            P.Wp[3][i] = v - hdt * (u * gr[6] + v * gr[7] + ((R)1.0 / r) * gr[3]);
+            P.Wp[1][i] = pp - hdt * (gam * pp * (gr[4] + gr[7]) + u * gr[2] + v * gr[3]);
+            const R metric = fabs(gr[0]) + fabs(gr[1]) + fabs(gr[2]) + fabs(gr[3]) + fabs(gr[4]) + fabs(gr[5]) +
+                             fabs(gr[6]) + fabs(gr[7]);
+            if (DBA && metric > (R)P.thr) s_nx[threadIdx.x / V] = 1;
+        }
+        __syncthreads();
+        if (DBA && threadIdx.x % V == 0 && blk >= 0) {
+            const int k = threadIdx.x / V;
+            f.next[blk] = (uint8_t)s_nx[k];
+            if (s_nx[k]) wake_faces_diag(g, f.wake_nxt, blk);
+        }
+        __syncthreads();
+    }
+}
+
+// Rusanov flux across one face (getFlux, KH_DBA.cu:662-697); outputs in the
+// order Mass, Energy, normal momentum, tangential momentum
+template <typename R>
+__device__ __forceinline__ void kh_getflux(R gam, R rho_L, R rho_R, R p_L, R p_R, R vx_L, R vx_R, R vy_L, R vy_R,
+                                           R& fM, R& fE, R& fX, R& fY)
+{
+    const R en_L = p_L / (gam - (R)1.0) + (R)0.5 * rho_L * (vx_L * vx_L + vy_L * vy_L);
+    const R en_R = p_R / (gam - (R)1.0) + (R)0.5 * rho_R * (vx_R * vx_R + vy_R * vy_R);
+    const R rho_star = (R)0.5 * (rho_L + rho_R);
+    const R momx_star = (R)0.5 * (rho_L * vx_L + rho_R * vx_R);
+    const R momy_star = (R)0.5 * (rho_L * vy_L + rho_R * vy_R);
+    const R en_star = (R)0.5 * (en_L + en_R);
+    const R p_star = (gam - (R)1.0) * (en_star - (R)0.5 * (momx_star * momx_star + momy_star * momy_star) / rho_star);
+    const R fMv = momx_star;
+    const R fXv = momx_star * momx_star / rho_star + p_star;
+    const R fYv = momx_star * momy_star / rho_star;
+    const R fEv = (en_star + p_star) * momx_star / rho_star;
+    const R C_L = sqrt(gam * p_L / rho_L) + fabs(vx_L);
+    const R C_R = sqrt(gam * p_R / rho_R) + fabs(vx_R);
+    const R C = (C_L >= C_R) ? C_L : C_R;
+    fM = fMv - C * (R)0.5 * (rho_L - rho_R);
+    fX = fXv - C * (R)0.5 * (rho_L * vx_L - rho_R * vx_R);
+    fY = fYv - C * (R)0.5 * (rho_L * vy_L - rho_R * vy_R);
+    fE = fEv - C * (R)0.5 * (en_L - en_R);
+}
+
+// --- stage 3: face states and fluxes (:630-660, :792-810) -----------------
+template <typename R, int B>
+__global__ void __launch_bounds__(kThreads) kh_flux(GridP g, KHP<R> P)
+{
+    constexpr int V = B * B;
+    const long long total = (long long)(*P.count) * V;
+    for (long long it = (long long)blockIdx.x * kThreads + threadIdx.x; it < total; it += (long long)gridDim.x * kThreads) {
+        int X, Y;
+        kh_cell(g, B, P.list[it / V], (int)(it % V), X, Y);
+        const int xp = wrapc(X + 1, g.nx, 0), yp = wrapc(Y + 1, g.ny, 0);
+        const size_t i = (size_t)X + (size_t)g.nx * Y;
+        const size_t ixp = (size_t)xp + (size_t)g.nx * Y, iyp = (size_t)X + (size_t)g.nx * yp;
+        const R dx = (R)P.dx, dy = (R)P.dy;
+        R fc[4][4];   // [rho, vx, vy, p][face 0..3]
+        const int wi[4] = {0, 2, 3, 1};      // prime / gradient slot of rho, vx, vy, p
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const R* w = P.Wp[wi[q]];
+            const R* gx = P.Gd[2 * (q == 0 ? 0 : (q == 1 ? 2 : (q == 2 ? 3 : 1)))];
+            const R* gy = P.Gd[2 * (q == 0 ? 0 : (q == 1 ? 2 : (q == 2 ? 3 : 1))) + 1];
+            fc[q][0] = w[ixp] - gx[ixp] * dx / (R)2.0;
+            fc[q][1] = w[i] + gx[i] * dx / (R)2.0;
+            fc[q][2] = w[iyp] - gy[iyp] * dy / (R)2.0;
+            fc[q][3] = w[i] + gy[i] * dy / (R)2.0;
+        }
+        const R gam = (R)P.gamma;
+        R fM, fE, fX, fY;
+        kh_getflux<R>(gam, fc[0][0], fc[0][1], fc[3][0], fc[3][1], fc[1][0], fc[1][1], fc[2][0], fc[2][1], fM, fE, fX, fY);
+        P.Fl[0][i] = fM; P.Fl[1][i] = fE; P.Fl[2][i] = fX; P.Fl[3][i] = fY;
+        // y faces: normal velocity vy, outputs land in Momy_y (normal) and Momx_y (tangential)
+        kh_getflux<R>(gam, fc[0][2], fc[0][3], fc[3][2], fc[3][3], fc[2][2], fc[2][3], fc[1][2], fc[1][3], fM, fE, fX, fY);
+        P.Fl[4][i] = fM; P.Fl[5][i] = fE; P.Fl[7][i] = fX; P.Fl[6][i] = fY;
+    }
+}
+
+// --- stage 4: apply fluxes (:818-841, Conserved :853-856) + change sums ----
+template <typename R, int B>
+__global__ void __launch_bounds__(kThreads) kh_apply(GridP g, FlagP f, KHP<R> P)
+{
+    constexpr int V = B * B;
+    constexpr int K = kThreads / V;
+    __shared__ double s_run[4][kThreads / 32];
+    __shared__ double s_bsum[4][K];
+    const long long total = (long long)(*P.count) * V;
+    for (long long c0 = (long long)blockIdx.x * kThreads; c0 < total; c0 += (long long)gridDim.x * kThreads) {
+        const long long it = c0 + threadIdx.x;
+        double ch[4] = {0.0, 0.0, 0.0, 0.0};
+        int blk = -1;
+        if (it < total) {
+            blk = P.list[it / V];
+            int X, Y;
+            kh_cell(g, B, blk, (int)(it % V), X, Y);
+            const int xm = wrapc(X - 1, g.nx, 0), ym = wrapc(Y - 1, g.ny, 0);
+            const size_t i = (size_t)X + (size_t)g.nx * Y;
+            const size_t ixm = (size_t)xm + (size_t)g.nx * Y, iym = (size_t)X + (size_t)g.nx * ym;
+            const R dtdx = (R)(P.dt * P.dx);
+            // field q takes flux_x slot fx[q] and flux_y slot fy[q]: Mass, Momx, Momy, Energy
+            const int fx[4] = {0, 2, 3, 1}, fy[4] = {4, 6, 7, 5};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const R* Fx = P.Fl[fx[q]];
+                const R* Fy = P.Fl[fy[q]];
+                const R c = dtdx * ((R)-1.0 * Fx[i] + Fx[ixm] - (R)1.0 * Fy[i] + Fy[iym]);
+                const R un = P.U[q][i] + c;
+                P.U[q][i] = un;
+                if (!isfinite(un)) raise_status(f.status, 5);
+                ch[q] = (double)c;
+            }
+        }
+        if (P.conserved) {
+            // Mass, Energy, Momx, Momy order for the sums
+            double cm[1] = {ch[0]}, ce[1] = {ch[3]}, cx[1] = {ch[1]}, cy[1] = {ch[2]};
+            block_tree_sums<V, 1>(cm, s_run[0], s_bsum[0], 0);
+            block_tree_sums<V, 1>(ce, s_run[1], s_bsum[1], 0);
+            block_tree_sums<V, 1>(cx, s_run[2], s_bsum[2], 0);
+            block_tree_sums<V, 1>(cy, s_run[3], s_bsum[3], 0);
+            __syncthreads();
+            if (threadIdx.x % V == 0 && blk >= 0) {
+                const int k = threadIdx.x / V;
+                for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + blk] = s_bsum[q][k];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace dba

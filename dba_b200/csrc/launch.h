@@ -1,0 +1,40 @@
+// launch.h -- host-side launchers for the step kernels.  Each is explicitly
+// instantiated for double in k_f64.cu (built with -fmad=false so FP64 results
+// are bit-identical to the CPU restatement) and for float in k_f32.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "k_common.cuh"
+#include "k_dendrite.cuh"
+#include "k_kh.cuh"
+#include "k_modelb.cuh"
+#include "k_reduce.cuh"
+
+namespace dba {
+
+enum { MODEL_DENDRITE = 0, MODEL_MODELB = 1, MODEL_KH = 2 };
+
+template <typename R> bool shape_supported(int model, int D, int B);
+template <typename R> int step_grid(int model, int D, int B, int sms);
+template <typename R>
+cudaError_t launch_dendrite(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
+                            const DenP<R>& P);
+template <typename R>
+cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
+                          const MBP<R>& P);
+template <typename R>
+cudaError_t launch_kh(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f, const KHP<R>& P);
+template <typename R> cudaError_t launch_correct(int grid, cudaStream_t st, const GridP& g, const CorrP<R>& P);
+// out[k] = buf[par[owner(cell)]][start + k*stride] for k < count (par may be null -> buffer 0)
+template <typename R>
+cudaError_t launch_gather(cudaStream_t st, const GridP& g, int B, int D, const R* b0, const R* b1, const uint8_t* par,
+                          size_t start, size_t stride, size_t count, double* out);
+// KH: recompute primitives from the conserved fields in every block flagged in `only` (all when null)
+template <typename R>
+cudaError_t launch_kh_prim_blocks(cudaStream_t st, const GridP& g, int B, const KHP<R>& P, const uint8_t* only);
+
+cudaError_t launch_reduce(cudaStream_t st, const double* bsum, int nb, int nq, double* l1, unsigned int* ticket,
+                          double* avg, double ncells);
+
+}  // namespace dba

@@ -1,0 +1,264 @@
+"""ctypes binding of include/dba.h and a small Simulation wrapper.
+
+The wrapper mirrors the reference programs' life cycle (ReadInput, Allocate,
+Initialize, time loop, output) one call per stage; see include/dba.h for the
+reference function each entry point replaces.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+MODELS = {"dendrite": 0, "modelb": 1, "kh": 2}
+FIELDS = {
+    0: ["p", "T"],
+    1: ["x", "y", "z", "b", "mu_x", "mu_y", "mu_z"],
+    2: ["Mass", "Momx", "Momy", "Energy", "rho", "p", "vx", "vy"],
+}
+DBA_ERR = {0: "ok", 1: "config", 2: "cuda", 3: "nomem", 4: "io", 5: "nonfinite", 6: "timeout", 7: "state", 8: "arg"}
+
+
+class DBAError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        msg = _lib().dba_strerror(code).decode() if _LIB is not None else DBA_ERR.get(code, "?")
+        super().__init__(f"{what}: DBA status {code} ({msg})")
+
+
+_d, _i, _u64 = ctypes.c_double, ctypes.c_int, ctypes.c_ulonglong
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("model", _i), ("nx", _i), ("ny", _i), ("nz", _i), ("t_total", _i), ("t_freq", _i), ("mode", _i),
+        ("dt", _d), ("dx", _d), ("dy", _d), ("dz", _d),
+        ("delta", _d), ("tau", _d), ("epsilon", _d), ("alpha", _d), ("gamma", _d), ("Delta", _d),
+        ("metric_p", _d), ("metric_T", _d),
+        ("chi_xy", _d), ("chi_xz", _d), ("chi_yz", _d), ("chi_xb", _d), ("chi_yb", _d), ("chi_zb", _d),
+        ("vx", _i), ("vy", _i), ("vz", _i), ("rx", _i), ("ry", _i), ("rz", _i), ("n", _i), ("m", _i),
+        ("eps_x", _d), ("eps_y", _d), ("eps_z", _d), ("eps_phi", _d),
+        ("mob_x", _d), ("mob_y", _d), ("mob_z", _d), ("mob_phi", _d),
+        ("x0", _d), ("y0", _d), ("z0", _d), ("K", _d), ("z_crit", _d), ("p_gel", _d), ("k_0", _d),
+        ("metric_eps", _d), ("kh_gamma", _d),
+        ("block", _i), ("precision", _i), ("bc", _i), ("conserved", _i), ("ic", _i),
+        ("seed", _u64), ("ic_radius", _d), ("ic_width", _d), ("ic_corner", _i),
+        ("noise_amp", _d), ("noise_amp_z", _d),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Obs(ctypes.Structure):
+    _fields_ = [("step", ctypes.c_long), ("time", _d), ("active_blocks", _i * 2), ("total_blocks", _i),
+                ("tip", _d), ("integral", _d * 4), ("vy_mode", _d), ("cell_updates", ctypes.c_long)]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [("nbx", _i), ("nby", _i), ("nbz", _i), ("nb", _i), ("dims", _i), ("nfields", _i),
+                ("nchannels", _i), ("device_bytes", ctypes.c_size_t), ("step", ctypes.c_long), ("grid_ctas", _i)]
+
+
+class Prof(ctypes.Structure):
+    _fields_ = [("steps", _i), ("step_ms", _d), ("stencil_ms", _d), ("reduce_ms", _d), ("correct_ms", _d),
+                ("active_blocks", ctypes.c_long), ("active_blocks_ch", ctypes.c_long * 2),
+                ("ch0_only_blocks", ctypes.c_long), ("cells_per_block", ctypes.c_long)]
+
+
+_LIB = None
+
+
+def lib_path():
+    return os.path.join(_HERE, "libdba_b200.so")
+
+
+def load_library():
+    """Load libdba_b200.so (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} is missing: build it with `python dba_b200/build.py`")
+        L = ctypes.CDLL(path)
+        P, V = ctypes.POINTER, ctypes.c_void_p
+        sig = {
+            "dba_config_default": (_i, [_i, P(Config)]),
+            "dba_parse_input": (_i, [ctypes.c_char_p, _i, P(Config)]),
+            "dba_create": (_i, [P(Config), P(V)]),
+            "dba_init": (_i, [V, P(_d)]),
+            "dba_step": (_i, [V, _i, _i]),
+            "dba_sync": (_i, [V]),
+            "dba_read_field": (_i, [V, _i, P(_d)]),
+            "dba_read_flags": (_i, [V, _i, P(ctypes.c_int32)]),
+            "dba_observables": (_i, [V, P(Obs)]),
+            "dba_tip": (_i, [V, P(_d)]),
+            "dba_write_vtk": (_i, [V, ctypes.c_char_p]),
+            "dba_write_active_vtk": (_i, [V, ctypes.c_char_p]),
+            "dba_checkpoint": (_i, [V, ctypes.c_char_p]),
+            "dba_restore": (_i, [V, ctypes.c_char_p]),
+            "dba_get_info": (_i, [V, P(Info)]),
+            "dba_get_config": (_i, [V, P(Config)]),
+            "dba_destroy": (None, [V]),
+            "dba_strerror": (ctypes.c_char_p, [_i]),
+            "dba_struct_size": (ctypes.c_size_t, [_i]),
+            "dba_step_profiled": (_i, [V, _i, _i, P(Prof)]),
+            "dba_get_stream": (_i, [V, P(V)]),
+            "dba_state_size": (_i, [V, P(ctypes.c_size_t)]),
+            "dba_save_state": (_i, [V, V, ctypes.c_size_t]),
+            "dba_load_state": (_i, [V, V, ctypes.c_size_t]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype, f.argtypes = res, args
+        for k, cls in ((0, Config), (1, Obs), (2, Info), (3, Prof)):
+            if L.dba_struct_size(k) != ctypes.sizeof(cls):
+                raise RuntimeError(f"struct layout mismatch for {cls.__name__}")
+        _LIB = L
+    return _LIB
+
+
+def _lib():
+    return load_library()
+
+
+def _check(code, what):
+    if code != 0:
+        raise DBAError(code, what)
+
+
+def config(model, **overrides):
+    """dba_config_default(model) with fields overridden by keyword."""
+    m = MODELS[model] if isinstance(model, str) else int(model)
+    c = Config()
+    _check(_lib().dba_config_default(m, ctypes.byref(c)), "dba_config_default")
+    for k, v in overrides.items():
+        if not hasattr(c, k):
+            raise KeyError(k)
+        setattr(c, k, v)
+    return c
+
+
+def parse_input(path, model):
+    m = MODELS[model] if isinstance(model, str) else int(model)
+    c = Config()
+    _check(_lib().dba_parse_input(str(path).encode(), m, ctypes.byref(c)), f"dba_parse_input({path})")
+    return c
+
+
+def _buf(buf):
+    if isinstance(buf, np.ndarray):
+        return ctypes.c_void_p(buf.ctypes.data), buf.nbytes
+    # torch tensor (e.g. pinned host memory)
+    return ctypes.c_void_p(buf.data_ptr()), buf.numel() * buf.element_size()
+
+
+class Simulation:
+    """One engine context on the current CUDA device."""
+
+    def __init__(self, cfg):
+        self._L = _lib()
+        self.cfg = cfg
+        self._h = ctypes.c_void_p()
+        _check(self._L.dba_create(ctypes.byref(cfg), ctypes.byref(self._h)), "dba_create")
+        self.shape = (cfg.nz, cfg.ny, cfg.nx)
+        self.n = cfg.nx * cfg.ny * cfg.nz
+        self.fields = FIELDS[cfg.model]
+        self.info = self.get_info()
+
+    def get_info(self):
+        inf = Info()
+        _check(self._L.dba_get_info(self._h, ctypes.byref(inf)), "dba_get_info")
+        return inf
+
+    def init(self, ic=None):
+        if ic is None:
+            _check(self._L.dba_init(self._h, None), "dba_init")
+        else:
+            a = np.ascontiguousarray(np.concatenate([np.asarray(f, np.float64).ravel() for f in ic]))
+            _check(self._L.dba_init(self._h, a.ctypes.data_as(ctypes.POINTER(_d))), "dba_init")
+        return self
+
+    def step(self, n=1, mode=1):
+        _check(self._L.dba_step(self._h, int(n), int(mode)), "dba_step")
+
+    def sync(self):
+        _check(self._L.dba_sync(self._h), "dba_sync")
+
+    def field(self, name):
+        fid = self.fields.index(name) if isinstance(name, str) else int(name)
+        out = np.empty(self.n, np.float64)
+        _check(self._L.dba_read_field(self._h, fid, out.ctypes.data_as(ctypes.POINTER(_d))), "dba_read_field")
+        return out.reshape(self.shape)
+
+    def flags(self, which=0):
+        out = np.empty(self.info.nb, np.int32)
+        _check(self._L.dba_read_flags(self._h, int(which), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))),
+               "dba_read_flags")
+        return out
+
+    def tip(self):
+        v = _d()
+        _check(self._L.dba_tip(self._h, ctypes.byref(v)), "dba_tip")
+        return v.value
+
+    def observables(self):
+        o = Obs()
+        _check(self._L.dba_observables(self._h, ctypes.byref(o)), "dba_observables")
+        return {"step": o.step, "time": o.time, "active_blocks": list(o.active_blocks), "total_blocks": o.total_blocks,
+                "tip": o.tip, "integral": list(o.integral), "vy_mode": o.vy_mode, "cell_updates": o.cell_updates}
+
+    def step_profiled(self, n, mode=1):
+        p = Prof()
+        _check(self._L.dba_step_profiled(self._h, int(n), int(mode), ctypes.byref(p)), "dba_step_profiled")
+        return {k: (list(getattr(p, k)) if k == "active_blocks_ch" else getattr(p, k)) for k, _ in p._fields_}
+
+    @property
+    def stream(self):
+        v = ctypes.c_void_p()
+        _check(self._L.dba_get_stream(self._h, ctypes.byref(v)), "dba_get_stream")
+        return v.value or 0
+
+    def state_size(self):
+        n = ctypes.c_size_t()
+        _check(self._L.dba_state_size(self._h, ctypes.byref(n)), "dba_state_size")
+        return n.value
+
+    def save_state(self, buf):
+        """buf: a writable host buffer (numpy uint8 array or pinned torch tensor data_ptr holder)."""
+        ptr, size = _buf(buf)
+        _check(self._L.dba_save_state(self._h, ptr, size), "dba_save_state")
+
+    def load_state(self, buf):
+        ptr, size = _buf(buf)
+        _check(self._L.dba_load_state(self._h, ptr, size), "dba_load_state")
+
+    def write_vtk(self, path):
+        _check(self._L.dba_write_vtk(self._h, str(path).encode()), "dba_write_vtk")
+
+    def write_active_vtk(self, path):
+        _check(self._L.dba_write_active_vtk(self._h, str(path).encode()), "dba_write_active_vtk")
+
+    def checkpoint(self, path):
+        _check(self._L.dba_checkpoint(self._h, str(path).encode()), "dba_checkpoint")
+
+    def restore(self, path):
+        _check(self._L.dba_restore(self._h, str(path).encode()), "dba_restore")
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.dba_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

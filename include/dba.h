@@ -1,0 +1,237 @@
+/*
+ * dba.h -- C ABI of the B200 dynamic-block-activation (DBA) stencil engine.
+ *
+ * The reference (zhangruoyao68/DBA) has no library API: each model is a
+ * program that reads ./Input.txt, allocates unified-memory arrays, runs a
+ * fixed kernel sequence per time step and writes .vtk/.out files.  These
+ * entry points replace the pieces of those programs, so a host program (the
+ * dba_run executable in this repository, the Python package, or a third
+ * party) can drive the same path.  Plain C types only; every function returns
+ * a status code (DBA_OK or a DBA_ERR_*), never exits the process.
+ *
+ * Threading: one dba_ctx is used by one host thread at a time.  Each context
+ * owns a CUDA stream and all of its device memory; separate contexts may run
+ * concurrently.
+ */
+#ifndef DBA_H
+#define DBA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DBA_ABI_VERSION 1
+
+/* ---- status codes ---- */
+#define DBA_OK 0
+#define DBA_ERR_CONFIG 1      /* invalid or unsupported configuration */
+#define DBA_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define DBA_ERR_NOMEM 3       /* device or host allocation failed */
+#define DBA_ERR_IO 4          /* file could not be opened / parsed */
+#define DBA_ERR_NONFINITE 5   /* a kernel produced NaN/inf in a state field */
+#define DBA_ERR_TIMEOUT 6     /* a bounded device wait gave up */
+#define DBA_ERR_STATE 7       /* call out of order (e.g. step before init) */
+#define DBA_ERR_ARG 8         /* bad argument (null pointer, bad field id) */
+
+/* ---- enumerations ---- */
+#define DBA_MODEL_DENDRITE 0  /* Kobayashi p/T, example_Dendritic_growth/ */
+#define DBA_MODEL_MODELB 1    /* reactive ternary Cahn-Hilliard, example_Reactive_ModelB/ */
+#define DBA_MODEL_KH 2        /* 2-D compressible Euler, example_Kelvin_Helmholtz/ */
+
+#define DBA_PREC_F64 0        /* FP64 stencils; bit-exact with the CPU restatement */
+#define DBA_PREC_F32 1        /* FP32 stencils, FP64 conserved sums and tip tracking */
+
+#define DBA_BC_PERIODIC 0     /* reference: wrap in cells and in block indices */
+#define DBA_BC_ZEROFLUX 1     /* mirror (clamped) neighbours, no block wrap */
+
+#define DBA_MODE_REGULAR 0    /* every block updated (reference mode 0) */
+#define DBA_MODE_DBA 1        /* only active blocks updated (reference mode 1) */
+
+#define DBA_IC_REFERENCE 0    /* the reference program's own initial condition */
+#define DBA_IC_TANH_SEED 1    /* dendrite: tanh-profile solid seed of radius ic_radius */
+#define DBA_IC_SHARP_BANDS 2  /* KH: sharp |y-0.5|<0.25 bands plus seeded white noise */
+
+/* ---- configuration: the reference's Input.txt values plus engine options ---- */
+typedef struct dba_config {
+    int model;                 /* DBA_MODEL_* */
+    int nx, ny, nz;            /* cells; nz == 1 selects the 2-D stencils */
+    int t_total, t_freq;       /* steps and output period (used by dba_run) */
+    int mode;                  /* DBA_MODE_* requested by Input.txt */
+    double dt, dx, dy, dz;
+    /* dendrite (example_Dendritic_growth/kernel.cu:40-64) */
+    double delta, tau, epsilon, alpha, gamma, Delta, metric_p, metric_T;
+    /* Model B (example_Reactive_ModelB/kernel.cu:49-87) */
+    double chi_xy, chi_xz, chi_yz, chi_xb, chi_yb, chi_zb;
+    int vx, vy, vz, rx, ry, rz, n, m;
+    double eps_x, eps_y, eps_z, eps_phi;
+    double mob_x, mob_y, mob_z, mob_phi;
+    double x0, y0, z0, K, z_crit, p_gel, k_0;
+    double metric_eps;         /* Model B and KH wake-up threshold (Metric_eps) */
+    /* KH (example_Kelvin_Helmholtz/KH_DBA.cu:66-85) */
+    double kh_gamma;           /* adiabatic index; the reference hard-codes 5/3 */
+    /* engine options (not in the reference's Input.txt) */
+    int block;                 /* DBA block edge in cells (4 = the reference's dendrite/Model B, 8 = KH) */
+    int precision;             /* DBA_PREC_* */
+    int bc;                    /* DBA_BC_* */
+    int conserved;             /* Model B / KH: the Conserved/ variant (global change removed each step) */
+    int ic;                    /* DBA_IC_* used by dba_init(ctx, NULL) */
+    unsigned long long seed;   /* Model B noise / KH noise seed (mt19937_64) */
+    double ic_radius, ic_width;/* dendrite tanh seed */
+    int ic_corner;             /* dendrite tanh seed at cell (0,0,0) instead of the centre */
+    double noise_amp, noise_amp_z; /* Model B: x,y and z uniform-noise amplitudes (0.05, 0.001) */
+} dba_config;
+
+typedef struct dba_ctx dba_ctx;
+
+/* observables computed on the device at the current step */
+typedef struct dba_obs {
+    long step;                 /* completed steps */
+    double time;               /* simulated time */
+    int active_blocks[2];      /* blocks active for the NEXT step, per channel (dendrite: p, T) */
+    int total_blocks;
+    double tip;                /* dendrite growth_front at x = Nx/2 (NaN if no p < 0.5 found) */
+    double integral[4];        /* dendrite: sum p, sum T; Model B: sum x,y,z,b; KH: sum Mass,Energy,Momx,Momy */
+    double vy_mode;            /* KH: amplitude of the vy mode (Calc_Vy_mode) */
+    long cell_updates;         /* active cell-updates accumulated since dba_init */
+} dba_obs;
+
+typedef struct dba_info {
+    int nbx, nby, nbz, nb;     /* block counts */
+    int dims;                  /* 2 or 3 */
+    int nfields;               /* readable fields */
+    int nchannels;             /* activity channels (2 for dendrite p/T, else 1) */
+    size_t device_bytes;       /* device memory held by the context */
+    long step;
+    int grid_ctas;             /* CTAs per step launch */
+} dba_info;
+
+/* ---- configuration ---- */
+
+/* Defaults of the reference's Input.txt for `model`
+ * (example_Dendritic_growth/Input.txt, example_Reactive_ModelB/Input.txt,
+ * example_Kelvin_Helmholtz/Input.txt) with engine options set to parity mode. */
+int dba_config_default(int model, dba_config* cfg);
+
+/* Replaces ReadInput (example_Dendritic_growth/kernel.cu:67-112,
+ * example_Reactive_ModelB/kernel.cu:90-142, example_Kelvin_Helmholtz/KH_DBA.cu:88-122):
+ * reads the reference's positional Input.txt grammar for `model`.  Fields not
+ * in the file keep their dba_config_default values.  Lines after the
+ * reference grammar may hold `key = value` engine options (block, precision,
+ * bc, conserved, ic, seed, ic_radius, ic_width, ic_corner, gamma_kh,
+ * noise_amp, noise_amp_z). */
+int dba_parse_input(const char* path, int model, dba_config* cfg);
+
+/* ---- lifetime ---- */
+
+/* Replaces Allocate (example_Dendritic_growth/kernel.cu:115-135 and the
+ * models' twins): validates `cfg` and allocates device state on the current
+ * CUDA device. */
+int dba_create(const dba_config* cfg, dba_ctx** out);
+
+/* Replaces Initialize (example_Dendritic_growth/kernel.cu:138-178,
+ * example_Reactive_ModelB/kernel.cu:173-238 with its cuRAND draw :1032-1042,
+ * example_Kelvin_Helmholtz/KH_DBA.cu:1047-1130 + getConserved :335-372).
+ * ic == NULL: the initial condition cfg->ic describes.  Otherwise host FP64
+ * fields, each nx*ny*nz x-fastest: dendrite p,T; Model B x,y,z; KH rho,p,vx,vy.
+ * All blocks start active; the step counter is reset. */
+int dba_init(dba_ctx* ctx, const double* ic);
+
+/* Replaces the body of the time loop of main()
+ * (example_Dendritic_growth/kernel.cu:913-990, example_Reactive_ModelB/kernel.cu:1057-1161,
+ * Conserved/kernel.cu:1095-1190, example_Kelvin_Helmholtz/KH_DBA.cu:1384-1500):
+ * enqueues nsteps steps in `mode` on the context's stream.  Asynchronous;
+ * errors raised on the device are reported by dba_sync. */
+int dba_step(dba_ctx* ctx, int nsteps, int mode);
+
+/* Waits for the context's stream and returns the first device-side status
+ * (DBA_ERR_NONFINITE, DBA_ERR_TIMEOUT) or a CUDA error. */
+int dba_sync(dba_ctx* ctx);
+
+/* Replaces the host reads of the reference's unified-memory fields (the VTK
+ * writers and Integral read them directly): copies field `field` as FP64 into
+ * host[nx*ny*nz].  Field ids: dendrite 0 p, 1 T; Model B 0 x, 1 y, 2 z, 3 b,
+ * 4 mu_x, 5 mu_y, 6 mu_z; KH 0 Mass, 1 Momx, 2 Momy, 3 Energy, 4 rho, 5 p,
+ * 6 vx, 7 vy (primitives recomputed from the conserved fields). */
+int dba_read_field(dba_ctx* ctx, int field, double* host);
+
+/* Replaces the host reads of wake_up / wake_up_next (Output_wakeup,
+ * example_Dendritic_growth/kernel.cu:711-757): which = 2*channel + 0 for the
+ * wake flags of the next step, 2*channel + 1 for the *_next flags the last
+ * step produced.  host[nb] receives 0/1. */
+int dba_read_flags(dba_ctx* ctx, int which, int32_t* host);
+
+/* Replaces Calc_RealTime_Values / growth_front / Integral / Calc_Vy_mode
+ * (example_Dendritic_growth/kernel.cu:759-863, example_Reactive_ModelB/kernel.cu:920-1010,
+ * example_Kelvin_Helmholtz/KH_DBA.cu:1273-1327). */
+int dba_observables(dba_ctx* ctx, dba_obs* obs);
+
+/* Replaces growth_front at x = Nx/2 (example_Dendritic_growth/kernel.cu:759-773)
+ * alone: gathers one column on the device, cheap enough to poll every few
+ * steps.  Dendrite only. */
+int dba_tip(dba_ctx* ctx, double* tip);
+
+/* Replaces Output_vtk / write_output_vtk (example_Dendritic_growth/kernel.cu:637-707,
+ * example_Reactive_ModelB/kernel.cu:766-879, example_Kelvin_Helmholtz/KH_DBA.cu:1132-1202):
+ * ASCII legacy VTK, the reference's header and value formatting. */
+int dba_write_vtk(dba_ctx* ctx, const char* path);
+
+/* Replaces Output_wakeup (example_Dendritic_growth/kernel.cu:711-757,
+ * example_Reactive_ModelB/kernel.cu:882-917, example_Kelvin_Helmholtz/KH_DBA.cu:1205-1240). */
+int dba_write_active_vtk(dba_ctx* ctx, const char* path);
+
+/* No reference counterpart (the reference has no checkpoint): binary
+ * snapshot of every state field, flag, parity bit and counter; restoring and
+ * stepping is bit-identical to not having stopped. */
+int dba_checkpoint(dba_ctx* ctx, const char* path);
+int dba_restore(dba_ctx* ctx, const char* path);
+
+int dba_get_info(dba_ctx* ctx, dba_info* info);
+
+/* Copy of the configuration the context was created with. */
+int dba_get_config(dba_ctx* ctx, dba_config* cfg);
+
+/* per-kernel device time of profiled steps (dba_step_profiled) */
+typedef struct dba_prof {
+    int steps;                 /* steps profiled */
+    double step_ms;            /* device time of all profiled steps */
+    double stencil_ms;         /* device time in the stencil kernel(s): the fused step kernel, or KH's four stages */
+    double reduce_ms;          /* conserved-change reduction */
+    double correct_ms;         /* conserved correction */
+    long active_blocks;        /* block-steps processed (active in any channel) */
+    long active_blocks_ch[2];  /* per channel */
+    long ch0_only_blocks;      /* dendrite: p-active but not T-active block-steps */
+    long cells_per_block;
+} dba_prof;
+
+/* No reference counterpart (the reference brackets each kernel with
+ * cudaEventRecord/cudaEventSynchronize, example_Dendritic_growth/kernel.cu:919-986):
+ * runs nsteps steps without graph capture, with CUDA events around each kernel
+ * class on the context's stream, and returns the device times. */
+int dba_step_profiled(dba_ctx* ctx, int nsteps, int mode, dba_prof* out);
+
+/* The context's CUDA stream (cudaStream_t), for callers that time or order work on it. */
+int dba_get_stream(dba_ctx* ctx, void** stream);
+
+/* No reference counterpart: the checkpoint as an in-memory blob.  dba_save_state
+ * copies device state into host[size] (size from dba_state_size), dba_load_state
+ * copies it back; both are asynchronous on the context's stream when host is
+ * pinned memory and complete before returning otherwise. */
+int dba_state_size(dba_ctx* ctx, size_t* size);
+int dba_save_state(dba_ctx* ctx, void* host, size_t size);
+int dba_load_state(dba_ctx* ctx, const void* host, size_t size);
+
+/* Replaces FreeMemory (example_Dendritic_growth/kernel.cu:866-879). */
+void dba_destroy(dba_ctx* ctx);
+
+const char* dba_strerror(int status);
+
+/* sizeof(dba_config), sizeof(dba_obs), sizeof(dba_info): lets a binding check its struct layout. */
+size_t dba_struct_size(int which);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DBA_H */

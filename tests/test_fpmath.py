@@ -1,0 +1,52 @@
+"""The shared FP64 atan/log/exp (dba_b200/csrc/fpmath.h) against mpmath: <= 2.5 ulp,
+C99 special values.  Run through the CPU build of the same header."""
+import math
+import random
+
+import mpmath as mp
+import pytest
+
+from oracle_lib import lib
+
+mp.mp.dps = 40
+FN = {0: mp.exp, 1: mp.log, 2: mp.atan}
+
+
+def ulp_err(which, x):
+    y = lib().oracle_fm(which, x)
+    t = FN[which](mp.mpf(x))
+    tf = float(t)
+    if tf == 0.0:
+        return abs(y) / 5e-324
+    return float(abs(mp.mpf(y) - t) / math.ulp(tf))
+
+
+@pytest.mark.parametrize("which,lo,hi,logscale", [
+    (0, -700, 700, False), (0, -2, 2, False), (1, -700, 700, True), (1, 0.01, 3.0, False),
+    (2, -8, 8, False), (2, -1e6, 1e6, False)])
+def test_ulp_error(which, lo, hi, logscale):
+    rng = random.Random(1000 + which)
+    worst = 0.0
+    for _ in range(3000):
+        x = rng.uniform(lo, hi)
+        if logscale:
+            x = math.exp(x)
+        worst = max(worst, ulp_err(which, x))
+    assert worst <= 2.5, worst
+
+
+def test_special_values():
+    L = lib()
+    assert L.oracle_fm(0, 0.0) == 1.0
+    assert L.oracle_fm(0, 800.0) == math.inf
+    assert L.oracle_fm(0, -800.0) == 0.0
+    assert math.isnan(L.oracle_fm(0, math.nan))
+    assert L.oracle_fm(1, 1.0) == 0.0
+    assert L.oracle_fm(1, 0.0) == -math.inf
+    assert math.isnan(L.oracle_fm(1, -1.0))
+    assert L.oracle_fm(1, math.inf) == math.inf
+    assert abs(L.oracle_fm(1, 5e-324) - math.log(5e-324)) < 1e-12
+    assert L.oracle_fm(2, 0.0) == 0.0
+    assert L.oracle_fm(2, math.inf) == pytest.approx(math.pi / 2, rel=0, abs=1e-16)
+    assert L.oracle_fm(2, -math.inf) == pytest.approx(-math.pi / 2, rel=0, abs=1e-16)
+    assert L.oracle_fm(2, 1.0) == pytest.approx(math.pi / 4, rel=2e-16)
