@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark of the DBA stencil hot path (active cell-updates/s, HBM roofline).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+A step is one time step of the DBA path over the whole grid.  Default workload
+`modelb_2048_fp32_conserved`: reactive Model B on a 2048^2 periodic grid, FP32
+stencils with FP64 conserved-change sums, 16x16 blocks, conserved DBA.  The
+state is pre-rolled (untimed) to the middle of the 50 000-step run so the timed
+steps see a representative active set, then W warm-up and K timed steps run on
+the engine's own CUDA stream, bracketed by CUDA events (max over ranks).
+
+Multi-GPU: the path does not shard in this build (one domain per GPU), so
+`--gpus N` runs N independent replicas, one process per GPU, and `value` is the
+sum of their active cell-updates divided by the slowest rank's time.
+
+`--impl reference` times the reference's own serial CPU program for the same
+model (its functions driven step by step by oracle/_ref/*_cpu_steps, built from
+the reference sources) on this host; rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# bytes read + written per active cell-update by the algorithm (state fields only)
+ALG_BYTES = {"dendrite": 4, "modelb": 6, "kh": 8}   # x element size
+
+WORKLOADS = {
+    # C1: reactive Model B, conserved DBA.  Symmetric quench inside the z-b
+    # spinodal (x0=y0=0.05, z0=0.45, uniform noise +-0.01, chi_zb=3), mobility 1,
+    # gradient coefficient 1, reaction rate 1e-4, dt=0.001 (0.005 diverges).
+    "modelb_2048_fp32_conserved": dict(
+        model="modelb", nx=2048, ny=2048, nz=1, block=16, precision=1, conserved=1, mode=1, t_total=50000,
+        params=dict(dt=0.001, chi_zb=3.0, eps_x=1.0, eps_y=1.0, eps_z=1.0, k_0=1e-4, metric_eps=1e-3, x0=0.05,
+                    y0=0.05, z0=0.45, noise_amp=0.02, noise_amp_z=0.02)),
+    # C0: 2-D dendrite, FP64, 512^2, tanh seed r=10 at the centre, zero-flux walls, 8x8 blocks
+    "dendrite_512_fp64": dict(
+        model="dendrite", nx=512, ny=512, nz=1, block=8, precision=0, conserved=0, mode=1, t_total=10000,
+        params=dict(Delta=0.55, delta=0.05, metric_p=1e-3, metric_T=1e-5, ic=1, ic_radius=10.0, ic_width=2.0, bc=1)),
+    # C2: KH 4096^2 FP32, 16x16 blocks, gamma 1.4, sharp bands + seeded noise
+    "kh_4096_fp32": dict(
+        model="kh", nx=4096, ny=4096, nz=1, block=16, precision=1, conserved=0, mode=1, t_total=50000,
+        params=dict(dt=1.0 / 4096 * 0.4 / 3.0, dx=1.0 / 4096, dy=1.0 / 4096, kh_gamma=1.4, metric_eps=1.0, ic=2,
+                    noise_amp=1e-4)),
+}
+
+
+def make_config(w):
+    import dba_b200
+    c = dba_b200.config(w["model"], nx=w["nx"], ny=w["ny"], nz=w["nz"], block=w["block"],
+                        precision=w["precision"], conserved=w["conserved"])
+    for k, v in w["params"].items():
+        setattr(c, k, v)
+    c.t_total = w["t_total"]
+    return c
+
+
+def hbm_peak():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.flush()
+        try:
+            rows = [r.split(",") for r in open(self.out.name).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_ours(args, w):
+    import datetime
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import dba_b200
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    cfg = make_config(w)
+    sim = dba_b200.Simulation(cfg).init()
+    stream = torch.cuda.ExternalStream(sim.stream)
+    # pre-roll to mid-run (untimed), then warm-up
+    preroll = w["t_total"] // 2 if args.preroll < 0 else args.preroll
+    if preroll:
+        sim.step(preroll, w["mode"])
+    sim.step(args.warmup, w["mode"])
+    sim.sync()
+    # host copy of this state: the end-to-end run below starts from it
+    blob = torch.empty(sim.state_size(), dtype=torch.uint8, pin_memory=True)
+    sim.save_state(blob)
+    prof0 = sim.step_profiled(1, w["mode"])   # also a final warm-up of the direct-launch path
+    sim.load_state(blob)
+    sim.sync()
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    st0 = sim.cell_updates()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        sim.step(args.steps, w["mode"])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    status = sim._L.dba_sync(sim._h)
+    ms = ev0.elapsed_time(ev1)
+    cells = sim.cell_updates() - st0
+    t_max = ms
+    cells_all = cells
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+        c = torch.tensor([float(cells)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        cells_all = float(c.item())
+
+    # dominant kernel: the fused stencil kernel, timed per launch with CUDA events on the same stream
+    sim.load_state(blob)
+    nprof = min(args.steps, 200)
+    prof = sim.step_profiled(nprof, w["mode"])
+    esz = 8 if w["precision"] == 0 else 4
+    per_cell = ALG_BYTES[w["model"]] * esz
+    if w["model"] == "dendrite":
+        alg = esz * (2 * prof["active_blocks_ch"][0] + 2 * prof["active_blocks_ch"][1] + prof["ch0_only_blocks"]) \
+            * prof["cells_per_block"]
+    else:
+        alg = per_cell * prof["active_blocks"] * prof["cells_per_block"]
+    achieved = alg / (prof["stencil_ms"] * 1e-3) / 1e9 if prof["stencil_ms"] > 0 else 0.0
+    peak, peak_kind = hbm_peak()
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", f"{args.workload}.traffic.json")
+    if os.path.exists(tfile) and prof["active_blocks"]:
+        try:
+            tj = json.load(open(tfile))
+            traffic = tj["dram_bytes_per_active_cell"] * prof["active_blocks"] * prof["cells_per_block"] / nprof
+        except Exception:
+            traffic = None
+
+    # end to end through the public API: host state in pinned memory -> device, K steps, fields -> host
+    n = cfg.nx * cfg.ny * cfg.nz
+    nf = {"dendrite": 2, "modelb": 3, "kh": 4}[w["model"]]
+    out_host = np.empty((nf, n))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.load_state(blob)
+    st_e0 = sim.cell_updates()
+    sim.step(args.steps, w["mode"])
+    for q in range(nf):
+        out_host[q] = sim.field(q).ravel()
+    t_e2e = (time.perf_counter() - t0) * 1e3
+    cells_e2e = sim.cell_updates() - st_e0
+    h2d = blob.numel()
+    d2h = out_host.nbytes
+    if world > 1:
+        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+        c = torch.tensor([float(cells_e2e)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        cells_e2e = float(c.item())
+
+    result = None
+    if rank == 0:
+        value = cells_all / (t_max * 1e-3)
+        total_blocks = sim.info.nb
+        active_frac = cells / max(1, args.steps) / (total_blocks * prof["cells_per_block"])
+        result = {
+            "metric": "active cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if w["precision"] else "f64",
+            "data": "synthetic (seeded initial condition)",
+            "config": {"workload": args.workload, "model": w["model"], "grid": [cfg.nx, cfg.ny, cfg.nz],
+                       "block": cfg.block, "conserved": bool(cfg.conserved), "mode": "DBA" if w["mode"] else "regular",
+                       "preroll_steps": preroll, "active_fraction": active_frac,
+                       "l2": "state larger than L2 (%.0f MB resident), no flush" % (sim.info.device_bytes / 1e6),
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": cells_e2e / (t_e2e * 1e-3), "unit": "cell-updates/s",
+                    "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if peak else None, "traffic": traffic,
+                         "kernel": f"{w['model']}_step", "peak_kind": peak_kind,
+                         "alg_bytes_per_active_cell": per_cell, "kernel_ms_avg": prof["stencil_ms"] / nprof,
+                         "frac_of_8tbs_spec": achieved / 8000.0},
+            "step_breakdown_ms": {"stencil": prof["stencil_ms"] / nprof, "reduce": prof["reduce_ms"] / nprof,
+                                  "correct": prof["correct_ms"] / nprof},
+            "gpu_launches": args.steps * launches_per_step(w),
+            "clocks": clk.summary(),
+            "status": status,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline(w, seconds=args.cpu_seconds)
+    sim.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def launches_per_step(w):
+    if w["model"] == "kh":
+        return 5 + (2 if w["conserved"] else 0)
+    return 1 + (2 if w["conserved"] and w["model"] == "modelb" else 0)
+
+
+def _ref_input(w, nx, ny):
+    p = w["params"]
+    if w["model"] == "modelb":
+        return (f"{nx} {ny} 1\n10 5 {p['dt']}\n1 1 1\n0 0 0 0 0 {p.get('chi_zb', 4)}\n1 1 2\n1 1 2\n1 1\n"
+                f"{p['eps_x']} {p['eps_y']} {p['eps_z']} 0.01\n1 1 1 1\n{p['x0']} {p['y0']} {p['z0']}\n100 0.4 1\n"
+                f"{p['k_0']}\n{p['metric_eps']}\n0\n")
+    if w["model"] == "kh":
+        return f"{nx} {ny} 1\n10 5 {p['dt']}\n{p['dx']} {p['dy']} {p['dx']}\n0\n0\n"
+    raise ValueError(w["model"])
+
+
+def time_reference_cpu(w, nsteps):
+    """Wall time of nsteps steps of the reference's serial CPU program on the workload's grid."""
+    binary = {"modelb": "modelb_cpu_steps", "kh": "kh_cpu_steps"}.get(w["model"])
+    path = os.path.join(ROOT, "oracle", "_ref", binary) if binary else None
+    d = tempfile.mkdtemp()
+    if path and os.path.exists(path):
+        with open(os.path.join(d, "Input.txt"), "w") as f:
+            f.write(_ref_input(w, w["nx"], w["ny"]))
+        out = subprocess.run([path, os.path.join(d, "Input.txt"), str(nsteps), "-"], capture_output=True, text=True,
+                             check=True).stdout
+        secs = float([ln for ln in out.splitlines() if ln.startswith("LOOP_SECONDS")][-1].split()[1])
+        return secs, "reference", f"{binary} (reference CPU_version functions, regular mode, FP64)"
+    # the reference's dendrite CPU program is single precision with fixed ghosts; time the FP64 restatement
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from cases import DENDRITE_REF
+    from oracle_lib import OracleDendrite
+    prm = dict(DENDRITE_REF, **{k: v for k, v in w["params"].items() if k in DENDRITE_REF})
+    o = OracleDendrite(w["nx"], w["ny"], w["nz"], w["block"], prm, bc=w["params"].get("bc", 0))
+    o.init_cone()
+    t0 = time.perf_counter()
+    o.step(nsteps, 0)
+    return time.perf_counter() - t0, "port", "oracle restatement, regular mode, FP64"
+
+
+def cpu_baseline(w, seconds=15.0):
+    cells = w["nx"] * w["ny"] * w["nz"]
+    # size the sample to about `seconds` of CPU time from a short probe
+    t1, kind, what = time_reference_cpu(w, 1)
+    n = max(1, min(200, int(seconds / max(t1, 1e-3))))
+    t, kind, what = time_reference_cpu(w, n)
+    return {"value": cells * n / t, "unit": "cell-updates/s", "cores": 1, "kind": kind,
+            "sample": f"{what}: {w['nx']}x{w['ny']}x{w['nz']} grid, {n} steps (all cells updated), {t:.2f} s, 1 thread"}
+
+
+def run_reference(args, w):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return None
+    # each bench step is one reference time step on the full grid; the warm-up
+    # steps are timed in a separate run and subtracted
+    secs, kind, what = time_reference_cpu(w, args.warmup + args.steps)
+    if args.warmup:
+        t_w, _, _ = time_reference_cpu(w, args.warmup)
+        secs = max(secs - t_w, 1e-9)
+    cells = w["nx"] * w["ny"] * w["nz"] * args.steps
+    value = cells / secs
+    return {
+        "metric": "active cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded initial condition)",
+        "impl": "reference",
+        "config": {"workload": args.workload, "model": w["model"], "grid": [w["nx"], w["ny"], w["nz"]],
+                   "mode": "regular (the reference CPU program has no DBA)"},
+        "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": 1, "kind": kind,
+                         "sample": f"{what}: {w['nx']}x{w['ny']}x{w['nz']}, {args.steps} timed steps"},
+        "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="modelb_2048_fp32_conserved", choices=sorted(WORKLOADS))
+    ap.add_argument("--preroll", type=int, default=-1, help="untimed steps before warm-up (default: half the run)")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        if args.steps > 40:
+            args.steps = 40   # each reference step is a full dense CPU step; keep the run to minutes
+        if args.warmup > 2:
+            args.warmup = 2
+        res = run_reference(args, w)
+    else:
+        res = run_ours(args, w)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -765,6 +765,11 @@ int dba_get_info(dba_ctx* c, dba_info* info)
     info->device_bytes = bytes;
     info->step = c->step;
     info->grid_ctas = c->grid;
+    unsigned long long stats[4] = {0, 0, 0, 0};
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    DBA_TRY(cudaMemcpy(stats, c->stats, sizeof stats, cudaMemcpyDeviceToHost));
+    info->active_block_steps = (long)stats[2];
+    info->cells_per_block = (long)(c->n / c->g.nb);
     return DBA_OK;
 }
 

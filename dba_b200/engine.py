@@ -58,7 +58,8 @@ class Obs(ctypes.Structure):
 
 class Info(ctypes.Structure):
     _fields_ = [("nbx", _i), ("nby", _i), ("nbz", _i), ("nb", _i), ("dims", _i), ("nfields", _i),
-                ("nchannels", _i), ("device_bytes", ctypes.c_size_t), ("step", ctypes.c_long), ("grid_ctas", _i)]
+                ("nchannels", _i), ("device_bytes", ctypes.c_size_t), ("step", ctypes.c_long), ("grid_ctas", _i),
+                ("active_block_steps", ctypes.c_long), ("cells_per_block", ctypes.c_long)]
 
 
 class Prof(ctypes.Structure):
@@ -197,6 +198,11 @@ class Simulation:
         _check(self._L.dba_read_flags(self._h, int(which), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))),
                "dba_read_flags")
         return out
+
+    def cell_updates(self):
+        """Active cell-updates (cells of blocks active in any channel) since init."""
+        inf = self.get_info()
+        return inf.active_block_steps * inf.cells_per_block
 
     def tip(self):
         v = _d()

@@ -106,6 +106,8 @@ typedef struct dba_info {
     size_t device_bytes;       /* device memory held by the context */
     long step;
     int grid_ctas;             /* CTAs per step launch */
+    long active_block_steps;   /* blocks processed (active in any channel), summed over steps since dba_init */
+    long cells_per_block;
 } dba_info;
 
 /* ---- configuration ---- */

@@ -4,9 +4,12 @@
 // extrap_in_time :325, calc_flux :438, apply_flux :499) in the order of its
 // main() (:710-790) for N steps and writes Mass, Momx, Momy, Energy, rho, p,
 // vx, vy as raw FP64.  The reference file is compiled from where it lies.
+// With out.bin == "-" nothing is written and the step loop's wall time is
+// printed instead (the timed CPU baseline).
 #define main dba_reference_program_main
 #include REF_SRC
 #undef main
+#include <chrono>
 #include <cstdio>
 
 int main(int argc, char** argv)
@@ -23,6 +26,7 @@ int main(int argc, char** argv)
     Initialize(V.rho, V.p, V.vx, V.vy, P);
     getConserved(V.Mass, V.Energy, V.Momx, V.Momy, V.rho, V.p, V.vx, V.vy, P);
     int nsteps = std::atoi(argv[2]);
+    auto t0 = std::chrono::steady_clock::now();
     for (int t = 1; t <= nsteps; ++t) {
         getPrimitive(V.rho, V.p, V.vx, V.vy, V.Mass, V.Energy, V.Momx, V.Momy, P);
         extrap_in_time(V.rho, V.p, V.vx, V.vy, V.rho_dx, V.rho_dy, V.p_dx, V.p_dy, V.vx_dx, V.vx_dy, V.vy_dx,
@@ -32,6 +36,11 @@ int main(int argc, char** argv)
                   V.flux_Momy_x, V.flux_Mass_y, V.flux_Energy_y, V.flux_Momx_y, V.flux_Momy_y, P);
         apply_flux(V.Mass, V.Energy, V.Momx, V.Momy, V.flux_Mass_x, V.flux_Energy_x, V.flux_Momx_x, V.flux_Momy_x,
                    V.flux_Mass_y, V.flux_Energy_y, V.flux_Momx_y, V.flux_Momy_y, P);
+    }
+    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (std::string(argv[3]) == "-") {
+        std::printf("LOOP_SECONDS %.9f\n", secs);
+        return 0;
     }
     FILE* f = std::fopen(argv[3], "wb");
     if (!f) return 1;

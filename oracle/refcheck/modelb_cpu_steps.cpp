@@ -4,10 +4,13 @@
 // for N steps from the mt19937_64(1234) initial condition of its main()
 // (:540-549) and writes x, y, z, b, dfdx, dfdy, dfdz as raw FP64.
 // The reference file is compiled from where it lies (REF_SRC); its main() is
-// renamed so this one drives it.
+// renamed so this one drives it.  With out.bin == "-" nothing is written and
+// the wall time of the step loop (steady_clock, seconds) is printed instead:
+// the timed CPU baseline.
 #define main dba_reference_program_main
 #include REF_SRC
 #undef main
+#include <chrono>
 #include <cstdio>
 
 int main(int argc, char** argv)
@@ -30,11 +33,17 @@ int main(int argc, char** argv)
     }
     Initialize(V.x_old, V.y_old, V.z_old, V.b, V.phi_old, P);
     int nsteps = std::atoi(argv[2]);
+    auto t0 = std::chrono::steady_clock::now();
     for (int t = 1; t <= nsteps; ++t) {
         Calc_mu(V.x_old, V.y_old, V.z_old, V.b, V.phi_old, V.dfdx, V.dfdy, V.dfdz, P);
         Update(V.x_new, V.y_new, V.z_new, V.phi_new, V.x_old, V.y_old, V.z_old, V.phi_old, V.b, V.dfdx, V.dfdy,
                V.dfdz, P);
         Swap_regular(V.x_old, V.x_new, V.y_old, V.y_new, V.z_old, V.z_new, P);
+    }
+    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (std::string(argv[3]) == "-") {
+        std::printf("LOOP_SECONDS %.9f\n", secs);
+        return 0;
     }
     FILE* f = std::fopen(argv[3], "wb");
     if (!f) return 1;
