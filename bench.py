@@ -127,6 +127,20 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def aggregate(ms, cells, world, device="cuda"):
+    """Replica aggregation: the slowest rank's time and the sum of all ranks' cell-updates.
+    Every rank takes the same collective steps in the same order."""
+    if world <= 1:
+        return ms, cells
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(cells)], device=device, dtype=torch.float64)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(c.item())
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -177,15 +191,7 @@ def run_ours(args, w):
     status = sim._L.dba_sync(sim._h)
     ms = ev0.elapsed_time(ev1)
     cells = sim.cell_updates() - st0
-    t_max = ms
-    cells_all = cells
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-        c = torch.tensor([float(cells)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        cells_all = float(c.item())
+    t_max, cells_all = aggregate(ms, cells, world)
 
     # dominant kernel: the fused stencil kernel, timed per launch with CUDA events on the same stream
     sim.load_state(blob)
@@ -226,13 +232,7 @@ def run_ours(args, w):
     cells_e2e = sim.cell_updates() - st_e0
     h2d = blob.numel()
     d2h = out_host.nbytes
-    if world > 1:
-        t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
-        c = torch.tensor([float(cells_e2e)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        cells_e2e = float(c.item())
+    t_e2e, cells_e2e = aggregate(t_e2e, cells_e2e, world)
 
     result = None
     if rank == 0:

@@ -55,6 +55,13 @@ struct dba_ctx {
     long step = 0;
     double time = 0.0;
     bool initialized = false;
+    // FP32 2-D Model B conserved: lazy correction state (k_modelb_fast.cuh)
+    bool lazy = false;
+    double* stamp = nullptr;          // [3][nb]
+    double* cum = nullptr;            // [3]
+    double* cta_part = nullptr;       // [3][grid]
+    double* lavg = nullptr;           // [3]
+    unsigned int* lticket = nullptr;
     cudaGraphExec_t graphs[6][2] = {};
     bool use_graphs = true;
     int last_error = DBA_OK;
@@ -206,6 +213,19 @@ CorrP<R> corr_params(dba_ctx* c, long s)
     return P;
 }
 
+LazyP lazy_params(dba_ctx* c, bool conserved_step)
+{
+    LazyP L{};
+    L.stamp = c->stamp;
+    L.cum = c->cum;
+    L.cta_part = c->cta_part;
+    L.avg = c->lavg;
+    L.ticket = c->lticket;
+    L.ncells = (double)c->n;
+    L.lazy = (c->lazy && conserved_step) ? 1 : 0;
+    return L;
+}
+
 template <typename R>
 cudaError_t enqueue_step_t(dba_ctx* c, long s, bool dba_mode)
 {
@@ -216,8 +236,9 @@ cudaError_t enqueue_step_t(dba_ctx* c, long s, bool dba_mode)
         return launch_dendrite<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<R>(c));
     case DBA_MODEL_MODELB: {
         MBP<R> P = mb_params<R>(c, dba_mode);
-        e = launch_modelb<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P);
-        if (e != cudaSuccess || !P.conserved) return e;
+        LazyP L = lazy_params(c, P.conserved != 0);
+        e = launch_modelb<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L);
+        if (e != cudaSuccess || !P.conserved || c->lazy) return e;
         break;
     }
     case DBA_MODEL_KH: {
@@ -504,6 +525,18 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
     }
     c->grid = c->esz == 8 ? step_grid<double>(cfg->model, c->D, c->B, c->sms) : step_grid<float>(cfg->model, c->D, c->B, c->sms);
     if (c->grid < 1) c->grid = c->sms;
+    if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->conserved && modelb_uses_fast<float>(c->D, c->B)) {
+        c->lazy = true;
+        c->stamp = (double*)dev_alloc(c, 3 * nb * sizeof(double), &err);
+        if (!err) c->cum = (double*)dev_alloc(c, 3 * sizeof(double), &err);
+        if (!err) c->cta_part = (double*)dev_alloc(c, 3 * (size_t)c->grid * sizeof(double), &err);
+        if (!err) c->lavg = (double*)dev_alloc(c, 3 * sizeof(double), &err);
+        if (!err) c->lticket = (unsigned int*)dev_alloc(c, sizeof(unsigned int), &err);
+        if (err) {
+            dba_destroy(c);
+            return err;
+        }
+    }
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         dba_destroy(c);
@@ -626,6 +659,24 @@ int dba_read_field(dba_ctx* c, int field, double* host)
     if (model == DBA_MODEL_DENDRITE)   // p and T have their own activity channel and buffer parity
         return gather(c, c->state[field][0], c->state[field][1], cur_par(c) + (size_t)field * c->g.nb, 0, 1, c->n, host);
     if (model == DBA_MODEL_MODELB) {
+        if (c->lazy && field < 4) {
+            // true values: stored - (C - stamp[owner]) per field (lazy conserved correction)
+            std::vector<double> tmp;
+            const int nq = field < 3 ? 1 : 3;
+            if (nq == 3) tmp.resize(2 * c->n);
+            for (int q = field < 3 ? field : 0, k = 0; k < nq; ++q, ++k) {
+                double* dst = (k == 0) ? host : tmp.data() + (k - 1) * c->n;
+                cudaError_t e = launch_gather_lazy(c->st, c->g, c->B, (const float*)c->state[q][0],
+                                                   (const float*)c->state[q][1], cur_par(c), c->stamp + (size_t)q * c->g.nb,
+                                                   c->cum + q, c->n, c->staging);
+                if (e == cudaSuccess) e = cudaMemcpyAsync(dst, c->staging, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+                if (e != cudaSuccess) return cuda_status(e);
+            }
+            if (nq == 3)
+                for (size_t i = 0; i < c->n; ++i) host[i] = 1.0 - host[i] - tmp[i] - tmp[c->n + i];
+            return DBA_OK;
+        }
         if (field < 3) return gather(c, c->state[field][0], c->state[field][1], cur_par(c), 0, 1, c->n, host);
         if (field >= 4) return gather(c, c->aux[field - 4], c->aux[field - 4], nullptr, 0, 1, c->n, host);
         // b = 1 - x - y - z of the current state (Update, kernel.cu:434)
@@ -787,7 +838,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
     if (nsteps < 1 || (mode != 0 && mode != 1)) return DBA_ERR_ARG;
     std::memset(out, 0, sizeof *out);
     const bool dba_mode = mode == DBA_MODE_DBA;
-    const bool cons = c->nsum && c->cfg.conserved && dba_mode;
+    const bool cons = c->nsum && c->cfg.conserved && dba_mode && !c->lazy;
     std::vector<cudaEvent_t> ev((size_t)nsteps * 4 + 2);
     for (auto& e : ev) DBA_TRY(cudaEventCreate(&e));
     unsigned long long s0[4], s1[4];
@@ -803,14 +854,22 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
         if (r == cudaSuccess) {
             if (c->esz == 8) {
                 if (c->cfg.model == DBA_MODEL_DENDRITE) r = launch_dendrite<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<double>(c));
-                else if (c->cfg.model == DBA_MODEL_MODELB) r = launch_modelb<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, mb_params<double>(c, dba_mode));
+                else if (c->cfg.model == DBA_MODEL_MODELB) {
+                    MBP<double> P = mb_params<double>(c, dba_mode);
+                    LazyP L = lazy_params(c, P.conserved != 0);
+                    r = launch_modelb<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L);
+                }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
                     if (r == cudaSuccess) r = launch_kh<double>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_params<double>(c, dba_mode));
                 }
             } else {
                 if (c->cfg.model == DBA_MODEL_DENDRITE) r = launch_dendrite<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<float>(c));
-                else if (c->cfg.model == DBA_MODEL_MODELB) r = launch_modelb<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, mb_params<float>(c, dba_mode));
+                else if (c->cfg.model == DBA_MODEL_MODELB) {
+                    MBP<float> P = mb_params<float>(c, dba_mode);
+                    LazyP L = lazy_params(c, P.conserved != 0);
+                    r = launch_modelb<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L);
+                }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
                     if (r == cudaSuccess) r = launch_kh<float>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_params<float>(c, dba_mode));

@@ -66,28 +66,32 @@ __device__ __forceinline__ int block_nb(const GridP& g, int b, int dx, int dy, i
     return bx + g.nbx * (by + g.nby * bz);
 }
 
+__device__ __forceinline__ void wake_one(const GridP& g, uint8_t* w, int b, int dx, int dy, int dz)
+{
+    const int nb = block_nb(g, b, dx, dy, dz);
+    if (nb >= 0) w[nb] = 1;
+}
+
 // self + 6 faces (example_Dendritic_growth/kernel.cu:596-628)
 __device__ __forceinline__ void wake_faces(const GridP& g, uint8_t* w, int b)
 {
     w[b] = 1;
-    const int d[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        int nb = block_nb(g, b, d[k][0], d[k][1], d[k][2]);
-        if (nb >= 0) w[nb] = 1;
-    }
+    wake_one(g, w, b, -1, 0, 0);
+    wake_one(g, w, b, 1, 0, 0);
+    wake_one(g, w, b, 0, -1, 0);
+    wake_one(g, w, b, 0, 1, 0);
+    wake_one(g, w, b, 0, 0, -1);
+    wake_one(g, w, b, 0, 0, 1);
 }
 
 // self + faces + 4 in-plane diagonals (example_Kelvin_Helmholtz/KH_DBA.cu:1026-1039)
 __device__ __forceinline__ void wake_faces_diag(const GridP& g, uint8_t* w, int b)
 {
     wake_faces(g, w, b);
-    const int d[4][2] = {{-1, -1}, {-1, 1}, {1, -1}, {1, 1}};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int nb = block_nb(g, b, d[k][0], d[k][1], 0);
-        if (nb >= 0) w[nb] = 1;
-    }
+    wake_one(g, w, b, -1, -1, 0);
+    wake_one(g, w, b, -1, 1, 0);
+    wake_one(g, w, b, 1, -1, 0);
+    wake_one(g, w, b, 1, 1, 0);
 }
 
 __device__ __forceinline__ void raise_status(int* status, int code)

@@ -48,7 +48,9 @@ template <typename R>
 int step_grid(int model, int D, int B, int sms)
 {
 #define XD(d, b) if (D == d && B == b) return grid_of<R>((const void*)dendrite_step<R, d, b, true>, 0, sms);
-#define XM(d, b) if (D == d && B == b) { size_t sm; mb_prepare<R, d, b>(sm); return grid_of<R>((const void*)modelb_step<R, d, b, true>, sm, sms); }
+#define XM(d, b) if (D == d && B == b) { size_t sm; mb_prepare<R, d, b>(sm); \
+    if constexpr (sizeof(R) == 4 && d == 2) return grid_of<R>((const void*)modelb_fast_step<b, true>, MBFastShape<b>::smem, sms); \
+    return grid_of<R>((const void*)modelb_step<R, d, b, true>, sm, sms); }
 #define XK(b) if (B == b) return grid_of<R>((const void*)kh_extrap<R, b, true>, 0, sms);
     if (model == MODEL_DENDRITE) { DBA_DEN_SHAPES(XD) }
     if (model == MODEL_MODELB) { DBA_MB_SHAPES(XM) }
@@ -75,9 +77,32 @@ cudaError_t launch_dendrite(int D, int B, bool dba_mode, int grid, cudaStream_t 
 }
 
 template <typename R>
-cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
-                          const MBP<R>& P)
+bool modelb_uses_fast(int D, int B)
 {
+    return sizeof(R) == 4 && D == 2 && (B == 4 || B == 8 || B == 16 || B == 32);
+}
+
+template <typename R>
+cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
+                          const MBP<R>& P, const LazyP* lz)
+{
+    if constexpr (sizeof(R) == 4) {
+        if (modelb_uses_fast<R>(D, B)) {
+            LazyP L{};
+            if (lz) L = *lz;
+            const MBFastP FP = make_fast_params(P);
+            const MBFastBuf FB = make_fast_buf(P);
+#define XF(b)                                                                                   \
+    if (B == b) {                                                                               \
+        const size_t sm = MBFastShape<b>::smem;                                                 \
+        if (dba_mode) modelb_fast_step<b, true><<<grid, kThreads, sm, st>>>(g, f, FP, FB, L);   \
+        else modelb_fast_step<b, false><<<grid, kThreads, sm, st>>>(g, f, FP, FB, L);           \
+        return cudaGetLastError();                                                              \
+    }
+            XF(4) XF(8) XF(16) XF(32)
+#undef XF
+        }
+    }
 #define XM(d, b)                                                                            \
     if (D == d && B == b) {                                                                 \
         size_t sm;                                                                          \
@@ -88,6 +113,7 @@ cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st
     }
     DBA_MB_SHAPES(XM)
 #undef XM
+    (void)lz;
     return cudaErrorInvalidValue;
 }
 
@@ -176,7 +202,8 @@ cudaError_t launch_kh_prim_blocks(cudaStream_t st, const GridP& g, int B, const 
 template bool shape_supported<REAL_T>(int, int, int);
 template int step_grid<REAL_T>(int, int, int, int);
 template cudaError_t launch_dendrite<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const DenP<REAL_T>&);
-template cudaError_t launch_modelb<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const MBP<REAL_T>&);
+template cudaError_t launch_modelb<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const MBP<REAL_T>&, const LazyP*);
+template bool modelb_uses_fast<REAL_T>(int, int);
 template cudaError_t launch_kh<REAL_T>(int, bool, int, cudaStream_t, const GridP&, const FlagP&, const KHP<REAL_T>&);
 template cudaError_t launch_correct<REAL_T>(int, cudaStream_t, const GridP&, const CorrP<REAL_T>&);
 template cudaError_t launch_gather<REAL_T>(cudaStream_t, const GridP&, int, int, const REAL_T*, const REAL_T*,

@@ -1,0 +1,351 @@
+// k_modelb_fast.cuh -- FP32 2-D Model B step (the throughput path).
+//
+// Same DBA semantics as modelb_step (k_modelb.cuh): potentials recomputed for
+// halo cells whose block is active, persisted (stale) potentials read where it
+// is not, per-block ping-pong buffers.  What changes for speed:
+//   * staging looks up owner parity (and conserved offset) once per neighbour
+//     block, not per cell;
+//   * the reference's 27-term Laplacian is evaluated in its exact 2-D form
+//     (Nz == 1: weights -10/3, 2/3, 1/6 on centre, faces, diagonals);
+//   * __logf/__expf, float constants and reciprocals precomputed on the host;
+//   * tile rows padded so each warp's shared-memory accesses are conflict-free;
+//   * only the ring of cells that neighbours can read is persisted;
+//   * conserved DBA is lazy: the reference subtracts the mean change from every
+//     cell every step (Conserved/kernel.cu:526-553), a dense pass.  Here a device
+//     scalar C accumulates the means (FP64) and every block carries the value of
+//     C at its last update (its stamp); a cell's value is stored - (C - stamp),
+//     applied when the cell is read.  The mean itself is reduced inside this
+//     kernel: each CTA sums its own blocks in a fixed order, and the last CTA to
+//     finish (atomic ticket) sums the CTA partials and advances C.  One kernel
+//     per step, no dense pass, no host round trip.
+#pragma once
+
+#include "k_common.cuh"
+#include "k_modelb.cuh"
+
+namespace dba {
+
+struct LazyP {
+    double* stamp;      // [3][nb] value of C at each block's last update
+    double* cum;        // [3] C: accumulated mean changes
+    double* cta_part;   // [3][grid] per-CTA change sums
+    double* avg;        // [3] last step's mean change (observability)
+    unsigned int* ticket;
+    double ncells;
+    int lazy;           // conserved DBA in this launch
+};
+
+// all constants in float, computed once on the host (no conversions or divisions in the kernel)
+struct MBFastP {
+    float inv_dx2, c0x, c0y, c0z, irx, iry, irz;
+    float chi_xy, chi_xz, chi_yz, chi_xb, chi_yb, chi_zb;
+    float ex, ey, ez, phi_logK;        // phi_logK = phi_term + log(K)/rz
+    float nvx, mvy, dvz, dtvx, dtvy, dtvz, dn, dm, Mx, My, Mz, k0, thr;
+    int conserved;
+};
+
+struct MBFastBuf {
+    float* x[2];
+    float* y[2];
+    float* z[2];
+    float* mu[3];
+};
+
+inline MBFastP make_fast_params(const MBP<float>& P)
+{
+    MBFastP q;
+    q.inv_dx2 = (float)P.inv_dx2;
+    q.c0x = (float)P.c0x; q.c0y = (float)P.c0y; q.c0z = (float)P.c0z;
+    q.irx = (float)(1.0 / P.rx); q.iry = (float)(1.0 / P.ry); q.irz = (float)(1.0 / P.rz);
+    q.chi_xy = (float)P.chi_xy; q.chi_xz = (float)P.chi_xz; q.chi_yz = (float)P.chi_yz;
+    q.chi_xb = (float)P.chi_xb; q.chi_yb = (float)P.chi_yb; q.chi_zb = (float)P.chi_zb;
+    q.ex = (float)P.ex; q.ey = (float)P.ey; q.ez = (float)P.ez;
+    q.phi_logK = (float)(P.phi_term + P.logK_rz);
+    q.nvx = (float)P.nvx; q.mvy = (float)P.mvy; q.dvz = (float)P.dvz;
+    q.dtvx = (float)P.dtvx; q.dtvy = (float)P.dtvy; q.dtvz = (float)P.dtvz;
+    q.dn = (float)P.dn; q.dm = (float)P.dm;
+    q.Mx = (float)P.Mx; q.My = (float)P.My; q.Mz = (float)P.Mz; q.k0 = (float)P.k0; q.thr = (float)P.thr;
+    q.conserved = P.conserved;
+    return q;
+}
+
+inline MBFastBuf make_fast_buf(const MBP<float>& P)
+{
+    MBFastBuf b;
+    for (int q = 0; q < 2; ++q) {
+        b.x[q] = P.x[q];
+        b.y[q] = P.y[q];
+        b.z[q] = P.z[q];
+    }
+    for (int q = 0; q < 3; ++q) b.mu[q] = P.mu[q];
+    return b;
+}
+
+// Shared-memory row stride of a tile of width w for blocks of edge B: a warp
+// covers 32/B rows of B cells, so a stride that shifts successive rows by B
+// banks keeps those accesses conflict-free.
+template <int B> constexpr int tile_stride(int w) { return B == 16 ? 48 : (B == 8 ? 40 : w); }
+
+template <int B> struct MBFastShape {
+    static constexpr int E = B + 4, F = B + 2, SE = tile_stride<B>(B + 4), SF = tile_stride<B>(B + 2);
+    static constexpr int TV = E * SE, FV = F * SF;   // tile footprints including row padding
+    static constexpr int V = B * B, K = V >= kThreads ? 1 : kThreads / V;
+    static constexpr size_t smem = sizeof(float) * 3 * (size_t)K * (TV + FV);
+};
+
+// 2-D form of the 27-point Laplacian (kernel.cu:332-344 with z wrapped onto the cell)
+__device__ __forceinline__ float lap9(const float* c, int i, int sy, float inv_dx2)
+{
+    const float cc = (float)(-10.0 / 3.0), cf = (float)(2.0 / 3.0), cd = (float)(1.0 / 6.0);
+    const float faces = (c[i + 1] + c[i - 1]) + (c[i + sy] + c[i - sy]);
+    const float diag = (c[i + 1 + sy] + c[i - 1 + sy]) + (c[i + 1 - sy] + c[i - 1 - sy]);
+    return inv_dx2 * (cc * c[i] + cf * faces + cd * diag);
+}
+
+template <int B, bool DBA>
+__global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, MBFastP P, MBFastBuf Q, LazyP L)
+{
+    using S = MBFastShape<B>;
+    constexpr int NT = kThreads, V = B * B, E = S::E, F = S::F, SE = S::SE, SF = S::SF, TV = S::TV, FV = S::FV;
+    constexpr int NE = E * E, NF = F * F;
+    constexpr int K = S::K;
+    constexpr int CPT = V >= NT ? V / NT : 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float* sx = reinterpret_cast<float*>(smem_raw);
+    float* sy = sx + K * TV;
+    float* sz = sy + K * TV;
+    float* mx = sz + K * TV;
+    float* my = mx + K * FV;
+    float* mz = my + K * FV;
+    __shared__ int s_list[NT], s_lmeta[NT];
+    __shared__ int s_cnt;
+    __shared__ int s_blk[K], s_meta[K], s_nx[K];
+    __shared__ unsigned char s_rp[K][9], s_ra[K][9];
+    __shared__ float s_ro[K][9][3];     // conserved offset C - stamp per neighbour block
+    __shared__ double s_run[3][(NT / 32) * CPT];
+    __shared__ double s_bsum[3][K];
+    __shared__ double s_C[3];
+    __shared__ bool s_last;
+
+    const int tid = threadIdx.x;
+    const int G = gridDim.x;
+    const int nb = g.nb;
+    const float inv_dx2 = P.inv_dx2;
+    if (tid < 3) s_C[tid] = L.lazy ? L.cum[tid] : 0.0;
+    __syncthreads();
+
+    for (long long j0 = 0; blockIdx.x + (long long)G * j0 < nb; j0 += NT) {
+        const long long bl = blockIdx.x + (long long)G * (j0 + tid);
+        const bool valid = bl < nb;
+        const int b = (int)bl;
+        int act = 0, meta = 0;
+        if (valid) {
+            int pp = f.par_cur[b];
+            act = DBA ? (f.wake_cur[b] ? 1 : 0) : 1;
+            f.wake_clr[b] = 0;
+            if (!DBA) f.wake_nxt[b] = 1;
+            f.par_nxt[b] = (uint8_t)(pp ^ act);
+            if (P.conserved && !act) {
+                f.bsum[b] = 0.0;
+                f.bsum[nb + b] = 0.0;
+                f.bsum[2 * nb + b] = 0.0;
+            }
+            meta = act | (pp << 2);
+        }
+        count_stats(f.stats, act, valid);
+        if (tid == 0) s_cnt = 0;
+        __syncthreads();
+        list_append(valid && act, b, meta, s_list, s_lmeta, &s_cnt);
+        __syncthreads();
+        const int cnt = s_cnt;
+
+        for (int q0 = 0; q0 < cnt; q0 += K) {
+            if (tid < K) {
+                int q = q0 + tid;
+                s_blk[tid] = q < cnt ? s_list[q] : -1;
+                s_meta[tid] = q < cnt ? s_lmeta[q] : 0;
+                s_nx[tid] = 0;
+            }
+            __syncthreads();
+            if (tid < K * 9) {   // per-neighbour parity, activity and conserved offset
+                const int k = tid / 9, r = tid % 9;
+                const int blk = s_blk[k];
+                if (blk >= 0) {
+                    const int bx = blk % g.nbx, by = blk / g.nbx;
+                    int nx_ = bx + (r % 3) - 1, ny_ = by + (r / 3) - 1;
+                    nx_ = nx_ < 0 ? g.nbx - 1 : (nx_ >= g.nbx ? 0 : nx_);
+                    ny_ = ny_ < 0 ? g.nby - 1 : (ny_ >= g.nby ? 0 : ny_);
+                    const int ob = nx_ + g.nbx * ny_;
+                    s_rp[k][r] = f.par_cur[ob];
+                    s_ra[k][r] = DBA ? (f.wake_cur[ob] ? 1 : 0) : 1;
+#pragma unroll
+                    for (int q = 0; q < 3; ++q)
+                        s_ro[k][r][q] = L.lazy ? (float)(s_C[q] - L.stamp[(size_t)q * nb + ob]) : 0.f;
+                }
+            }
+            __syncthreads();
+            // 1. stage x, y, z (block + 2-cell halo) at their true values
+            for (int i = tid; i < K * NE; i += NT) {
+                const int k = i / NE;
+                const int blk = s_blk[k];
+                if (blk < 0) continue;
+                const int j = i - k * NE;
+                const int ly = j / E, lx = j - ly * E;
+                const int r = (lx < 2 ? 0 : (lx < 2 + B ? 1 : 2)) + 3 * (ly < 2 ? 0 : (ly < 2 + B ? 1 : 2));
+                const int bx = blk % g.nbx, by = blk / g.nbx;
+                int gx = bx * B + lx - 2, gy = by * B + ly - 2;
+                gx += gx < 0 ? g.nx : (gx >= g.nx ? -g.nx : 0);
+                gy += gy < 0 ? g.ny : (gy >= g.ny ? -g.ny : 0);
+                const size_t gi = (size_t)gx + (size_t)g.nx * gy;
+                const int par = s_rp[k][r];
+                const int si = k * TV + lx + SE * ly;
+                sx[si] = Q.x[par][gi] - s_ro[k][r][0];
+                sy[si] = Q.y[par][gi] - s_ro[k][r][1];
+                sz[si] = Q.z[par][gi] - s_ro[k][r][2];
+            }
+            __syncthreads();
+            // 2. potentials on block + 1-cell halo (Calc_mu, kernel.cu:371-388)
+            for (int i = tid; i < K * NF; i += NT) {
+                const int k = i / NF;
+                const int blk = s_blk[k];
+                if (blk < 0) continue;
+                const int j = i - k * NF;
+                const int fy = j / F, fx = j - fy * F;
+                const int r = (fx < 1 ? 0 : (fx < 1 + B ? 1 : 2)) + 3 * (fy < 1 ? 0 : (fy < 1 + B ? 1 : 2));
+                const int bx = blk % g.nbx, by = blk / g.nbx;
+                int gx = bx * B + fx - 1, gy = by * B + fy - 1;
+                gx += gx < 0 ? g.nx : (gx >= g.nx ? -g.nx : 0);
+                gy += gy < 0 ? g.ny : (gy >= g.ny ? -g.ny : 0);
+                const size_t gi = (size_t)gx + (size_t)g.nx * gy;
+                const int mi = k * FV + fx + SF * fy;
+                if (r == 4 || s_ra[k][r]) {
+                    const int ti = k * TV + (fx + 1) + SE * (fy + 1);
+                    const float X = sx[ti], Y = sy[ti], Z = sz[ti];
+                    const float bb = 1.f - X - Y - Z;
+                    const float lapx = lap9(sx, ti, SE, inv_dx2);
+                    const float lapy = lap9(sy, ti, SE, inv_dx2);
+                    const float lapz = lap9(sz, ti, SE, inv_dx2);
+                    const float lb = __logf(bb);
+                    const float sumb = P.chi_xb * X + P.chi_yb * Y + P.chi_zb * Z;   // common subtrahend
+                    const float ux = P.c0x + P.chi_xy * Y + P.chi_xz * Z + P.chi_xb * bb - sumb +
+                                     __logf(X) * P.irx - lb - P.ex * lapx;
+                    const float uy = P.c0y + P.chi_xy * X + P.chi_yz * Z + P.chi_yb * bb - sumb +
+                                     __logf(Y) * P.iry - lb - P.ey * lapy;
+                    const float uz = P.c0z + P.chi_xz * X + P.chi_yz * Y + P.chi_zb * bb - sumb +
+                                     __logf(Z) * P.irz - lb - P.ez * lapz - P.phi_logK;
+                    mx[mi] = ux;
+                    my[mi] = uy;
+                    mz[mi] = uz;
+                    if (r == 4) {
+                        // persist the ring that neighbour blocks may read later
+                        if (fx == 1 || fx == B || fy == 1 || fy == B) {
+                            Q.mu[0][gi] = ux;
+                            Q.mu[1][gi] = uy;
+                            Q.mu[2][gi] = uz;
+                        }
+                        if (fabsf(lapz) > P.thr) s_nx[k] = 1;
+                    }
+                } else {
+                    mx[mi] = Q.mu[0][gi];
+                    my[mi] = Q.mu[1][gi];
+                    mz[mi] = Q.mu[2][gi];
+                }
+            }
+            __syncthreads();
+            // 3. update (Update, kernel.cu:419-434; Conserved/kernel.cu:428-440)
+            double chg[3][CPT];
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) {
+                chg[0][c] = chg[1][c] = chg[2][c] = 0.0;
+                const int k = (V >= NT) ? 0 : tid / V;
+                const int v = (V >= NT) ? tid + c * NT : tid - k * V;
+                const int blk = s_blk[k];
+                if (blk < 0) continue;
+                const int m = s_meta[k];
+                const int ly = v / B, lx = v - ly * B;
+                const int fi = k * FV + (lx + 1) + SF * (ly + 1);
+                const int ti = k * TV + (lx + 2) + SE * (ly + 2);
+                const int bx = blk % g.nbx, by = blk / g.nbx;
+                const size_t gi = (size_t)(bx * B + lx) + (size_t)g.nx * (size_t)(by * B + ly);
+                const float Rr = P.k0 * (__expf(P.nvx * mx[fi] + P.mvy * my[fi]) - __expf(P.dvz * mz[fi]));
+                const float cx = P.dtvx * (P.Mx * lap9(mx, fi, SF, inv_dx2) - P.dn * Rr);
+                const float cy = P.dtvy * (P.My * lap9(my, fi, SF, inv_dx2) - P.dm * Rr);
+                const float cz = P.dtvz * (P.Mz * lap9(mz, fi, SF, inv_dx2) + Rr);
+                const float xn = sx[ti] + cx, yn = sy[ti] + cy, zn = sz[ti] + cz;
+                const int dst = ((m >> 2) & 1) ^ 1;
+                Q.x[dst][gi] = xn;
+                Q.y[dst][gi] = yn;
+                Q.z[dst][gi] = zn;
+                if (!isfinite(xn) || !isfinite(yn) || !isfinite(zn)) raise_status(f.status, 5);
+                chg[0][c] = (double)cx;
+                chg[1][c] = (double)cy;
+                chg[2][c] = (double)cz;
+            }
+            if (P.conserved) {
+                block_tree_sums<V, CPT>(chg[0], s_run[0], s_bsum[0], 0);
+                block_tree_sums<V, CPT>(chg[1], s_run[1], s_bsum[1], 0);
+                block_tree_sums<V, CPT>(chg[2], s_run[2], s_bsum[2], 0);
+            }
+            __syncthreads();
+            if (tid < K) {
+                const int blk = s_blk[tid];
+                if (blk >= 0) {
+                    if (P.conserved) {
+                        f.bsum[blk] = s_bsum[0][tid];
+                        f.bsum[nb + blk] = s_bsum[1][tid];
+                        f.bsum[2 * nb + blk] = s_bsum[2][tid];
+                    }
+                    if (L.lazy)
+                        for (int q = 0; q < 3; ++q) L.stamp[(size_t)q * nb + blk] = s_C[q];
+                    if (DBA) {
+                        f.next[blk] = (uint8_t)s_nx[tid];
+                        if (s_nx[tid]) wake_faces(g, f.wake_nxt, blk);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (!L.lazy) return;
+    // conserved mean change: fixed-order CTA partials, then the last CTA finishes
+    if (tid < 3) {
+        double s = 0.0;
+        for (long long b2 = blockIdx.x; b2 < nb; b2 += G) s += f.bsum[(size_t)tid * nb + b2];
+        L.cta_part[(size_t)tid * G + blockIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = (atomicAdd(L.ticket, 1u) == (unsigned)G - 1);
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const int warp = tid >> 5, lane = tid & 31;
+    if (warp < 3) {
+        double s = 0.0;
+        for (int c = lane; c < G; c += 32) s += ((volatile double*)L.cta_part)[(size_t)warp * G + c];
+#pragma unroll
+        for (int h = 16; h >= 1; h /= 2) s += __shfl_down_sync(0xffffffffu, s, h);
+        if (lane == 0) {
+            const double a = s / L.ncells;
+            L.avg[warp] = a;
+            L.cum[warp] = s_C[warp] + a;
+        }
+    }
+    if (tid == 0) *L.ticket = 0u;
+}
+
+// FP32 lazy-conserved readback: value = stored - (C - stamp[owner])
+static __global__ void __launch_bounds__(kThreads) gather_lazy_kernel(GridP g, int B, const float* b0, const float* b1,
+                                                                      const uint8_t* par, const double* stamp_q,
+                                                                      const double* cum_q, size_t count, double* out)
+{
+    const double C = *cum_q;
+    for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < count; i += (size_t)gridDim.x * kThreads) {
+        const int x = (int)(i % g.nx), y = (int)(i / g.nx);
+        const int ob = x / B + g.nbx * (y / B);
+        const float v = par[ob] ? b1[i] : b0[i];
+        out[i] = (double)v - (C - stamp_q[ob]);
+    }
+}
+
+}  // namespace dba

@@ -9,6 +9,7 @@
 #include "k_dendrite.cuh"
 #include "k_kh.cuh"
 #include "k_modelb.cuh"
+#include "k_modelb_fast.cuh"
 #include "k_reduce.cuh"
 
 namespace dba {
@@ -20,9 +21,15 @@ template <typename R> int step_grid(int model, int D, int B, int sms);
 template <typename R>
 cudaError_t launch_dendrite(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
                             const DenP<R>& P);
+// FP32 2-D uses the fast kernel (lazy conserved correction, reduction fused);
+// `lz` may be null for FP64.
 template <typename R>
 cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
-                          const MBP<R>& P);
+                          const MBP<R>& P, const LazyP* lz);
+template <typename R> bool modelb_uses_fast(int D, int B);
+cudaError_t launch_gather_lazy(cudaStream_t st, const GridP& g, int B, const float* b0, const float* b1,
+                               const uint8_t* par, const double* stamp_q, const double* cum_q, size_t count,
+                               double* out);
 template <typename R>
 cudaError_t launch_kh(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f, const KHP<R>& P);
 template <typename R> cudaError_t launch_correct(int grid, cudaStream_t st, const GridP& g, const CorrP<R>& P);
