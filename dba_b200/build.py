@@ -26,7 +26,7 @@ UNITS = [
     ("api.cu", ["-fmad=false"]),
 ]
 HEADERS = ["fpmath.h", "fpmath_coeffs.h", "k_common.cuh", "k_dendrite.cuh", "k_modelb.cuh", "k_kh.cuh",
-           "k_reduce.cuh", "k_inst.cuh", "launch.h"]
+           "k_reduce.cuh", "k_inst.cuh", "launch.h", "k_modelb_fast.cuh", "k_batch.cuh"]
 
 
 def _newer(target, deps):

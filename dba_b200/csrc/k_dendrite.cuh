@@ -108,8 +108,8 @@ __global__ void __launch_bounds__(kThreads) dendrite_step(GridP g, FlagP f, DenP
                 const int gz = (D == 3) ? wrapc(bz * B + lz - 1, g.nz, g.bc) : 0;
                 const int ob = gx / B + g.nbx * (gy / B + g.nby * ((D == 3) ? gz / B : 0));
                 const size_t gi = (size_t)gx + (size_t)g.nx * ((size_t)gy + (size_t)g.ny * gz);
-                sp[i] = P.p[f.par_cur[ob]][gi];
-                sT[i] = P.T[f.par_cur[nb + ob]][gi];
+                sp[i] = (f.par_cur[ob] ? P.p[1] : P.p[0])[gi];
+                sT[i] = (f.par_cur[nb + ob] ? P.T[1] : P.T[0])[gi];
             }
             __syncthreads();
 #pragma unroll
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kThreads) dendrite_step(GridP g, FlagP f, DenP
                     const R mm = f2 * atan_r<R>(gam * sigma * Tc);
                     const R pchg = f3 * (eps2 * lapP + pc * (1 - pc) * (pc - (R)0.5 + mm));
                     pn = pc + dt * pchg;
-                    P.p[((m >> 2) & 1) ^ 1][gi] = pn;
+                    ((m & 4) ? P.p[0] : P.p[1])[gi] = pn;
                     if (pn >= thr_p && pn <= thr_p_hi) s_np[k] = 1;
                     if (!isfinite(pn)) raise_status(f.status, 5);
                 }
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(kThreads) dendrite_step(GridP g, FlagP f, DenP
                     } else {
                         Tn = Tc + dt * lapT + pn - pc;
                     }
-                    P.T[((m >> 3) & 1) ^ 1][gi] = Tn;
+                    ((m & 8) ? P.T[0] : P.T[1])[gi] = Tn;
                     if (fabs(Tn - Tc) >= thr_T) s_nT[k] = 1;
                     if (!isfinite(Tn)) raise_status(f.status, 5);
                 }

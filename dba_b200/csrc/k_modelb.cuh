@@ -155,9 +155,9 @@ __global__ void __launch_bounds__(kThreads) modelb_step(GridP g, FlagP f, MBP<R>
                 const int ob = gx / B + g.nbx * (gy / B + g.nby * ((D == 3) ? gz / B : 0));
                 const size_t gi = (size_t)gx + (size_t)g.nx * ((size_t)gy + (size_t)g.ny * gz);
                 const int par = f.par_cur[ob];
-                sx[i] = P.x[par][gi];
-                sy[i] = P.y[par][gi];
-                sz[i] = P.z[par][gi];
+                sx[i] = (par ? P.x[1] : P.x[0])[gi];
+                sy[i] = (par ? P.y[1] : P.y[0])[gi];
+                sz[i] = (par ? P.z[1] : P.z[0])[gi];
             }
             __syncthreads();
             // 2. potentials on the block plus a 1-cell halo (Calc_mu, kernel.cu:371-388)
@@ -228,9 +228,9 @@ __global__ void __launch_bounds__(kThreads) modelb_step(GridP g, FlagP f, MBP<R>
                 const R cz = (R)P.dtvz * ((R)P.Mz * lap27<R>(mz, fi, FY, FZ, inv_dx2) + Rr);
                 const R xn = sx[ti] + cx, yn = sy[ti] + cy, zn = sz[ti] + cz;
                 const int dst = ((m >> 2) & 1) ^ 1;
-                P.x[dst][gi] = xn;
-                P.y[dst][gi] = yn;
-                P.z[dst][gi] = zn;
+                (dst ? P.x[1] : P.x[0])[gi] = xn;
+                (dst ? P.y[1] : P.y[0])[gi] = yn;
+                (dst ? P.z[1] : P.z[0])[gi] = zn;
                 if (!isfinite(xn) || !isfinite(yn) || !isfinite(zn)) raise_status(f.status, 5);
                 chg[0][c] = (double)cx;
                 chg[1][c] = (double)cy;

@@ -10,14 +10,16 @@
 //   * __logf/__expf, float constants and reciprocals precomputed on the host;
 //   * tile rows padded so each warp's shared-memory accesses are conflict-free;
 //   * only the ring of cells that neighbours can read is persisted;
-//   * conserved DBA is lazy: the reference subtracts the mean change from every
-//     cell every step (Conserved/kernel.cu:526-553), a dense pass.  Here a device
-//     scalar C accumulates the means (FP64) and every block carries the value of
-//     C at its last update (its stamp); a cell's value is stored - (C - stamp),
-//     applied when the cell is read.  The mean itself is reduced inside this
-//     kernel: each CTA sums its own blocks in a fixed order, and the last CTA to
-//     finish (atomic ticket) sums the CTA partials and advances C.  One kernel
-//     per step, no dense pass, no host round trip.
+//   * conserved DBA is lazy.  The reference subtracts the mean change from every
+//     cell every step (Conserved/kernel.cu:526-553), a dense pass.  That
+//     correction is the same for every cell, so here the stored values carry
+//     only the raw changes and a device FP64 scalar C (per field) accumulates
+//     the means: a cell's value is stored - C, formed when it is staged or read
+//     back.  (Subtracting a tiny mean from an FP32 value directly would round it
+//     away.)  The mean itself is reduced inside this kernel: each CTA sums its
+//     own blocks in a fixed order, and the last CTA to finish (atomic ticket)
+//     sums the CTA partials and advances C.  One kernel per step, no dense pass,
+//     no host round trip.
 #pragma once
 
 #include "k_common.cuh"
@@ -26,8 +28,7 @@
 namespace dba {
 
 struct LazyP {
-    double* stamp;      // [3][nb] value of C at each block's last update
-    double* cum;        // [3] C: accumulated mean changes
+    double* cum;        // [3] C: accumulated mean changes (value = stored - C)
     double* cta_part;   // [3][grid] per-CTA change sums
     double* avg;        // [3] last step's mean change (observability)
     unsigned int* ticket;
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
     __shared__ int s_cnt;
     __shared__ int s_blk[K], s_meta[K], s_nx[K];
     __shared__ unsigned char s_rp[K][9], s_ra[K][9];
-    __shared__ float s_ro[K][9][3];     // conserved offset C - stamp per neighbour block
+    __shared__ float s_Cf[3];           // conserved offset C as float
     __shared__ double s_run[3][(NT / 32) * CPT];
     __shared__ double s_bsum[3][K];
     __shared__ double s_C[3];
@@ -131,7 +132,10 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
     const int G = gridDim.x;
     const int nb = g.nb;
     const float inv_dx2 = P.inv_dx2;
-    if (tid < 3) s_C[tid] = L.lazy ? L.cum[tid] : 0.0;
+    if (tid < 3) {
+        s_C[tid] = L.lazy ? L.cum[tid] : 0.0;
+        s_Cf[tid] = (float)s_C[tid];
+    }
     __syncthreads();
 
     for (long long j0 = 0; blockIdx.x + (long long)G * j0 < nb; j0 += NT) {
@@ -167,7 +171,7 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 s_nx[tid] = 0;
             }
             __syncthreads();
-            if (tid < K * 9) {   // per-neighbour parity, activity and conserved offset
+            if (tid < K * 9) {   // per-neighbour parity and activity
                 const int k = tid / 9, r = tid % 9;
                 const int blk = s_blk[k];
                 if (blk >= 0) {
@@ -178,13 +182,10 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                     const int ob = nx_ + g.nbx * ny_;
                     s_rp[k][r] = f.par_cur[ob];
                     s_ra[k][r] = DBA ? (f.wake_cur[ob] ? 1 : 0) : 1;
-#pragma unroll
-                    for (int q = 0; q < 3; ++q)
-                        s_ro[k][r][q] = L.lazy ? (float)(s_C[q] - L.stamp[(size_t)q * nb + ob]) : 0.f;
                 }
             }
             __syncthreads();
-            // 1. stage x, y, z (block + 2-cell halo) at their true values
+            // 1. stage x, y, z (block + 2-cell halo)
             for (int i = tid; i < K * NE; i += NT) {
                 const int k = i / NE;
                 const int blk = s_blk[k];
@@ -199,9 +200,11 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 const size_t gi = (size_t)gx + (size_t)g.nx * gy;
                 const int par = s_rp[k][r];
                 const int si = k * TV + lx + SE * ly;
-                sx[si] = Q.x[par][gi] - s_ro[k][r][0];
-                sy[si] = Q.y[par][gi] - s_ro[k][r][1];
-                sz[si] = Q.z[par][gi] - s_ro[k][r][2];
+                // stored values; the conserved offset is subtracted where values are used
+                // pointwise (Laplacians are unchanged by a uniform offset)
+                sx[si] = (par ? Q.x[1] : Q.x[0])[gi];
+                sy[si] = (par ? Q.y[1] : Q.y[0])[gi];
+                sz[si] = (par ? Q.z[1] : Q.z[0])[gi];
             }
             __syncthreads();
             // 2. potentials on block + 1-cell halo (Calc_mu, kernel.cu:371-388)
@@ -220,7 +223,7 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 const int mi = k * FV + fx + SF * fy;
                 if (r == 4 || s_ra[k][r]) {
                     const int ti = k * TV + (fx + 1) + SE * (fy + 1);
-                    const float X = sx[ti], Y = sy[ti], Z = sz[ti];
+                    const float X = sx[ti] - s_Cf[0], Y = sy[ti] - s_Cf[1], Z = sz[ti] - s_Cf[2];
                     const float bb = 1.f - X - Y - Z;
                     const float lapx = lap9(sx, ti, SE, inv_dx2);
                     const float lapy = lap9(sy, ti, SE, inv_dx2);
@@ -271,11 +274,12 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 const float cx = P.dtvx * (P.Mx * lap9(mx, fi, SF, inv_dx2) - P.dn * Rr);
                 const float cy = P.dtvy * (P.My * lap9(my, fi, SF, inv_dx2) - P.dm * Rr);
                 const float cz = P.dtvz * (P.Mz * lap9(mz, fi, SF, inv_dx2) + Rr);
+                // stored values carry raw changes (value = stored - C)
                 const float xn = sx[ti] + cx, yn = sy[ti] + cy, zn = sz[ti] + cz;
                 const int dst = ((m >> 2) & 1) ^ 1;
-                Q.x[dst][gi] = xn;
-                Q.y[dst][gi] = yn;
-                Q.z[dst][gi] = zn;
+                (dst ? Q.x[1] : Q.x[0])[gi] = xn;
+                (dst ? Q.y[1] : Q.y[0])[gi] = yn;
+                (dst ? Q.z[1] : Q.z[0])[gi] = zn;
                 if (!isfinite(xn) || !isfinite(yn) || !isfinite(zn)) raise_status(f.status, 5);
                 chg[0][c] = (double)cx;
                 chg[1][c] = (double)cy;
@@ -295,8 +299,6 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                         f.bsum[nb + blk] = s_bsum[1][tid];
                         f.bsum[2 * nb + blk] = s_bsum[2][tid];
                     }
-                    if (L.lazy)
-                        for (int q = 0; q < 3; ++q) L.stamp[(size_t)q * nb + blk] = s_C[q];
                     if (DBA) {
                         f.next[blk] = (uint8_t)s_nx[tid];
                         if (s_nx[tid]) wake_faces(g, f.wake_nxt, blk);
@@ -334,17 +336,17 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
     if (tid == 0) *L.ticket = 0u;
 }
 
-// FP32 lazy-conserved readback: value = stored - (C - stamp[owner])
+// FP32 lazy-conserved readback: value = stored - C
 static __global__ void __launch_bounds__(kThreads) gather_lazy_kernel(GridP g, int B, const float* b0, const float* b1,
-                                                                      const uint8_t* par, const double* stamp_q,
-                                                                      const double* cum_q, size_t count, double* out)
+                                                                      const uint8_t* par, const double* cum_q,
+                                                                      size_t count, double* out)
 {
     const double C = *cum_q;
     for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < count; i += (size_t)gridDim.x * kThreads) {
         const int x = (int)(i % g.nx), y = (int)(i / g.nx);
         const int ob = x / B + g.nbx * (y / B);
         const float v = par[ob] ? b1[i] : b0[i];
-        out[i] = (double)v - (C - stamp_q[ob]);
+        out[i] = (double)v - C;
     }
 }
 

@@ -28,8 +28,7 @@ cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st
                           const MBP<R>& P, const LazyP* lz);
 template <typename R> bool modelb_uses_fast(int D, int B);
 cudaError_t launch_gather_lazy(cudaStream_t st, const GridP& g, int B, const float* b0, const float* b1,
-                               const uint8_t* par, const double* stamp_q, const double* cum_q, size_t count,
-                               double* out);
+                               const uint8_t* par, const double* cum_q, size_t count, double* out);
 template <typename R>
 cudaError_t launch_kh(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f, const KHP<R>& P);
 template <typename R> cudaError_t launch_correct(int grid, cudaStream_t st, const GridP& g, const CorrP<R>& P);

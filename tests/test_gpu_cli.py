@@ -1,0 +1,74 @@
+"""dba_run, the drop-in for the reference programs: run in a directory holding an
+Input.txt and check that the reference's output files appear with the reference's
+names, headers and column counts, and that the fields it writes match the library."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "dba_b200", "bin", "dba_run")
+pytestmark = pytest.mark.gpu
+
+
+def run(tmp_path, model, text, *extra):
+    (tmp_path / "Input.txt").write_text(text)
+    r = subprocess.run([BIN, model, *extra, "--quiet"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return tmp_path
+
+
+def read_vtk_scalars(path, name):
+    lines = open(path).read().split("\n")
+    i = next(k for k, l in enumerate(lines) if l.startswith(f"SCALARS {name} "))
+    return np.array(lines[i + 2].split(), dtype=float)
+
+
+def test_dendrite_outputs(tmp_path):
+    d = run(tmp_path, "dendrite", "64 64 1\n200 100 0.00005\n0.02 0.02 0.02\n0.5 0.0003 0.01 0.9 40.\n0.25\n1\n0.01\n1e-5\n",
+            "--vtk")
+    rt = open(d / "RTValues.out").read().splitlines()
+    assert rt[0] == "Time Vel Act_portion_p Act_portion_T Steps_per_second"
+    assert [r.split()[0] for r in rt[1:]] == ["100", "200"] and all(len(r.split()) == 5 for r in rt[1:])
+    tips = open(d / "tip_profile.out").read().splitlines()
+    assert len(tips) == 2 and len(tips[0].split()) == 21
+    head = open(d / "output_DBA_200.vtk").read().split("\n")[:5]
+    assert head == ["# vtk DataFile Version 2.0", "OUTPUT by Roy Zhang", "ASCII", "DATASET RECTILINEAR_GRID",
+                    "DIMENSIONS 64 64 1"]
+    assert os.path.exists(d / "Active_200.vtk")
+
+
+def test_modelb_outputs_match_library(tmp_path):
+    import dba_b200
+    text = ("32 32 1\n20 10 0.001\n1 1 1\n0 0 0 0 0 4\n1 1 2\n1 1 2\n1 1\n4 4 4 0.01\n1 1 1 1\n0.2 0.2 0.01\n"
+            "100 0.4 1\n1\n1e-3\n1\n")
+    d = run(tmp_path, "modelb", text)
+    assert sorted(f for f in os.listdir(d) if f.endswith(".vtk")) == \
+        ["Wakeup_10.vtk", "Wakeup_20.vtk", "output_0.vtk", "output_10.vtk", "output_20.vtk"]
+    integ = open(d / "Integral.out").read().splitlines()
+    assert [l.split()[0] for l in integ] == ["0", "10", "20"]
+    rt = open(d / "RTvalues.out").read().splitlines()
+    assert rt[0] == "Time Act_portion_p Steps_per_second"
+    # the VTK values are the library's fields at ostream precision 6
+    cfg = dba_b200.parse_input(d / "Input.txt", "modelb")
+    sim = dba_b200.Simulation(cfg).init()
+    sim.step(20, cfg.mode)
+    x = sim.field("x").ravel()
+    v = read_vtk_scalars(d / "output_20.vtk", "X")
+    assert np.allclose(v, x, rtol=1e-5, atol=0)
+
+
+def test_kh_outputs(tmp_path):
+    d = run(tmp_path, "kh", "64 64 1\n20 10 0.0002\n0.002 0.002 0.002\n1\n10\nconserved = 1\n")
+    for f in ("output_1_0.vtk", "output_1_10.vtk", "output_1_20.vtk", "Active_10.vtk", "Active_20.vtk",
+              "Wakeup_portion.out", "Integral.out", "VY_mode.out"):
+        assert os.path.exists(d / f), f
+    integ = open(d / "Integral.out").read().splitlines()
+    assert len(integ) == 3 and all(len(l.split()) == 5 for l in integ)
+    assert len(open(d / "VY_mode.out").read().splitlines()) == 2
+
+
+def test_missing_input_exits_1(tmp_path):
+    r = subprocess.run([BIN, "kh"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1
