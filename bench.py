@@ -215,6 +215,12 @@ def run_ours(args, w):
         except Exception:
             traffic = None
 
+    # the same state advanced in regular (dense, every block) mode, for the DBA-vs-dense comparison
+    sim.load_state(blob)
+    dense = sim.step_profiled(nprof, 0)
+    sim.load_state(blob)
+    dba_p = sim.step_profiled(nprof, w["mode"])
+
     # end to end through the public API: host state in pinned memory -> device, K steps, fields -> host
     n = cfg.nx * cfg.ny * cfg.nz
     nf = {"dendrite": 2, "modelb": 3, "kh": 4}[w["model"]]
@@ -258,6 +264,10 @@ def run_ours(args, w):
                          "frac_of_8tbs_spec": achieved / 8000.0},
             "step_breakdown_ms": {"stencil": prof["stencil_ms"] / nprof, "reduce": prof["reduce_ms"] / nprof,
                                   "correct": prof["correct_ms"] / nprof},
+            "vs_dense": {"dba_ms_per_step": dba_p["step_ms"] / nprof, "dense_ms_per_step": dense["step_ms"] / nprof,
+                         "dense_over_dba_time": dense["step_ms"] / dba_p["step_ms"] if dba_p["step_ms"] else None,
+                         "dense_cell_updates_per_s": dense["active_blocks"] * dense["cells_per_block"] /
+                         (dense["step_ms"] * 1e-3) if dense["step_ms"] else None},
             "gpu_launches": args.steps * launches_per_step(w),
             "clocks": clk.summary(),
             "status": status,
@@ -274,7 +284,9 @@ def run_ours(args, w):
 def launches_per_step(w):
     if w["model"] == "kh":
         return 5 + (2 if w["conserved"] else 0)
-    return 1 + (2 if w["conserved"] and w["model"] == "modelb" else 0)
+    if w["model"] == "modelb" and w["conserved"] and not (w["precision"] == 1 and w["nz"] == 1):
+        return 3   # FP64 / 3-D conserved: step, reduce, correct
+    return 1       # FP32 2-D conserved Model B: the reduction is inside the step kernel
 
 
 def _ref_input(w, nx, ny):
