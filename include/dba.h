@@ -225,6 +225,25 @@ int dba_state_size(dba_ctx* ctx, size_t* size);
 int dba_save_state(dba_ctx* ctx, void* host, size_t size);
 int dba_load_state(dba_ctx* ctx, const void* host, size_t size);
 
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * -- work enqueued while a stream is captured into a CUDA graph, latency-critical
+ * loops that must not take an allocation's implicit device synchronisation, or
+ * hosts whose device memory belongs to another allocator: the conserved-DBA
+ * mean change, computed with the same fixed-order reduction dba_step uses,
+ * allocating nothing.  Its scratch is a fixed array inside the library
+ * (32 KiB + 256 B on every GPU that loads it, held until exit).
+ *   block_sums: device pointer, nfields x nb FP64 per-block sums of the change
+ *   mean_out:   device pointer, nfields FP64 results: sum / ncells
+ *   stream:     cudaStream_t to enqueue on (NULL = legacy default stream)
+ * Limits: nb <= DBA_NOALLOC_MAX_BLOCKS, 1 <= nfields <= DBA_NOALLOC_MAX_FIELDS;
+ * larger sizes return DBA_ERR_ARG.  The first call on a device looks up the
+ * array's device address (make it before any stream capture).  All calls share
+ * the array: calls that overlap on the GPU race.  Asynchronous on `stream`. */
+#define DBA_NOALLOC_MAX_BLOCKS (1 << 20)
+#define DBA_NOALLOC_MAX_FIELDS 4
+int dba_mean_change_noalloc(const double* block_sums, int nb, int nfields, double ncells, double* mean_out,
+                            void* stream);
+
 /* Replaces FreeMemory (example_Dendritic_growth/kernel.cu:866-879). */
 void dba_destroy(dba_ctx* ctx);
 
