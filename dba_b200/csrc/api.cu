@@ -57,8 +57,8 @@ struct dba_ctx {
     bool initialized = false;
     // FP32 2-D Model B conserved: lazy correction state (k_modelb_fast.cuh)
     bool lazy = false;
-    double* cum = nullptr;            // [3]
-    double* cta_part = nullptr;       // [3][grid]
+    long long* total = nullptr;       // [3] fixed-point total of stored changes
+    long long* cta_part = nullptr;    // [3][grid]
     double* lavg = nullptr;           // [3]
     unsigned int* lticket = nullptr;
     cudaGraphExec_t graphs[6][2] = {};
@@ -215,7 +215,7 @@ CorrP<R> corr_params(dba_ctx* c, long s)
 LazyP lazy_params(dba_ctx* c, bool conserved_step)
 {
     LazyP L{};
-    L.cum = c->cum;
+    L.total = c->total;
     L.cta_part = c->cta_part;
     L.avg = c->lavg;
     L.ticket = c->lticket;
@@ -525,8 +525,8 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
     if (c->grid < 1) c->grid = c->sms;
     if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->conserved && modelb_uses_fast<float>(c->D, c->B)) {
         c->lazy = true;
-        c->cum = (double*)dev_alloc(c, 3 * sizeof(double), &err);
-        if (!err) c->cta_part = (double*)dev_alloc(c, 3 * (size_t)c->grid * sizeof(double), &err);
+        c->total = (long long*)dev_alloc(c, 3 * sizeof(long long), &err);
+        if (!err) c->cta_part = (long long*)dev_alloc(c, 3 * (size_t)c->grid * sizeof(long long), &err);
         if (!err) c->lavg = (double*)dev_alloc(c, 3 * sizeof(double), &err);
         if (!err) c->lticket = (unsigned int*)dev_alloc(c, sizeof(unsigned int), &err);
         if (err) {
@@ -657,14 +657,14 @@ int dba_read_field(dba_ctx* c, int field, double* host)
         return gather(c, c->state[field][0], c->state[field][1], cur_par(c) + (size_t)field * c->g.nb, 0, 1, c->n, host);
     if (model == DBA_MODEL_MODELB) {
         if (c->lazy && field < 4) {
-            // true values: stored - C per field (lazy conserved correction)
+            // true values: stored - total / (2^40 N) per field (lazy conserved correction)
             std::vector<double> tmp;
             const int nq = field < 3 ? 1 : 3;
             if (nq == 3) tmp.resize(2 * c->n);
             for (int q = field < 3 ? field : 0, k = 0; k < nq; ++q, ++k) {
                 double* dst = (k == 0) ? host : tmp.data() + (k - 1) * c->n;
                 cudaError_t e = launch_gather_lazy(c->st, c->g, c->B, (const float*)c->state[q][0],
-                                                   (const float*)c->state[q][1], cur_par(c), c->cum + q, c->n,
+                                                   (const float*)c->state[q][1], cur_par(c), c->total + q, c->n,
                                                    c->staging);
                 if (e == cudaSuccess) e = cudaMemcpyAsync(dst, c->staging, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);

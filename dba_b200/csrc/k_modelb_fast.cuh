@@ -13,13 +13,16 @@
 //   * conserved DBA is lazy.  The reference subtracts the mean change from every
 //     cell every step (Conserved/kernel.cu:526-553), a dense pass.  That
 //     correction is the same for every cell, so here the stored values carry
-//     only the raw changes and a device FP64 scalar C (per field) accumulates
-//     the means: a cell's value is stored - C, formed when it is staged or read
-//     back.  (Subtracting a tiny mean from an FP32 value directly would round it
-//     away.)  The mean itself is reduced inside this kernel: each CTA sums its
-//     own blocks in a fixed order, and the last CTA to finish (atomic ticket)
-//     sums the CTA partials and advances C.  One kernel per step, no dense pass,
-//     no host round trip.
+//     only the raw changes and the total of all stored changes is accumulated
+//     exactly in fixed point (int64, units of 2^-40); a cell's value is
+//     stored - total / (2^40 * Ncells), formed when it is staged or read back.
+//     The changes summed are the ones actually stored (x_new - x in FP32,
+//     exact), converted to fixed point exactly, reduced with warp
+//     __reduce_add_sync and shared/global int64 atomics -- order-independent,
+//     so the result is deterministic and the field totals are conserved to the
+//     rounding of the final FP64 division.  The last CTA to finish (atomic
+//     ticket) folds the CTA totals into the running total.  One kernel per
+//     step, no dense pass, no host round trip.
 #pragma once
 
 #include "k_common.cuh"
@@ -28,13 +31,31 @@
 namespace dba {
 
 struct LazyP {
-    double* cum;        // [3] C: accumulated mean changes (value = stored - C)
-    double* cta_part;   // [3][grid] per-CTA change sums
+    long long* total;   // [3] all stored changes so far, fixed point 2^-40 (value = stored - total/(2^40 N))
+    long long* cta_part;// [3][grid] this step's per-CTA change totals
     double* avg;        // [3] last step's mean change (observability)
     unsigned int* ticket;
     double ncells;
     int lazy;           // conserved DBA in this launch
 };
+
+constexpr double kFixScale = 1099511627776.0;       // 2^40
+constexpr double kFixUnit = 1.0 / 1099511627776.0;  // 2^-40
+
+// exact fixed-point image of an FP32 change (|d| < 2^23, ulp(d) >= 2^-40 for
+// field values above 2^-17)
+__device__ __forceinline__ long long to_fix(float d) { return __float2ll_rn(d * 1099511627776.0f); }
+
+// warp total of int64 values without 64-bit shuffles: split into a signed high
+// part and a 24-bit low part, each summed with one __reduce_add_sync
+__device__ __forceinline__ long long warp_sum_fix(long long v)
+{
+    const int hi = (int)(v >> 24);
+    const int lo = (int)(v & 0xffffff);
+    const int shi = __reduce_add_sync(0xffffffffu, hi);
+    const int slo = __reduce_add_sync(0xffffffffu, lo);
+    return ((long long)shi << 24) + (long long)slo;
+}
 
 // all constants in float, computed once on the host (no conversions or divisions in the kernel)
 struct MBFastP {
@@ -123,8 +144,7 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
     __shared__ int s_blk[K], s_meta[K], s_nx[K];
     __shared__ unsigned char s_rp[K][9], s_ra[K][9];
     __shared__ float s_Cf[3];           // conserved offset C as float
-    __shared__ double s_run[3][(NT / 32) * CPT];
-    __shared__ double s_bsum[3][K];
+    __shared__ unsigned long long s_fix[3];   // this CTA's change total (fixed point)
     __shared__ double s_C[3];
     __shared__ bool s_last;
 
@@ -133,8 +153,9 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
     const int nb = g.nb;
     const float inv_dx2 = P.inv_dx2;
     if (tid < 3) {
-        s_C[tid] = L.lazy ? L.cum[tid] : 0.0;
+        s_C[tid] = L.lazy ? (double)L.total[tid] * kFixUnit / L.ncells : 0.0;
         s_Cf[tid] = (float)s_C[tid];
+        s_fix[tid] = 0ull;
     }
     __syncthreads();
 
@@ -149,11 +170,6 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
             f.wake_clr[b] = 0;
             if (!DBA) f.wake_nxt[b] = 1;
             f.par_nxt[b] = (uint8_t)(pp ^ act);
-            if (P.conserved && !act) {
-                f.bsum[b] = 0.0;
-                f.bsum[nb + b] = 0.0;
-                f.bsum[2 * nb + b] = 0.0;
-            }
             meta = act | (pp << 2);
         }
         count_stats(f.stats, act, valid);
@@ -170,11 +186,11 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 s_meta[tid] = q < cnt ? s_lmeta[q] : 0;
                 s_nx[tid] = 0;
             }
-            __syncthreads();
             if (tid < K * 9) {   // per-neighbour parity and activity
                 const int k = tid / 9, r = tid % 9;
-                const int blk = s_blk[k];
-                if (blk >= 0) {
+                const int q = q0 + k;
+                if (q < cnt) {
+                    const int blk = s_list[q];
                     const int bx = blk % g.nbx, by = blk / g.nbx;
                     int nx_ = bx + (r % 3) - 1, ny_ = by + (r / 3) - 1;
                     nx_ = nx_ < 0 ? g.nbx - 1 : (nx_ >= g.nbx ? 0 : nx_);
@@ -256,10 +272,9 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
             }
             __syncthreads();
             // 3. update (Update, kernel.cu:419-434; Conserved/kernel.cu:428-440)
-            double chg[3][CPT];
+            long long fx_[3] = {0, 0, 0};
 #pragma unroll
             for (int c = 0; c < CPT; ++c) {
-                chg[0][c] = chg[1][c] = chg[2][c] = 0.0;
                 const int k = (V >= NT) ? 0 : tid / V;
                 const int v = (V >= NT) ? tid + c * NT : tid - k * V;
                 const int blk = s_blk[k];
@@ -275,30 +290,30 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 const float cy = P.dtvy * (P.My * lap9(my, fi, SF, inv_dx2) - P.dm * Rr);
                 const float cz = P.dtvz * (P.Mz * lap9(mz, fi, SF, inv_dx2) + Rr);
                 // stored values carry raw changes (value = stored - C)
-                const float xn = sx[ti] + cx, yn = sy[ti] + cy, zn = sz[ti] + cz;
+                const float x0 = sx[ti], y0 = sy[ti], z0 = sz[ti];
+                const float xn = x0 + cx, yn = y0 + cy, zn = z0 + cz;
                 const int dst = ((m >> 2) & 1) ^ 1;
                 (dst ? Q.x[1] : Q.x[0])[gi] = xn;
                 (dst ? Q.y[1] : Q.y[0])[gi] = yn;
                 (dst ? Q.z[1] : Q.z[0])[gi] = zn;
                 if (!isfinite(xn) || !isfinite(yn) || !isfinite(zn)) raise_status(f.status, 5);
-                chg[0][c] = (double)cx;
-                chg[1][c] = (double)cy;
-                chg[2][c] = (double)cz;
+                if (L.lazy) {   // the change actually stored (exact in FP32), in fixed point
+                    fx_[0] += to_fix(xn - x0);
+                    fx_[1] += to_fix(yn - y0);
+                    fx_[2] += to_fix(zn - z0);
+                }
             }
-            if (P.conserved) {
-                block_tree_sums<V, CPT>(chg[0], s_run[0], s_bsum[0], 0);
-                block_tree_sums<V, CPT>(chg[1], s_run[1], s_bsum[1], 0);
-                block_tree_sums<V, CPT>(chg[2], s_run[2], s_bsum[2], 0);
+            if (L.lazy) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    const long long w = warp_sum_fix(fx_[q]);
+                    if ((tid & 31) == 0 && w) atomicAdd(&s_fix[q], (unsigned long long)w);
+                }
             }
             __syncthreads();
             if (tid < K) {
                 const int blk = s_blk[tid];
                 if (blk >= 0) {
-                    if (P.conserved) {
-                        f.bsum[blk] = s_bsum[0][tid];
-                        f.bsum[nb + blk] = s_bsum[1][tid];
-                        f.bsum[2 * nb + blk] = s_bsum[2][tid];
-                    }
                     if (DBA) {
                         f.next[blk] = (uint8_t)s_nx[tid];
                         if (s_nx[tid]) wake_faces(g, f.wake_nxt, blk);
@@ -309,12 +324,8 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
         }
     }
     if (!L.lazy) return;
-    // conserved mean change: fixed-order CTA partials, then the last CTA finishes
-    if (tid < 3) {
-        double s = 0.0;
-        for (long long b2 = blockIdx.x; b2 < nb; b2 += G) s += f.bsum[(size_t)tid * nb + b2];
-        L.cta_part[(size_t)tid * G + blockIdx.x] = s;
-    }
+    // conserved change: CTA totals, then the last CTA folds them into the running total
+    if (tid < 3) L.cta_part[(size_t)tid * G + blockIdx.x] = (long long)s_fix[tid];
     __threadfence();
     __syncthreads();
     if (tid == 0) s_last = (atomicAdd(L.ticket, 1u) == (unsigned)G - 1);
@@ -323,25 +334,24 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
     __threadfence();
     const int warp = tid >> 5, lane = tid & 31;
     if (warp < 3) {
-        double s = 0.0;
-        for (int c = lane; c < G; c += 32) s += ((volatile double*)L.cta_part)[(size_t)warp * G + c];
+        long long t = 0;
+        for (int c = lane; c < G; c += 32) t += ((volatile long long*)L.cta_part)[(size_t)warp * G + c];
 #pragma unroll
-        for (int h = 16; h >= 1; h /= 2) s += __shfl_down_sync(0xffffffffu, s, h);
+        for (int h = 16; h >= 1; h /= 2) t += __shfl_down_sync(0xffffffffu, t, h);
         if (lane == 0) {
-            const double a = s / L.ncells;
-            L.avg[warp] = a;
-            L.cum[warp] = s_C[warp] + a;
+            L.avg[warp] = (double)t * kFixUnit / L.ncells;
+            L.total[warp] += t;
         }
     }
     if (tid == 0) *L.ticket = 0u;
 }
 
-// FP32 lazy-conserved readback: value = stored - C
+// FP32 lazy-conserved readback: value = stored - total / (2^40 N)
 static __global__ void __launch_bounds__(kThreads) gather_lazy_kernel(GridP g, int B, const float* b0, const float* b1,
-                                                                      const uint8_t* par, const double* cum_q,
+                                                                      const uint8_t* par, const long long* total_q,
                                                                       size_t count, double* out)
 {
-    const double C = *cum_q;
+    const double C = (double)(*total_q) * kFixUnit / (double)count;
     for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < count; i += (size_t)gridDim.x * kThreads) {
         const int x = (int)(i % g.nx), y = (int)(i / g.nx);
         const int ob = x / B + g.nbx * (y / B);
