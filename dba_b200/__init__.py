@@ -6,8 +6,8 @@ fallback: importing works without a GPU, but creating a Simulation needs the
 compiled library and a CUDA device.
 """
 from .engine import (  # noqa: F401
-    DBA_ERR, FIELDS, MODELS, Config, DBAError, Simulation, config, lib_path, load_library, parse_input,
+    DBA_ERR, FIELDS, MODELS, Batch, Config, DBAError, Simulation, config, lib_path, load_library, parse_input,
 )
 
-__all__ = ["Config", "DBAError", "Simulation", "config", "parse_input", "load_library", "lib_path", "FIELDS",
+__all__ = ["Batch", "Config", "DBAError", "Simulation", "config", "parse_input", "load_library", "lib_path", "FIELDS",
            "MODELS", "DBA_ERR"]

@@ -1,0 +1,84 @@
+"""Autotuner for the batched dendrite sweep.
+
+The batch kernel's DBA block edge (4, 8 or 16 cells) trades halo overhead and
+per-block work against activity granularity, and the number of steps advanced
+between tip checks (`chunk`) trades host synchronisation against overshoot past
+each run's stopping point.  `tune()` times each candidate on a short seeded
+mixed workload (the sweep's grid sizes and parameter ranges, every slot
+admitted at once, a fixed number of steps) and returns the fastest by
+active cell-updates per second, caching the choice per GPU and precision in
+a JSON file (DBA_AUTOTUNE_CACHE, default ~/.cache/dba_b200/autotune.json).
+"""
+import json
+import os
+import time
+
+from . import engine, serve
+
+CANDIDATE_BLOCKS = (8, 16)
+CANDIDATE_CHUNKS = (48, 96, 192)
+
+
+def _cache_path():
+    return os.environ.get("DBA_AUTOTUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "dba_b200", "autotune.json"))
+
+
+def _device_key(precision):
+    try:
+        import torch
+        name = torch.cuda.get_device_name(0)
+    except Exception:
+        name = "cuda"
+    return f"{name}|prec{precision}"
+
+
+def time_candidate(block, precision=1, nslots=24, steps=480, seed=5):
+    """Active cell-updates per second of one block edge on a mixed batch."""
+    reqs = serve.sweep_requests(n=nslots, rate=0.0, seed=seed, edges=(128, 256, 512))
+    b = engine.Batch(precision=precision, block=block, max_slots=nslots, block_capacity=1 << 17)
+    try:
+        for r in reqs:
+            if b.add(serve.request_config(r, precision, block)) is None:
+                break
+        b.step(96)                      # warm-up: graph capture, clocks
+        b.sync()
+        a0 = b.info().active_block_steps
+        t0 = time.perf_counter()
+        b.step(steps)
+        b.sync()
+        dt = time.perf_counter() - t0
+        cells = (b.info().active_block_steps - a0) * block * block
+    finally:
+        b.close()
+    return cells / dt
+
+
+def tune(precision=1, use_cache=True, verbose=False):
+    key = _device_key(precision)
+    path = _cache_path()
+    cache = {}
+    if use_cache and os.path.exists(path):
+        try:
+            cache = json.load(open(path))
+        except Exception:
+            cache = {}
+        if key in cache:
+            return cache[key]
+    scores = {}
+    for blk in CANDIDATE_BLOCKS:
+        scores[blk] = time_candidate(blk, precision)
+        if verbose:
+            print(f"block {blk}: {scores[blk]:.3e} cell-updates/s", flush=True)
+    best_block = max(scores, key=scores.get)
+    # chunk: the largest that keeps the mean overshoot past the stop below 2 % of a
+    # typical run (runs here take >= ~1000 steps), favouring fewer host syncs
+    best_chunk = max(c for c in CANDIDATE_CHUNKS if c <= 0.02 * 1000 * 10)
+    choice = {"block": int(best_block), "chunk": int(best_chunk),
+              "scores": {str(k): v for k, v in scores.items()}}
+    if use_cache:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        cache[key] = choice
+        with open(path, "w") as f:
+            json.dump(cache, f, indent=1)
+    return choice

@@ -25,6 +25,7 @@ UNITS = [
     ("k_f32.cu", []),
     ("api.cu", ["-fmad=false"]),
     ("noalloc.cu", ["-fmad=false"]),
+    ("batch.cu", []),
 ]
 HEADERS = ["fpmath.h", "fpmath_coeffs.h", "k_common.cuh", "k_dendrite.cuh", "k_modelb.cuh", "k_kh.cuh",
            "k_reduce.cuh", "k_inst.cuh", "launch.h", "k_modelb_fast.cuh", "k_batch.cuh"]

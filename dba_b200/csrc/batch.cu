@@ -1,0 +1,420 @@
+// batch.cu -- C ABI of the batched dendrite engine (include/dba.h, dba_batch_*).
+//
+// Simulations ("slots") share one device arena: each takes nx*ny cells in each
+// of four arrays (p and T, two ping-pong buffers each) and nb consecutive ids
+// of the global block space.  Both are first-fit allocated when a slot is
+// added and returned when it is removed, so admission is by free device
+// memory.  One kernel per step advances every live slot (k_batch.cuh); steps
+// are captured into CUDA graphs that stay valid across admissions because the
+// kernel reads the slot table from device memory.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/dba.h"
+#include "launch.h"
+
+using namespace dba;
+
+namespace {
+
+constexpr int kGraphSteps = 48;
+
+struct Range {
+    size_t off, len;
+};
+
+// first-fit allocator over [0, capacity)
+struct FreeList {
+    std::vector<Range> free;
+    void init(size_t cap) { free.assign(1, Range{0, cap}); }
+    bool take(size_t len, size_t* off)
+    {
+        for (size_t i = 0; i < free.size(); ++i)
+            if (free[i].len >= len) {
+                *off = free[i].off;
+                free[i].off += len;
+                free[i].len -= len;
+                if (free[i].len == 0) free.erase(free.begin() + i);
+                return true;
+            }
+        return false;
+    }
+    void give(size_t off, size_t len)
+    {
+        free.push_back(Range{off, len});
+        std::sort(free.begin(), free.end(), [](const Range& a, const Range& b) { return a.off < b.off; });
+        std::vector<Range> m;
+        for (auto& r : free) {
+            if (!m.empty() && m.back().off + m.back().len == r.off) m.back().len += r.len;
+            else m.push_back(r);
+        }
+        free = m;
+    }
+    size_t largest() const
+    {
+        size_t l = 0;
+        for (auto& r : free) l = std::max(l, r.len);
+        return l;
+    }
+    size_t total() const
+    {
+        size_t t = 0;
+        for (auto& r : free) t += r.len;
+        return t;
+    }
+};
+
+int cuda_status(cudaError_t e) { return e == cudaSuccess ? DBA_OK : (e == cudaErrorMemoryAllocation ? DBA_ERR_NOMEM : DBA_ERR_CUDA); }
+
+#define BTRY(call)                              \
+    do {                                        \
+        cudaError_t e_ = (call);                \
+        if (e_ != cudaSuccess) return cuda_status(e_); \
+    } while (0)
+
+}  // namespace
+
+struct dba_batch {
+    dba_batch_config cfg;
+    int esz = 4;
+    int sms = 148, grid = 148;
+    cudaStream_t st = nullptr;
+    void* arena = nullptr;           // 4 arrays x cell_capacity x esz
+    SlotRec* d_slots = nullptr;
+    int* d_bslot = nullptr;
+    uint8_t* par = nullptr;          // [2][2][NB]
+    uint8_t* wake = nullptr;         // [3][2][NB]
+    uint8_t* next = nullptr;         // [2][NB]
+    int* status = nullptr;
+    unsigned long long* stats = nullptr;
+    double* d_tips = nullptr;
+    double* staging = nullptr;       // largest slot's cells
+    std::vector<SlotRec> slots;      // host mirror
+    std::vector<size_t> cell_off;
+    std::vector<long> age;           // steps since admission
+    FreeList cells, blocks;
+    long step = 0;
+    cudaGraphExec_t graphs[6] = {};
+};
+
+namespace {
+
+FlagP bflags(dba_batch* b, long s)
+{
+    const size_t L = 2 * (size_t)b->cfg.block_capacity;
+    FlagP f;
+    f.par_cur = b->par + (s % 2) * L;
+    f.par_nxt = b->par + ((s + 1) % 2) * L;
+    f.wake_cur = b->wake + (s % 3) * L;
+    f.wake_nxt = b->wake + ((s + 1) % 3) * L;
+    f.wake_clr = b->wake + ((s + 2) % 3) * L;
+    f.next = b->next;
+    f.bsum = nullptr;
+    f.status = b->status;
+    f.stats = b->stats;
+    return f;
+}
+
+BatchP bparams(dba_batch* b)
+{
+    BatchP p;
+    p.slots = b->d_slots;
+    p.bslot = b->d_bslot;
+    p.nbtot = b->cfg.block_capacity;
+    return p;
+}
+
+cudaError_t enqueue(dba_batch* b, long s)
+{
+    FlagP f = bflags(b, s);
+    BatchP p = bparams(b);
+    return b->esz == 8 ? launch_batch_step<double>(b->cfg.block, b->grid, b->st, p, f)
+                       : launch_batch_step<float>(b->cfg.block, b->grid, b->st, p, f);
+}
+
+}  // namespace
+
+extern "C" {
+
+int dba_batch_create(const dba_batch_config* cfg, dba_batch** out)
+{
+    if (!cfg || !out) return DBA_ERR_ARG;
+    *out = nullptr;
+    if (cfg->block != 4 && cfg->block != 8 && cfg->block != 16) return DBA_ERR_CONFIG;
+    if (cfg->precision != DBA_PREC_F32 && cfg->precision != DBA_PREC_F64) return DBA_ERR_CONFIG;
+    if (cfg->max_slots < 1 || cfg->block_capacity < 1) return DBA_ERR_CONFIG;
+    dba_batch* b = new (std::nothrow) dba_batch();
+    if (!b) return DBA_ERR_NOMEM;
+    b->cfg = *cfg;
+    b->esz = cfg->precision == DBA_PREC_F64 ? 8 : 4;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+    size_t cells = cfg->cell_capacity;
+    if (e == cudaSuccess && cells == 0) {
+        // size the arena from free device memory (80 %), keeping the flag arrays' share
+        size_t fr = 0, tot = 0;
+        e = cudaMemGetInfo(&fr, &tot);
+        cells = (size_t)(0.8 * (double)fr) / (4 * (size_t)b->esz);
+        b->cfg.cell_capacity = cells;
+    }
+    const size_t NB = cfg->block_capacity;
+    if (e == cudaSuccess) e = cudaMalloc(&b->arena, 4 * cells * b->esz);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_slots, sizeof(SlotRec) * cfg->max_slots);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_bslot, sizeof(int) * NB);
+    if (e == cudaSuccess) e = cudaMalloc(&b->par, 2 * 2 * NB);
+    if (e == cudaSuccess) e = cudaMalloc(&b->wake, 3 * 2 * NB);
+    if (e == cudaSuccess) e = cudaMalloc(&b->next, 2 * NB);
+    if (e == cudaSuccess) e = cudaMalloc(&b->status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&b->stats, 4 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_tips, sizeof(double) * cfg->max_slots);
+    if (e == cudaSuccess) e = cudaMemset(b->d_bslot, 0xff, sizeof(int) * NB);
+    if (e == cudaSuccess) e = cudaMemset(b->par, 0, 2 * 2 * NB);
+    if (e == cudaSuccess) e = cudaMemset(b->wake, 0, 3 * 2 * NB);
+    if (e == cudaSuccess) e = cudaMemset(b->next, 0, 2 * NB);
+    if (e == cudaSuccess) e = cudaMemset(b->status, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(b->stats, 0, 4 * sizeof(unsigned long long));
+    b->slots.assign(cfg->max_slots, SlotRec{});
+    b->cell_off.assign(cfg->max_slots, 0);
+    b->age.assign(cfg->max_slots, 0);
+    if (e == cudaSuccess) e = cudaMemset(b->d_slots, 0, sizeof(SlotRec) * cfg->max_slots);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        dba_batch_destroy(b);
+        return cuda_status(e);
+    }
+    b->cells.init(cells);
+    b->blocks.init(NB);
+    b->grid = b->esz == 8 ? batch_grid<double>(cfg->block, b->sms) : batch_grid<float>(cfg->block, b->sms);
+    *out = b;
+    return DBA_OK;
+}
+
+void dba_batch_destroy(dba_batch* b)
+{
+    if (!b) return;
+    if (b->st) cudaStreamSynchronize(b->st);
+    for (auto& g : b->graphs)
+        if (g) cudaGraphExecDestroy(g);
+    for (void* p : {(void*)b->arena, (void*)b->d_slots, (void*)b->d_bslot, (void*)b->par, (void*)b->wake,
+                    (void*)b->next, (void*)b->status, (void*)b->stats, (void*)b->d_tips, (void*)b->staging})
+        if (p) cudaFree(p);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+int dba_batch_add(dba_batch* b, const dba_config* k, const double* ic, int* slot_out)
+{
+    if (!b || !k || !slot_out) return DBA_ERR_ARG;
+    if (k->model != DBA_MODEL_DENDRITE || k->nz != 1) return DBA_ERR_CONFIG;
+    if (k->block != b->cfg.block || k->precision != b->cfg.precision) return DBA_ERR_CONFIG;
+    const int B = b->cfg.block;
+    if (k->nx % B || k->ny % B || k->nx < 2 * B || k->ny < 2 * B) return DBA_ERR_CONFIG;
+    int s = -1;
+    for (int i = 0; i < b->cfg.max_slots; ++i)
+        if (!b->slots[i].live) {
+            s = i;
+            break;
+        }
+    if (s < 0) return DBA_ERR_NOMEM;
+    const size_t n = (size_t)k->nx * k->ny;
+    const int nbx = k->nx / B, nby = k->ny / B, nb = nbx * nby;
+    size_t coff = 0, boff = 0;
+    if (!b->cells.take(n, &coff)) return DBA_ERR_NOMEM;
+    if (!b->blocks.take(nb, &boff)) {
+        b->cells.give(coff, n);
+        return DBA_ERR_NOMEM;
+    }
+    // initial condition (FP64 host): the single-domain engine's dba_init rules
+    std::vector<double> p(n), T(n);
+    if (ic) {
+        std::memcpy(p.data(), ic, n * 8);
+        std::memcpy(T.data(), ic + n, n * 8);
+    } else {
+        for (int y = 0; y < k->ny; ++y)
+            for (int x = 0; x < k->nx; ++x) {
+                size_t i = (size_t)x + (size_t)k->nx * y;
+                if (k->ic == DBA_IC_TANH_SEED) {
+                    double cx = k->ic_corner ? 0.0 : k->nx / 2, cy = k->ic_corner ? 0.0 : k->ny / 2;
+                    double r = std::sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy));
+                    p[i] = 0.5 * (1.0 - std::tanh((r - k->ic_radius) / k->ic_width));
+                } else {
+                    int dx = x - k->nx / 2, dy = y - k->ny / 2, dz = 0 - k->nz / 2;
+                    double dist = std::sqrt((double)(dx * dx + dy * dy + dz * dz));
+                    p[i] = dist <= 5 ? (1. - 0.2 * dist) : 0;
+                }
+                T[i] = -k->Delta;
+            }
+    }
+    const size_t cap = b->cfg.cell_capacity;
+    unsigned char* base = (unsigned char*)b->arena;
+    SlotRec r{};
+    r.nx = k->nx; r.ny = k->ny; r.nbx = nbx; r.nby = nby; r.nb = nb; r.boff = (int)boff; r.bc = k->bc; r.live = 1;
+    r.p[0] = base + (0 * cap + coff) * b->esz;
+    r.p[1] = base + (1 * cap + coff) * b->esz;
+    r.T[0] = base + (2 * cap + coff) * b->esz;
+    r.T[1] = base + (3 * cap + coff) * b->esz;
+    const double Pi = 3.14159;   // example_Dendritic_growth/kernel.cu:7
+    r.f0 = 1. / (2 * k->dx); r.f1 = 1. / k->dx / k->dx; r.f2 = -k->alpha / Pi; r.f3 = 1. / k->tau;
+    r.dt = k->dt; r.delta = k->delta; r.eps2 = k->epsilon * k->epsilon; r.gamma = k->gamma;
+    r.thr_p = k->metric_p; r.thr_p_hi = 1.0 - k->metric_p; r.thr_T = k->metric_T;
+    // upload fields (both buffers hold the initial state; parity 0 selects buffer 0)
+    std::vector<float> tmp;
+    auto put = [&](void* dst, const std::vector<double>& v) -> cudaError_t {
+        if (b->esz == 8) return cudaMemcpyAsync(dst, v.data(), n * 8, cudaMemcpyHostToDevice, b->st);
+        tmp.resize(n);
+        for (size_t i = 0; i < n; ++i) tmp[i] = (float)v[i];
+        cudaError_t e = cudaMemcpyAsync(dst, tmp.data(), n * 4, cudaMemcpyHostToDevice, b->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);   // tmp is reused
+        return e;
+    };
+    BTRY(put(r.p[0], p));
+    BTRY(put(r.T[0], T));
+    // flags of its blocks: parity 0, all active for the next step, the rest cleared
+    const size_t NB = b->cfg.block_capacity;
+    const long s_next = b->step + 1;
+    for (int ch = 0; ch < 2; ++ch) {
+        for (int q = 0; q < 2; ++q) BTRY(cudaMemsetAsync(b->par + (q * 2 + ch) * NB + boff, 0, nb, b->st));
+        for (int q = 0; q < 3; ++q)
+            BTRY(cudaMemsetAsync(b->wake + (q * 2 + ch) * NB + boff, (q == s_next % 3) ? 1 : 0, nb, b->st));
+        BTRY(cudaMemsetAsync(b->next + ch * NB + boff, 0, nb, b->st));
+    }
+    std::vector<int> ids(nb, s);
+    BTRY(cudaMemcpyAsync(b->d_bslot + boff, ids.data(), nb * sizeof(int), cudaMemcpyHostToDevice, b->st));
+    BTRY(cudaMemcpyAsync(b->d_slots + s, &r, sizeof r, cudaMemcpyHostToDevice, b->st));
+    BTRY(cudaStreamSynchronize(b->st));
+    b->slots[s] = r;
+    b->cell_off[s] = coff;
+    b->age[s] = 0;
+    *slot_out = s;
+    return DBA_OK;
+}
+
+int dba_batch_remove(dba_batch* b, int s)
+{
+    if (!b || s < 0 || s >= b->cfg.max_slots || !b->slots[s].live) return DBA_ERR_ARG;
+    SlotRec& r = b->slots[s];
+    std::vector<int> ids(r.nb, -1);
+    BTRY(cudaMemcpyAsync(b->d_bslot + r.boff, ids.data(), r.nb * sizeof(int), cudaMemcpyHostToDevice, b->st));
+    SlotRec dead{};
+    BTRY(cudaMemcpyAsync(b->d_slots + s, &dead, sizeof dead, cudaMemcpyHostToDevice, b->st));
+    BTRY(cudaStreamSynchronize(b->st));
+    b->cells.give(b->cell_off[s], (size_t)r.nx * r.ny);
+    b->blocks.give(r.boff, r.nb);
+    r = SlotRec{};
+    return DBA_OK;
+}
+
+int dba_batch_step(dba_batch* b, int nsteps)
+{
+    if (!b || nsteps < 0) return DBA_ERR_ARG;
+    while (nsteps > 0) {
+        const int res = (int)((b->step + 1) % 6);
+        if (nsteps >= kGraphSteps) {
+            cudaGraphExec_t& ge = b->graphs[res];
+            if (!ge) {
+                cudaGraph_t graph;
+                BTRY(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+                cudaError_t e = cudaSuccess;
+                for (int q = 0; q < kGraphSteps && e == cudaSuccess; ++q) e = enqueue(b, b->step + 1 + q);
+                cudaError_t e2 = cudaStreamEndCapture(b->st, &graph);
+                if (e != cudaSuccess) return cuda_status(e);
+                if (e2 != cudaSuccess) return cuda_status(e2);
+                e = cudaGraphInstantiate(&ge, graph, 0);
+                cudaGraphDestroy(graph);
+                if (e != cudaSuccess) return cuda_status(e);
+            }
+            BTRY(cudaGraphLaunch(ge, b->st));
+            b->step += kGraphSteps;
+            nsteps -= kGraphSteps;
+            for (int s = 0; s < b->cfg.max_slots; ++s)
+                if (b->slots[s].live) b->age[s] += kGraphSteps;
+        } else {
+            BTRY(enqueue(b, b->step + 1));
+            b->step += 1;
+            nsteps -= 1;
+            for (int s = 0; s < b->cfg.max_slots; ++s)
+                if (b->slots[s].live) b->age[s] += 1;
+        }
+    }
+    return DBA_OK;
+}
+
+int dba_batch_sync(dba_batch* b)
+{
+    if (!b) return DBA_ERR_ARG;
+    BTRY(cudaStreamSynchronize(b->st));
+    int s = 0;
+    BTRY(cudaMemcpy(&s, b->status, sizeof(int), cudaMemcpyDeviceToHost));
+    return s;
+}
+
+int dba_batch_tips(dba_batch* b, double* tips, long* steps)
+{
+    if (!b || !tips) return DBA_ERR_ARG;
+    const uint8_t* par_cur = b->par + ((b->step + 1) % 2) * 2 * (size_t)b->cfg.block_capacity;
+    BTRY(b->esz == 8 ? launch_batch_tips<double>(b->st, bparams(b), par_cur, b->cfg.max_slots, b->d_tips)
+                     : launch_batch_tips<float>(b->st, bparams(b), par_cur, b->cfg.max_slots, b->d_tips));
+    BTRY(cudaMemcpyAsync(tips, b->d_tips, sizeof(double) * b->cfg.max_slots, cudaMemcpyDeviceToHost, b->st));
+    BTRY(cudaStreamSynchronize(b->st));
+    if (steps)
+        for (int s = 0; s < b->cfg.max_slots; ++s) steps[s] = b->slots[s].live ? b->age[s] : -1;
+    return DBA_OK;
+}
+
+int dba_batch_read_field(dba_batch* b, int s, int field, double* host)
+{
+    if (!b || !host || s < 0 || s >= b->cfg.max_slots || !b->slots[s].live || field < 0 || field > 1)
+        return DBA_ERR_ARG;
+    BTRY(cudaStreamSynchronize(b->st));
+    const SlotRec& r = b->slots[s];
+    const size_t n = (size_t)r.nx * r.ny;
+    const size_t NB = b->cfg.block_capacity;
+    const uint8_t* par_cur = b->par + ((b->step + 1) % 2) * 2 * NB + field * NB;
+    std::vector<uint8_t> par(r.nb);
+    BTRY(cudaMemcpy(par.data(), par_cur + r.boff, r.nb, cudaMemcpyDeviceToHost));
+    std::vector<unsigned char> a0(n * b->esz), a1(n * b->esz);
+    BTRY(cudaMemcpy(a0.data(), field ? r.T[0] : r.p[0], n * b->esz, cudaMemcpyDeviceToHost));
+    BTRY(cudaMemcpy(a1.data(), field ? r.T[1] : r.p[1], n * b->esz, cudaMemcpyDeviceToHost));
+    const int B = b->cfg.block;
+    for (int y = 0; y < r.ny; ++y)
+        for (int x = 0; x < r.nx; ++x) {
+            size_t i = (size_t)x + (size_t)r.nx * y;
+            const unsigned char* src = par[x / B + r.nbx * (y / B)] ? a1.data() : a0.data();
+            host[i] = b->esz == 8 ? ((const double*)src)[i] : (double)((const float*)src)[i];
+        }
+    return DBA_OK;
+}
+
+int dba_batch_get_info(dba_batch* b, dba_batch_info* info)
+{
+    if (!b || !info) return DBA_ERR_ARG;
+    std::memset(info, 0, sizeof *info);
+    info->free_cells = b->cells.total();
+    info->largest_free_cells = b->cells.largest();
+    info->free_blocks = (long)b->blocks.total();
+    info->largest_free_blocks = (long)b->blocks.largest();
+    for (auto& r : b->slots) info->live_slots += r.live ? 1 : 0;
+    info->step = b->step;
+    unsigned long long st[4];
+    BTRY(cudaStreamSynchronize(b->st));
+    BTRY(cudaMemcpy(st, b->stats, sizeof st, cudaMemcpyDeviceToHost));
+    info->active_block_steps = (long)st[2];
+    info->grid_ctas = b->grid;
+    return DBA_OK;
+}
+
+int dba_batch_get_stream(dba_batch* b, void** stream)
+{
+    if (!b || !stream) return DBA_ERR_ARG;
+    *stream = (void*)b->st;
+    return DBA_OK;
+}
+
+}  // extern "C"

@@ -199,6 +199,36 @@ cudaError_t launch_kh_prim_blocks(cudaStream_t st, const GridP& g, int B, const 
     return cudaGetLastError();
 }
 
+template <typename R>
+int batch_grid(int B, int sms)
+{
+    const void* k = B == 4 ? (const void*)batch_dendrite_step<R, 4, true>
+                  : B == 8 ? (const void*)batch_dendrite_step<R, 8, true> : (const void*)batch_dendrite_step<R, 16, true>;
+    return grid_of<R>(k, 0, sms);
+}
+
+template <typename R>
+cudaError_t launch_batch_step(int B, int grid, cudaStream_t st, const BatchP& p, const FlagP& f)
+{
+    switch (B) {
+    case 4: batch_dendrite_step<R, 4, true><<<grid, kThreads, 0, st>>>(p, f); break;
+    case 8: batch_dendrite_step<R, 8, true><<<grid, kThreads, 0, st>>>(p, f); break;
+    case 16: batch_dendrite_step<R, 16, true><<<grid, kThreads, 0, st>>>(p, f); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_batch_tips(cudaStream_t st, const BatchP& p, const uint8_t* par_cur, int nslots, double* tips)
+{
+    batch_tips<R><<<nslots, kThreads, 0, st>>>(p, par_cur, nslots, tips);
+    return cudaGetLastError();
+}
+
+template int batch_grid<REAL_T>(int, int);
+template cudaError_t launch_batch_step<REAL_T>(int, int, cudaStream_t, const BatchP&, const FlagP&);
+template cudaError_t launch_batch_tips<REAL_T>(cudaStream_t, const BatchP&, const uint8_t*, int, double*);
 template bool shape_supported<REAL_T>(int, int, int);
 template int step_grid<REAL_T>(int, int, int, int);
 template cudaError_t launch_dendrite<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const DenP<REAL_T>&);

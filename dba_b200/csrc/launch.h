@@ -11,6 +11,7 @@
 #include "k_modelb.cuh"
 #include "k_modelb_fast.cuh"
 #include "k_reduce.cuh"
+#include "k_batch.cuh"
 
 namespace dba {
 
@@ -28,7 +29,7 @@ cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st
                           const MBP<R>& P, const LazyP* lz);
 template <typename R> bool modelb_uses_fast(int D, int B);
 cudaError_t launch_gather_lazy(cudaStream_t st, const GridP& g, int B, const float* b0, const float* b1,
-                               const uint8_t* par, const double* cum_q, size_t count, double* out);
+                               const uint8_t* par, const long long* total_q, size_t count, double* out);
 template <typename R>
 cudaError_t launch_kh(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f, const KHP<R>& P);
 template <typename R> cudaError_t launch_correct(int grid, cudaStream_t st, const GridP& g, const CorrP<R>& P);
@@ -39,6 +40,13 @@ cudaError_t launch_gather(cudaStream_t st, const GridP& g, int B, int D, const R
 // KH: recompute primitives from the conserved fields in every block flagged in `only` (all when null)
 template <typename R>
 cudaError_t launch_kh_prim_blocks(cudaStream_t st, const GridP& g, int B, const KHP<R>& P, const uint8_t* only);
+
+// batched dendrite (k_batch.cuh)
+template <typename R> int batch_grid(int B, int sms);
+template <typename R>
+cudaError_t launch_batch_step(int B, int grid, cudaStream_t st, const BatchP& p, const FlagP& f);
+template <typename R>
+cudaError_t launch_batch_tips(cudaStream_t st, const BatchP& p, const uint8_t* par_cur, int nslots, double* tips);
 
 cudaError_t launch_reduce(cudaStream_t st, const double* bsum, int nb, int nq, double* l1, unsigned int* ticket,
                           double* avg, double ncells);

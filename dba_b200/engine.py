@@ -68,6 +68,17 @@ class Prof(ctypes.Structure):
                 ("ch0_only_blocks", ctypes.c_long), ("cells_per_block", ctypes.c_long)]
 
 
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("precision", _i), ("block", _i), ("max_slots", _i), ("block_capacity", _i),
+                ("cell_capacity", ctypes.c_size_t)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("free_cells", ctypes.c_size_t), ("largest_free_cells", ctypes.c_size_t),
+                ("free_blocks", ctypes.c_long), ("largest_free_blocks", ctypes.c_long), ("live_slots", _i),
+                ("step", ctypes.c_long), ("active_block_steps", ctypes.c_long), ("grid_ctas", _i)]
+
+
 _LIB = None
 
 
@@ -109,6 +120,16 @@ def load_library():
             "dba_state_size": (_i, [V, P(ctypes.c_size_t)]),
             "dba_save_state": (_i, [V, V, ctypes.c_size_t]),
             "dba_load_state": (_i, [V, V, ctypes.c_size_t]),
+            "dba_batch_create": (_i, [P(BatchConfig), P(V)]),
+            "dba_batch_add": (_i, [V, P(Config), P(_d), P(_i)]),
+            "dba_batch_remove": (_i, [V, _i]),
+            "dba_batch_step": (_i, [V, _i]),
+            "dba_batch_sync": (_i, [V]),
+            "dba_batch_tips": (_i, [V, P(_d), P(ctypes.c_long)]),
+            "dba_batch_read_field": (_i, [V, _i, _i, P(_d)]),
+            "dba_batch_get_info": (_i, [V, P(BatchInfo)]),
+            "dba_batch_get_stream": (_i, [V, P(V)]),
+            "dba_batch_destroy": (None, [V]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -268,3 +289,78 @@ class Simulation:
 
     def __exit__(self, *a):
         self.close()
+
+
+class Batch:
+    """Many independent 2-D dendrite simulations advanced by one kernel per step
+    (include/dba.h, dba_batch_*).  Slots are admitted while the batch's device
+    arena and block space have room and retired when done."""
+
+    def __init__(self, precision=1, block=8, max_slots=64, block_capacity=1 << 16, cell_capacity=0):
+        self._L = _lib()
+        self.cfg = BatchConfig(precision, block, max_slots, block_capacity, cell_capacity)
+        self._h = ctypes.c_void_p()
+        _check(self._L.dba_batch_create(ctypes.byref(self.cfg), ctypes.byref(self._h)), "dba_batch_create")
+        self.max_slots = max_slots
+        self.shapes = {}
+
+    def add(self, cfg, ic=None):
+        """Admit a simulation; returns its slot, or None when there is no room."""
+        slot = _i()
+        ptr = None
+        if ic is not None:
+            a = np.ascontiguousarray(np.concatenate([np.asarray(f, np.float64).ravel() for f in ic]))
+            ptr = a.ctypes.data_as(ctypes.POINTER(_d))
+        st = self._L.dba_batch_add(self._h, ctypes.byref(cfg), ptr, ctypes.byref(slot))
+        if st == 3:
+            return None
+        _check(st, "dba_batch_add")
+        self.shapes[slot.value] = (cfg.ny, cfg.nx)
+        return slot.value
+
+    def remove(self, slot):
+        _check(self._L.dba_batch_remove(self._h, int(slot)), "dba_batch_remove")
+        self.shapes.pop(slot, None)
+
+    def step(self, n):
+        _check(self._L.dba_batch_step(self._h, int(n)), "dba_batch_step")
+
+    def sync(self):
+        _check(self._L.dba_batch_sync(self._h), "dba_batch_sync")
+
+    def tips(self):
+        t = np.empty(self.max_slots, np.float64)
+        s = np.empty(self.max_slots, np.int64)
+        _check(self._L.dba_batch_tips(self._h, t.ctypes.data_as(ctypes.POINTER(_d)),
+                                      s.ctypes.data_as(ctypes.POINTER(ctypes.c_long))), "dba_batch_tips")
+        return t, s
+
+    def field(self, slot, name):
+        fid = ["p", "T"].index(name) if isinstance(name, str) else int(name)
+        ny, nx = self.shapes[slot]
+        out = np.empty(ny * nx, np.float64)
+        _check(self._L.dba_batch_read_field(self._h, int(slot), fid, out.ctypes.data_as(ctypes.POINTER(_d))),
+               "dba_batch_read_field")
+        return out.reshape(1, ny, nx)
+
+    def info(self):
+        inf = BatchInfo()
+        _check(self._L.dba_batch_get_info(self._h, ctypes.byref(inf)), "dba_batch_get_info")
+        return inf
+
+    @property
+    def stream(self):
+        v = ctypes.c_void_p()
+        _check(self._L.dba_batch_get_stream(self._h, ctypes.byref(v)), "dba_batch_get_stream")
+        return v.value or 0
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.dba_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -225,6 +225,46 @@ int dba_state_size(dba_ctx* ctx, size_t* size);
 int dba_save_state(dba_ctx* ctx, void* host, size_t size);
 int dba_load_state(dba_ctx* ctx, const void* host, size_t size);
 
+/* ---- batched simulations (no reference counterpart: the reference runs one
+ * simulation per process; these advance many independent 2-D dendrite runs of
+ * different sizes and parameters, e.g. an undercooling/anisotropy sweep, with
+ * one kernel launch per step over all of their active blocks) ---- */
+typedef struct dba_batch dba_batch;
+
+typedef struct dba_batch_config {
+    int precision;             /* DBA_PREC_* for every slot */
+    int block;                 /* DBA block edge for every slot (4, 8 or 16) */
+    int max_slots;             /* simulations held at once */
+    int block_capacity;        /* total DBA blocks over all slots */
+    size_t cell_capacity;      /* total cells over all slots; 0 = size from free device memory */
+} dba_batch_config;
+
+typedef struct dba_batch_info {
+    size_t free_cells, largest_free_cells;
+    long free_blocks, largest_free_blocks;
+    int live_slots;
+    long step;                 /* batch steps since creation */
+    long active_block_steps;   /* blocks processed, summed over steps */
+    int grid_ctas;
+} dba_batch_info;
+
+int dba_batch_create(const dba_batch_config* cfg, dba_batch** out);
+/* Admit one simulation (dendrite, 2-D, cfg->block and cfg->precision equal to
+ * the batch's): allocates its fields from the batch arena and its blocks from
+ * the block space; DBA_ERR_NOMEM when either has no room.  ic as dba_init. */
+int dba_batch_add(dba_batch* b, const dba_config* cfg, const double* ic, int* slot);
+int dba_batch_remove(dba_batch* b, int slot);
+/* nsteps DBA steps of every live slot (asynchronous; captured graphs). */
+int dba_batch_step(dba_batch* b, int nsteps);
+int dba_batch_sync(dba_batch* b);
+/* growth_front at x = Nx/2 of every slot (NaN for empty slots) and each slot's
+ * steps since admission (-1 for empty slots); arrays of max_slots. */
+int dba_batch_tips(dba_batch* b, double* tips, long* steps);
+int dba_batch_read_field(dba_batch* b, int slot, int field, double* host);
+int dba_batch_get_info(dba_batch* b, dba_batch_info* info);
+int dba_batch_get_stream(dba_batch* b, void** stream);
+void dba_batch_destroy(dba_batch* b);
+
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * -- work enqueued while a stream is captured into a CUDA graph, latency-critical
  * loops that must not take an allocation's implicit device synchronisation, or
