@@ -57,6 +57,7 @@ struct dba_ctx {
     bool initialized = false;
     // FP32 2-D Model B conserved: lazy correction state (k_modelb_fast.cuh)
     bool lazy = false;
+    bool tiles = false;               // FP32 2-D Model B on 32x32-cell tiles (k_modelb_tile.cuh)
     long long* total = nullptr;       // [3] fixed-point total of stored changes
     long long* cta_part = nullptr;    // [3][grid]
     double* lavg = nullptr;           // [3]
@@ -235,7 +236,7 @@ cudaError_t enqueue_step_t(dba_ctx* c, long s, bool dba_mode)
     case DBA_MODEL_MODELB: {
         MBP<R> P = mb_params<R>(c, dba_mode);
         LazyP L = lazy_params(c, P.conserved != 0);
-        e = launch_modelb<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L);
+        e = launch_modelb<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
         if (e != cudaSuccess || !P.conserved || c->lazy) return e;
         break;
     }
@@ -428,6 +429,7 @@ int dba_config_default(int model, dba_config* k)
     k->seed = 1234ULL;
     k->noise_amp = 0.05;
     k->noise_amp_z = 0.001;
+    k->tiles = 1;
     k->kh_gamma = 5.0 / 3.0;
     k->ic_radius = 10.0;
     k->ic_width = 2.0;
@@ -523,6 +525,10 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
     }
     c->grid = c->esz == 8 ? step_grid<double>(cfg->model, c->D, c->B, c->sms) : step_grid<float>(cfg->model, c->D, c->B, c->sms);
     if (c->grid < 1) c->grid = c->sms;
+    if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->tiles && modelb_tiles_ok(c->D, c->B, cfg->nx, cfg->ny)) {
+        c->tiles = true;
+        c->grid = modelb_tile_grid(c->B, c->sms, (cfg->nx / 32) * (cfg->ny / 32));
+    }
     if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->conserved && modelb_uses_fast<float>(c->D, c->B)) {
         c->lazy = true;
         c->total = (long long*)dev_alloc(c, 3 * sizeof(long long), &err);
@@ -854,7 +860,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 else if (c->cfg.model == DBA_MODEL_MODELB) {
                     MBP<double> P = mb_params<double>(c, dba_mode);
                     LazyP L = lazy_params(c, P.conserved != 0);
-                    r = launch_modelb<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L);
+                    r = launch_modelb<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
                 }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
@@ -865,7 +871,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 else if (c->cfg.model == DBA_MODEL_MODELB) {
                     MBP<float> P = mb_params<float>(c, dba_mode);
                     LazyP L = lazy_params(c, P.conserved != 0);
-                    r = launch_modelb<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L);
+                    r = launch_modelb<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
                 }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);

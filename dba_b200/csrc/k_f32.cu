@@ -14,4 +14,43 @@ cudaError_t launch_gather_lazy(cudaStream_t st, const GridP& g, int B, const flo
     return cudaGetLastError();
 }
 
+bool modelb_tiles_ok(int D, int B, int nx, int ny)
+{
+    return D == 2 && (B == 8 || B == 16) && nx % MBTile<16>::T == 0 && ny % MBTile<16>::T == 0;
+}
+
+template <int B>
+static int tile_grid_b(int sms, int ntiles)
+{
+    const size_t sm = MBTile<B>::smem;
+    cudaFuncSetAttribute(modelb_tile_step<B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(modelb_tile_step<B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, modelb_tile_step<B, true>, MBTile<B>::NT, sm) != cudaSuccess ||
+        occ < 1)
+        occ = 1;
+    const int g = occ * sms;
+    return g < ntiles ? g : ntiles;
+}
+
+int modelb_tile_grid(int B, int sms, int ntiles)
+{
+    return B == 8 ? tile_grid_b<8>(sms, ntiles) : tile_grid_b<16>(sms, ntiles);
+}
+
+cudaError_t launch_modelb_tiles(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
+                                const MBFastP& P, const MBFastBuf& Q, const LazyP& L)
+{
+#define XT(b)                                                                                         \
+    if (B == b) {                                                                                     \
+        const size_t sm = MBTile<b>::smem;                                                            \
+        if (dba_mode) modelb_tile_step<b, true><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, Q, L);      \
+        else modelb_tile_step<b, false><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, Q, L);              \
+        return cudaGetLastError();                                                                    \
+    }
+    XT(8) XT(16)
+#undef XT
+    return cudaErrorInvalidValue;
+}
+
 }  // namespace dba

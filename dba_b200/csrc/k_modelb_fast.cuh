@@ -44,7 +44,7 @@ constexpr double kFixUnit = 1.0 / 1099511627776.0;  // 2^-40
 
 // exact fixed-point image of an FP32 change (|d| < 2^23, ulp(d) >= 2^-40 for
 // field values above 2^-17)
-__device__ __forceinline__ long long to_fix(float d) { return __float2ll_rn(d * 1099511627776.0f); }
+__device__ __forceinline__ long long to_fix(float d) { return __float2ll_rn(__fmul_rn(d, 1099511627776.0f)); }
 
 // warp total of int64 values without 64-bit shuffles: split into a signed high
 // part and a 24-bit low part, each summed with one __reduce_add_sync
@@ -115,13 +115,54 @@ template <int B> struct MBFastShape {
     static constexpr size_t smem = sizeof(float) * 3 * (size_t)K * (TV + FV);
 };
 
-// 2-D form of the 27-point Laplacian (kernel.cu:332-344 with z wrapped onto the cell)
-__device__ __forceinline__ float lap9(const float* c, int i, int sy, float inv_dx2)
+// ---- FP32 point formulas shared by every 2-D Model B kernel.  Each operation
+// is an explicitly rounded intrinsic (no compiler contraction choices), so two
+// kernels that use these helpers produce bit-identical values. ----
+
+// 2-D form of the 27-point Laplacian (kernel.cu:332-344 with z wrapped onto the
+// cell) from row data: h = right + left neighbour of a row, c = its centre,
+// m / 0 / p = rows y-1, y, y+1
+__device__ __forceinline__ float lap9_rows(float hm, float cm, float h0, float c0, float hp, float cp, float inv_dx2)
 {
     const float cc = (float)(-10.0 / 3.0), cf = (float)(2.0 / 3.0), cd = (float)(1.0 / 6.0);
-    const float faces = (c[i + 1] + c[i - 1]) + (c[i + sy] + c[i - sy]);
-    const float diag = (c[i + 1 + sy] + c[i - 1 + sy]) + (c[i + 1 - sy] + c[i - 1 - sy]);
-    return inv_dx2 * (cc * c[i] + cf * faces + cd * diag);
+    const float faces = __fadd_rn(h0, __fadd_rn(cp, cm));
+    const float diag = __fadd_rn(hp, hm);
+    return __fmul_rn(inv_dx2, __fmaf_rn(cd, diag, __fmaf_rn(cf, faces, __fmul_rn(cc, c0))));
+}
+
+__device__ __forceinline__ float lap9(const float* c, int i, int sy, float inv_dx2)
+{
+    return lap9_rows(__fadd_rn(c[i + 1 - sy], c[i - 1 - sy]), c[i - sy], __fadd_rn(c[i + 1], c[i - 1]), c[i],
+                     __fadd_rn(c[i + 1 + sy], c[i - 1 + sy]), c[i + sy], inv_dx2);
+}
+
+// chemical potentials (Calc_mu, kernel.cu:371-388) from pointwise values and Laplacians
+__device__ __forceinline__ void mb_potentials(const MBFastP& P, float X, float Y, float Z, float lapx, float lapy,
+                                              float lapz, float& ux, float& uy, float& uz)
+{
+    const float bb = __fsub_rn(__fsub_rn(__fsub_rn(1.f, X), Y), Z);
+    const float lb = __logf(bb);
+    const float sumb = __fmaf_rn(P.chi_zb, Z, __fmaf_rn(P.chi_yb, Y, __fmul_rn(P.chi_xb, X)));   // common subtrahend
+    float u = __fmaf_rn(P.chi_xb, bb, __fmaf_rn(P.chi_xz, Z, __fmaf_rn(P.chi_xy, Y, P.c0x)));
+    u = __fsub_rn(__fmaf_rn(__logf(X), P.irx, __fsub_rn(u, sumb)), lb);
+    ux = __fmaf_rn(-P.ex, lapx, u);
+    u = __fmaf_rn(P.chi_yb, bb, __fmaf_rn(P.chi_yz, Z, __fmaf_rn(P.chi_xy, X, P.c0y)));
+    u = __fsub_rn(__fmaf_rn(__logf(Y), P.iry, __fsub_rn(u, sumb)), lb);
+    uy = __fmaf_rn(-P.ey, lapy, u);
+    u = __fmaf_rn(P.chi_zb, bb, __fmaf_rn(P.chi_yz, Y, __fmaf_rn(P.chi_xz, X, P.c0z)));
+    u = __fsub_rn(__fmaf_rn(__logf(Z), P.irz, __fsub_rn(u, sumb)), lb);
+    uz = __fsub_rn(__fmaf_rn(-P.ez, lapz, u), P.phi_logK);
+}
+
+// per-step changes (Update, kernel.cu:419-434) from the potentials at the cell and their Laplacians
+__device__ __forceinline__ void mb_changes(const MBFastP& P, float mx, float my, float mz, float lmx, float lmy,
+                                           float lmz, float& cx, float& cy, float& cz)
+{
+    const float Rr = __fmul_rn(P.k0, __fsub_rn(__expf(__fmaf_rn(P.nvx, mx, __fmul_rn(P.mvy, my))),
+                                               __expf(__fmul_rn(P.dvz, mz))));
+    cx = __fmul_rn(P.dtvx, __fmaf_rn(P.Mx, lmx, -__fmul_rn(P.dn, Rr)));
+    cy = __fmul_rn(P.dtvy, __fmaf_rn(P.My, lmy, -__fmul_rn(P.dm, Rr)));
+    cz = __fmul_rn(P.dtvz, __fmaf_rn(P.Mz, lmz, Rr));
 }
 
 template <int B, bool DBA>
@@ -239,19 +280,13 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 const int mi = k * FV + fx + SF * fy;
                 if (r == 4 || s_ra[k][r]) {
                     const int ti = k * TV + (fx + 1) + SE * (fy + 1);
-                    const float X = sx[ti] - s_Cf[0], Y = sy[ti] - s_Cf[1], Z = sz[ti] - s_Cf[2];
-                    const float bb = 1.f - X - Y - Z;
+                    const float X = __fsub_rn(sx[ti], s_Cf[0]), Y = __fsub_rn(sy[ti], s_Cf[1]);
+                    const float Z = __fsub_rn(sz[ti], s_Cf[2]);
                     const float lapx = lap9(sx, ti, SE, inv_dx2);
                     const float lapy = lap9(sy, ti, SE, inv_dx2);
                     const float lapz = lap9(sz, ti, SE, inv_dx2);
-                    const float lb = __logf(bb);
-                    const float sumb = P.chi_xb * X + P.chi_yb * Y + P.chi_zb * Z;   // common subtrahend
-                    const float ux = P.c0x + P.chi_xy * Y + P.chi_xz * Z + P.chi_xb * bb - sumb +
-                                     __logf(X) * P.irx - lb - P.ex * lapx;
-                    const float uy = P.c0y + P.chi_xy * X + P.chi_yz * Z + P.chi_yb * bb - sumb +
-                                     __logf(Y) * P.iry - lb - P.ey * lapy;
-                    const float uz = P.c0z + P.chi_xz * X + P.chi_yz * Y + P.chi_zb * bb - sumb +
-                                     __logf(Z) * P.irz - lb - P.ez * lapz - P.phi_logK;
+                    float ux, uy, uz;
+                    mb_potentials(P, X, Y, Z, lapx, lapy, lapz, ux, uy, uz);
                     mx[mi] = ux;
                     my[mi] = uy;
                     mz[mi] = uz;
@@ -285,22 +320,21 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 const int ti = k * TV + (lx + 2) + SE * (ly + 2);
                 const int bx = blk % g.nbx, by = blk / g.nbx;
                 const size_t gi = (size_t)(bx * B + lx) + (size_t)g.nx * (size_t)(by * B + ly);
-                const float Rr = P.k0 * (__expf(P.nvx * mx[fi] + P.mvy * my[fi]) - __expf(P.dvz * mz[fi]));
-                const float cx = P.dtvx * (P.Mx * lap9(mx, fi, SF, inv_dx2) - P.dn * Rr);
-                const float cy = P.dtvy * (P.My * lap9(my, fi, SF, inv_dx2) - P.dm * Rr);
-                const float cz = P.dtvz * (P.Mz * lap9(mz, fi, SF, inv_dx2) + Rr);
+                float cx, cy, cz;
+                mb_changes(P, mx[fi], my[fi], mz[fi], lap9(mx, fi, SF, inv_dx2), lap9(my, fi, SF, inv_dx2),
+                           lap9(mz, fi, SF, inv_dx2), cx, cy, cz);
                 // stored values carry raw changes (value = stored - C)
                 const float x0 = sx[ti], y0 = sy[ti], z0 = sz[ti];
-                const float xn = x0 + cx, yn = y0 + cy, zn = z0 + cz;
+                const float xn = __fadd_rn(x0, cx), yn = __fadd_rn(y0, cy), zn = __fadd_rn(z0, cz);
                 const int dst = ((m >> 2) & 1) ^ 1;
                 (dst ? Q.x[1] : Q.x[0])[gi] = xn;
                 (dst ? Q.y[1] : Q.y[0])[gi] = yn;
                 (dst ? Q.z[1] : Q.z[0])[gi] = zn;
                 if (!isfinite(xn) || !isfinite(yn) || !isfinite(zn)) raise_status(f.status, 5);
                 if (L.lazy) {   // the change actually stored (exact in FP32), in fixed point
-                    fx_[0] += to_fix(xn - x0);
-                    fx_[1] += to_fix(yn - y0);
-                    fx_[2] += to_fix(zn - z0);
+                    fx_[0] += to_fix(__fsub_rn(xn, x0));
+                    fx_[1] += to_fix(__fsub_rn(yn, y0));
+                    fx_[2] += to_fix(__fsub_rn(zn, z0));
                 }
             }
             if (L.lazy) {

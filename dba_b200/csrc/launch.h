@@ -10,6 +10,7 @@
 #include "k_kh.cuh"
 #include "k_modelb.cuh"
 #include "k_modelb_fast.cuh"
+#include "k_modelb_tile.cuh"
 #include "k_reduce.cuh"
 #include "k_batch.cuh"
 
@@ -22,12 +23,18 @@ template <typename R> int step_grid(int model, int D, int B, int sms);
 template <typename R>
 cudaError_t launch_dendrite(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
                             const DenP<R>& P);
-// FP32 2-D uses the fast kernel (lazy conserved correction, reduction fused);
-// `lz` may be null for FP64.
+// FP32 2-D uses the fast kernels (lazy conserved correction, reduction fused):
+// the 32x32-cell tile kernel when `tiles` (see modelb_tiles_ok), else one block
+// at a time.  `lz` may be null for FP64.
 template <typename R>
 cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
-                          const MBP<R>& P, const LazyP* lz);
+                          const MBP<R>& P, const LazyP* lz, bool tiles);
 template <typename R> bool modelb_uses_fast(int D, int B);
+bool modelb_tiles_ok(int D, int B, int nx, int ny);
+// persistent grid of the tile kernel (also sets its shared-memory limit on the current device)
+int modelb_tile_grid(int B, int sms, int ntiles);
+cudaError_t launch_modelb_tiles(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
+                                const MBFastP& P, const MBFastBuf& Q, const LazyP& L);
 cudaError_t launch_gather_lazy(cudaStream_t st, const GridP& g, int B, const float* b0, const float* b1,
                                const uint8_t* par, const long long* total_q, size_t count, double* out);
 template <typename R>

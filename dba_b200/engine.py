@@ -44,7 +44,7 @@ class Config(ctypes.Structure):
         ("metric_eps", _d), ("kh_gamma", _d),
         ("block", _i), ("precision", _i), ("bc", _i), ("conserved", _i), ("ic", _i),
         ("seed", _u64), ("ic_radius", _d), ("ic_width", _d), ("ic_corner", _i),
-        ("noise_amp", _d), ("noise_amp_z", _d),
+        ("noise_amp", _d), ("noise_amp_z", _d), ("tiles", _i),
     ]
 
     def as_dict(self):

@@ -82,6 +82,8 @@ typedef struct dba_config {
     double ic_radius, ic_width;/* dendrite tanh seed */
     int ic_corner;             /* dendrite tanh seed at cell (0,0,0) instead of the centre */
     double noise_amp, noise_amp_z; /* Model B: x,y and z uniform-noise amplitudes (0.05, 0.001) */
+    int tiles;                 /* FP32 2-D Model B: 1 (default) = 32x32-cell tile kernel when nx, ny are multiples
+                                  of 32 and block is 8 or 16; 0 = one-block-at-a-time kernel */
 } dba_config;
 
 typedef struct dba_ctx dba_ctx;
