@@ -58,10 +58,7 @@ struct dba_ctx {
     // FP32 2-D Model B conserved: lazy correction state (k_modelb_fast.cuh)
     bool lazy = false;
     bool tiles = false;               // FP32 2-D Model B on 32x32-cell tiles (k_modelb_tile.cuh)
-    long long* total = nullptr;       // [3] fixed-point total of stored changes
-    long long* cta_part = nullptr;    // [3][grid]
-    double* lavg = nullptr;           // [3]
-    unsigned int* lticket = nullptr;
+    long long* lz = nullptr;          // tot[2][3] then chg[3][3]: rotating fixed-point totals (LazyP)
     cudaGraphExec_t graphs[6][2] = {};
     bool use_graphs = true;
     int last_error = DBA_OK;
@@ -213,15 +210,21 @@ CorrP<R> corr_params(dba_ctx* c, long s)
     return P;
 }
 
-LazyP lazy_params(dba_ctx* c, bool conserved_step)
+// lazy conserved totals seen by the launch of step s (rotation described at LazyP)
+LazyP lazy_params(dba_ctx* c, long s, bool conserved_step)
 {
     LazyP L{};
-    L.total = c->total;
-    L.cta_part = c->cta_part;
-    L.avg = c->lavg;
-    L.ticket = c->lticket;
+    if (!c->lazy) return L;
+    long long* tot = c->lz;
+    long long* chg = c->lz + 6;
+    L.tot_prev = tot + 3 * ((s + 1) % 2);
+    L.tot_cur = tot + 3 * (s % 2);
+    L.chg_prev = chg + 3 * ((s + 2) % 3);
+    L.chg_clear = chg + 3 * ((s + 1) % 3);
+    L.chg_cur = reinterpret_cast<unsigned long long*>(chg + 3 * (s % 3));
     L.ncells = (double)c->n;
-    L.lazy = (c->lazy && conserved_step) ? 1 : 0;
+    L.lazy = 1;
+    L.accumulate = conserved_step ? 1 : 0;
     return L;
 }
 
@@ -235,7 +238,7 @@ cudaError_t enqueue_step_t(dba_ctx* c, long s, bool dba_mode)
         return launch_dendrite<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<R>(c));
     case DBA_MODEL_MODELB: {
         MBP<R> P = mb_params<R>(c, dba_mode);
-        LazyP L = lazy_params(c, P.conserved != 0);
+        LazyP L = lazy_params(c, s, P.conserved != 0);
         e = launch_modelb<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
         if (e != cudaSuccess || !P.conserved || c->lazy) return e;
         break;
@@ -531,10 +534,7 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
     }
     if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->conserved && modelb_uses_fast<float>(c->D, c->B)) {
         c->lazy = true;
-        c->total = (long long*)dev_alloc(c, 3 * sizeof(long long), &err);
-        if (!err) c->cta_part = (long long*)dev_alloc(c, 3 * (size_t)c->grid * sizeof(long long), &err);
-        if (!err) c->lavg = (double*)dev_alloc(c, 3 * sizeof(double), &err);
-        if (!err) c->lticket = (unsigned int*)dev_alloc(c, sizeof(unsigned int), &err);
+        c->lz = (long long*)dev_alloc(c, 15 * sizeof(long long), &err);
         if (err) {
             dba_destroy(c);
             return err;
@@ -663,14 +663,17 @@ int dba_read_field(dba_ctx* c, int field, double* host)
         return gather(c, c->state[field][0], c->state[field][1], cur_par(c) + (size_t)field * c->g.nb, 0, 1, c->n, host);
     if (model == DBA_MODEL_MODELB) {
         if (c->lazy && field < 4) {
-            // true values: stored - total / (2^40 N) per field (lazy conserved correction)
+            // true values: stored - T / (2^40 N) per field (lazy conserved correction), T as the
+            // next step's launch will form it
+            const long sn = c->step + 1;
             std::vector<double> tmp;
             const int nq = field < 3 ? 1 : 3;
             if (nq == 3) tmp.resize(2 * c->n);
             for (int q = field < 3 ? field : 0, k = 0; k < nq; ++q, ++k) {
                 double* dst = (k == 0) ? host : tmp.data() + (k - 1) * c->n;
                 cudaError_t e = launch_gather_lazy(c->st, c->g, c->B, (const float*)c->state[q][0],
-                                                   (const float*)c->state[q][1], cur_par(c), c->total + q, c->n,
+                                                   (const float*)c->state[q][1], cur_par(c),
+                                                   c->lz + 3 * ((sn + 1) % 2) + q, c->lz + 6 + 3 * ((sn + 2) % 3) + q, c->n,
                                                    c->staging);
                 if (e == cudaSuccess) e = cudaMemcpyAsync(dst, c->staging, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
@@ -859,7 +862,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 if (c->cfg.model == DBA_MODEL_DENDRITE) r = launch_dendrite<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<double>(c));
                 else if (c->cfg.model == DBA_MODEL_MODELB) {
                     MBP<double> P = mb_params<double>(c, dba_mode);
-                    LazyP L = lazy_params(c, P.conserved != 0);
+                    LazyP L = lazy_params(c, s, P.conserved != 0);
                     r = launch_modelb<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
                 }
                 else {
@@ -870,7 +873,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 if (c->cfg.model == DBA_MODEL_DENDRITE) r = launch_dendrite<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<float>(c));
                 else if (c->cfg.model == DBA_MODEL_MODELB) {
                     MBP<float> P = mb_params<float>(c, dba_mode);
-                    LazyP L = lazy_params(c, P.conserved != 0);
+                    LazyP L = lazy_params(c, s, P.conserved != 0);
                     r = launch_modelb<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
                 }
                 else {

@@ -84,6 +84,18 @@ __device__ __forceinline__ void wake_faces(const GridP& g, uint8_t* w, int b)
     wake_one(g, w, b, 0, 0, 1);
 }
 
+// self + 4 faces of block (bx, by) of a periodic 2-D block grid; the z faces of
+// wake_faces wrap onto the block itself when there is one block layer
+__device__ __forceinline__ void wake_faces_2d(uint8_t* w, int bx, int by, int nbx, int nby)
+{
+    const int row = by * nbx;
+    w[bx + row] = 1;
+    w[(bx == 0 ? nbx - 1 : bx - 1) + row] = 1;
+    w[(bx == nbx - 1 ? 0 : bx + 1) + row] = 1;
+    w[bx + (by == 0 ? nby - 1 : by - 1) * nbx] = 1;
+    w[bx + (by == nby - 1 ? 0 : by + 1) * nbx] = 1;
+}
+
 // self + faces + 4 in-plane diagonals (example_Kelvin_Helmholtz/KH_DBA.cu:1026-1039)
 __device__ __forceinline__ void wake_faces_diag(const GridP& g, uint8_t* w, int b)
 {

@@ -7,7 +7,7 @@
 //     block, not per cell;
 //   * the reference's 27-term Laplacian is evaluated in its exact 2-D form
 //     (Nz == 1: weights -10/3, 2/3, 1/6 on centre, faces, diagonals);
-//   * __logf/__expf, float constants and reciprocals precomputed on the host;
+//   * base-2 hardware log/exp, float constants and reciprocals precomputed on the host;
 //   * tile rows padded so each warp's shared-memory accesses are conflict-free;
 //   * only the ring of cells that neighbours can read is persisted;
 //   * conserved DBA is lazy.  The reference subtracts the mean change from every
@@ -20,9 +20,11 @@
 //     exact), converted to fixed point exactly, reduced with warp
 //     __reduce_add_sync and shared/global int64 atomics -- order-independent,
 //     so the result is deterministic and the field totals are conserved to the
-//     rounding of the final FP64 division.  The last CTA to finish (atomic
-//     ticket) folds the CTA totals into the running total.  One kernel per
-//     step, no dense pass, no host round trip.
+//     rounding of the final FP64 division.  The running total is rotated with
+//     the step index (LazyP), so no CTA waits for another and there is no
+//     end-of-launch fold.  The offset applies in every mode once a context is
+//     lazy: regular steps keep it, only conserved DBA steps add to it.  One
+//     kernel per step, no dense pass, no host round trip.
 #pragma once
 
 #include "k_common.cuh"
@@ -30,14 +32,37 @@
 
 namespace dba {
 
+// Lazy conserved state of the launch for step s.  A field value is its stored
+// value minus T / (2^40 N), T the fixed-point total of every conserved change
+// stored so far.  The totals rotate with the step index so that no CTA has to
+// wait for another within a launch:
+//   T(s) = tot[(s+1) % 2] + chg[(s+2) % 3]   (total before step s-1 + changes of step s-1)
+// Step s writes T(s) to tot[s % 2] and clears chg[(s+1) % 3] (CTA 0; that slot
+// held the changes of step s-2, last read by step s-1), and every CTA adds its
+// changes of step s into chg[s % 3] with 64-bit integer atomics (exact, order
+// independent).
 struct LazyP {
-    long long* total;   // [3] all stored changes so far, fixed point 2^-40 (value = stored - total/(2^40 N))
-    long long* cta_part;// [3][grid] this step's per-CTA change totals
-    double* avg;        // [3] last step's mean change (observability)
-    unsigned int* ticket;
+    const long long* tot_prev;    // tot[(s+1) % 2]
+    const long long* chg_prev;    // chg[(s+2) % 3]
+    long long* tot_cur;           // tot[s % 2]
+    long long* chg_clear;         // chg[(s+1) % 3]
+    unsigned long long* chg_cur;  // chg[s % 3]
     double ncells;
-    int lazy;           // conserved DBA in this launch
+    int lazy;           // stored values carry the offset (every step of an FP32 2-D conserved context)
+    int accumulate;     // conserved DBA step: this step's stored changes are summed
 };
+
+// offset of field q at the start of a launch; CTA 0 also advances the rotation
+__device__ __forceinline__ float lazy_offset(const LazyP& L, int q)
+{
+    if (!L.lazy) return 0.f;
+    const long long T = L.tot_prev[q] + L.chg_prev[q];
+    if (blockIdx.x == 0) {
+        L.tot_cur[q] = T;
+        L.chg_clear[q] = 0;
+    }
+    return (float)((double)T * (1.0 / 1099511627776.0) / L.ncells);
+}
 
 constexpr double kFixScale = 1099511627776.0;       // 2^40
 constexpr double kFixUnit = 1.0 / 1099511627776.0;  // 2^-40
@@ -136,21 +161,39 @@ __device__ __forceinline__ float lap9(const float* c, int i, int sy, float inv_d
                      __fadd_rn(c[i + 1 + sy], c[i - 1 + sy]), c[i + sy], inv_dx2);
 }
 
+// Natural log and exponential by change of base onto the hardware base-2
+// approximations (PTX lg2.approx / ex2.approx, flush-to-zero forms):
+// ln x = log2(x) ln 2,  e^x = 2^(x log2 e).  Relative error ~2^-22; the fields
+// never approach the denormal range.
+__device__ __forceinline__ float ln_approx(float x)
+{
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return __fmul_rn(r, 0.693147180559945309f);
+}
+
+__device__ __forceinline__ float exp_approx(float x)
+{
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(__fmul_rn(x, 1.442695040888963407f)));
+    return r;
+}
+
 // chemical potentials (Calc_mu, kernel.cu:371-388) from pointwise values and Laplacians
 __device__ __forceinline__ void mb_potentials(const MBFastP& P, float X, float Y, float Z, float lapx, float lapy,
                                               float lapz, float& ux, float& uy, float& uz)
 {
     const float bb = __fsub_rn(__fsub_rn(__fsub_rn(1.f, X), Y), Z);
-    const float lb = __logf(bb);
+    const float lb = ln_approx(bb);
     const float sumb = __fmaf_rn(P.chi_zb, Z, __fmaf_rn(P.chi_yb, Y, __fmul_rn(P.chi_xb, X)));   // common subtrahend
     float u = __fmaf_rn(P.chi_xb, bb, __fmaf_rn(P.chi_xz, Z, __fmaf_rn(P.chi_xy, Y, P.c0x)));
-    u = __fsub_rn(__fmaf_rn(__logf(X), P.irx, __fsub_rn(u, sumb)), lb);
+    u = __fsub_rn(__fmaf_rn(ln_approx(X), P.irx, __fsub_rn(u, sumb)), lb);
     ux = __fmaf_rn(-P.ex, lapx, u);
     u = __fmaf_rn(P.chi_yb, bb, __fmaf_rn(P.chi_yz, Z, __fmaf_rn(P.chi_xy, X, P.c0y)));
-    u = __fsub_rn(__fmaf_rn(__logf(Y), P.iry, __fsub_rn(u, sumb)), lb);
+    u = __fsub_rn(__fmaf_rn(ln_approx(Y), P.iry, __fsub_rn(u, sumb)), lb);
     uy = __fmaf_rn(-P.ey, lapy, u);
     u = __fmaf_rn(P.chi_zb, bb, __fmaf_rn(P.chi_yz, Y, __fmaf_rn(P.chi_xz, X, P.c0z)));
-    u = __fsub_rn(__fmaf_rn(__logf(Z), P.irz, __fsub_rn(u, sumb)), lb);
+    u = __fsub_rn(__fmaf_rn(ln_approx(Z), P.irz, __fsub_rn(u, sumb)), lb);
     uz = __fsub_rn(__fmaf_rn(-P.ez, lapz, u), P.phi_logK);
 }
 
@@ -158,8 +201,8 @@ __device__ __forceinline__ void mb_potentials(const MBFastP& P, float X, float Y
 __device__ __forceinline__ void mb_changes(const MBFastP& P, float mx, float my, float mz, float lmx, float lmy,
                                            float lmz, float& cx, float& cy, float& cz)
 {
-    const float Rr = __fmul_rn(P.k0, __fsub_rn(__expf(__fmaf_rn(P.nvx, mx, __fmul_rn(P.mvy, my))),
-                                               __expf(__fmul_rn(P.dvz, mz))));
+    const float Rr = __fmul_rn(P.k0, __fsub_rn(exp_approx(__fmaf_rn(P.nvx, mx, __fmul_rn(P.mvy, my))),
+                                               exp_approx(__fmul_rn(P.dvz, mz))));
     cx = __fmul_rn(P.dtvx, __fmaf_rn(P.Mx, lmx, -__fmul_rn(P.dn, Rr)));
     cy = __fmul_rn(P.dtvy, __fmaf_rn(P.My, lmy, -__fmul_rn(P.dm, Rr)));
     cz = __fmul_rn(P.dtvz, __fmaf_rn(P.Mz, lmz, Rr));
@@ -186,19 +229,17 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
     __shared__ unsigned char s_rp[K][9], s_ra[K][9];
     __shared__ float s_Cf[3];           // conserved offset C as float
     __shared__ unsigned long long s_fix[3];   // this CTA's change total (fixed point)
-    __shared__ double s_C[3];
-    __shared__ bool s_last;
 
     const int tid = threadIdx.x;
     const int G = gridDim.x;
     const int nb = g.nb;
     const float inv_dx2 = P.inv_dx2;
     if (tid < 3) {
-        s_C[tid] = L.lazy ? (double)L.total[tid] * kFixUnit / L.ncells : 0.0;
-        s_Cf[tid] = (float)s_C[tid];
+        s_Cf[tid] = lazy_offset(L, tid);
         s_fix[tid] = 0ull;
     }
     __syncthreads();
+    const float Cx = s_Cf[0], Cy = s_Cf[1], Cz = s_Cf[2];
 
     for (long long j0 = 0; blockIdx.x + (long long)G * j0 < nb; j0 += NT) {
         const long long bl = blockIdx.x + (long long)G * (j0 + tid);
@@ -280,8 +321,7 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 const int mi = k * FV + fx + SF * fy;
                 if (r == 4 || s_ra[k][r]) {
                     const int ti = k * TV + (fx + 1) + SE * (fy + 1);
-                    const float X = __fsub_rn(sx[ti], s_Cf[0]), Y = __fsub_rn(sy[ti], s_Cf[1]);
-                    const float Z = __fsub_rn(sz[ti], s_Cf[2]);
+                    const float X = __fsub_rn(sx[ti], Cx), Y = __fsub_rn(sy[ti], Cy), Z = __fsub_rn(sz[ti], Cz);
                     const float lapx = lap9(sx, ti, SE, inv_dx2);
                     const float lapy = lap9(sy, ti, SE, inv_dx2);
                     const float lapz = lap9(sz, ti, SE, inv_dx2);
@@ -331,13 +371,13 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 (dst ? Q.y[1] : Q.y[0])[gi] = yn;
                 (dst ? Q.z[1] : Q.z[0])[gi] = zn;
                 if (!isfinite(xn) || !isfinite(yn) || !isfinite(zn)) raise_status(f.status, 5);
-                if (L.lazy) {   // the change actually stored (exact in FP32), in fixed point
+                if (L.accumulate) {   // the change actually stored (exact in FP32), in fixed point
                     fx_[0] += to_fix(__fsub_rn(xn, x0));
                     fx_[1] += to_fix(__fsub_rn(yn, y0));
                     fx_[2] += to_fix(__fsub_rn(zn, z0));
                 }
             }
-            if (L.lazy) {
+            if (L.accumulate) {
 #pragma unroll
                 for (int q = 0; q < 3; ++q) {
                     const long long w = warp_sum_fix(fx_[q]);
@@ -357,35 +397,18 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
             __syncthreads();
         }
     }
-    if (!L.lazy) return;
-    // conserved change: CTA totals, then the last CTA folds them into the running total
-    if (tid < 3) L.cta_part[(size_t)tid * G + blockIdx.x] = (long long)s_fix[tid];
-    __threadfence();
+    if (!L.accumulate) return;
     __syncthreads();
-    if (tid == 0) s_last = (atomicAdd(L.ticket, 1u) == (unsigned)G - 1);
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    const int warp = tid >> 5, lane = tid & 31;
-    if (warp < 3) {
-        long long t = 0;
-        for (int c = lane; c < G; c += 32) t += ((volatile long long*)L.cta_part)[(size_t)warp * G + c];
-#pragma unroll
-        for (int h = 16; h >= 1; h /= 2) t += __shfl_down_sync(0xffffffffu, t, h);
-        if (lane == 0) {
-            L.avg[warp] = (double)t * kFixUnit / L.ncells;
-            L.total[warp] += t;
-        }
-    }
-    if (tid == 0) *L.ticket = 0u;
+    if (tid < 3 && s_fix[tid]) atomicAdd(&L.chg_cur[tid], s_fix[tid]);
 }
 
-// FP32 lazy-conserved readback: value = stored - total / (2^40 N)
+// FP32 lazy-conserved readback: value = stored - T / (2^40 N), T = tot_q + chg_q
 static __global__ void __launch_bounds__(kThreads) gather_lazy_kernel(GridP g, int B, const float* b0, const float* b1,
-                                                                      const uint8_t* par, const long long* total_q,
-                                                                      size_t count, double* out)
+                                                                      const uint8_t* par, const long long* tot_q,
+                                                                      const long long* chg_q, size_t count,
+                                                                      double* out)
 {
-    const double C = (double)(*total_q) * kFixUnit / (double)count;
+    const double C = (double)(*tot_q + *chg_q) * kFixUnit / (double)count;
     for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < count; i += (size_t)gridDim.x * kThreads) {
         const int x = (int)(i % g.nx), y = (int)(i / g.nx);
         const int ob = x / B + g.nbx * (y / B);

@@ -14,12 +14,13 @@
 //   * each thread owns a 4-row strip of one column and slides a 3-row window
 //     down it, so the Laplacians reuse row sums instead of re-reading 9 cells;
 //   * the 1-cell potential ring around the tile is computed (active owner) or
-//     loaded from the persisted ring (inactive owner) by 132 threads;
+//     loaded from the persisted ring (inactive owner), 17 cells per warp;
 //   * a block persists its ring potentials only when its own wake-up test is
 //     negative: a block whose test is positive is active next step (it wakes
 //     itself), so its ring from this step is never read as stale;
-//   * conserved DBA (lazy): the exact fixed-point change totals are kept per
-//     thread over all its tiles and reduced once per launch.
+//   * conserved DBA (lazy): each thread sums its stored changes exactly in FP64
+//     over all its tiles; the sums are turned into fixed point and reduced once
+//     per launch, giving the same totals as a per-cell fixed-point sum.
 #pragma once
 
 #include "k_common.cuh"
@@ -34,16 +35,19 @@ template <int B> struct MBTile {
     static constexpr int NBT = TB * TB;       // blocks per tile
     static constexpr int RB = TB + 2;         // neighbourhood edge in blocks
     static constexpr int SR = T + 4;          // staged rows: 2-cell halo above and below
-    static constexpr int SP = T + 8;          // staged row pitch: 4-cell (16-byte) halo left and right
+    static constexpr int SW = T + 8;          // staged row width: 4-cell (16-byte) halo left and right
+    static constexpr int SP = SW + 4;         // row pitch: rows shift by 12 banks, so column accesses
+                                              // of the ring spread over 8 banks
     static constexpr int SV = SR * SP;        // one staged field
-    static constexpr int NQ = SR * (SP / 4);  // 16-byte pieces per staged field
+    static constexpr int NQ = SR * (SW / 4);  // 16-byte pieces per staged field
     static constexpr int MP = T + 4;          // potential row pitch (T + 2 used)
     static constexpr int MV = (T + 2) * MP;   // one potential field
     static constexpr int RING = 4 * T + 4;    // potential cells around the tile
+    static constexpr int RPW = (RING + NT / 32 - 1) / (NT / 32);   // ring cells per warp
     static constexpr int TPP = NT / NBT;      // tiles per scan pass
     static constexpr int ROWS = T * T / NT;   // rows per thread strip
     static constexpr size_t smem = sizeof(float) * (2 * 3 * SV + 3 * MV);
-    static_assert(T % B == 0 && B % ROWS == 0 && NBT <= 16 && NQ <= 2 * NT && RING <= NT, "tile shape");
+    static_assert(T % B == 0 && B % ROWS == 0 && NBT <= 16 && NQ <= 2 * NT && RPW <= 32, "tile shape");
 };
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
@@ -60,8 +64,8 @@ template <int B, bool DBA>
 __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBFastP P, MBFastBuf Q, LazyP L)
 {
     using S = MBTile<B>;
-    constexpr int NT = S::NT, T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, SP = S::SP, SV = S::SV;
-    constexpr int NQ = S::NQ, MP = S::MP, MV = S::MV, RING = S::RING, TPP = S::TPP, ROWS = S::ROWS;
+    constexpr int NT = S::NT, T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, SW = S::SW, SP = S::SP, SV = S::SV;
+    constexpr int NQ = S::NQ, MP = S::MP, MV = S::MV, RING = S::RING, RPW = S::RPW, TPP = S::TPP, ROWS = S::ROWS;
     extern __shared__ __align__(128) float smem_f[];
     float* stage = smem_f;               // [2][3][SV]
     float* mu = smem_f + 2 * 3 * SV;     // [3][MV]
@@ -72,7 +76,6 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
     __shared__ int s_nx[NBT];
     __shared__ float s_Cf[3];
     __shared__ unsigned long long s_fix[3];
-    __shared__ bool s_last;
 
     const int tid = threadIdx.x;
     const int G = gridDim.x;
@@ -80,7 +83,7 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
     const size_t nx = (size_t)g.nx;
     const float inv_dx2 = P.inv_dx2;
     if (tid < 3) {
-        s_Cf[tid] = L.lazy ? (float)((double)L.total[tid] * kFixUnit / L.ncells) : 0.f;
+        s_Cf[tid] = lazy_offset(L, tid);
         s_fix[tid] = 0ull;
     }
 
@@ -89,7 +92,7 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         const int p = tid + h * NT;
-        const int r = p / (SP / 4), c4 = p - r * (SP / 4);
+        const int r = p / (SW / 4), c4 = p - r * (SW / 4);
         q_soff[h] = r * SP + 4 * c4;
         q_lx[h] = 4 * c4 - 4;
         q_ly[h] = r - 2;
@@ -97,14 +100,18 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
     }
     const int tx = tid & 31, ly0 = (tid >> 5) * ROWS;
     const int kb = tx / B + TB * (ly0 / B);     // tile block of this strip
+    // ring cell of this thread: 17 per warp, so every warp carries the same share
+    const int rg_p = (tid >> 5) * RPW + (tid & 31);
+    const bool rg_on = (tid & 31) < RPW && rg_p < RING;
     int rg_lx = 0, rg_ly = 0;
-    if (tid < T + 2) { rg_ly = -1; rg_lx = tid - 1; }
-    else if (tid < 2 * (T + 2)) { rg_ly = T; rg_lx = tid - (T + 2) - 1; }
-    else if (tid < 2 * (T + 2) + T) { rg_lx = -1; rg_ly = tid - 2 * (T + 2); }
-    else { rg_lx = T; rg_ly = tid - 2 * (T + 2) - T; }
+    if (rg_p < T + 2) { rg_ly = -1; rg_lx = rg_p - 1; }
+    else if (rg_p < 2 * (T + 2)) { rg_ly = T; rg_lx = rg_p - (T + 2) - 1; }
+    else if (rg_p < 2 * (T + 2) + T) { rg_lx = -1; rg_ly = rg_p - 2 * (T + 2); }
+    else { rg_lx = T; rg_ly = rg_p - 2 * (T + 2) - T; }
     const int rg_reg = (rg_lx + B) / B + RB * ((rg_ly + B) / B);
-    long long fsum[3] = {0, 0, 0};
+    double fsum[3] = {0.0, 0.0, 0.0};   // this thread's stored changes (exact: see below)
     __syncthreads();
+    const float Cx = s_Cf[0], Cy = s_Cf[1], Cz = s_Cf[2];
 
     auto build_nbr = [&](int idx, int st) {
         if (tid < RB * RB) {
@@ -207,8 +214,8 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
                     const float lapy = lap9_rows(hym, cym, hy0, cy0, hyp, cyp, inv_dx2);
                     const float lapz = lap9_rows(hzm, czm, hz0, cz0, hzp, czp, inv_dx2);
                     float ux, uy, uz;
-                    mb_potentials(P, __fsub_rn(cx0, s_Cf[0]), __fsub_rn(cy0, s_Cf[1]), __fsub_rn(cz0, s_Cf[2]),
-                                  lapx, lapy, lapz, ux, uy, uz);
+                    mb_potentials(P, __fsub_rn(cx0, Cx), __fsub_rn(cy0, Cy), __fsub_rn(cz0, Cz), lapx, lapy, lapz,
+                                  ux, uy, uz);
                     const int mi = (ly0 + r + 1) * MP + tx + 1;
                     mu[mi] = ux;
                     mu[MV + mi] = uy;
@@ -230,13 +237,13 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
                     mu[2 * MV + mi] = Q.mu[2][gi];
                 }
             }
-            if (tid < RING) {
+            if (rg_on) {
                 const int mi = (rg_ly + 1) * MP + rg_lx + 1;
                 if (s_nact[st][rg_reg]) {
                     const int si = (rg_ly + 2) * SP + rg_lx + 4;
                     float ux, uy, uz;
-                    mb_potentials(P, __fsub_rn(sx[si], s_Cf[0]), __fsub_rn(sy[si], s_Cf[1]),
-                                  __fsub_rn(sz[si], s_Cf[2]), lap9(sx, si, SP, inv_dx2), lap9(sy, si, SP, inv_dx2),
+                    mb_potentials(P, __fsub_rn(sx[si], Cx), __fsub_rn(sy[si], Cy), __fsub_rn(sz[si], Cz),
+                                  lap9(sx, si, SP, inv_dx2), lap9(sy, si, SP, inv_dx2),
                                   lap9(sz, si, SP, inv_dx2), ux, uy, uz);
                     mu[mi] = ux;
                     mu[MV + mi] = uy;
@@ -258,6 +265,7 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
                 float* oz = dst ? Q.z[1] : Q.z[0];
                 const bool persist = DBA && !s_nx[kb];
                 const bool edge_x = (tx % B) == 0 || (tx % B) == B - 1;
+                const bool ring_top = (ly0 % B) == 0, ring_bot = ((ly0 + ROWS - 1) % B) == B - 1;
                 int mi = ly0 * MP + tx + 1;           // potential row ly0 - 1
                 const float* m0 = mu;
                 const float* m1 = mu + MV;
@@ -289,12 +297,15 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
                     oy[gi] = yn;
                     oz[gi] = zn;
                     bad |= !(fabsf(xn) < INFINITY && fabsf(yn) < INFINITY && fabsf(zn) < INFINITY);
-                    if (L.lazy) {   // the change actually stored (exact in FP32), in fixed point
-                        fsum[0] += to_fix(__fsub_rn(xn, x0));
-                        fsum[1] += to_fix(__fsub_rn(yn, y0));
-                        fsum[2] += to_fix(__fsub_rn(zn, z0));
+                    if (L.accumulate) {
+                        // the change actually stored (exact in FP32).  With stored values above
+                        // 2^-17 each is a multiple of 2^-40, so while a thread's partial sums stay
+                        // below 2^13 they are exact in FP64 and convert exactly to fixed point.
+                        fsum[0] += (double)__fsub_rn(xn, x0);
+                        fsum[1] += (double)__fsub_rn(yn, y0);
+                        fsum[2] += (double)__fsub_rn(zn, z0);
                     }
-                    if (persist && (edge_x || (ly % B) == 0 || (ly % B) == B - 1)) {
+                    if (persist && (edge_x || (r == 0 && ring_top) || (r == ROWS - 1 && ring_bot))) {
                         Q.mu[0][gi] = cx0;
                         Q.mu[1][gi] = cy0;
                         Q.mu[2][gi] = cz0;
@@ -308,38 +319,21 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
             if (DBA && tid < NBT && ((tm >> tid) & 1u)) {
                 const int b = ((tile % ntx) * TB + tid % TB) + g.nbx * ((tile / ntx) * TB + tid / TB);
                 f.next[b] = (uint8_t)s_nx[tid];
-                if (s_nx[tid]) wake_faces(g, f.wake_nxt, b);
+                if (s_nx[tid])
+                    wake_faces_2d(f.wake_nxt, (tile % ntx) * TB + tid % TB, (tile / ntx) * TB + tid / TB, g.nbx, g.nby);
             }
         }
         __syncthreads();                         // list and buffers reused by the next scan pass
     }
-    if (!L.lazy) return;
-    // conserved change: thread totals -> CTA totals -> last CTA folds them into the running total
+    if (!L.accumulate) return;
+    // conserved change: thread totals -> CTA totals -> this step's total (64-bit integer atomics)
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-        const long long w = warp_sum_fix(fsum[q]);
+        const long long w = warp_sum_fix(__double2ll_rn(fsum[q] * kFixScale));
         if ((tid & 31) == 0 && w) atomicAdd(&s_fix[q], (unsigned long long)w);
     }
     __syncthreads();
-    if (tid < 3) L.cta_part[(size_t)tid * G + blockIdx.x] = (long long)s_fix[tid];
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) s_last = (atomicAdd(L.ticket, 1u) == (unsigned)G - 1);
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    const int warp = tid >> 5, lane = tid & 31;
-    if (warp < 3) {
-        long long t = 0;
-        for (int c = lane; c < G; c += 32) t += ((volatile long long*)L.cta_part)[(size_t)warp * G + c];
-#pragma unroll
-        for (int h = 16; h >= 1; h /= 2) t += __shfl_down_sync(0xffffffffu, t, h);
-        if (lane == 0) {
-            L.avg[warp] = (double)t * kFixUnit / L.ncells;
-            L.total[warp] += t;
-        }
-    }
-    if (tid == 0) *L.ticket = 0u;
+    if (tid < 3 && s_fix[tid]) atomicAdd(&L.chg_cur[tid], s_fix[tid]);
 }
 
 }  // namespace dba

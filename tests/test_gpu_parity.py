@@ -197,6 +197,25 @@ def test_modelb_fp32_lazy_conserved_mass():
         assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-4, f
 
 
+@pytest.mark.parametrize("tiles", [1, 0])
+def test_modelb_fp32_lazy_offset_across_mode_switches(tiles):
+    """The lazy conserved offset of an FP32 context applies in every mode: conserved
+    DBA steps, then regular steps (offset kept, not accumulated), then DBA again,
+    track the FP64 oracle running the same sequence with its dense correction."""
+    prm = dict(MODELB_REF, metric_eps=1e-3)
+    o = OracleModelB(64, 64, 1, 16, prm, conserved=1)
+    o.init_mt()
+    s = dba_b200.Simulation(modelb_cfg(prm, 64, 64, 1, 16, precision=1, conserved=1, tiles=tiles)).init()
+    # FP32 error grows with the step count (with k_0 = 1 the approximate exp/log of the
+    # reaction bias the mean change slightly); the bound follows it
+    for n, mode, tol in ((100, 1, 1e-4), (100, 0, 1e-4), (60, 1, 3e-4)):
+        o.step(n, mode)
+        s.step(n, mode)
+        for f in ("x", "y", "z"):
+            a, b = s.field(f), o.field(f)
+            assert np.linalg.norm(a - b) / np.linalg.norm(b) <= tol, (f, n, mode)
+
+
 @pytest.mark.parametrize("B", [4, 8, 32])
 def test_modelb_fp32_fast_path_block_edges(B):
     prm = dict(MODELB_REF, metric_eps=1e-3)
