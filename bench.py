@@ -14,6 +14,11 @@ Multi-GPU: the path does not shard in this build (one domain per GPU), so
 `--gpus N` runs N independent replicas, one process per GPU, and `value` is the
 sum of their active cell-updates divided by the slowest rank's time.
 
+At N=1 the line also carries `sweep`: the batched/served 2-D dendrite
+parameter sweep (256 seeded requests, Poisson arrivals, admission by device
+memory, autotuned block edge and threads) against the same requests run one at
+a time -- runs/s of both and p50/p99 time to completion (`--no-sweep` skips it).
+
 `--impl reference` times the reference's own serial CPU program for the same
 model (its functions driven step by step by oracle/_ref/*_cpu_steps, built from
 the reference sources) on this host; rank 0 only.
@@ -215,11 +220,24 @@ def run_ours(args, w):
         except Exception:
             traffic = None
 
-    # the same state advanced in regular (dense, every block) mode, for the DBA-vs-dense comparison
-    sim.load_state(blob)
-    dense = sim.step_profiled(nprof, 0)
-    sim.load_state(blob)
-    dba_p = sim.step_profiled(nprof, w["mode"])
+    # the same state advanced in regular (dense, every block) mode and in the workload's mode, both
+    # through the captured-graph path and timed with CUDA events, for the DBA-vs-dense comparison
+    def graph_ms(mode):
+        sim.load_state(blob)
+        sim.step(3, mode)
+        sim.load_state(blob)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        c0 = sim.cell_updates()
+        e0.record(stream)
+        sim.step(ncmp, mode)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / ncmp, (sim.cell_updates() - c0) / ncmp
+
+    ncmp = min(args.steps, 1000)
+    dense_ms, dense_cells = graph_ms(0)
+    dba_ms, _ = graph_ms(w["mode"])
 
     # end to end through the public API: host state in pinned memory -> device, K steps, fields -> host
     n = cfg.nx * cfg.ny * cfg.nz
@@ -264,16 +282,18 @@ def run_ours(args, w):
                          "frac_of_8tbs_spec": achieved / 8000.0},
             "step_breakdown_ms": {"stencil": prof["stencil_ms"] / nprof, "reduce": prof["reduce_ms"] / nprof,
                                   "correct": prof["correct_ms"] / nprof},
-            "vs_dense": {"dba_ms_per_step": dba_p["step_ms"] / nprof, "dense_ms_per_step": dense["step_ms"] / nprof,
-                         "dense_over_dba_time": dense["step_ms"] / dba_p["step_ms"] if dba_p["step_ms"] else None,
-                         "dense_cell_updates_per_s": dense["active_blocks"] * dense["cells_per_block"] /
-                         (dense["step_ms"] * 1e-3) if dense["step_ms"] else None},
+            "vs_dense": {"dba_ms_per_step": dba_ms, "dense_ms_per_step": dense_ms,
+                         "dense_over_dba_time": dense_ms / dba_ms if dba_ms else None,
+                         "dense_cell_updates_per_s": dense_cells / (dense_ms * 1e-3) if dense_ms else None,
+                         "steps": ncmp, "timing": "captured graphs, CUDA events, same starting state"},
             "gpu_launches": args.steps * launches_per_step(w),
             "clocks": clk.summary(),
             "status": status,
         }
         if world == 1 and not args.no_cpu_baseline:
             result["cpu_baseline"] = cpu_baseline(w, seconds=args.cpu_seconds)
+        if world == 1 and not args.no_sweep:
+            result["sweep"] = run_sweep(args)
     sim.close()
     if world > 1:
         dist.barrier()
@@ -334,6 +354,47 @@ def cpu_baseline(w, seconds=15.0):
             "sample": f"{what}: {w['nx']}x{w['ny']}x{w['nz']} grid, {n} steps (all cells updated), {t:.2f} s, 1 thread"}
 
 
+def run_sweep(args):
+    """Batched/served 2-D dendrite parameter sweep against sequential single-simulation runs.
+
+    Seeded requests (grid edge from {128, 256, 512, 1024}, undercooling and
+    anisotropy uniform, seed radius 8, FP32, each run until its tip reaches 80 %
+    of the domain half-width) arrive as a Poisson stream.  The server admits
+    them by device memory into one batch (one kernel launch per step over the
+    merged active blocks of every admitted run, captured in CUDA graphs), with
+    the block edge and threads per CTA picked by the autotuner.  The same
+    requests are then run one at a time, each in its own context.  Reported:
+    runs/s of both, p50/p99 time to completion of the served run, and how far
+    each served result is from its sequential twin."""
+    from dba_b200 import autotune, serve
+
+    choice = autotune.tune(precision=1, use_cache=False)
+    reqs = serve.sweep_requests(n=args.sweep_requests, rate=args.sweep_rate, seed=args.sweep_seed)
+    srv = serve.SweepServer(precision=1, block=choice["block"], threads=choice["threads"], chunk=choice["chunk"])
+    t0 = time.perf_counter()
+    res = srv.run(reqs)
+    t_batched = time.perf_counter() - t0
+    srv.close()
+    summ = serve.summarize(res)
+    t0 = time.perf_counter()
+    seq = serve.run_sequential(reqs, precision=1, block=choice["block"], chunk=choice["chunk"])
+    t_seq = time.perf_counter() - t0
+    by_id = {r["id"]: r for r in seq}
+    tip_rel = max(abs(r["tip"] - by_id[r["id"]]["tip"]) / max(abs(by_id[r["id"]]["tip"]), 1e-30) for r in res)
+    same_steps = sum(r["steps"] == by_id[r["id"]]["steps"] for r in res)
+    return {
+        "requests": len(reqs), "arrival_rate_per_s": args.sweep_rate, "seed": args.sweep_seed,
+        "autotune": {"block": choice["block"], "threads": choice["threads"], "chunk": choice["chunk"]},
+        "batched_runs_per_s": summ["runs_per_s"], "sequential_runs_per_s": len(seq) / t_seq,
+        "speedup": (summ["runs_per_s"] * t_seq / len(seq)) if summ["runs_per_s"] else None,
+        "p50_latency_s": summ.get("p50_latency_s"), "p99_latency_s": summ.get("p99_latency_s"),
+        "makespan_s": summ["makespan_s"], "sequential_wall_s": t_seq,
+        "completed": summ["completed"], "completed_sequential": int(sum(r["completed"] for r in seq)),
+        "max_tip_rel_diff_vs_sequential": tip_rel, "same_stop_step": same_steps,
+        "note": "makespan from first arrival to last completion; sequential runs back to back, FP32 both",
+    }
+
+
 def run_reference(args, w):
     world, rank, local = dist_setup()
     if rank != 0:
@@ -369,6 +430,10 @@ def main():
     ap.add_argument("--preroll", type=int, default=-1, help="untimed steps before warm-up (default: half the run)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the batched dendrite sweep section")
+    ap.add_argument("--sweep-requests", type=int, default=256)
+    ap.add_argument("--sweep-rate", type=float, default=200.0, help="Poisson arrival rate, requests per second")
+    ap.add_argument("--sweep-seed", type=int, default=0)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -133,8 +133,8 @@ cudaError_t enqueue(dba_batch* b, long s)
 {
     FlagP f = bflags(b, s);
     BatchP p = bparams(b);
-    return b->esz == 8 ? launch_batch_step<double>(b->cfg.block, b->grid, b->st, p, f)
-                       : launch_batch_step<float>(b->cfg.block, b->grid, b->st, p, f);
+    return b->esz == 8 ? launch_batch_step<double>(b->cfg.block, b->cfg.threads, b->grid, b->st, p, f)
+                       : launch_batch_step<float>(b->cfg.block, b->cfg.threads, b->grid, b->st, p, f);
 }
 
 }  // namespace
@@ -148,9 +148,11 @@ int dba_batch_create(const dba_batch_config* cfg, dba_batch** out)
     if (cfg->block != 4 && cfg->block != 8 && cfg->block != 16) return DBA_ERR_CONFIG;
     if (cfg->precision != DBA_PREC_F32 && cfg->precision != DBA_PREC_F64) return DBA_ERR_CONFIG;
     if (cfg->max_slots < 1 || cfg->block_capacity < 1) return DBA_ERR_CONFIG;
+    if (cfg->threads != 0 && cfg->threads != 128 && cfg->threads != 256 && cfg->threads != 512) return DBA_ERR_CONFIG;
     dba_batch* b = new (std::nothrow) dba_batch();
     if (!b) return DBA_ERR_NOMEM;
     b->cfg = *cfg;
+    if (b->cfg.threads == 0) b->cfg.threads = 256;
     b->esz = cfg->precision == DBA_PREC_F64 ? 8 : 4;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -191,7 +193,8 @@ int dba_batch_create(const dba_batch_config* cfg, dba_batch** out)
     }
     b->cells.init(cells);
     b->blocks.init(NB);
-    b->grid = b->esz == 8 ? batch_grid<double>(cfg->block, b->sms) : batch_grid<float>(cfg->block, b->sms);
+    b->grid = b->esz == 8 ? batch_grid<double>(b->cfg.block, b->cfg.threads, b->sms)
+                          : batch_grid<float>(b->cfg.block, b->cfg.threads, b->sms);
     *out = b;
     return DBA_OK;
 }

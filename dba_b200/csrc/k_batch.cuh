@@ -31,10 +31,9 @@ struct BatchP {
     int nbtot;             // size of the global block space
 };
 
-template <typename R, int B, bool DBA>
-__global__ void __launch_bounds__(kThreads) batch_dendrite_step(BatchP bp, FlagP f)
+template <typename R, int B, int NT, bool DBA>
+__global__ void __launch_bounds__(NT) batch_dendrite_step(BatchP bp, FlagP f)
 {
-    constexpr int NT = kThreads;
     constexpr int V = B * B;
     constexpr int E = B + 2;
     constexpr int TV = E * E;

@@ -201,23 +201,38 @@ cudaError_t launch_kh_prim_blocks(cudaStream_t st, const GridP& g, int B, const 
     return cudaGetLastError();
 }
 
-template <typename R>
-int batch_grid(int B, int sms)
+template <typename R, int NT>
+static const void* batch_kernel(int B)
 {
-    const void* k = B == 4 ? (const void*)batch_dendrite_step<R, 4, true>
-                  : B == 8 ? (const void*)batch_dendrite_step<R, 8, true> : (const void*)batch_dendrite_step<R, 16, true>;
-    return grid_of<R>(k, 0, sms);
+    return B == 4 ? (const void*)batch_dendrite_step<R, 4, NT, true>
+         : B == 8 ? (const void*)batch_dendrite_step<R, 8, NT, true> : (const void*)batch_dendrite_step<R, 16, NT, true>;
 }
 
 template <typename R>
-cudaError_t launch_batch_step(int B, int grid, cudaStream_t st, const BatchP& p, const FlagP& f)
+int batch_grid(int B, int threads, int sms)
 {
-    switch (B) {
-    case 4: batch_dendrite_step<R, 4, true><<<grid, kThreads, 0, st>>>(p, f); break;
-    case 8: batch_dendrite_step<R, 8, true><<<grid, kThreads, 0, st>>>(p, f); break;
-    case 16: batch_dendrite_step<R, 16, true><<<grid, kThreads, 0, st>>>(p, f); break;
-    default: return cudaErrorInvalidValue;
-    }
+    const void* k = threads == 128 ? batch_kernel<R, 128>(B) : (threads == 512 ? batch_kernel<R, 512>(B) : batch_kernel<R, 256>(B));
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, 0) != cudaSuccess || occ < 1) occ = 1;
+    return occ * sms;
+}
+
+template <typename R, int NT>
+static void batch_launch_nt(int B, int grid, cudaStream_t st, const BatchP& p, const FlagP& f)
+{
+    if (B == 4) batch_dendrite_step<R, 4, NT, true><<<grid, NT, 0, st>>>(p, f);
+    else if (B == 8) batch_dendrite_step<R, 8, NT, true><<<grid, NT, 0, st>>>(p, f);
+    else batch_dendrite_step<R, 16, NT, true><<<grid, NT, 0, st>>>(p, f);
+}
+
+template <typename R>
+cudaError_t launch_batch_step(int B, int threads, int grid, cudaStream_t st, const BatchP& p, const FlagP& f)
+{
+    if (B != 4 && B != 8 && B != 16) return cudaErrorInvalidValue;
+    if (threads == 128) batch_launch_nt<R, 128>(B, grid, st, p, f);
+    else if (threads == 256) batch_launch_nt<R, 256>(B, grid, st, p, f);
+    else if (threads == 512) batch_launch_nt<R, 512>(B, grid, st, p, f);
+    else return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 
@@ -228,8 +243,8 @@ cudaError_t launch_batch_tips(cudaStream_t st, const BatchP& p, const uint8_t* p
     return cudaGetLastError();
 }
 
-template int batch_grid<REAL_T>(int, int);
-template cudaError_t launch_batch_step<REAL_T>(int, int, cudaStream_t, const BatchP&, const FlagP&);
+template int batch_grid<REAL_T>(int, int, int);
+template cudaError_t launch_batch_step<REAL_T>(int, int, int, cudaStream_t, const BatchP&, const FlagP&);
 template cudaError_t launch_batch_tips<REAL_T>(cudaStream_t, const BatchP&, const uint8_t*, int, double*);
 template bool shape_supported<REAL_T>(int, int, int);
 template int step_grid<REAL_T>(int, int, int, int);

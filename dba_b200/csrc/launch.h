@@ -50,9 +50,9 @@ template <typename R>
 cudaError_t launch_kh_prim_blocks(cudaStream_t st, const GridP& g, int B, const KHP<R>& P, const uint8_t* only);
 
 // batched dendrite (k_batch.cuh)
-template <typename R> int batch_grid(int B, int sms);
+template <typename R> int batch_grid(int B, int threads, int sms);
 template <typename R>
-cudaError_t launch_batch_step(int B, int grid, cudaStream_t st, const BatchP& p, const FlagP& f);
+cudaError_t launch_batch_step(int B, int threads, int grid, cudaStream_t st, const BatchP& p, const FlagP& f);
 template <typename R>
 cudaError_t launch_batch_tips(cudaStream_t st, const BatchP& p, const uint8_t* par_cur, int nslots, double* tips);
 

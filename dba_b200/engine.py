@@ -70,7 +70,7 @@ class Prof(ctypes.Structure):
 
 class BatchConfig(ctypes.Structure):
     _fields_ = [("precision", _i), ("block", _i), ("max_slots", _i), ("block_capacity", _i),
-                ("cell_capacity", ctypes.c_size_t)]
+                ("cell_capacity", ctypes.c_size_t), ("threads", _i)]
 
 
 class BatchInfo(ctypes.Structure):
@@ -296,9 +296,9 @@ class Batch:
     (include/dba.h, dba_batch_*).  Slots are admitted while the batch's device
     arena and block space have room and retired when done."""
 
-    def __init__(self, precision=1, block=8, max_slots=64, block_capacity=1 << 16, cell_capacity=0):
+    def __init__(self, precision=1, block=8, max_slots=64, block_capacity=1 << 16, cell_capacity=0, threads=256):
         self._L = _lib()
-        self.cfg = BatchConfig(precision, block, max_slots, block_capacity, cell_capacity)
+        self.cfg = BatchConfig(precision, block, max_slots, block_capacity, cell_capacity, threads)
         self._h = ctypes.c_void_p()
         _check(self._L.dba_batch_create(ctypes.byref(self.cfg), ctypes.byref(self._h)), "dba_batch_create")
         self.max_slots = max_slots

@@ -66,9 +66,9 @@ def _done(tip, edge, target):
 
 class SweepServer:
     def __init__(self, precision=1, block=8, max_slots=128, block_capacity=1 << 17, cell_capacity=0, chunk=96,
-                 target=0.8, max_steps=200000):
+                 target=0.8, max_steps=200000, threads=256):
         self.batch = engine.Batch(precision=precision, block=block, max_slots=max_slots,
-                                  block_capacity=block_capacity, cell_capacity=cell_capacity)
+                                  block_capacity=block_capacity, cell_capacity=cell_capacity, threads=threads)
         self.precision, self.block, self.chunk = precision, block, chunk
         self.target, self.max_steps = target, max_steps
 

@@ -239,6 +239,7 @@ typedef struct dba_batch_config {
     int max_slots;             /* simulations held at once */
     int block_capacity;        /* total DBA blocks over all slots */
     size_t cell_capacity;      /* total cells over all slots; 0 = size from free device memory */
+    int threads;               /* threads per CTA of the batch kernel: 128, 256 or 512 (0 = 256) */
 } dba_batch_config;
 
 typedef struct dba_batch_info {

@@ -88,3 +88,24 @@ def test_server_completes_sweep_and_matches_single_runs():
         assert abs(s["tip"] - r["tip"]) <= 0.01 * abs(s["tip"])
     summ = serve.summarize(res)
     assert summ["p99_latency_s"] >= summ["p50_latency_s"] > 0
+
+
+def test_sweep_fp32_error_vs_fp64():
+    """A sweep run in FP32 against the same run in FP64 (FP64 slots are bit-exact with
+    the CPU restatement): tip velocity within 1 %, relative L2 of p and T <= 1e-4."""
+    req = _req(128, 0.45, 0.04)
+    out = {}
+    for prec in (1, 0):
+        b = dba_b200.Batch(precision=prec, block=8, max_slots=2, block_capacity=1 << 12, cell_capacity=1 << 16)
+        s = b.add(serve.request_config(req, precision=prec))
+        b.step(480)
+        t1, _ = b.tips()
+        b.step(480)
+        t2, steps = b.tips()
+        out[prec] = dict(v=(t2[s] - t1[s]) / 480.0, tip=t2[s], p=b.field(s, "p"), T=b.field(s, "T"))
+        b.close()
+    f32, f64 = out[1], out[0]
+    assert f64["tip"] >= 0.6 * 64                                     # the tip has crossed most of the half-width
+    assert abs(f32["v"] - f64["v"]) <= 0.01 * abs(f64["v"])
+    for k in ("p", "T"):
+        assert np.linalg.norm(f32[k] - f64[k]) / np.linalg.norm(f64[k]) <= 1e-4, k
