@@ -729,14 +729,17 @@ int dba_tip(dba_ctx* c, double* tip)
     if (!c->initialized) return DBA_ERR_STATE;
     const dba_config& k = c->cfg;
     std::vector<double> col(k.ny);
-    size_t start = (size_t)(k.nx / 2) + (size_t)k.nx * (size_t)k.ny * (size_t)(k.nz / 2);
+    // growth_front (example_Dendritic_growth/kernel.cu:759-773): along +y from the seed centre,
+    // (Nx/2, Ny/2, Nz/2), or from cell (0, 0, 0) for a corner seed
+    const int ox = k.ic_corner ? 0 : k.nx / 2, oy = k.ic_corner ? 0 : k.ny / 2, oz = k.ic_corner ? 0 : k.nz / 2;
+    size_t start = (size_t)ox + (size_t)k.nx * (size_t)k.ny * (size_t)oz;
     int st = gather(c, c->state[0][0], c->state[0][1], cur_par(c), start, (size_t)k.nx, (size_t)k.ny, col.data());
     if (st) return st;
-    // growth_front (example_Dendritic_growth/kernel.cu:759-773)
     *tip = NAN;
-    for (int y = k.ny / 2; y < k.ny; ++y)
+    for (int y = oy > 0 ? oy : 1; y < k.ny; ++y)
         if (col[y] < 0.5) {
-            *tip = (col[y - 1] - 0.5) / (col[y - 1] - col[y]) + y - 1 - k.ny / 2;
+            // corner seed: no crossing when the corner cell itself is liquid
+            if (!k.ic_corner || col[y - 1] >= 0.5) *tip = (col[y - 1] - 0.5) / (col[y - 1] - col[y]) + y - 1 - oy;
             break;
         }
     return DBA_OK;
