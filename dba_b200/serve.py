@@ -149,3 +149,26 @@ def summarize(results, makespan=None):
         out["p50_latency_s"] = float(np.percentile(lat, 50))
         out["p99_latency_s"] = float(np.percentile(lat, 99))
     return out
+
+
+def main(argv=None):
+    """python -m dba_b200.serve: run one seeded sweep through the server and print its summary."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=200.0, help="Poisson arrivals per second (0: all at once)")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--precision", type=int, default=1, help="1 FP32, 0 FP64")
+    ap.add_argument("--block", type=int, default=8)
+    ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--chunk", type=int, default=96)
+    a = ap.parse_args(argv)
+    srv = SweepServer(precision=a.precision, block=a.block, threads=a.threads, chunk=a.chunk)
+    res = srv.run(sweep_requests(n=a.requests, rate=a.rate, seed=a.seed))
+    srv.close()
+    print(json.dumps(summarize(res)))
+
+
+if __name__ == "__main__":
+    main()
