@@ -319,8 +319,8 @@ def run_ours(args, w):
 
 
 def launches_per_step(w):
-    if w["model"] == "kh":
-        return 5 + (2 if w["conserved"] else 0)
+    if w["model"] == "kh":   # one tile kernel per step (grids of 16-cell multiples, blocks 8 or 16)
+        return 1 + (2 if w["conserved"] else 0)
     if w["model"] == "modelb" and w["conserved"] and not (w["precision"] == 1 and w["nz"] == 1):
         return 3   # FP64 / 3-D conserved: step, reduce, correct
     return 1       # FP32 2-D conserved Model B: the reduction is inside the step kernel

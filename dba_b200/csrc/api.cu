@@ -58,6 +58,7 @@ struct dba_ctx {
     // FP32 2-D Model B conserved: lazy correction state (k_modelb_fast.cuh)
     bool lazy = false;
     bool tiles = false;               // FP32 2-D Model B on 32x32-cell tiles (k_modelb_tile.cuh)
+    bool kh_tiles = false;            // KH one-kernel step on 16x16-cell tiles (k_kh_tile.cuh)
     long long* lz = nullptr;          // tot[2][3] then chg[3][3]: rotating fixed-point totals (LazyP)
     cudaGraphExec_t graphs[6][2] = {};
     bool use_graphs = true;
@@ -178,6 +179,28 @@ KHP<R> kh_params(dba_ctx* c, bool dba_mode)
     P.conserved = (k.conserved && dba_mode) ? 1 : 0;
     P.list = c->list;
     P.count = c->count;
+    for (int q = 0; q < 4; ++q) P.U1[q] = (R*)c->state[q][c->kh_tiles ? 1 : 0];
+    P.upar = c->kh_tiles ? cur_par(c) : nullptr;
+    return P;
+}
+
+template <typename R>
+KHTileP<R> kh_tile_params(dba_ctx* c, bool dba_mode)
+{
+    const dba_config& k = c->cfg;
+    KHTileP<R> P;
+    for (int q = 0; q < 4; ++q) {
+        P.U[q][0] = (R*)c->state[q][0];
+        P.U[q][1] = (R*)c->state[q][1];
+        P.W[q] = (R*)c->aux[q];
+        P.Wp[q] = (R*)c->aux[12 + q];
+    }
+    for (int q = 0; q < 8; ++q) {
+        P.Gd[q] = (R*)c->aux[4 + q];
+        P.Fl[q] = (R*)c->aux[16 + q];
+    }
+    P.dt = k.dt; P.dx = k.dx; P.dy = k.dy; P.vol = k.dx * k.dy; P.gamma = k.kh_gamma; P.thr = k.metric_eps;
+    P.conserved = (k.conserved && dba_mode) ? 1 : 0;
     return P;
 }
 
@@ -200,12 +223,13 @@ CorrP<R> corr_params(dba_ctx* c, long s)
     } else {
         for (int q = 0; q < 4; ++q) {
             P.f[q][0] = (R*)c->state[q][0];
-            P.f[q][1] = (R*)c->state[q][0];
+            P.f[q][1] = (R*)c->state[q][c->kh_tiles ? 1 : 0];
         }
         // sums are Mass, Energy, Momx, Momy; fields are Mass, Momx, Momy, Energy
         P.map[0] = 0; P.map[1] = 3; P.map[2] = 1; P.map[3] = 2;
         P.nq = 4;
-        P.par = nullptr;
+        // the tile kernel ping-pongs U per block (after step s); the stage kernels update in place
+        P.par = c->kh_tiles ? c->par + ((s + 1) % 2) * (size_t)c->nch * c->g.nb : nullptr;
     }
     return P;
 }
@@ -244,6 +268,12 @@ cudaError_t enqueue_step_t(dba_ctx* c, long s, bool dba_mode)
         break;
     }
     case DBA_MODEL_KH: {
+        if (c->kh_tiles) {
+            const KHTileP<R> T = kh_tile_params<R>(c, dba_mode);
+            e = launch_kh_tile<R>(c->B, dba_mode, c->grid, c->st, c->g, f, T);
+            if (e != cudaSuccess || !T.conserved) return e;
+            break;
+        }
         KHP<R> P = kh_params<R>(c, dba_mode);
         e = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
         if (e != cudaSuccess) return e;
@@ -500,7 +530,10 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
     const size_t fb = c->n * c->esz;
     const size_t nb = c->g.nb;
     if (cfg->model == DBA_MODEL_KH) {
+        c->kh_tiles = cfg->tiles && kh_tiles_ok(c->D, c->B, cfg->nx, cfg->ny);
         for (int q = 0; q < 4 && !err; ++q) c->state[q][0] = dev_alloc(c, fb, &err);
+        if (c->kh_tiles)
+            for (int q = 0; q < 4 && !err; ++q) c->state[q][1] = dev_alloc(c, fb, &err);
         for (int q = 0; q < 24 && !err; ++q) c->aux[q] = dev_alloc(c, fb, &err);
         if (!err) c->list = (int*)dev_alloc(c, nb * sizeof(int), &err);
         if (!err) c->count = (int*)dev_alloc(c, sizeof(int), &err);
@@ -528,6 +561,10 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
     }
     c->grid = c->esz == 8 ? step_grid<double>(cfg->model, c->D, c->B, c->sms) : step_grid<float>(cfg->model, c->D, c->B, c->sms);
     if (c->grid < 1) c->grid = c->sms;
+    if (c->kh_tiles) {
+        const int nt = (cfg->nx / 16) * (cfg->ny / 16);
+        c->grid = c->esz == 8 ? kh_tile_grid<double>(c->B, c->sms, nt) : kh_tile_grid<float>(c->B, c->sms, nt);
+    }
     if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->tiles && modelb_tiles_ok(c->D, c->B, cfg->nx, cfg->ny)) {
         c->tiles = true;
         c->grid = modelb_tile_grid(c->B, c->sms, (cfg->nx / 32) * (cfg->ny / 32));
@@ -695,7 +732,9 @@ int dba_read_field(dba_ctx* c, int field, double* host)
         return DBA_OK;
     }
     // KH
-    if (field < 4) return gather(c, c->state[field][0], c->state[field][0], nullptr, 0, 1, c->n, host);
+    if (field < 4)
+        return c->kh_tiles ? gather(c, c->state[field][0], c->state[field][1], cur_par(c), 0, 1, c->n, host)
+                           : gather(c, c->state[field][0], c->state[field][0], nullptr, 0, 1, c->n, host);
     // primitives as the reference's output path computes them: getPrimitive for the
     // blocks active in the next step (KH_DBA.cu:1518), stale values elsewhere
     {
@@ -870,7 +909,8 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
-                    if (r == cudaSuccess) r = launch_kh<double>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_params<double>(c, dba_mode));
+                    if (c->kh_tiles) r = launch_kh_tile<double>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_tile_params<double>(c, dba_mode));
+                    else if (r == cudaSuccess) r = launch_kh<double>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_params<double>(c, dba_mode));
                 }
             } else {
                 if (c->cfg.model == DBA_MODEL_DENDRITE) r = launch_dendrite<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<float>(c));
@@ -881,7 +921,8 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
-                    if (r == cudaSuccess) r = launch_kh<float>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_params<float>(c, dba_mode));
+                    if (c->kh_tiles) r = launch_kh_tile<float>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_tile_params<float>(c, dba_mode));
+                    else if (r == cudaSuccess) r = launch_kh<float>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_params<float>(c, dba_mode));
                 }
             }
         }

@@ -51,6 +51,9 @@ __device__ __forceinline__ int wrapc(int v, int n, int bc)
     return v;
 }
 
+// periodic wrap of an index at most one period outside [0, n)
+__device__ __forceinline__ int wrap_p(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
 // block neighbour for the wake-up scatter; -1 when it falls off a zero-flux edge
 __device__ __forceinline__ int block_nb(const GridP& g, int b, int dx, int dy, int dz)
 {

@@ -139,6 +139,42 @@ cudaError_t launch_kh(int B, bool dba_mode, int grid, cudaStream_t st, const Gri
     return cudaErrorInvalidValue;
 }
 
+template <typename R, int B>
+static int kh_tile_grid_b(int sms, int ntiles)
+{
+    const size_t sm = KHTile<R, B>::smem;
+    cudaFuncSetAttribute(kh_tile_step<R, B, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(kh_tile_step<R, B, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kh_tile_step<R, B, true>, KHTile<R, B>::NT, sm) != cudaSuccess ||
+        occ < 1)
+        occ = 1;
+    const int g = occ * sms;
+    return g < ntiles ? g : ntiles;
+}
+
+template <typename R>
+int kh_tile_grid(int B, int sms, int ntiles)
+{
+    return B == 8 ? kh_tile_grid_b<R, 8>(sms, ntiles) : kh_tile_grid_b<R, 16>(sms, ntiles);
+}
+
+template <typename R>
+cudaError_t launch_kh_tile(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
+                           const KHTileP<R>& P)
+{
+#define XT(b)                                                                                          \
+    if (B == b) {                                                                                      \
+        const size_t sm = KHTile<R, b>::smem;                                                          \
+        if (dba_mode) kh_tile_step<R, b, true><<<grid, KHTile<R, b>::NT, sm, st>>>(g, f, P);           \
+        else kh_tile_step<R, b, false><<<grid, KHTile<R, b>::NT, sm, st>>>(g, f, P);                   \
+        return cudaGetLastError();                                                                     \
+    }
+    XT(8) XT(16)
+#undef XT
+    return cudaErrorInvalidValue;
+}
+
 template <typename R>
 cudaError_t launch_correct(int grid, cudaStream_t st, const GridP& g, const CorrP<R>& P)
 {
@@ -178,12 +214,13 @@ __global__ void __launch_bounds__(kThreads) kh_prim_blocks(GridP g, int B, KHP<R
     const size_t n = (size_t)g.nx * g.ny;
     for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (size_t)gridDim.x * kThreads) {
         const int x = (int)(i % g.nx), y = (int)(i / g.nx);
-        if (only && !only[x / B + g.nbx * (y / B)]) continue;
+        const int ob = x / B + g.nbx * (y / B);
+        if (only && !only[ob]) continue;
         const R vol = (R)P.vol, gm1 = (R)(P.gamma - 1.0);
-        const R r = P.U[0][i] / vol;
-        const R u = P.U[1][i] / r / vol;
-        const R v = P.U[2][i] / r / vol;
-        const R pp = (P.U[3][i] / vol - (R)0.5 * r * (u * u + v * v)) * gm1;
+        const bool alt = P.upar && P.upar[ob];
+        R r, pp, u, v;
+        kh_prim_of<R>((alt ? P.U1 : P.U)[0][i], (alt ? P.U1 : P.U)[1][i], (alt ? P.U1 : P.U)[2][i],
+                      (alt ? P.U1 : P.U)[3][i], vol, gm1, r, pp, u, v);
         P.W[0][i] = r;
         P.W[1][i] = pp;
         P.W[2][i] = u;
@@ -253,6 +290,8 @@ template cudaError_t launch_modelb<REAL_T>(int, int, bool, int, cudaStream_t, co
 template bool modelb_uses_fast<REAL_T>(int, int);
 template cudaError_t launch_kh<REAL_T>(int, bool, int, cudaStream_t, const GridP&, const FlagP&, const KHP<REAL_T>&);
 template cudaError_t launch_correct<REAL_T>(int, cudaStream_t, const GridP&, const CorrP<REAL_T>&);
+template int kh_tile_grid<REAL_T>(int, int, int);
+template cudaError_t launch_kh_tile<REAL_T>(int, bool, int, cudaStream_t, const GridP&, const FlagP&, const KHTileP<REAL_T>&);
 template cudaError_t launch_gather<REAL_T>(cudaStream_t, const GridP&, int, int, const REAL_T*, const REAL_T*,
                                            const uint8_t*, size_t, size_t, size_t, double*);
 template cudaError_t launch_kh_prim_blocks<REAL_T>(cudaStream_t, const GridP&, int, const KHP<REAL_T>&, const uint8_t*);

@@ -30,7 +30,84 @@ struct KHP {
     int conserved;
     int* list;        // compacted active blocks of this step
     int* count;       // number of entries in list
+    R* U1[4];         // second buffers of U when the fused kernel ping-pongs them (== U otherwise)
+    const uint8_t* upar;  // per-block buffer of U (null: U updated in place)
 };
+
+// ---- KH point formulas.  Every operation is an explicit intrinsic in the
+// reference's evaluation order, so the stage kernels below and the fused kernel
+// (k_kh_tile.cuh) give the same bits in each precision (in FP64 they equal the
+// plain operators of the -fmad=false build). ----
+__device__ __forceinline__ float ka(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double ka(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float ks(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double ks(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float km(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double km(double a, double b) { return __dmul_rn(a, b); }
+// FP32 (the throughput precision) divides and takes square roots with the PTX
+// approximations (div.approx: a times the approximate reciprocal of b, <= 2 ulp;
+// sqrt.approx, <= 1 ulp-ish), which are a few instructions instead of an
+// IEEE-rounded sequence; FP64 keeps IEEE rounding (bit-exact with the CPU restatement).
+__device__ __forceinline__ float kd(float a, float b)
+{
+    float r;
+    asm("div.approx.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ double kd(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float kq(float a)
+{
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
+__device__ __forceinline__ double kq(double a) { return __dsqrt_rn(a); }
+
+// getPrimitive (KH_DBA.cu:461-475): rho, p, vx, vy from Mass, Momx, Momy, Energy
+template <typename R>
+__device__ __forceinline__ void kh_prim_of(R U0, R U1, R U2, R U3, R vol, R gm1, R& r, R& p, R& u, R& v)
+{
+    r = kd(U0, vol);
+    u = kd(kd(U1, r), vol);
+    v = kd(kd(U2, r), vol);
+    p = km(ks(kd(U3, vol), km(km((R)0.5, r), ka(km(u, u), km(v, v)))), gm1);
+}
+
+// central gradient (Grad_x / Grad_y, KH_DBA.cu:249-275)
+template <typename R>
+__device__ __forceinline__ R kh_grad(R wp, R wm, R h) { return kd(kd(ks(wp, wm), (R)2.0), h); }
+
+// half-step states (extrap_in_time, KH_DBA.cu:524-531); gr = rho_dx rho_dy p_dx p_dy vx_dx vx_dy vy_dx vy_dy
+template <typename R>
+__device__ __forceinline__ void kh_prime_of(R r, R pp, R u, R v, const R* gr, R hdt, R gam, R& rp, R& ppp, R& up, R& vp)
+{
+    rp = ks(r, km(hdt, ka(ka(ka(km(u, gr[0]), km(r, gr[4])), km(v, gr[1])), km(r, gr[7]))));
+    up = ks(u, km(hdt, ka(ka(km(u, gr[4]), km(v, gr[5])), km(kd((R)1.0, r), gr[2]))));
+    vp = ks(v, km(hdt, ka(ka(km(u, gr[6]), km(v, gr[7])), km(kd((R)1.0, r), gr[3]))));
+    ppp = ks(pp, km(hdt, ka(ka(km(km(gam, pp), ka(gr[4], gr[7])), km(u, gr[2])), km(v, gr[3]))));
+}
+
+// wake-up metric (KH_DBA.cu:614-617): sum of |gradients| in order
+template <typename R>
+__device__ __forceinline__ R kh_metric(const R* gr)
+{
+    R m = fabs(gr[0]);
+#pragma unroll
+    for (int q = 1; q < 8; ++q) m = ka(m, fabs(gr[q]));
+    return m;
+}
+
+// face state extrapolated from a cell (extrapolateInSpaceToFace, KH_DBA.cu:630-660):
+// towards the -side face w - g h / 2, towards the +side face w + g h / 2
+template <typename R> __device__ __forceinline__ R kh_face_m(R w, R g, R h) { return ks(w, kd(km(g, h), (R)2.0)); }
+template <typename R> __device__ __forceinline__ R kh_face_p(R w, R g, R h) { return ka(w, kd(km(g, h), (R)2.0)); }
+
+// conserved-field change of one cell (applyFluxes, KH_DBA.cu:818-841)
+template <typename R>
+__device__ __forceinline__ R kh_change(R dtdx, R f_own, R f_xm, R g_own, R g_ym)
+{
+    return km(dtdx, ka(ks(ka(-f_own, f_xm), g_own), g_ym));
+}
 
 // --- scan: flag bookkeeping and the compacted active list -----------------
 template <bool DBA>
@@ -77,10 +154,8 @@ __global__ void __launch_bounds__(kThreads) kh_prim(GridP g, KHP<R> P)
         kh_cell(g, B, P.list[it / V], (int)(it % V), X, Y);
         const size_t i = (size_t)X + (size_t)g.nx * Y;
         const R vol = (R)P.vol, gm1 = (R)(P.gamma - 1.0);
-        const R r = P.U[0][i] / vol;
-        const R u = P.U[1][i] / r / vol;
-        const R v = P.U[2][i] / r / vol;
-        const R pp = (P.U[3][i] / vol - (R)0.5 * r * (u * u + v * v)) * gm1;
+        R r, pp, u, v;
+        kh_prim_of<R>(P.U[0][i], P.U[1][i], P.U[2][i], P.U[3][i], vol, gm1, r, pp, u, v);
         P.W[0][i] = r;
         P.W[1][i] = pp;
         P.W[2][i] = u;
@@ -115,19 +190,20 @@ __global__ void __launch_bounds__(kThreads) kh_extrap(GridP g, FlagP f, KHP<R> P
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const R* w = P.W[q == 0 ? 0 : (q == 1 ? 1 : (q == 2 ? 2 : 3))];
-                gr[2 * q] = (w[ixp] - w[ixm]) / (R)2.0 / dx;
-                gr[2 * q + 1] = (w[iyp] - w[iym]) / (R)2.0 / dy;
+                gr[2 * q] = kh_grad<R>(w[ixp], w[ixm], dx);
+                gr[2 * q + 1] = kh_grad<R>(w[iyp], w[iym], dy);
             }
             // gr: rho_dx rho_dy p_dx p_dy vx_dx vx_dy vy_dx vy_dy
 #pragma unroll
             for (int q = 0; q < 8; ++q) P.Gd[q][i] = gr[q];
             const R r = P.W[0][i], pp = P.W[1][i], u = P.W[2][i], v = P.W[3][i];
-            P.Wp[0][i] = r - hdt * (u * gr[0] + r * gr[4] + v * gr[1] + r * gr[7]);
-            P.Wp[2][i] = u - hdt * (u * gr[4] + v * gr[5] + ((R)1.0 / r) * gr[2]);
-            P.Wp[3][i] = v - hdt * (u * gr[6] + v * gr[7] + ((R)1.0 / r) * gr[3]);
-            P.Wp[1][i] = pp - hdt * (gam * pp * (gr[4] + gr[7]) + u * gr[2] + v * gr[3]);
-            const R metric = fabs(gr[0]) + fabs(gr[1]) + fabs(gr[2]) + fabs(gr[3]) + fabs(gr[4]) + fabs(gr[5]) +
-                             fabs(gr[6]) + fabs(gr[7]);
+            R rp, ppp, up, vp;
+            kh_prime_of<R>(r, pp, u, v, gr, hdt, gam, rp, ppp, up, vp);
+            P.Wp[0][i] = rp;
+            P.Wp[2][i] = up;
+            P.Wp[3][i] = vp;
+            P.Wp[1][i] = ppp;
+            const R metric = kh_metric<R>(gr);
             if (DBA && metric > (R)P.thr) s_nx[threadIdx.x / V] = 1;
         }
         __syncthreads();
@@ -146,24 +222,26 @@ template <typename R>
 __device__ __forceinline__ void kh_getflux(R gam, R rho_L, R rho_R, R p_L, R p_R, R vx_L, R vx_R, R vy_L, R vy_R,
                                            R& fM, R& fE, R& fX, R& fY)
 {
-    const R en_L = p_L / (gam - (R)1.0) + (R)0.5 * rho_L * (vx_L * vx_L + vy_L * vy_L);
-    const R en_R = p_R / (gam - (R)1.0) + (R)0.5 * rho_R * (vx_R * vx_R + vy_R * vy_R);
-    const R rho_star = (R)0.5 * (rho_L + rho_R);
-    const R momx_star = (R)0.5 * (rho_L * vx_L + rho_R * vx_R);
-    const R momy_star = (R)0.5 * (rho_L * vy_L + rho_R * vy_R);
-    const R en_star = (R)0.5 * (en_L + en_R);
-    const R p_star = (gam - (R)1.0) * (en_star - (R)0.5 * (momx_star * momx_star + momy_star * momy_star) / rho_star);
+    const R g1 = ks(gam, (R)1.0), h = (R)0.5;
+    const R en_L = ka(kd(p_L, g1), km(km(h, rho_L), ka(km(vx_L, vx_L), km(vy_L, vy_L))));
+    const R en_R = ka(kd(p_R, g1), km(km(h, rho_R), ka(km(vx_R, vx_R), km(vy_R, vy_R))));
+    const R rho_star = km(h, ka(rho_L, rho_R));
+    const R momx_star = km(h, ka(km(rho_L, vx_L), km(rho_R, vx_R)));
+    const R momy_star = km(h, ka(km(rho_L, vy_L), km(rho_R, vy_R)));
+    const R en_star = km(h, ka(en_L, en_R));
+    const R p_star = km(g1, ks(en_star, kd(km(h, ka(km(momx_star, momx_star), km(momy_star, momy_star))), rho_star)));
     const R fMv = momx_star;
-    const R fXv = momx_star * momx_star / rho_star + p_star;
-    const R fYv = momx_star * momy_star / rho_star;
-    const R fEv = (en_star + p_star) * momx_star / rho_star;
-    const R C_L = sqrt(gam * p_L / rho_L) + fabs(vx_L);
-    const R C_R = sqrt(gam * p_R / rho_R) + fabs(vx_R);
+    const R fXv = ka(kd(km(momx_star, momx_star), rho_star), p_star);
+    const R fYv = kd(km(momx_star, momy_star), rho_star);
+    const R fEv = kd(km(ka(en_star, p_star), momx_star), rho_star);
+    const R C_L = ka(kq(kd(km(gam, p_L), rho_L)), (R)fabs(vx_L));
+    const R C_R = ka(kq(kd(km(gam, p_R), rho_R)), (R)fabs(vx_R));
     const R C = (C_L >= C_R) ? C_L : C_R;
-    fM = fMv - C * (R)0.5 * (rho_L - rho_R);
-    fX = fXv - C * (R)0.5 * (rho_L * vx_L - rho_R * vx_R);
-    fY = fYv - C * (R)0.5 * (rho_L * vy_L - rho_R * vy_R);
-    fE = fEv - C * (R)0.5 * (en_L - en_R);
+    const R Ch = km(C, h);
+    fM = ks(fMv, km(Ch, ks(rho_L, rho_R)));
+    fX = ks(fXv, km(Ch, ks(km(rho_L, vx_L), km(rho_R, vx_R))));
+    fY = ks(fYv, km(Ch, ks(km(rho_L, vy_L), km(rho_R, vy_R))));
+    fE = ks(fEv, km(Ch, ks(en_L, en_R)));
 }
 
 // --- stage 3: face states and fluxes (:630-660, :792-810) -----------------
@@ -186,10 +264,10 @@ __global__ void __launch_bounds__(kThreads) kh_flux(GridP g, KHP<R> P)
             const R* w = P.Wp[wi[q]];
             const R* gx = P.Gd[2 * (q == 0 ? 0 : (q == 1 ? 2 : (q == 2 ? 3 : 1)))];
             const R* gy = P.Gd[2 * (q == 0 ? 0 : (q == 1 ? 2 : (q == 2 ? 3 : 1))) + 1];
-            fc[q][0] = w[ixp] - gx[ixp] * dx / (R)2.0;
-            fc[q][1] = w[i] + gx[i] * dx / (R)2.0;
-            fc[q][2] = w[iyp] - gy[iyp] * dy / (R)2.0;
-            fc[q][3] = w[i] + gy[i] * dy / (R)2.0;
+            fc[q][0] = kh_face_m<R>(w[ixp], gx[ixp], dx);
+            fc[q][1] = kh_face_p<R>(w[i], gx[i], dx);
+            fc[q][2] = kh_face_m<R>(w[iyp], gy[iyp], dy);
+            fc[q][3] = kh_face_p<R>(w[i], gy[i], dy);
         }
         const R gam = (R)P.gamma;
         R fM, fE, fX, fY;
@@ -228,8 +306,8 @@ __global__ void __launch_bounds__(kThreads) kh_apply(GridP g, FlagP f, KHP<R> P)
             for (int q = 0; q < 4; ++q) {
                 const R* Fx = P.Fl[fx[q]];
                 const R* Fy = P.Fl[fy[q]];
-                const R c = dtdx * ((R)-1.0 * Fx[i] + Fx[ixm] - (R)1.0 * Fy[i] + Fy[iym]);
-                const R un = P.U[q][i] + c;
+                const R c = kh_change<R>(dtdx, Fx[i], Fx[ixm], Fy[i], Fy[iym]);
+                const R un = ka(P.U[q][i], c);
                 P.U[q][i] = un;
                 if (!isfinite(un)) raise_status(f.status, 5);
                 ch[q] = (double)c;

@@ -58,7 +58,6 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-__device__ __forceinline__ int wrap_p(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
 template <int B, bool DBA>
 __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBFastP P, MBFastBuf Q, LazyP L)

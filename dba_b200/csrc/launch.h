@@ -8,6 +8,7 @@
 #include "k_common.cuh"
 #include "k_dendrite.cuh"
 #include "k_kh.cuh"
+#include "k_kh_tile.cuh"
 #include "k_modelb.cuh"
 #include "k_modelb_fast.cuh"
 #include "k_modelb_tile.cuh"
@@ -41,6 +42,15 @@ cudaError_t launch_gather_lazy(cudaStream_t st, const GridP& g, int B, const flo
 template <typename R>
 cudaError_t launch_kh(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f, const KHP<R>& P);
 template <typename R> cudaError_t launch_correct(int grid, cudaStream_t st, const GridP& g, const CorrP<R>& P);
+// one-kernel KH step on 16x16-cell tiles (k_kh_tile.cuh) when kh_tiles_ok
+inline bool kh_tiles_ok(int D, int B, int nx, int ny)
+{
+    return D == 2 && (B == 8 || B == 16) && nx % 16 == 0 && ny % 16 == 0;
+}
+template <typename R> int kh_tile_grid(int B, int sms, int ntiles);
+template <typename R>
+cudaError_t launch_kh_tile(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
+                           const KHTileP<R>& P);
 // out[k] = buf[par[owner(cell)]][start + k*stride] for k < count (par may be null -> buffer 0)
 template <typename R>
 cudaError_t launch_gather(cudaStream_t st, const GridP& g, int B, int D, const R* b0, const R* b1, const uint8_t* par,
