@@ -60,11 +60,12 @@ WORKLOADS = {
         model="dendrite", nx=512, ny=512, nz=512, block=8, precision=1, conserved=0, mode=1, t_total=20000,
         params=dict(Delta=1.15, delta=0.2, metric_p=1e-3, metric_T=1e-5, ic=1, ic_radius=10.0, ic_width=2.0, bc=1,
                     ic_corner=1)),
-    # C2: KH 4096^2 FP32, 16x16 blocks, gamma 1.4, sharp bands + seeded noise
+    # C2: KH 4096^2 FP32, 16x16 blocks, gamma 1.4, sharp bands + seeded noise, CFL 0.4 chosen on the device
+    # (t = 2 is ~49 000 steps at the layer's ~2.4 maximum signal speed)
     "kh_4096_fp32": dict(
-        model="kh", nx=4096, ny=4096, nz=1, block=16, precision=1, conserved=0, mode=1, t_total=50000,
+        model="kh", nx=4096, ny=4096, nz=1, block=16, precision=1, conserved=0, mode=1, t_total=49000,
         params=dict(dt=1.0 / 4096 * 0.4 / 3.0, dx=1.0 / 4096, dy=1.0 / 4096, kh_gamma=1.4, metric_eps=1.0, ic=2,
-                    noise_amp=1e-4)),
+                    noise_amp=1e-4, cfl=0.4)),
 }
 
 

@@ -3,6 +3,7 @@
 // observables and checkpoints.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -59,6 +60,9 @@ struct dba_ctx {
     bool lazy = false;
     bool tiles = false;               // FP32 2-D Model B on 32x32-cell tiles (k_modelb_tile.cuh)
     bool kh_tiles = false;            // KH one-kernel step on 16x16-cell tiles (k_kh_tile.cuh)
+    float* kvmax = nullptr;           // KH tiles: per-block largest signal speed (CFL)
+    unsigned* kgmax = nullptr;        // KH tiles: rotating maxima of the CFL speed, float bits [3]
+    double* ktime = nullptr;          // KH tiles: simulated time accumulated on the device (CFL)
     long long* lz = nullptr;          // tot[2][3] then chg[3][3]: rotating fixed-point totals (LazyP)
     cudaGraphExec_t graphs[6][2] = {};
     bool use_graphs = true;
@@ -118,6 +122,10 @@ FlagP flags_for(dba_ctx* c, long s)
 }
 
 // current-buffer parity / next-step wake flags after `step` completed steps
+// the time step the host adds to its clock; with a device-chosen (CFL) step the
+// device keeps the clock
+double host_dt(const dba_ctx* c) { return c->cfg.cfl > 0 ? 0.0 : c->cfg.dt; }
+
 const uint8_t* cur_par(dba_ctx* c) { return c->par + ((c->step + 1) % 2) * (size_t)c->nch * c->g.nb; }
 const uint8_t* next_wake(dba_ctx* c) { return c->wake + ((c->step + 1) % 3) * (size_t)c->nch * c->g.nb; }
 
@@ -185,7 +193,7 @@ KHP<R> kh_params(dba_ctx* c, bool dba_mode)
 }
 
 template <typename R>
-KHTileP<R> kh_tile_params(dba_ctx* c, bool dba_mode)
+KHTileP<R> kh_tile_params(dba_ctx* c, bool dba_mode, long s)
 {
     const dba_config& k = c->cfg;
     KHTileP<R> P;
@@ -201,6 +209,13 @@ KHTileP<R> kh_tile_params(dba_ctx* c, bool dba_mode)
     }
     P.dt = k.dt; P.dx = k.dx; P.dy = k.dy; P.vol = k.dx * k.dy; P.gamma = k.kh_gamma; P.thr = k.metric_eps;
     P.conserved = (k.conserved && dba_mode) ? 1 : 0;
+    P.cfl = k.cfl;
+    P.hmin = k.dx < k.dy ? k.dx : k.dy;
+    P.vmax = c->kvmax;
+    P.gmax_prev = c->kgmax + (s + 2) % 3;
+    P.gmax_cur = c->kgmax + s % 3;
+    P.gmax_clear = c->kgmax + (s + 1) % 3;
+    P.time = c->ktime;
     return P;
 }
 
@@ -269,7 +284,7 @@ cudaError_t enqueue_step_t(dba_ctx* c, long s, bool dba_mode)
     }
     case DBA_MODEL_KH: {
         if (c->kh_tiles) {
-            const KHTileP<R> T = kh_tile_params<R>(c, dba_mode);
+            const KHTileP<R> T = kh_tile_params<R>(c, dba_mode, s);
             e = launch_kh_tile<R>(c->B, dba_mode, c->grid, c->st, c->g, f, T);
             if (e != cudaSuccess || !T.conserved) return e;
             break;
@@ -306,6 +321,8 @@ int validate(const dba_config* k)
     if (k->nx < 4 || k->ny < 4 || (k->nz > 1 && k->nz < 4)) return DBA_ERR_CONFIG;
     if (k->model == DBA_MODEL_KH && k->nz != 1) return DBA_ERR_CONFIG;
     if (k->model != DBA_MODEL_DENDRITE && k->bc != DBA_BC_PERIODIC) return DBA_ERR_CONFIG;
+    if (k->cfl < 0 || (k->cfl > 0 && !(k->model == DBA_MODEL_KH && k->tiles && kh_tiles_ok(k->nz == 1 ? 2 : 3, B, k->nx, k->ny))))
+        return DBA_ERR_CONFIG;   // the CFL step lives in the KH tile kernel
     if (k->precision != DBA_PREC_F64 && k->precision != DBA_PREC_F32) return DBA_ERR_CONFIG;
     if (k->dt <= 0 || k->dx <= 0) return DBA_ERR_CONFIG;
     size_t nb = (size_t)(k->nx / B) * (k->ny / B) * (k->nz == 1 ? 1 : k->nz / B);
@@ -532,8 +549,12 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
     if (cfg->model == DBA_MODEL_KH) {
         c->kh_tiles = cfg->tiles && kh_tiles_ok(c->D, c->B, cfg->nx, cfg->ny);
         for (int q = 0; q < 4 && !err; ++q) c->state[q][0] = dev_alloc(c, fb, &err);
-        if (c->kh_tiles)
+        if (c->kh_tiles) {
             for (int q = 0; q < 4 && !err; ++q) c->state[q][1] = dev_alloc(c, fb, &err);
+            if (!err) c->kvmax = (float*)dev_alloc(c, nb * sizeof(float), &err);
+            if (!err) c->kgmax = (unsigned*)dev_alloc(c, 3 * sizeof(unsigned), &err);
+            if (!err) c->ktime = (double*)dev_alloc(c, sizeof(double), &err);
+        }
         for (int q = 0; q < 24 && !err; ++q) c->aux[q] = dev_alloc(c, fb, &err);
         if (!err) c->list = (int*)dev_alloc(c, nb * sizeof(int), &err);
         if (!err) c->count = (int*)dev_alloc(c, sizeof(int), &err);
@@ -629,6 +650,24 @@ int dba_init(dba_ctx* c, const double* ic)
         }
         for (int q = 0; q < 4 && !st; ++q) st = upload_any(c, c->state[q][0], U.data() + q * n, n);
         for (int q = 0; q < 4 && !st; ++q) st = upload_any(c, c->aux[q], src + q * n, n);   // initial primitives
+        if (!st && c->kh_tiles) {
+            // CFL state: every block's largest signal speed c + |v| of the initial state; the
+            // maximum goes to the slot the first step reads
+            std::vector<float> vb(c->g.nb, 0.f);
+            float vmax = 0.f;
+            for (int Y = 0; Y < k.ny; ++Y)
+                for (int X = 0; X < k.nx; ++X) {
+                    const size_t i = (size_t)X + (size_t)k.nx * Y;
+                    const double sp = std::sqrt(gamma * p[i] / rho[i]) + std::sqrt(vx[i] * vx[i] + vy[i] * vy[i]);
+                    float& b = vb[X / c->B + c->g.nbx * (Y / c->B)];
+                    b = std::max(b, (float)sp);
+                    vmax = std::max(vmax, (float)sp);
+                }
+            unsigned bits = 0;
+            std::memcpy(&bits, &vmax, sizeof bits);
+            st = cuda_status(cudaMemcpy(c->kvmax, vb.data(), vb.size() * sizeof(float), cudaMemcpyHostToDevice));
+            if (!st) st = cuda_status(cudaMemcpy(c->kgmax + 0, &bits, sizeof bits, cudaMemcpyHostToDevice));   // step 1 reads slot 0
+        }
     } else {
         for (int q = 0; q < c->nstate && !st; ++q) st = upload_any(c, c->state[q][0], src + q * c->n, c->n);
     }
@@ -667,12 +706,12 @@ int dba_step(dba_ctx* c, int nsteps, int mode)
             DBA_TRY(cudaGraphLaunch(ge, c->st));
             c->step += kGraphSteps;
             nsteps -= kGraphSteps;
-            c->time += kGraphSteps * c->cfg.dt;
+            c->time += kGraphSteps * host_dt(c);
         } else {
             DBA_TRY(enqueue_step(c, c->step + 1, dba_mode));
             c->step += 1;
             nsteps -= 1;
-            c->time += c->cfg.dt;
+            c->time += host_dt(c);
         }
     }
     return DBA_OK;
@@ -791,6 +830,18 @@ int dba_observables(dba_ctx* c, dba_obs* o)
     std::memset(o, 0, sizeof *o);
     o->step = c->step;
     o->time = c->time;
+    o->dt = c->cfg.dt;
+    if (c->cfg.cfl > 0 && c->kh_tiles) {
+        // device clock, and the step the next launch takes: cfl * hmin / (maximum after the last step)
+        unsigned bits = 0;
+        DBA_TRY(cudaStreamSynchronize(c->st));
+        DBA_TRY(cudaMemcpy(&o->time, c->ktime, sizeof(double), cudaMemcpyDeviceToHost));
+        DBA_TRY(cudaMemcpy(&bits, c->kgmax + (c->step + 3) % 3, sizeof bits, cudaMemcpyDeviceToHost));
+        float m = 0.f;
+        std::memcpy(&m, &bits, sizeof m);
+        const double h = c->cfg.dx < c->cfg.dy ? c->cfg.dx : c->cfg.dy;
+        o->dt = c->cfg.cfl * h / (double)m;
+    }
     o->total_blocks = c->g.nb;
     o->tip = NAN;
     o->vy_mode = NAN;
@@ -909,7 +960,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
-                    if (c->kh_tiles) r = launch_kh_tile<double>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_tile_params<double>(c, dba_mode));
+                    if (c->kh_tiles) r = launch_kh_tile<double>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_tile_params<double>(c, dba_mode, s));
                     else if (r == cudaSuccess) r = launch_kh<double>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_params<double>(c, dba_mode));
                 }
             } else {
@@ -921,7 +972,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
-                    if (c->kh_tiles) r = launch_kh_tile<float>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_tile_params<float>(c, dba_mode));
+                    if (c->kh_tiles) r = launch_kh_tile<float>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_tile_params<float>(c, dba_mode, s));
                     else if (r == cudaSuccess) r = launch_kh<float>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_params<float>(c, dba_mode));
                 }
             }
@@ -935,7 +986,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
         if (r == cudaSuccess) r = cudaEventRecord(e[3], c->st);
         if (r != cudaSuccess) st = cuda_status(r);
         c->step += 1;
-        c->time += c->cfg.dt;
+        c->time += host_dt(c);
     }
     cudaEvent_t& last = ev[ev.size() - 1];
     if (!st) st = cuda_status(cudaEventRecord(last, c->st));

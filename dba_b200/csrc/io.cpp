@@ -30,6 +30,7 @@ void apply_option(dba_config* c, const std::string& key, const std::string& val)
     else if (key == "noise_amp") c->noise_amp = d();
     else if (key == "noise_amp_z") c->noise_amp_z = d();
     else if (key == "tiles") c->tiles = i();
+    else if (key == "cfl") c->cfl = d();
 }
 
 template <class T> void vtk_coords(std::ofstream& o, const char* axis, int n)

@@ -38,7 +38,26 @@ struct KHTileP {
     R* Fl[8];         // persisted fluxes (Mass_x Energy_x Momx_x Momy_x Mass_y Energy_y Momx_y Momy_y)
     double dt, dx, dy, vol, gamma, thr;
     int conserved;
+    // CFL time step (cfl > 0).  Each block's largest signal speed c + |v| of its
+    // current state is kept in vmax; every launch folds all blocks' values into
+    // its own slot of a 3-slot rotation of maxima (float bits, unsigned atomicMax,
+    // exact and order-independent), and step s takes dt = cfl * hmin / max of step
+    // s-1.  CTA 0 clears the slot the next launch fills and adds dt to the
+    // simulated time.
+    double cfl, hmin;
+    float* vmax;                  // [nb]
+    const unsigned* gmax_prev;    // maximum after the previous step (read)
+    unsigned* gmax_cur;           // this step's maximum (atomicMax)
+    unsigned* gmax_clear;         // the slot the next step fills
+    double* time;                 // simulated time
 };
+
+// largest signal speed of a cell: sound speed + flow speed
+template <typename R>
+__device__ __forceinline__ float kh_speed(R r, R p, R u, R v, R gam)
+{
+    return (float)ka(kq(kd(km(gam, p), r)), kq(ka(km(u, u), km(v, v))));
+}
 
 template <typename R, int B> struct KHTile {
     static constexpr int NT = 256;
@@ -77,13 +96,31 @@ __global__ void __launch_bounds__(256) kh_tile_step(GridP g, FlagP f, KHTileP<R>
     __shared__ int s_nx[NBT];
     __shared__ double s_run[4][NT / 32];
     __shared__ double s_bsum[4][NBT];
+    __shared__ unsigned s_vblk[NBT];            // this tile's blocks' largest speed (float bits)
+    __shared__ unsigned s_vcta;                 // this CTA's largest speed over its blocks
+    __shared__ double s_dt;
 
     const int tid = threadIdx.x;
     const int G = gridDim.x;
     const int ntx = g.nx / T, nty = g.ny / T, ntiles = ntx * nty;
     const size_t nx = (size_t)g.nx;
+    const bool cfl = P.cfl > 0.0;
+    if (tid == 0) {
+        double dt = P.dt;
+        if (cfl) {
+            dt = P.cfl * P.hmin / (double)__uint_as_float(*P.gmax_prev);
+            if (blockIdx.x == 0) {
+                *P.gmax_clear = 0u;
+                *P.time += dt;
+            }
+        }
+        s_dt = dt;
+        s_vcta = 0u;
+    }
+    __syncthreads();
+    const double dtc = s_dt;
     const R vol = (R)P.vol, gm1 = (R)(P.gamma - 1.0), gam = (R)P.gamma;
-    const R dx = (R)P.dx, dy = (R)P.dy, hdt = (R)(0.5 * P.dt), dtdx = (R)(P.dt * P.dx);
+    const R dx = (R)P.dx, dy = (R)P.dy, hdt = (R)(0.5 * dtc), dtdx = (R)(dtc * P.dx);
     // this thread's own cell in the update phase: cell v of tile block kb (the
     // layout block_tree_sums expects)
     const int ukb = tid / V, uv = tid % V;
@@ -106,6 +143,7 @@ __global__ void __launch_bounds__(256) kh_tile_step(GridP g, FlagP f, KHTileP<R>
                 f.par_nxt[b] = (uint8_t)(pp ^ act);
                 if (P.conserved && !act)
                     for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = 0.0;
+                if (cfl && !act) atomicMax(&s_vcta, __float_as_uint(P.vmax[b]));
             }
             count_stats(f.stats, act, valid);
             const unsigned ma = __ballot_sync(0xffffffffu, valid && act);
@@ -131,7 +169,10 @@ __global__ void __launch_bounds__(256) kh_tile_step(GridP g, FlagP f, KHTileP<R>
                 s_npar[tid] = f.par_cur[ob];
                 s_nact[tid] = DBA ? (f.wake_cur[ob] ? 1 : 0) : 1;
             }
-            if (tid < NBT) s_nx[tid] = 0;
+            if (tid < NBT) {
+                s_nx[tid] = 0;
+                s_vblk[tid] = 0u;
+            }
             __syncthreads();
 
             // 1. primitives on tile + 2
@@ -263,8 +304,14 @@ __global__ void __launch_bounds__(256) kh_tile_step(GridP g, FlagP f, KHTileP<R>
                     P.U[q][dst][gi] = un;
                     bad |= !isfinite(un);
                     ch[q] = (double)c;
+                    if (cfl) sU[q * T * T + ui] = un;   // own cell only: new state for the speed below
                 }
                 if (bad) raise_status(f.status, 5);
+                if (cfl) {
+                    R r, pp, u, v;
+                    kh_prim_of<R>(sU[ui], sU[T * T + ui], sU[2 * T * T + ui], sU[3 * T * T + ui], vol, gm1, r, pp, u, v);
+                    atomicMax(&s_vblk[ukb], __float_as_uint(kh_speed<R>(r, pp, u, v, gam)));
+                }
                 if (DBA && !s_nx[ukb]) {
                     const int si = (uy + 2) * P2 + ux + 2, pi = (uy + 1) * P1 + ux + 1;
 #pragma unroll
@@ -297,9 +344,14 @@ __global__ void __launch_bounds__(256) kh_tile_step(GridP g, FlagP f, KHTileP<R>
                 block_tree_sums<V, 1>(cy, s_run[3], s_bsum[3], 0);
                 __syncthreads();
             }
+            if (cfl) __syncthreads();
             if (tid < NBT && ((tm >> tid) & 1u)) {
                 const int bx = tbx * TB + tid % TB, by = tby * TB + tid / TB;
                 const int b = bx + g.nbx * by;
+                if (cfl) {
+                    P.vmax[b] = __uint_as_float(s_vblk[tid]);
+                    atomicMax(&s_vcta, s_vblk[tid]);
+                }
                 if (P.conserved)
                     for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = s_bsum[q][tid];
                 if (DBA) {
@@ -311,6 +363,7 @@ __global__ void __launch_bounds__(256) kh_tile_step(GridP g, FlagP f, KHTileP<R>
         }
         __syncthreads();                          // list reused by the next scan pass
     }
+    if (cfl && tid == 0) atomicMax(P.gmax_cur, s_vcta);
 }
 
 }  // namespace dba

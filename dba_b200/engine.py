@@ -44,7 +44,7 @@ class Config(ctypes.Structure):
         ("metric_eps", _d), ("kh_gamma", _d),
         ("block", _i), ("precision", _i), ("bc", _i), ("conserved", _i), ("ic", _i),
         ("seed", _u64), ("ic_radius", _d), ("ic_width", _d), ("ic_corner", _i),
-        ("noise_amp", _d), ("noise_amp_z", _d), ("tiles", _i),
+        ("noise_amp", _d), ("noise_amp_z", _d), ("tiles", _i), ("cfl", _d),
     ]
 
     def as_dict(self):
@@ -53,7 +53,7 @@ class Config(ctypes.Structure):
 
 class Obs(ctypes.Structure):
     _fields_ = [("step", ctypes.c_long), ("time", _d), ("active_blocks", _i * 2), ("total_blocks", _i),
-                ("tip", _d), ("integral", _d * 4), ("vy_mode", _d), ("cell_updates", ctypes.c_long)]
+                ("tip", _d), ("integral", _d * 4), ("vy_mode", _d), ("cell_updates", ctypes.c_long), ("dt", _d)]
 
 
 class Info(ctypes.Structure):
@@ -234,7 +234,8 @@ class Simulation:
         o = Obs()
         _check(self._L.dba_observables(self._h, ctypes.byref(o)), "dba_observables")
         return {"step": o.step, "time": o.time, "active_blocks": list(o.active_blocks), "total_blocks": o.total_blocks,
-                "tip": o.tip, "integral": list(o.integral), "vy_mode": o.vy_mode, "cell_updates": o.cell_updates}
+                "tip": o.tip, "integral": list(o.integral), "vy_mode": o.vy_mode, "cell_updates": o.cell_updates,
+                "dt": o.dt}
 
     def step_profiled(self, n, mode=1):
         p = Prof()

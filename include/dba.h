@@ -82,8 +82,11 @@ typedef struct dba_config {
     double ic_radius, ic_width;/* dendrite tanh seed */
     int ic_corner;             /* dendrite tanh seed at cell (0,0,0) instead of the centre */
     double noise_amp, noise_amp_z; /* Model B: x,y and z uniform-noise amplitudes (0.05, 0.001) */
-    int tiles;                 /* FP32 2-D Model B: 1 (default) = 32x32-cell tile kernel when nx, ny are multiples
-                                  of 32 and block is 8 or 16; 0 = one-block-at-a-time kernel */
+    int tiles;                 /* 1 (default): tile kernels where the shape allows -- FP32 2-D Model B on 32x32
+                                  cells (nx, ny multiples of 32, block 8 or 16), KH on 16x16 cells (nx, ny
+                                  multiples of 16, block 8 or 16); 0: one-block Model B / four-stage KH kernels */
+    double cfl;                /* KH: > 0 picks each step's dt = cfl * min(dx, dy) / max(c + |v|) on the device
+                                  (tile kernel only); 0 (default): the fixed dt */
 } dba_config;
 
 typedef struct dba_ctx dba_ctx;
@@ -98,6 +101,7 @@ typedef struct dba_obs {
     double integral[4];        /* dendrite: sum p, sum T; Model B: sum x,y,z,b; KH: sum Mass,Energy,Momx,Momy */
     double vy_mode;            /* KH: amplitude of the vy mode (Calc_Vy_mode) */
     long cell_updates;         /* active cell-updates accumulated since dba_init */
+    double dt;                 /* time step the next step will take (KH with cfl > 0: set on the device) */
 } dba_obs;
 
 typedef struct dba_info {
