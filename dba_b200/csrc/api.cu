@@ -60,6 +60,7 @@ struct dba_ctx {
     bool lazy = false;
     bool tiles = false;               // FP32 2-D Model B on 32x32-cell tiles (k_modelb_tile.cuh)
     bool kh_tiles = false;            // KH one-kernel step on 16x16-cell tiles (k_kh_tile.cuh)
+    bool den_tiles = false;           // FP32 3-D dendrite on 32x8x8-cell tiles (k_dendrite_tile.cuh)
     float* kvmax = nullptr;           // KH tiles: per-block largest signal speed (CFL)
     unsigned* kgmax = nullptr;        // KH tiles: rotating maxima of the CFL speed, float bits [3]
     double* ktime = nullptr;          // KH tiles: simulated time accumulated on the device (CFL)
@@ -274,6 +275,8 @@ cudaError_t enqueue_step_t(dba_ctx* c, long s, bool dba_mode)
     cudaError_t e = cudaSuccess;
     switch (c->cfg.model) {
     case DBA_MODEL_DENDRITE:
+        if constexpr (sizeof(R) == 4)
+            if (c->den_tiles) return launch_dendrite3_tiles(dba_mode, c->grid, c->st, c->g, f, den_params<float>(c));
         return launch_dendrite<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<R>(c));
     case DBA_MODEL_MODELB: {
         MBP<R> P = mb_params<R>(c, dba_mode);
@@ -582,6 +585,10 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
     }
     c->grid = c->esz == 8 ? step_grid<double>(cfg->model, c->D, c->B, c->sms) : step_grid<float>(cfg->model, c->D, c->B, c->sms);
     if (c->grid < 1) c->grid = c->sms;
+    if (cfg->model == DBA_MODEL_DENDRITE && c->esz == 4 && cfg->tiles && dendrite_tiles_ok(c->D, c->B, cfg->nx)) {
+        c->den_tiles = true;
+        c->grid = dendrite3_tile_grid(c->sms, (cfg->nx / 32) * (cfg->ny / 8) * (cfg->nz / 8));
+    }
     if (c->kh_tiles) {
         const int nt = (cfg->nx / 16) * (cfg->ny / 16);
         c->grid = c->esz == 8 ? kh_tile_grid<double>(c->B, c->sms, nt) : kh_tile_grid<float>(c->B, c->sms, nt);
@@ -964,7 +971,9 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                     else if (r == cudaSuccess) r = launch_kh<double>(c->B, dba_mode, c->grid, c->st, c->g, f, kh_params<double>(c, dba_mode));
                 }
             } else {
-                if (c->cfg.model == DBA_MODEL_DENDRITE) r = launch_dendrite<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<float>(c));
+                if (c->cfg.model == DBA_MODEL_DENDRITE)
+                    r = c->den_tiles ? launch_dendrite3_tiles(dba_mode, c->grid, c->st, c->g, f, den_params<float>(c))
+                                     : launch_dendrite<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, den_params<float>(c));
                 else if (c->cfg.model == DBA_MODEL_MODELB) {
                     MBP<float> P = mb_params<float>(c, dba_mode);
                     LazyP L = lazy_params(c, s, P.conserved != 0);

@@ -122,34 +122,15 @@ __global__ void __launch_bounds__(NT) batch_dendrite_step(BatchP bp, FlagP f)
                 const R pc = sp[ti], Tc = sT[ti];
                 R pn = pc;
                 if (m & 1) {
-                    const R pxp = sp[ti + 1], pxm = sp[ti - 1], pyp = sp[ti + SY], pym = sp[ti - SY];
-                    const R dpx = (pxp - pxm) * f0;
-                    const R dpy = (pyp - pym) * f0;
-                    const R dpz = (pc - pc) * f0;
-                    const R lapP = (pxp + pxm + pyp + pym + pc + pc - 6 * pc) * f1;
-                    const R v2 = dpx * dpx + dpy * dpy + dpz * dpz;
-                    R sigma;
-                    if (v2 <= (R)1E-6)
-                        sigma = 1;
-                    else
-                        sigma = 1 - (R)r.delta * (1 - ((dpx * dpx) * (dpx * dpx) + (dpy * dpy) * (dpy * dpy) +
-                                                       (dpz * dpz) * (dpz * dpz)) / (v2 * v2));
-                    const R mm = f2 * atan_r<R>((R)r.gamma * sigma * Tc);
-                    const R pchg = f3 * ((R)r.eps2 * lapP + pc * (1 - pc) * (pc - (R)0.5 + mm));
-                    pn = pc + dt * pchg;
+                    pn = den_p_new<R>(pc, Tc, sp[ti + 1], sp[ti - 1], sp[ti + SY], sp[ti - SY], pc, pc, f0, f1, f2, f3,
+                                      dt, (R)r.delta, (R)r.eps2, (R)r.gamma);
                     ((m & 4) ? (R*)r.p[0] : (R*)r.p[1])[gi] = pn;
                     if (pn >= (R)r.thr_p && pn <= (R)r.thr_p_hi) s_np[k] = 1;
                     if (!isfinite(pn)) raise_status(f.status, 5);
                 }
                 if (m & 2) {
-                    const R lapT = (sT[ti + 1] + sT[ti - 1] + sT[ti + SY] + sT[ti - SY] + Tc + Tc - 6 * Tc) * f1;
-                    R Tn;
-                    if (DBA) {
-                        Tn = Tc + dt * lapT;
-                        if (m & 1) Tn = Tn + (pn - pc);
-                    } else {
-                        Tn = Tc + dt * lapT + pn - pc;
-                    }
+                    const R Tn = den_T_new<R, DBA>(Tc, sT[ti + 1], sT[ti - 1], sT[ti + SY], sT[ti - SY], Tc, Tc,
+                                                   (m & 1) != 0, pn, pc, f1, dt);
                     ((m & 8) ? (R*)r.T[0] : (R*)r.T[1])[gi] = Tn;
                     if (fabs(Tn - Tc) >= (R)r.thr_T) s_nT[k] = 1;
                     if (!isfinite(Tn)) raise_status(f.status, 5);

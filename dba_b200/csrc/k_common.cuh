@@ -51,6 +51,15 @@ __device__ __forceinline__ int wrapc(int v, int n, int bc)
     return v;
 }
 
+// 16-byte asynchronous global -> shared copies (both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 // periodic wrap of an index at most one period outside [0, n)
 __device__ __forceinline__ int wrap_p(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 

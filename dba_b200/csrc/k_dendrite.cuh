@@ -37,6 +37,54 @@ template <typename R> __device__ __forceinline__ R atan_r(R v);
 template <> __device__ __forceinline__ double atan_r<double>(double v) { return dba_atan(v); }
 template <> __device__ __forceinline__ float atan_r<float>(float v) { return atanf(v); }
 
+// explicitly rounded operations, so every kernel that advances dendrite cells
+// through den_p_new / den_T_new produces the same bits (in FP64 they equal the
+// plain operators of the -fmad=false build)
+__device__ __forceinline__ float da(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float ds(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float dm(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float dd(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double dd(double a, double b) { return __ddiv_rn(a, b); }
+
+// Evolve_p (example_Dendritic_growth/kernel.cu:220-241) for one cell from its
+// 6 neighbours (2-D: the z neighbours are the cell itself), in the reference's order
+template <typename R>
+__device__ __forceinline__ R den_p_new(R pc, R Tc, R pxp, R pxm, R pyp, R pym, R pzp, R pzm, R f0, R f1, R f2, R f3,
+                                       R dt, R delta, R eps2, R gam)
+{
+    const R dpx = dm(ds(pxp, pxm), f0);
+    const R dpy = dm(ds(pyp, pym), f0);
+    const R dpz = dm(ds(pzp, pzm), f0);
+    const R lapP = dm(ds(da(da(da(da(da(pxp, pxm), pyp), pym), pzp), pzm), dm((R)6, pc)), f1);
+    const R px2 = dm(dpx, dpx), py2 = dm(dpy, dpy), pz2 = dm(dpz, dpz);
+    const R v2 = da(da(px2, py2), pz2);
+    R sigma;
+    if (v2 <= (R)1E-6)
+        sigma = 1;
+    else
+        sigma = ds((R)1, dm(delta, ds((R)1, dd(da(da(dm(px2, px2), dm(py2, py2)), dm(pz2, pz2)), dm(v2, v2)))));
+    const R mm = dm(f2, atan_r<R>(dm(dm(gam, sigma), Tc)));
+    const R pchg = dm(f3, da(dm(eps2, lapP), dm(dm(pc, ds((R)1, pc)), da(ds(pc, (R)0.5), mm))));
+    return da(pc, dm(dt, pchg));
+}
+
+// Evolve_T (kernel.cu:286-289 regular, :468-489 DBA): T + dt lapT, plus the p
+// change in the reference's order for the mode
+template <typename R, bool DBA>
+__device__ __forceinline__ R den_T_new(R Tc, R Txp, R Txm, R Typ, R Tym, R Tzp, R Tzm, bool p_active, R pn, R pc,
+                                       R f1, R dt)
+{
+    const R lapT = dm(ds(da(da(da(da(da(Txp, Txm), Typ), Tym), Tzp), Tzm), dm((R)6, Tc)), f1);
+    if (DBA) {
+        R Tn = da(Tc, dm(dt, lapT));
+        return p_active ? da(Tn, ds(pn, pc)) : Tn;
+    }
+    return ds(da(da(Tc, dm(dt, lapT)), pn), pc);
+}
+
 template <typename R, int D, int B, bool DBA>
 __global__ void __launch_bounds__(kThreads) dendrite_step(GridP g, FlagP f, DenP<R> P)
 {
@@ -127,36 +175,15 @@ __global__ void __launch_bounds__(kThreads) dendrite_step(GridP g, FlagP f, DenP
                 const R pc = sp[ti], Tc = sT[ti];
                 R pn = pc;
                 if (m & 1) {   // Evolve_p (kernel.cu:220-241)
-                    const R pxp = sp[ti + 1], pxm = sp[ti - 1], pyp = sp[ti + SY], pym = sp[ti - SY];
-                    const R pzp = sp[ti + SZ], pzm = sp[ti - SZ];
-                    const R dpx = (pxp - pxm) * f0;
-                    const R dpy = (pyp - pym) * f0;
-                    const R dpz = (pzp - pzm) * f0;
-                    const R lapP = (pxp + pxm + pyp + pym + pzp + pzm - 6 * pc) * f1;
-                    const R v2 = dpx * dpx + dpy * dpy + dpz * dpz;
-                    R sigma;
-                    if (v2 <= (R)1E-6)
-                        sigma = 1;
-                    else
-                        sigma = 1 - delta * (1 - ((dpx * dpx) * (dpx * dpx) + (dpy * dpy) * (dpy * dpy) +
-                                                  (dpz * dpz) * (dpz * dpz)) / (v2 * v2));
-                    const R mm = f2 * atan_r<R>(gam * sigma * Tc);
-                    const R pchg = f3 * (eps2 * lapP + pc * (1 - pc) * (pc - (R)0.5 + mm));
-                    pn = pc + dt * pchg;
+                    pn = den_p_new<R>(pc, Tc, sp[ti + 1], sp[ti - 1], sp[ti + SY], sp[ti - SY], sp[ti + SZ], sp[ti - SZ],
+                                      f0, f1, f2, f3, dt, delta, eps2, gam);
                     ((m & 4) ? P.p[0] : P.p[1])[gi] = pn;
                     if (pn >= thr_p && pn <= thr_p_hi) s_np[k] = 1;
                     if (!isfinite(pn)) raise_status(f.status, 5);
                 }
                 if (m & 2) {   // Evolve_T (kernel.cu:286-289, :468-489)
-                    const R lapT = (sT[ti + 1] + sT[ti - 1] + sT[ti + SY] + sT[ti - SY] + sT[ti + SZ] + sT[ti - SZ] -
-                                    6 * Tc) * f1;
-                    R Tn;
-                    if (DBA) {
-                        Tn = Tc + dt * lapT;
-                        if (m & 1) Tn = Tn + (pn - pc);
-                    } else {
-                        Tn = Tc + dt * lapT + pn - pc;
-                    }
+                    const R Tn = den_T_new<R, DBA>(Tc, sT[ti + 1], sT[ti - 1], sT[ti + SY], sT[ti - SY], sT[ti + SZ],
+                                                   sT[ti - SZ], (m & 1) != 0, pn, pc, f1, dt);
                     ((m & 8) ? P.T[0] : P.T[1])[gi] = Tn;
                     if (fabs(Tn - Tc) >= thr_T) s_nT[k] = 1;
                     if (!isfinite(Tn)) raise_status(f.status, 5);

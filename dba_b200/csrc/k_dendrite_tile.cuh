@@ -1,0 +1,236 @@
+// k_dendrite_tile.cuh -- FP32 3-D dendrite step over 32x8x8-cell tiles.
+//
+// Same DBA semantics and the same point arithmetic as dendrite_step
+// (k_dendrite.cuh; den_p_new / den_T_new fix every rounding) for 8^3 blocks,
+// reorganised so that a CTA works on four x-adjacent blocks at a time:
+//
+//   * a tile is listed when any channel (p or T) of any of its blocks is
+//     active; only active channels of active blocks are updated;
+//   * p and T of the tile plus a 1-cell halo are staged in shared memory as
+//     40-float rows (x from X0-4 to X0+35): each row is five whole 32-byte
+//     sectors, where one 8-cell block row with its x halo touches three sectors
+//     for ten values.  16-byte cp.async pieces, each inside one block (whose
+//     parity picks the buffer), double-buffered so tile i+1 loads while tile i
+//     computes; pieces that fall outside a zero-flux wall are clamped cell by
+//     cell instead;
+//   * each thread owns one (x, y) column of the tile and slides a 3-plane
+//     window along z, so the z neighbours come from registers.
+#pragma once
+
+#include "k_common.cuh"
+#include "k_dendrite.cuh"
+
+namespace dba {
+
+struct DenTile {
+    static constexpr int NT = 256;
+    static constexpr int B = 8;
+    static constexpr int TX = 32;                // tile x extent (4 blocks)
+    static constexpr int TBX = TX / B;
+    static constexpr int SW = TX + 8;            // staged row: 4-cell (16-byte) halo each side
+    static constexpr int SP = SW + 4;            // row pitch
+    static constexpr int SR = B + 2;             // staged rows per plane (y) and planes (z)
+    static constexpr int PL = SR * SP;           // one staged plane
+    static constexpr int SV = SR * PL;           // one staged field
+    static constexpr int NQ = SR * SR * (SW / 4);// 16-byte pieces per field
+    static constexpr int RX = TBX + 2;           // neighbourhood extent in blocks: x
+    static constexpr int NR = RX * 3 * 3;        // neighbourhood blocks
+    static constexpr int TPP = NT / TBX;         // tiles per scan pass
+    static constexpr size_t smem = sizeof(float) * 2 * 2 * SV;   // [stage][p, T]
+    static_assert(TX * B == NT, "one column per thread");
+};
+
+template <bool DBA>
+__global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, DenP<float> P)
+{
+    using S = DenTile;
+    constexpr int NT = S::NT, B = S::B, TX = S::TX, TBX = S::TBX, SW = S::SW, SP = S::SP, SR = S::SR, PL = S::PL,
+                  SV = S::SV, NQ = S::NQ, RX = S::RX, NR = S::NR, TPP = S::TPP;
+    extern __shared__ __align__(128) float smem_f[];   // [stage][p|T][z][y][x]
+    __shared__ int s_tile[TPP];
+    __shared__ unsigned s_tmeta[TPP];   // bits 0-3 p-active blocks, 4-7 T-active, 8-11 p parity, 12-15 T parity
+    __shared__ int s_cnt;
+    __shared__ uint8_t s_par[2][2][NR];  // [stage][channel][neighbour block]
+    __shared__ int s_np[TBX], s_nT[TBX];
+
+    const int tid = threadIdx.x;
+    const int G = gridDim.x;
+    const int nb = g.nb;
+    const int ntx = g.nx / TX, nty = g.ny / B, ntz = g.nz / B;
+    const int ntiles = ntx * nty * ntz;
+    const size_t nx = (size_t)g.nx, nxy = (size_t)g.nx * g.ny;
+    const float f0 = (float)P.f0, f1 = (float)P.f1, f2 = (float)P.f2, f3 = (float)P.f3;
+    const float dt = (float)P.dt, delta = (float)P.delta, eps2 = (float)P.eps2, gam = (float)P.gamma;
+    const float thr_p = (float)P.thr_p, thr_p_hi = (float)P.thr_p_hi, thr_T = (float)P.thr_T;
+    const int cx = tid % TX, cy = tid / TX;       // this thread's column
+    const int kb = cx / B;                        // its block within the tile
+
+    auto tile_xyz = [&](int tile, int& X0, int& Y0, int& Z0) {
+        X0 = (tile % ntx) * TX;
+        Y0 = ((tile / ntx) % nty) * B;
+        Z0 = (tile / (ntx * nty)) * B;
+    };
+    auto build_nbr = [&](int idx, int st) {
+        for (int r = tid; r < NR; r += NT) {
+            int X0, Y0, Z0;
+            tile_xyz(s_tile[idx], X0, Y0, Z0);
+            const int rx = r % RX, ry = (r / RX) % 3, rz = r / (RX * 3);
+            int bx = X0 / B + rx - 1, by = Y0 / B + ry - 1, bz = Z0 / B + rz - 1;
+            // outside a zero-flux wall the clamped cells belong to the edge block
+            bx = bx < 0 ? (g.bc ? 0 : g.nbx - 1) : (bx >= g.nbx ? (g.bc ? g.nbx - 1 : 0) : bx);
+            by = by < 0 ? (g.bc ? 0 : g.nby - 1) : (by >= g.nby ? (g.bc ? g.nby - 1 : 0) : by);
+            bz = bz < 0 ? (g.bc ? 0 : g.nbz - 1) : (bz >= g.nbz ? (g.bc ? g.nbz - 1 : 0) : bz);
+            const int ob = bx + g.nbx * (by + g.nby * bz);
+            s_par[st][0][r] = f.par_cur[ob];
+            s_par[st][1][r] = f.par_cur[nb + ob];
+        }
+    };
+    auto issue = [&](int idx, int st) {
+        int X0, Y0, Z0;
+        tile_xyz(s_tile[idx], X0, Y0, Z0);
+        float* dst = smem_f + st * 2 * SV;
+        for (int q = tid; q < NQ; q += NT) {
+            const int c4 = q % (SW / 4), ry = (q / (SW / 4)) % SR, rz = q / ((SW / 4) * SR);
+            const int lx = 4 * c4 - 4, ly = ry - 1, lz = rz - 1;
+            const int reg = (lx + B) / B + RX * ((ly + B) / B + 3 * ((lz + B) / B));
+            const int gy = wrapc(Y0 + ly, g.ny, g.bc), gz = wrapc(Z0 + lz, g.nz, g.bc);
+            const int so = rz * PL + ry * SP + 4 * c4;
+            const int gx0 = X0 + lx;
+            const float* pb = s_par[st][0][reg] ? P.p[1] : P.p[0];
+            const float* Tb = s_par[st][1][reg] ? P.T[1] : P.T[0];
+            const size_t row = nx * ((size_t)gy + (size_t)g.ny * gz);
+            if (gx0 >= 0 && gx0 + 3 < g.nx) {
+                cp_async16(dst + so, pb + row + gx0);
+                cp_async16(dst + SV + so, Tb + row + gx0);
+            } else if (!g.bc) {                    // periodic: the piece wraps whole (nx is a multiple of 32)
+                const int gx = gx0 < 0 ? gx0 + g.nx : gx0 - g.nx;
+                cp_async16(dst + so, pb + row + gx);
+                cp_async16(dst + SV + so, Tb + row + gx);
+            } else {                               // zero-flux wall: clamp cell by cell
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int gx = wrapc(gx0 + e, g.nx, 1);
+                    dst[so + e] = pb[row + gx];
+                    dst[SV + so + e] = Tb[row + gx];
+                }
+            }
+        }
+        cp_async_commit();
+    };
+
+    for (long long j0 = 0; blockIdx.x + (long long)G * j0 < ntiles; j0 += TPP) {
+        // ---- scan: per-block bookkeeping of both channels, one list entry per tile
+        {
+            const long long tl = blockIdx.x + (long long)G * (j0 + tid / TBX);
+            const int kq = tid % TBX;
+            const bool valid = tl < ntiles;
+            const int tile = (int)tl;
+            int act = 0, pp = 0, pT = 0;
+            if (valid) {
+                int X0, Y0, Z0;
+                tile_xyz(tile, X0, Y0, Z0);
+                const int b = (X0 / B + kq) + g.nbx * (Y0 / B + g.nby * (Z0 / B));
+                pp = f.par_cur[b];
+                pT = f.par_cur[nb + b];
+                act = DBA ? ((f.wake_cur[b] ? 1 : 0) | (f.wake_cur[nb + b] ? 2 : 0)) : 3;
+                f.wake_clr[b] = 0;
+                f.wake_clr[nb + b] = 0;
+                if (!DBA) {
+                    f.wake_nxt[b] = 1;
+                    f.wake_nxt[nb + b] = 1;
+                }
+                f.par_nxt[b] = (uint8_t)(pp ^ (act & 1));
+                f.par_nxt[nb + b] = (uint8_t)(pT ^ ((act >> 1) & 1));
+            }
+            count_stats(f.stats, act, valid);
+            const unsigned m0 = __ballot_sync(0xffffffffu, valid && (act & 1));
+            const unsigned m1 = __ballot_sync(0xffffffffu, valid && (act & 2));
+            const unsigned m2 = __ballot_sync(0xffffffffu, valid && pp);
+            const unsigned m3 = __ballot_sync(0xffffffffu, valid && pT);
+            const int g0 = (tid & 31) & ~(TBX - 1);
+            const unsigned gm = (1u << TBX) - 1u;
+            const unsigned meta = ((m0 >> g0) & gm) | (((m1 >> g0) & gm) << 4) | (((m2 >> g0) & gm) << 8) |
+                                  (((m3 >> g0) & gm) << 12);
+            if (tid == 0) s_cnt = 0;
+            __syncthreads();
+            list_append(valid && kq == 0 && (meta & 0xffu) != 0, tile, (int)meta, s_tile,
+                        reinterpret_cast<int*>(s_tmeta), &s_cnt);
+            __syncthreads();
+        }
+        const int cnt = s_cnt;
+        if (cnt > 0) {
+            build_nbr(0, 0);
+            __syncthreads();
+            issue(0, 0);
+        }
+        for (int i = 0; i < cnt; ++i) {
+            const int st = i & 1;
+            if (i + 1 < cnt) build_nbr(i + 1, st ^ 1);
+            __syncthreads();                     // next table ready; stage st^1 free
+            if (tid < TBX) {
+                s_np[tid] = 0;
+                s_nT[tid] = 0;
+            }
+            if (i + 1 < cnt) issue(i + 1, st ^ 1);
+            else cp_async_commit();
+            cp_async_wait1();
+            __syncthreads();                     // tile i staged (plain stores of wall pieces included)
+            const unsigned tm = s_tmeta[i];
+            const bool pa = (tm >> kb) & 1u, Ta = (tm >> (4 + kb)) & 1u;
+            if (pa || Ta) {
+                int X0, Y0, Z0;
+                tile_xyz(s_tile[i], X0, Y0, Z0);
+                const float* sp = smem_f + st * 2 * SV;
+                const float* sT = sp + SV;
+                float* pout = ((tm >> (8 + kb)) & 1u) ? P.p[0] : P.p[1];
+                float* Tout = ((tm >> (12 + kb)) & 1u) ? P.T[0] : P.T[1];
+                int si = PL + (cy + 1) * SP + cx + 4;        // plane z = 0 of this column
+                float pm = sp[si - PL], pc = sp[si], Tm = sT[si - PL], Tc = sT[si];
+                bool wp = false, wT = false, bad = false;
+                const size_t gcol = (size_t)(X0 + cx) + nx * (size_t)(Y0 + cy);
+#pragma unroll 2
+                for (int z = 0; z < B; ++z) {
+                    const float pq = sp[si + PL], Tq = sT[si + PL];
+                    const size_t gi = gcol + nxy * (size_t)(Z0 + z);
+                    float pn = pc;
+                    if (pa) {
+                        pn = den_p_new<float>(pc, Tc, sp[si + 1], sp[si - 1], sp[si + SP], sp[si - SP], pq, pm, f0, f1,
+                                              f2, f3, dt, delta, eps2, gam);
+                        pout[gi] = pn;
+                        wp |= pn >= thr_p && pn <= thr_p_hi;
+                        bad |= !isfinite(pn);
+                    }
+                    if (Ta) {
+                        const float Tn = den_T_new<float, DBA>(Tc, sT[si + 1], sT[si - 1], sT[si + SP], sT[si - SP],
+                                                               Tq, Tm, pa, pn, pc, f1, dt);
+                        Tout[gi] = Tn;
+                        wT |= fabsf(Tn - Tc) >= thr_T;
+                        bad |= !isfinite(Tn);
+                    }
+                    pm = pc; pc = pq; Tm = Tc; Tc = Tq;
+                    si += PL;
+                }
+                if (bad) raise_status(f.status, 5);
+                if (DBA && wp) s_np[kb] = 1;
+                if (DBA && wT) s_nT[kb] = 1;
+            }
+            __syncthreads();
+            if (DBA && tid < TBX) {
+                int X0, Y0, Z0;
+                tile_xyz(s_tile[i], X0, Y0, Z0);
+                const int b = (X0 / B + tid) + g.nbx * (Y0 / B + g.nby * (Z0 / B));
+                if ((tm >> tid) & 1u) {
+                    f.next[b] = (uint8_t)s_np[tid];
+                    if (s_np[tid]) wake_faces(g, f.wake_nxt, b);
+                }
+                if ((tm >> (4 + tid)) & 1u) {
+                    f.next[nb + b] = (uint8_t)s_nT[tid];
+                    if (s_nT[tid]) wake_faces(g, f.wake_nxt + nb, b);
+                }
+            }
+        }
+        __syncthreads();                         // list and buffers reused by the next scan pass
+    }
+}
+
+}  // namespace dba

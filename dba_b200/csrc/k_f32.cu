@@ -34,6 +34,27 @@ static int tile_grid_b(int sms, int ntiles)
     return g < ntiles ? g : ntiles;
 }
 
+int dendrite3_tile_grid(int sms, int ntiles)
+{
+    const size_t sm = DenTile::smem;
+    cudaFuncSetAttribute(dendrite3_tile_step<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(dendrite3_tile_step<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, dendrite3_tile_step<true>, DenTile::NT, sm) != cudaSuccess ||
+        occ < 1)
+        occ = 1;
+    const int g = occ * sms;
+    return g < ntiles ? g : ntiles;
+}
+
+cudaError_t launch_dendrite3_tiles(bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
+                                   const DenP<float>& P)
+{
+    if (dba_mode) dendrite3_tile_step<true><<<grid, DenTile::NT, DenTile::smem, st>>>(g, f, P);
+    else dendrite3_tile_step<false><<<grid, DenTile::NT, DenTile::smem, st>>>(g, f, P);
+    return cudaGetLastError();
+}
+
 int modelb_tile_grid(int B, int sms, int ntiles)
 {
     return B == 8 ? tile_grid_b<8>(sms, ntiles) : tile_grid_b<16>(sms, ntiles);

@@ -14,7 +14,7 @@
 //   * each thread owns a 4-row strip of one column and slides a 3-row window
 //     down it, so the Laplacians reuse row sums instead of re-reading 9 cells;
 //   * the 1-cell potential ring around the tile is computed (active owner) or
-//     loaded from the persisted ring (inactive owner), 17 cells per warp;
+//     loaded from the persisted ring (inactive owner) by the first 132 threads;
 //   * a block persists its ring potentials only when its own wake-up test is
 //     negative: a block whose test is positive is active next step (it wakes
 //     itself), so its ring from this step is never read as stale;
@@ -43,20 +43,11 @@ template <int B> struct MBTile {
     static constexpr int MP = T + 4;          // potential row pitch (T + 2 used)
     static constexpr int MV = (T + 2) * MP;   // one potential field
     static constexpr int RING = 4 * T + 4;    // potential cells around the tile
-    static constexpr int RPW = (RING + NT / 32 - 1) / (NT / 32);   // ring cells per warp
     static constexpr int TPP = NT / NBT;      // tiles per scan pass
     static constexpr int ROWS = T * T / NT;   // rows per thread strip
     static constexpr size_t smem = sizeof(float) * (2 * 3 * SV + 3 * MV);
-    static_assert(T % B == 0 && B % ROWS == 0 && NBT <= 16 && NQ <= 2 * NT && RPW <= 32, "tile shape");
+    static_assert(T % B == 0 && B % ROWS == 0 && NBT <= 16 && NQ <= 2 * NT && RING <= NT, "tile shape");
 };
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 
 template <int B, bool DBA>
@@ -64,7 +55,7 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
 {
     using S = MBTile<B>;
     constexpr int NT = S::NT, T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, SW = S::SW, SP = S::SP, SV = S::SV;
-    constexpr int NQ = S::NQ, MP = S::MP, MV = S::MV, RING = S::RING, RPW = S::RPW, TPP = S::TPP, ROWS = S::ROWS;
+    constexpr int NQ = S::NQ, MP = S::MP, MV = S::MV, RING = S::RING, TPP = S::TPP, ROWS = S::ROWS;
     extern __shared__ __align__(128) float smem_f[];
     float* stage = smem_f;               // [2][3][SV]
     float* mu = smem_f + 2 * 3 * SV;     // [3][MV]
@@ -99,9 +90,10 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
     }
     const int tx = tid & 31, ly0 = (tid >> 5) * ROWS;
     const int kb = tx / B + TB * (ly0 / B);     // tile block of this strip
-    // ring cell of this thread: 17 per warp, so every warp carries the same share
-    const int rg_p = (tid >> 5) * RPW + (tid & 31);
-    const bool rg_on = (tid & 31) < RPW && rg_p < RING;
+    // ring cell of this thread: the first RING threads, so whole warps carry the
+    // ring (measured faster than spreading it thinly over every warp)
+    const int rg_p = tid;
+    const bool rg_on = tid < RING;
     int rg_lx = 0, rg_ly = 0;
     if (rg_p < T + 2) { rg_ly = -1; rg_lx = rg_p - 1; }
     else if (rg_p < 2 * (T + 2)) { rg_ly = T; rg_lx = rg_p - (T + 2) - 1; }

@@ -7,6 +7,7 @@
 
 #include "k_common.cuh"
 #include "k_dendrite.cuh"
+#include "k_dendrite_tile.cuh"
 #include "k_kh.cuh"
 #include "k_kh_tile.cuh"
 #include "k_modelb.cuh"
@@ -24,6 +25,11 @@ template <typename R> int step_grid(int model, int D, int B, int sms);
 template <typename R>
 cudaError_t launch_dendrite(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
                             const DenP<R>& P);
+// FP32 3-D dendrite on 32x8x8-cell tiles (k_dendrite_tile.cuh)
+inline bool dendrite_tiles_ok(int D, int B, int nx) { return D == 3 && B == 8 && nx % 32 == 0; }
+int dendrite3_tile_grid(int sms, int ntiles);
+cudaError_t launch_dendrite3_tiles(bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
+                                   const DenP<float>& P);
 // FP32 2-D uses the fast kernels (lazy conserved correction, reduction fused):
 // the 32x32-cell tile kernel when `tiles` (see modelb_tiles_ok), else one block
 // at a time.  `lz` may be null for FP64.

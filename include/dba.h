@@ -84,7 +84,8 @@ typedef struct dba_config {
     double noise_amp, noise_amp_z; /* Model B: x,y and z uniform-noise amplitudes (0.05, 0.001) */
     int tiles;                 /* 1 (default): tile kernels where the shape allows -- FP32 2-D Model B on 32x32
                                   cells (nx, ny multiples of 32, block 8 or 16), KH on 16x16 cells (nx, ny
-                                  multiples of 16, block 8 or 16); 0: one-block Model B / four-stage KH kernels */
+                                  multiples of 16, block 8 or 16), FP32 3-D dendrite on 32x8x8 cells (block 8,
+                                  nx a multiple of 32); 0: the one-block kernels and the four-stage KH kernels */
     double cfl;                /* KH: > 0 picks each step's dt = cfl * min(dx, dy) / max(c + |v|) on the device
                                   (tile kernel only); 0 (default): the fixed dt */
 } dba_config;
