@@ -439,9 +439,31 @@ int gather(dba_ctx* c, const void* b0, const void* b1, const uint8_t* par, size_
                         ? launch_gather<double>(c->st, c->g, c->B, c->D, (const double*)b0, (const double*)b1, par, start, stride, count, c->staging)
                         : launch_gather<float>(c->st, c->g, c->B, c->D, (const float*)b0, (const float*)b1, par, start, stride, count, c->staging);
     if (e != cudaSuccess) return cuda_status(e);
+    if (!host) return DBA_OK;   // device-side consumers read c->staging
     e = cudaMemcpyAsync(host, c->staging, count * sizeof(double), cudaMemcpyDeviceToHost, c->st);
     if (e != cudaSuccess) return cuda_status(e);
     return cuda_status(cudaStreamSynchronize(c->st));
+}
+
+// a state field's current values, as doubles, into c->staging (device only)
+int field_on_device(dba_ctx* c, int field)
+{
+    const int model = c->cfg.model;
+    const size_t nb = c->g.nb;
+    if (model == DBA_MODEL_DENDRITE && field < 2)
+        return gather(c, c->state[field][0], c->state[field][1], cur_par(c) + (size_t)field * nb, 0, 1, c->n, nullptr);
+    if (model == DBA_MODEL_MODELB && field < 3) {
+        if (!c->lazy) return gather(c, c->state[field][0], c->state[field][1], cur_par(c), 0, 1, c->n, nullptr);
+        const long sn = c->step + 1;
+        return cuda_status(launch_gather_lazy(c->st, c->g, c->B, (const float*)c->state[field][0],
+                                              (const float*)c->state[field][1], cur_par(c),
+                                              c->lz + 3 * ((sn + 1) % 2) + field, c->lz + 6 + 3 * ((sn + 2) % 3) + field,
+                                              c->n, c->staging));
+    }
+    if (model == DBA_MODEL_KH && field < 4)
+        return c->kh_tiles ? gather(c, c->state[field][0], c->state[field][1], cur_par(c), 0, 1, c->n, nullptr)
+                           : gather(c, c->state[field][0], c->state[field][0], nullptr, 0, 1, c->n, nullptr);
+    return DBA_ERR_ARG;
 }
 
 }  // namespace
@@ -1140,6 +1162,109 @@ int dba_restore(dba_ctx* c, const char* path)
     c->time = time;
     c->initialized = true;
     return DBA_OK;
+}
+
+int dba_tip_profile(dba_ctx* c, int field, int dz, int* tip_x, int* tip_x_max)
+{
+    // Extract_Tip (example_Dendritic_growth/Extract_Tip.cpp:68-87) on the device
+    if (!c || !tip_x || !tip_x_max || dz < 0) return DBA_ERR_ARG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    int st = field_on_device(c, field);
+    if (st) return st;
+    const int z0 = c->cfg.nz / 2;
+    const int nk = std::min(dz + 1, c->cfg.nz - z0);
+    int* d_tip = nullptr;
+    DBA_TRY(cudaMalloc(&d_tip, sizeof(int) * (size_t)(dz + 1)));
+    cudaError_t e = cudaMemsetAsync(d_tip, 0, sizeof(int) * (size_t)(dz + 1), c->st);
+    if (e == cudaSuccess) {
+        post_tip_kernel<<<4 * c->sms, 256, 0, c->st>>>(c->staging, c->cfg.nx, c->cfg.ny, c->cfg.nz, z0, nk, d_tip);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tip_x, d_tip, sizeof(int) * (size_t)(dz + 1), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    cudaFree(d_tip);
+    if (e != cudaSuccess) return cuda_status(e);
+    int m = 0;
+    for (int k = 0; k <= dz; ++k) m = std::max(m, tip_x[k]);
+    *tip_x_max = m;
+    return DBA_OK;
+}
+
+int dba_size_distribution(dba_ctx* c, int field, double* avg_out, long* volume_out, long* islands_out, long* sizes,
+                          long max_sizes)
+{
+    // coarsening_analysis (example_Reactive_ModelB/coarsening_analysis.cpp:46-165) on the device
+    if (!c || !avg_out || !volume_out || !islands_out || (max_sizes > 0 && !sizes)) return DBA_ERR_ARG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    int st = field_on_device(c, field);
+    if (st) return st;
+    const size_t n = c->n;
+    PostGrid pg{c->cfg.nx, c->cfg.ny, c->cfg.nz, n};
+    long long* lab = nullptr;
+    unsigned long long *size = nullptr, *first = nullptr, *small = nullptr;
+    // small: [0] max, [1] min, [2] volume, [3] pair count, then (first seed, size) pairs
+    const unsigned long long cap = max_sizes > 0 ? (unsigned long long)max_sizes : 0ull;
+    cudaError_t e = cudaMalloc(&lab, n * sizeof(long long));
+    if (e == cudaSuccess) e = cudaMalloc(&size, n * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&first, n * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&small, (4 + 2 * (size_t)cap) * sizeof(unsigned long long) + 16);
+    std::vector<unsigned long long> head(4, 0ull);
+    const double half = 0.5;
+    unsigned long long hb = 0;
+    std::memcpy(&hb, &half, sizeof hb);
+    head[0] = head[1] = (hb >> 63) ? ~hb : (hb | 0x8000000000000000ull);   // the tool starts Max = Min = 0.5
+    const int grid = 8 * c->sms;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(small, head.data(), 4 * sizeof(unsigned long long), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) {
+        post_minmax_kernel<<<grid, 256, 0, c->st>>>(c->staging, n, small);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(head.data(), small, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    double avg = 0.0;
+    if (e == cudaSuccess) {
+        double mx, mn;
+        for (int k = 0; k < 2; ++k) {
+            const unsigned long long o = head[k];
+            const unsigned long long b = (o >> 63) ? (o & 0x7fffffffffffffffull) : ~o;
+            std::memcpy(k == 0 ? &mx : &mn, &b, sizeof b);
+        }
+        avg = (mx + mn) / 2.;
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(size, 0, n * sizeof(unsigned long long), c->st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(first, 0xff, n * sizeof(unsigned long long), c->st);
+    if (e == cudaSuccess) {
+        post_init_kernel<<<grid, 256, 0, c->st>>>(c->staging, pg, avg, lab, small + 2);
+        post_union_kernel<<<grid, 256, 0, c->st>>>(pg, lab, c->status);
+        post_count_kernel<<<grid, 256, 0, c->st>>>(c->staging, pg, avg, lab, size, first);
+        post_collect_kernel<<<grid, 256, 0, c->st>>>(pg, lab, size, first, small + 4, small + 3, cap);
+        e = cudaGetLastError();
+    }
+    std::vector<unsigned long long> pairs;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(head.data(), small, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    const unsigned long long npairs = head[3];
+    if (e == cudaSuccess && cap) {
+        pairs.resize(2 * (size_t)std::min(npairs, cap));
+        if (!pairs.empty())
+            e = cudaMemcpy(pairs.data(), small + 4, pairs.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+    }
+    cudaFree(lab);
+    cudaFree(size);
+    cudaFree(first);
+    cudaFree(small);
+    if (e != cudaSuccess) return cuda_status(e);
+    // islands in the order of their first seed cell (the tool's scan order)
+    std::vector<std::pair<unsigned long long, unsigned long long>> byseed;
+    for (size_t k = 0; k + 1 < pairs.size(); k += 2) byseed.push_back({pairs[k], pairs[k + 1]});
+    std::sort(byseed.begin(), byseed.end());
+    for (size_t k = 0; k < byseed.size(); ++k) sizes[k] = (long)byseed[k].second;
+    *avg_out = avg;
+    *volume_out = (long)head[2];
+    *islands_out = (long)npairs;
+    return npairs > cap && max_sizes > 0 ? DBA_ERR_ARG : DBA_OK;
 }
 
 }  // extern "C"

@@ -96,7 +96,8 @@ double field_sum(dba_ctx* ctx, int field, size_t n)
 int main(int argc, char** argv)
 {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: %s dendrite|modelb|kh [Input.txt] [--vtk] [--quiet]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s dendrite|modelb|kh [Input.txt] [--vtk] [--quiet] [--tip-profile] [--size-dist]\n",
+                     argv[0]);
         return 2;
     }
     std::string mname = argv[1];
@@ -107,11 +108,13 @@ int main(int argc, char** argv)
         return 2;
     }
     std::string input = "Input.txt";
-    bool vtk = false;
+    bool vtk = false, tip_prof = false, size_dist = false;
     for (int a = 2; a < argc; ++a) {
         std::string s = argv[a];
         if (s == "--vtk") vtk = true;
         else if (s == "--quiet") quiet = true;
+        else if (s == "--tip-profile") tip_prof = true;   // Extract_Tip on the device at every output
+        else if (s == "--size-dist") size_dist = true;    // coarsening_analysis on the device at every output
         else input = s;
     }
     dba_config k;
@@ -129,8 +132,33 @@ int main(int argc, char** argv)
     const size_t n = (size_t)k.nx * k.ny * k.nz;
     const int mode = k.mode ? DBA_MODE_DBA : DBA_MODE_REGULAR;
 
+    // coarsening_analysis (example_Reactive_ModelB/coarsening_analysis.cpp:171-188) of the z field:
+    // sizes appended to size_dist.txt, "index,R_avg" to avg_radius.txt
+    long n_dist = 0;
+    auto droplets = [&]() {
+        double avg = 0;
+        long volume = 0, islands = 0;
+        std::vector<long> sizes(1 << 16);
+        int s = dba_size_distribution(ctx, 2, &avg, &volume, &islands, sizes.data(), (long)sizes.size());
+        if (s == DBA_ERR_ARG && islands > (long)sizes.size()) {
+            sizes.resize(islands);
+            s = dba_size_distribution(ctx, 2, &avg, &volume, &islands, sizes.data(), (long)sizes.size());
+        }
+        check(s, "dba_size_distribution");
+        std::ofstream d = open_append("size_dist.txt");
+        for (long i = 0; i < islands; ++i) d << sizes[i] << " ";
+        d << std::endl;
+        std::ofstream r = open_append("avg_radius.txt");
+        r << n_dist++ << "," << std::cbrt(volume * 0.75 / M_PI / islands) << std::endl;
+    };
+    // Extract_Tip (example_Dendritic_growth/Extract_Tip.cpp:68-108): one column per output
+    std::vector<std::string> tip_names;
+    std::vector<std::vector<int>> tip_cols;
+    std::vector<int> tip_max;
+
     if (model == DBA_MODEL_MODELB) {
         check(dba_write_vtk(ctx, "output_0.vtk"), "dba_write_vtk");
+        if (size_dist) droplets();
         std::ofstream o = open_append("Integral.out");
         o << 0 << " " << field_sum(ctx, 0, n) << " " << field_sum(ctx, 1, n) << " " << field_sum(ctx, 2, n) << " "
           << field_sum(ctx, 3, n) << std::endl;
@@ -170,10 +198,19 @@ int main(int argc, char** argv)
             std::ofstream tp = open_append("tip_profile.out");
             for (int ix = k.nx / 2 - 10; ix <= k.nx / 2 + 10; ix++) tp << growth_front(p, k, ix) << " ";
             tp << std::endl;
+            std::string pre = mode ? "output_DBA_" : "output_regular_";
             if (vtk) {
-                std::string pre = mode ? "output_DBA_" : "output_regular_";
                 check(dba_write_vtk(ctx, (pre + std::to_string(t) + ".vtk").c_str()), "dba_write_vtk");
                 if (mode) check(dba_write_active_vtk(ctx, ("Active_" + std::to_string(t) + ".vtk").c_str()), "vtk");
+            }
+            if (tip_prof) {
+                std::vector<int> col(41);
+                int m = 0;
+                check(dba_tip_profile(ctx, 0, 40, col.data(), &m), "dba_tip_profile");
+                tip_names.push_back(pre + std::to_string(t) + ".vtk");
+                tip_cols.push_back(col);
+                tip_max.push_back(m);
+                if (!quiet) std::cout << " Tip at x = " << m << std::endl;
             }
         } else if (model == DBA_MODEL_MODELB) {
             if (k.conserved) {
@@ -190,6 +227,7 @@ int main(int argc, char** argv)
               << field_sum(ctx, 3, n) << std::endl;
             check(dba_write_vtk(ctx, ("output_" + std::to_string(t) + ".vtk").c_str()), "dba_write_vtk");
             if (mode) check(dba_write_active_vtk(ctx, ("Wakeup_" + std::to_string(t) + ".vtk").c_str()), "vtk");
+            if (size_dist) droplets();
         } else {
             check(dba_write_vtk(ctx, ("output_" + std::to_string(k.mode) + "_" + std::to_string(t) + ".vtk").c_str()),
                   "dba_write_vtk");
@@ -211,6 +249,17 @@ int main(int argc, char** argv)
             o << t << " " << obs.vy_mode << std::endl;
         }
         win_start = std::chrono::steady_clock::now();
+    }
+    if (tip_prof && !tip_cols.empty()) {
+        std::ofstream o("Tip_Profile.dat");
+        o << "z ";
+        for (auto& s : tip_names) o << s << " ";
+        o << std::endl;
+        for (int i = 0; i < 41; i++) {
+            o << i << " ";
+            for (size_t c = 0; c < tip_cols.size(); ++c) o << tip_max[c] - tip_cols[c][i] << " ";
+            o << std::endl;
+        }
     }
     double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     if (!quiet) printf("The loop running time is: %f sec.\n", total);

@@ -15,6 +15,7 @@
 #include "k_modelb_tile.cuh"
 #include "k_reduce.cuh"
 #include "k_batch.cuh"
+#include "k_post.cuh"
 
 namespace dba {
 

@@ -115,6 +115,9 @@ def load_library():
             "dba_destroy": (None, [V]),
             "dba_strerror": (ctypes.c_char_p, [_i]),
             "dba_struct_size": (ctypes.c_size_t, [_i]),
+            "dba_tip_profile": (_i, [V, _i, _i, P(_i), P(_i)]),
+            "dba_size_distribution": (_i, [V, _i, P(_d), P(ctypes.c_long), P(ctypes.c_long), P(ctypes.c_long),
+                                           ctypes.c_long]),
             "dba_step_profiled": (_i, [V, _i, _i, P(Prof)]),
             "dba_get_stream": (_i, [V, P(V)]),
             "dba_state_size": (_i, [V, P(ctypes.c_size_t)]),
@@ -208,8 +211,11 @@ class Simulation:
     def sync(self):
         _check(self._L.dba_sync(self._h), "dba_sync")
 
+    def _fid(self, name):
+        return self.fields.index(name) if isinstance(name, str) else int(name)
+
     def field(self, name):
-        fid = self.fields.index(name) if isinstance(name, str) else int(name)
+        fid = self._fid(name)
         out = np.empty(self.n, np.float64)
         _check(self._L.dba_read_field(self._h, fid, out.ctypes.data_as(ctypes.POINTER(_d))), "dba_read_field")
         return out.reshape(self.shape)
@@ -236,6 +242,26 @@ class Simulation:
         return {"step": o.step, "time": o.time, "active_blocks": list(o.active_blocks), "total_blocks": o.total_blocks,
                 "tip": o.tip, "integral": list(o.integral), "vy_mode": o.vy_mode, "cell_updates": o.cell_updates,
                 "dt": o.dt}
+
+    def tip_profile(self, dz=40, field=0):
+        """Extract_Tip on the device: (tip_x[0..dz], tip_x_max) for planes Nz/2 .. Nz/2+dz."""
+        tip = np.zeros(dz + 1, np.int32)
+        m = _i()
+        _check(self._L.dba_tip_profile(self._h, int(self._fid(field)), int(dz),
+                                       tip.ctypes.data_as(ctypes.POINTER(_i)), ctypes.byref(m)), "dba_tip_profile")
+        return tip, m.value
+
+    def size_distribution(self, field, max_sizes=1 << 16):
+        """coarsening_analysis on the device: (avg, volume, island sizes in scan order)."""
+        fid = int(self._fid(field))
+        avg, vol, nis = _d(), ctypes.c_long(), ctypes.c_long()
+        sizes = np.zeros(max(1, max_sizes), np.int64)
+        st = self._L.dba_size_distribution(self._h, fid, ctypes.byref(avg), ctypes.byref(vol), ctypes.byref(nis),
+                                           sizes.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), int(max_sizes))
+        if st == 8 and nis.value > max_sizes:       # too many islands for the buffer: retry once, sized
+            return self.size_distribution(field, int(nis.value))
+        _check(st, "dba_size_distribution")
+        return avg.value, vol.value, sizes[:nis.value].copy()
 
     def step_profiled(self, n, mode=1):
         p = Prof()

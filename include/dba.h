@@ -289,6 +289,25 @@ void dba_batch_destroy(dba_batch* b);
  * the array: calls that overlap on the GPU race.  Asynchronous on `stream`. */
 #define DBA_NOALLOC_MAX_BLOCKS (1 << 20)
 #define DBA_NOALLOC_MAX_FIELDS 4
+/* ---- on-device post-processing (the reference's separate analysis tools, run on
+   the resident field instead of re-reading ASCII VTK files) ---- */
+
+/* Extract_Tip (example_Dendritic_growth/Extract_Tip.cpp:68-87) on state field `field`:
+   for z = Nz/2 + k, k = 0..dz, tip_x[k] = the largest x with value > 0.5 in plane z
+   (0 if none, or if the plane is beyond the grid); *tip_x_max = max over k.  The
+   tool's Tip_Profile.dat column is tip_x_max - tip_x[k]. */
+int dba_tip_profile(dba_ctx* ctx, int field, int dz, int* tip_x, int* tip_x_max);
+
+/* coarsening_analysis (example_Reactive_ModelB/coarsening_analysis.cpp:46-165) of state
+   field `field`: avg = (max(0.5, max f) + min(0.5, min f)) / 2; *volume = cells with
+   f > avg; islands = periodic 6-connected components grown from cells with f > avg
+   through cells with f >= avg; sizes[k] = cells of island k, islands ordered by their
+   first f > avg cell in x-fastest order (the tool's scan order).  max_sizes = 0 only
+   counts; returns DBA_ERR_ARG (with *islands set) when max_sizes is too small, and
+   DBA_ERR_TIMEOUT through dba_sync if the bounded union loop ever gives up. */
+int dba_size_distribution(dba_ctx* ctx, int field, double* avg, long* volume, long* islands, long* sizes,
+                          long max_sizes);
+
 int dba_mean_change_noalloc(const double* block_sums, int nb, int nfields, double ncells, double* mean_out,
                             void* stream);
 

@@ -828,4 +828,74 @@ void oracle_kh_get_flags(void* h, int* wake, int* next)
 }
 void oracle_kh_free(void* h) { delete (KH*)h; }
 
+// ---- post-processing tools -------------------------------------------------
+
+// Extract_Tip (example_Dendritic_growth/Extract_Tip.cpp:68-87): per z-plane of
+// [Nz/2, Nz/2 + dz] the largest x with value > 0.5 (0 if none; planes past the
+// grid stay 0), and their maximum
+void oracle_tip_profile(const double* f, int nx, int ny, int nz, int dz, int* tip_x, int* tip_x_max)
+{
+    for (int k = 0; k <= dz; ++k) tip_x[k] = 0;
+    for (int z = 0; z < nz; ++z) {
+        if (z < nz / 2 || z > nz / 2 + dz) continue;
+        int tip_loc = 0;
+        for (int y = 0; y < ny; ++y)
+            for (int x = 0; x < nx; ++x)
+                if (f[(size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * z)] > 0.5) tip_loc = std::max(tip_loc, x);
+        tip_x[z - nz / 2] = tip_loc;
+    }
+    int m = 0;
+    for (int k = 0; k <= dz; ++k) m = std::max(m, tip_x[k]);
+    *tip_x_max = m;
+}
+
+// coarsening_analysis (example_Reactive_ModelB/coarsening_analysis.cpp:46-165):
+// threshold from the extremes with 0.5 as the starting max and min, volume
+// above it, islands by flood fill in the tool's scan order (x fastest), grown
+// through cells >= avg with periodic 6-neighbours (an explicit stack and a
+// visited mask in place of the tool's recursion and zeroing).  Returns the
+// island count; sizes holds the first `cap` island sizes.
+long oracle_size_distribution(const double* f, int nx, int ny, int nz, double* avg_out, long* volume_out, long* sizes,
+                              long cap)
+{
+    const size_t n = (size_t)nx * ny * nz;
+    double Max = 0.5, Min = 0.5;
+    for (size_t i = 0; i < n; ++i) {
+        if (f[i] > Max) Max = f[i];
+        if (f[i] < Min) Min = f[i];
+    }
+    const double avg = (Max + Min) / 2.;
+    long volume = 0;
+    for (size_t i = 0; i < n; ++i) volume += f[i] > avg ? 1 : 0;
+    std::vector<unsigned char> seen(n, 0);
+    std::vector<size_t> stack;
+    long islands = 0;
+    for (size_t i = 0; i < n; ++i) {
+        if (!(f[i] > avg) || seen[i]) continue;
+        long size = 0;
+        stack.assign(1, i);
+        while (!stack.empty()) {
+            const size_t c = stack.back();
+            stack.pop_back();
+            if (seen[c] || f[c] < avg) continue;
+            seen[c] = 1;
+            ++size;
+            const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((size_t)nx * ny));
+            const int xs[2] = {x == 0 ? nx - 1 : x - 1, x == nx - 1 ? 0 : x + 1};
+            const int ys[2] = {y == 0 ? ny - 1 : y - 1, y == ny - 1 ? 0 : y + 1};
+            const int zs[2] = {z == 0 ? nz - 1 : z - 1, z == nz - 1 ? 0 : z + 1};
+            for (int k = 0; k < 2; ++k) {
+                stack.push_back((size_t)xs[k] + (size_t)nx * ((size_t)y + (size_t)ny * z));
+                stack.push_back((size_t)x + (size_t)nx * ((size_t)ys[k] + (size_t)ny * z));
+                stack.push_back((size_t)x + (size_t)nx * ((size_t)y + (size_t)ny * zs[k]));
+            }
+        }
+        if (islands < cap) sizes[islands] = size;
+        ++islands;
+    }
+    *avg_out = avg;
+    *volume_out = volume;
+    return islands;
+}
+
 }  // extern "C"

@@ -32,6 +32,11 @@ def lib():
             "oracle_dendrite_step": (None, [vp, ctypes.c_int, ctypes.c_int]),
             "oracle_dendrite_get": (None, [vp, _D, _D, _I, _I, _I, _I]),
             "oracle_dendrite_tip": (ctypes.c_double, [vp]),
+            "oracle_tip_profile": (None, [_D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _I,
+                                          ctypes.POINTER(ctypes.c_int)]),
+            "oracle_size_distribution": (ctypes.c_long, [_D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D,
+                                                         ctypes.POINTER(ctypes.c_long), ctypes.POINTER(ctypes.c_long),
+                                                         ctypes.c_long]),
             "oracle_dendrite_free": (None, [vp]),
             "oracle_modelb_new": (vp, [ctypes.c_int] * 5 + [_D, ctypes.c_int, ctypes.c_int]),
             "oracle_modelb_init_uniform": (None, [vp, _D, _D, _D, ctypes.c_double, ctypes.c_double]),
@@ -184,3 +189,25 @@ class OracleKH:
         if getattr(self, "h", None):
             lib().oracle_kh_free(self.h)
             self.h = None
+
+
+def tip_profile(f, dz=40):
+    """Extract_Tip restated (oracle): f is (nz, ny, nx)."""
+    nz, ny, nx = f.shape
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    tip = np.zeros(dz + 1, np.int32)
+    m = ctypes.c_int()
+    lib().oracle_tip_profile(dptr(f), nx, ny, nz, dz, iptr(tip), ctypes.byref(m))
+    return tip, m.value
+
+
+def size_distribution(f, cap=1 << 20):
+    """coarsening_analysis restated (oracle): (avg, volume, island sizes in scan order)."""
+    nz, ny, nx = f.shape
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    sizes = np.zeros(cap, np.int64)
+    avg = ctypes.c_double()
+    vol = ctypes.c_long()
+    n = lib().oracle_size_distribution(dptr(f), nx, ny, nz, ctypes.byref(avg), ctypes.byref(vol),
+                                       sizes.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), cap)
+    return avg.value, vol.value, sizes[:min(n, cap)].copy()

@@ -72,3 +72,34 @@ def test_kh_outputs(tmp_path):
 def test_missing_input_exits_1(tmp_path):
     r = subprocess.run([BIN, "kh"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
     assert r.returncode == 1
+
+
+def test_modelb_size_distribution_outputs(tmp_path):
+    """--size-dist: coarsening_analysis's size_dist.txt and avg_radius.txt, from the device field,
+    matching the restated tool on the z field of the same run."""
+    import oracle_lib as ol
+    text = ("64 64 1\n3000 1500 0.001\n1 1 1\n0 0 0 0 0 3\n1 1 2\n1 1 2\n1 1\n1 1 1 0.01\n1 1 1 1\n"
+            "0.05 0.05 0.45\n100 0.4 1\n1e-4\n1e-3\n1\nnoise_amp = 0.02\nnoise_amp_z = 0.02\n")
+    d = run(tmp_path, "modelb", text, "--size-dist")
+    radius = open(d / "avg_radius.txt").read().splitlines()
+    assert [r.split(",")[0] for r in radius] == ["0", "1", "2"]
+    dist = open(d / "size_dist.txt").read().splitlines()
+    assert len(dist) == 3
+    import dba_b200
+    cfg = dba_b200.parse_input(d / "Input.txt", "modelb")
+    sim = dba_b200.Simulation(cfg).init()
+    sim.step(3000, cfg.mode)
+    avg, vol, sizes = ol.size_distribution(sim.field("z"))
+    assert len(sizes) > 0
+    assert [int(v) for v in dist[2].split()] == sizes.tolist()
+    assert float(radius[2].split(",")[1]) == pytest.approx(np.cbrt(vol * 0.75 / np.pi / len(sizes)), rel=1e-5)
+
+
+def test_dendrite_tip_profile_output(tmp_path):
+    """--tip-profile: Extract_Tip's Tip_Profile.dat (one column per output time)."""
+    d = run(tmp_path, "dendrite", "32 32 48\n200 100 0.00005\n0.02 0.02 0.02\n0.5 0.0003 0.01 0.9 40.\n0.25\n1\n0.01\n1e-5\n",
+            "--tip-profile")
+    lines = open(d / "Tip_Profile.dat").read().splitlines()
+    assert lines[0].split() == ["z", "output_DBA_100.vtk", "output_DBA_200.vtk"]
+    assert len(lines) == 42 and [l.split()[0] for l in lines[1:]] == [str(i) for i in range(41)]
+    assert all(len(l.split()) == 3 for l in lines[1:])
