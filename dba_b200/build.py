@@ -62,12 +62,13 @@ def build(verbose=False, jobs=4):
     io_obj = os.path.join(BUILD, "io.o")
     objs.append(io_obj)
     if _newer(io_obj, [io_src] + hdrs):
-        procs.append(subprocess.Popen([CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-c", io_src, "-o", io_obj]))
+        procs.append(subprocess.Popen([CXX, "-O2", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-c", io_src,
+                                       "-o", io_obj]))
     bad = [p for p in procs if p.wait() != 0]
     if bad:
         raise RuntimeError("compilation failed")
     if _newer(LIB, objs):
-        _run([NVCC] + GENCODE + ["-shared", "-o", LIB] + objs + ["-lcudart"], verbose)
+        _run([NVCC] + GENCODE + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"], verbose)
     run_src = os.path.join(CSRC, "dba_run.cpp")
     if os.path.exists(run_src) and _newer(BIN, [run_src, LIB]):
         _run([CXX, "-O2", "-std=c++17", run_src, "-o", BIN, "-L" + HERE, "-ldba_b200",

@@ -639,6 +639,7 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
 void dba_destroy(dba_ctx* c)
 {
     if (!c) return;
+    dba_wait_io(c);   // background VTR writers hold only snapshots, but report into this context's status
     if (c->st) cudaStreamSynchronize(c->st);
     for (auto& row : c->graphs)
         for (auto& gexec : row)

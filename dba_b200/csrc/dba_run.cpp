@@ -96,7 +96,8 @@ double field_sum(dba_ctx* ctx, int field, size_t n)
 int main(int argc, char** argv)
 {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: %s dendrite|modelb|kh [Input.txt] [--vtk] [--quiet] [--tip-profile] [--size-dist]\n",
+        std::fprintf(stderr,
+                     "usage: %s dendrite|modelb|kh [Input.txt] [--vtk] [--quiet] [--tip-profile] [--size-dist] [--vtr[=N]]\n",
                      argv[0]);
         return 2;
     }
@@ -109,12 +110,14 @@ int main(int argc, char** argv)
     }
     std::string input = "Input.txt";
     bool vtk = false, tip_prof = false, size_dist = false;
+    int vtr = 0;   // pieces of a binary .vtr / .pvtr written in the background at every output (0: none)
     for (int a = 2; a < argc; ++a) {
         std::string s = argv[a];
         if (s == "--vtk") vtk = true;
         else if (s == "--quiet") quiet = true;
         else if (s == "--tip-profile") tip_prof = true;   // Extract_Tip on the device at every output
         else if (s == "--size-dist") size_dist = true;    // coarsening_analysis on the device at every output
+        else if (s.rfind("--vtr", 0) == 0) vtr = s.size() > 6 ? std::max(1, std::atoi(s.c_str() + 6)) : 1;
         else input = s;
     }
     dba_config k;
@@ -248,8 +251,11 @@ int main(int argc, char** argv)
             std::ofstream o = open_append("VY_mode.out");
             o << t << " " << obs.vy_mode << std::endl;
         }
+        if (vtr) check(dba_write_vtr(ctx, ("output_" + std::to_string(t)).c_str(), vtr, DBA_VTR_BINARY | DBA_VTR_ASYNC),
+                       "dba_write_vtr");
         win_start = std::chrono::steady_clock::now();
     }
+    check(dba_wait_io(ctx), "dba_wait_io");
     if (tip_prof && !tip_cols.empty()) {
         std::ofstream o("Tip_Profile.dat");
         o << "z ";

@@ -8,6 +8,11 @@
 #include <string>
 #include <vector>
 
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+
 #include "../../include/dba.h"
 
 namespace {
@@ -215,6 +220,241 @@ int dba_write_active_vtk(dba_ctx* ctx, const char* path)
     if (k.model != DBA_MODEL_DENDRITE) o << std::endl;
     o.close();
     return o.fail() ? DBA_ERR_IO : DBA_OK;
+}
+
+}  // extern "C"
+
+
+// ---------------------------------------------------------------------------
+// VTK XML RectilinearGrid output (.vtr, and a .pvtr index of y-slab pieces), as
+// the reference's CUDA-MPI writers (example_Dendritic_growth/CUDA-MPI/
+// dendrite_kernels.cu:875-1060: Float32 fields, Int8 per-cell activity, one
+// piece per y slab).  ASCII like the reference, or appended raw binary; the file
+// can be formatted and written on a background thread from a host snapshot
+// while the GPU keeps stepping (dba_wait_io joins those writers).
+namespace {
+
+struct VtrJob {
+    dba_config k;
+    std::string base;
+    int pieces = 1, flags = 0;
+    std::vector<std::string> names;          // point fields
+    std::vector<std::vector<float>> fields;  // x-fastest, whole grid
+    std::vector<std::string> act_names;      // per-cell activity of each channel
+    std::vector<std::vector<int8_t>> act;
+};
+
+std::mutex g_io_mutex;
+std::map<const dba_ctx*, std::vector<std::thread>> g_writers;
+std::map<const dba_ctx*, int> g_io_status;
+
+void y_slab(int ny, int pieces, int r, int& y0, int& y1)   // rows [y0, y1] of piece r
+{
+    const int lo = ny / pieces, extra = ny % pieces;
+    y0 = r * lo + std::min(r, extra);
+    y1 = y0 + lo + (r < extra ? 1 : 0) - 1;
+}
+
+int write_piece(const VtrJob& j, const std::string& path, int y0, int y1)
+{
+    const dba_config& k = j.k;
+    const bool bin = (j.flags & DBA_VTR_BINARY) != 0;
+    // a piece shares the boundary row with the next one, as the reference's pieces do
+    const int ye = std::min(y1 + 1, k.ny - 1);
+    std::ofstream o(path, std::ios::binary);
+    if (!o.is_open()) return DBA_ERR_IO;
+    const size_t nxz = (size_t)k.nx, rows = (size_t)(ye - y0 + 1), nz = (size_t)k.nz;
+    const size_t npt = nxz * rows * nz;
+    o << "<VTKFile type=\"RectilinearGrid\" version=\"2.0\" byte_order=\"LittleEndian\" header_type=\"UInt64\">\n";
+    o << "<RectilinearGrid WholeExtent=\"0 " << k.nx - 1 << " " << y0 << " " << ye << " 0 " << k.nz - 1 << "\">\n";
+    o << "<Piece Extent=\"0 " << k.nx - 1 << " " << y0 << " " << ye << " 0 " << k.nz - 1 << "\">\n";
+    o << "<PointData>\n";
+    unsigned long long offset = 0;
+    auto head = [&](const char* type, const std::string& name, size_t bytes) {
+        o << "<DataArray type=\"" << type << "\" Name=\"" << name << "\" format=\"" << (bin ? "appended" : "ascii") << "\"";
+        if (bin) {
+            o << " offset=\"" << offset << "\"/>\n";
+            offset += 8 + bytes;
+        } else {
+            o << ">\n";
+        }
+    };
+    auto cell = [&](size_t x, size_t y, size_t z) { return x + (size_t)k.nx * ((size_t)y + (size_t)k.ny * z); };
+    for (size_t f = 0; f < j.fields.size(); ++f) {
+        head("Float32", j.names[f], npt * sizeof(float));
+        if (!bin) {
+            for (size_t z = 0; z < nz; ++z)
+                for (int y = y0; y <= ye; ++y)
+                    for (size_t x = 0; x < nxz; ++x) o << j.fields[f][cell(x, y, z)] << " ";
+            o << "\n</DataArray>\n";
+        }
+    }
+    for (size_t f = 0; f < j.act.size(); ++f) {
+        head("Int8", j.act_names[f], npt);
+        if (!bin) {
+            for (size_t z = 0; z < nz; ++z)
+                for (int y = y0; y <= ye; ++y)
+                    for (size_t x = 0; x < nxz; ++x) o << (int)j.act[f][cell(x, y, z)] << " ";
+            o << "\n</DataArray>\n";
+        }
+    }
+    o << "</PointData>\n<CellData>\n</CellData>\n<Coordinates>\n";
+    const char* axis[3] = {"x", "y", "z"};
+    const int lo[3] = {0, y0, 0}, hi[3] = {k.nx - 1, ye, k.nz - 1};
+    for (int a = 0; a < 3; ++a) {
+        const size_t m = (size_t)(hi[a] - lo[a] + 1);
+        head("Float32", std::string("Array ") + axis[a], m * sizeof(float));
+        if (!bin) {
+            for (int v = lo[a]; v <= hi[a]; ++v) o << v << " ";
+            o << "\n</DataArray>\n";
+        }
+    }
+    o << "</Coordinates>\n</Piece>\n</RectilinearGrid>\n";
+    if (bin) {
+        o << "<AppendedData encoding=\"raw\">\n_";
+        auto block = [&](const void* p, unsigned long long bytes) {
+            o.write(reinterpret_cast<const char*>(&bytes), sizeof bytes);
+            o.write(reinterpret_cast<const char*>(p), (std::streamsize)bytes);
+        };
+        std::vector<float> buf(npt);
+        std::vector<int8_t> bb(npt);
+        for (const auto& fv : j.fields) {
+            size_t q = 0;
+            for (size_t z = 0; z < nz; ++z)
+                for (int y = y0; y <= ye; ++y)
+                    for (size_t x = 0; x < nxz; ++x) buf[q++] = fv[cell(x, y, z)];
+            block(buf.data(), npt * sizeof(float));
+        }
+        for (const auto& av : j.act) {
+            size_t q = 0;
+            for (size_t z = 0; z < nz; ++z)
+                for (int y = y0; y <= ye; ++y)
+                    for (size_t x = 0; x < nxz; ++x) bb[q++] = av[cell(x, y, z)];
+            block(bb.data(), npt);
+        }
+        for (int a = 0; a < 3; ++a) {
+            std::vector<float> c;
+            for (int v = lo[a]; v <= hi[a]; ++v) c.push_back((float)v);
+            block(c.data(), c.size() * sizeof(float));
+        }
+        o << "\n</AppendedData>\n";
+    }
+    o << "</VTKFile>\n";
+    return o.good() ? DBA_OK : DBA_ERR_IO;
+}
+
+int write_job(const VtrJob& j)
+{
+    if (j.pieces <= 1) return write_piece(j, j.base + ".vtr", 0, j.k.ny - 1);
+    // write_output_pvtr (dendrite_kernels.cu:875-925): the index of the pieces
+    std::ofstream o(j.base + ".pvtr");
+    if (!o.is_open()) return DBA_ERR_IO;
+    const dba_config& k = j.k;
+    o << "<VTKFile type=\"PRectilinearGrid\" version=\"2.0\" byte_order=\"LittleEndian\" header_type=\"UInt64\">\n";
+    o << "<PRectilinearGrid WholeExtent=\"0 " << k.nx - 1 << " 0 " << k.ny - 1 << " 0 " << k.nz - 1 << "\" GhostLevel=\"0\">\n";
+    o << "<PPointData>\n";
+    for (auto& nm : j.names) o << "<PDataArray type=\"Float32\" Name=\"" << nm << "\"/>\n";
+    for (auto& nm : j.act_names) o << "<PDataArray type=\"Int8\" Name=\"" << nm << "\"/>\n";
+    o << "</PPointData>\n<PCoordinates>\n";
+    for (int a = 0; a < 3; ++a) o << "<PDataArray type=\"Float32\"/>\n";
+    o << "</PCoordinates>\n";
+    std::string stem = j.base;
+    const size_t slash = stem.find_last_of('/');
+    if (slash != std::string::npos) stem = stem.substr(slash + 1);
+    int st = DBA_OK;
+    for (int r = 0; r < j.pieces; ++r) {
+        int y0, y1;
+        y_slab(k.ny, j.pieces, r, y0, y1);
+        const int ye = std::min(y1 + 1, k.ny - 1);
+        o << "<Piece Extent=\"0 " << k.nx - 1 << " " << y0 << " " << ye << " 0 " << k.nz - 1 << "\" Source=\"" << stem << "_"
+          << r << ".vtr\"/>\n";
+        const int s = write_piece(j, j.base + "_" + std::to_string(r) + ".vtr", y0, y1);
+        if (s && !st) st = s;
+    }
+    o << "</PRectilinearGrid>\n</VTKFile>\n";
+    return o.good() ? st : DBA_ERR_IO;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dba_wait_io(dba_ctx* ctx)
+{
+    std::vector<std::thread> ws;
+    {
+        std::lock_guard<std::mutex> g(g_io_mutex);
+        auto it = g_writers.find(ctx);
+        if (it != g_writers.end()) {
+            ws.swap(it->second);
+            g_writers.erase(it);
+        }
+    }
+    for (auto& w : ws) w.join();
+    std::lock_guard<std::mutex> g(g_io_mutex);
+    auto it = g_io_status.find(ctx);
+    int st = DBA_OK;
+    if (it != g_io_status.end()) {
+        st = it->second;
+        g_io_status.erase(it);
+    }
+    return st;
+}
+
+int dba_write_vtr(dba_ctx* ctx, const char* base, int pieces, int flags)
+{
+    if (!ctx || !base || pieces < 1) return DBA_ERR_ARG;
+    auto j = std::make_shared<VtrJob>();
+    int st = dba_get_config(ctx, &j->k);
+    if (st) return st;
+    dba_info info;
+    if ((st = dba_get_info(ctx, &info))) return st;
+    if (pieces > j->k.ny) return DBA_ERR_ARG;
+    j->base = base;
+    j->pieces = pieces;
+    j->flags = flags;
+    const dba_config& k = j->k;
+    const size_t n = (size_t)k.nx * k.ny * k.nz;
+    std::vector<double> a(n);
+    auto take = [&](int id, const char* name) -> int {
+        int s = dba_read_field(ctx, id, a.data());
+        if (s) return s;
+        j->names.push_back(name);
+        j->fields.emplace_back(a.begin(), a.end());
+        return DBA_OK;
+    };
+    if (k.model == DBA_MODEL_DENDRITE) {
+        if ((st = take(0, "phi")) || (st = take(1, "T"))) return st;
+    } else if (k.model == DBA_MODEL_MODELB) {
+        if ((st = take(0, "X")) || (st = take(1, "Y")) || (st = take(2, "Z")) || (st = take(3, "B"))) return st;
+    } else {
+        if ((st = take(4, "rho")) || (st = take(5, "p")) || (st = take(6, "vx")) || (st = take(7, "vy"))) return st;
+    }
+    // per-cell activity of the next step, per channel (the reference's active_phi / active_T)
+    const char* cn[2] = {k.model == DBA_MODEL_DENDRITE ? "active_phi" : "active", "active_T"};
+    for (int ch = 0; ch < info.nchannels; ++ch) {
+        std::vector<int32_t> fl(info.nb);
+        if ((st = dba_read_flags(ctx, 2 * ch, fl.data()))) return st;
+        const int B = k.block;
+        std::vector<int8_t> cellw(n);
+        for (int z = 0; z < k.nz; ++z)
+            for (int y = 0; y < k.ny; ++y)
+                for (int x = 0; x < k.nx; ++x)
+                    cellw[(size_t)x + (size_t)k.nx * ((size_t)y + (size_t)k.ny * z)] =
+                        (int8_t)(fl[x / B + info.nbx * (y / B + info.nby * (z / B))] ? 1 : 0);
+        j->act_names.push_back(cn[ch]);
+        j->act.push_back(std::move(cellw));
+    }
+    if (!(flags & DBA_VTR_ASYNC)) return write_job(*j);
+    std::lock_guard<std::mutex> g(g_io_mutex);
+    g_writers[ctx].emplace_back([ctx, j]() {
+        const int s = write_job(*j);
+        if (s) {
+            std::lock_guard<std::mutex> g2(g_io_mutex);
+            if (!g_io_status[ctx]) g_io_status[ctx] = s;
+        }
+    });
+    return DBA_OK;
 }
 
 }  // extern "C"

@@ -116,6 +116,8 @@ def load_library():
             "dba_strerror": (ctypes.c_char_p, [_i]),
             "dba_struct_size": (ctypes.c_size_t, [_i]),
             "dba_tip_profile": (_i, [V, _i, _i, P(_i), P(_i)]),
+            "dba_write_vtr": (_i, [V, ctypes.c_char_p, _i, _i]),
+            "dba_wait_io": (_i, [V]),
             "dba_size_distribution": (_i, [V, _i, P(_d), P(ctypes.c_long), P(ctypes.c_long), P(ctypes.c_long),
                                            ctypes.c_long]),
             "dba_step_profiled": (_i, [V, _i, _i, P(Prof)]),
@@ -242,6 +244,15 @@ class Simulation:
         return {"step": o.step, "time": o.time, "active_blocks": list(o.active_blocks), "total_blocks": o.total_blocks,
                 "tip": o.tip, "integral": list(o.integral), "vy_mode": o.vy_mode, "cell_updates": o.cell_updates,
                 "dt": o.dt}
+
+    def write_vtr(self, base, pieces=1, binary=True, background=False):
+        """VTK XML RectilinearGrid output: <base>.vtr, or <base>_<r>.vtr pieces and <base>.pvtr."""
+        flags = (1 if binary else 0) | (2 if background else 0)
+        _check(self._L.dba_write_vtr(self._h, str(base).encode(), int(pieces), flags), "dba_write_vtr")
+
+    def wait_io(self):
+        """Join background writers; raises the first write error."""
+        _check(self._L.dba_wait_io(self._h), "dba_wait_io")
 
     def tip_profile(self, dz=40, field=0):
         """Extract_Tip on the device: (tip_x[0..dz], tip_x_max) for planes Nz/2 .. Nz/2+dz."""

@@ -289,6 +289,20 @@ void dba_batch_destroy(dba_batch* b);
  * the array: calls that overlap on the GPU race.  Asynchronous on `stream`. */
 #define DBA_NOALLOC_MAX_BLOCKS (1 << 20)
 #define DBA_NOALLOC_MAX_FIELDS 4
+/* ---- VTK XML RectilinearGrid output (the reference's CUDA-MPI write_output_vtr /
+   write_output_pvtr, example_Dendritic_growth/CUDA-MPI/dendrite_kernels.cu:875-1060) ----
+   Writes <base>.vtr, or with pieces > 1 <base>_<r>.vtr for r < pieces (y slabs that
+   share their boundary row) and the index <base>.pvtr.  Fields as Float32 (dendrite
+   phi, T; Model B X, Y, Z, B; KH rho, p, vx, vy) and the next step's activity per
+   cell as Int8 (active_phi / active_T, or active).  DBA_VTR_BINARY: appended raw
+   data instead of ASCII.  DBA_VTR_ASYNC: the fields are read now and the files are
+   formatted and written by a background thread; dba_wait_io joins the context's
+   writers and returns the first write error (dba_destroy waits too). */
+#define DBA_VTR_BINARY 1
+#define DBA_VTR_ASYNC 2
+int dba_write_vtr(dba_ctx* ctx, const char* base, int pieces, int flags);
+int dba_wait_io(dba_ctx* ctx);
+
 /* ---- on-device post-processing (the reference's separate analysis tools, run on
    the resident field instead of re-reading ASCII VTK files) ---- */
 
