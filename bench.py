@@ -14,7 +14,10 @@ Multi-GPU: the path does not shard in this build (one domain per GPU), so
 `--gpus N` runs N independent replicas, one process per GPU, and `value` is the
 sum of their active cell-updates divided by the slowest rank's time.
 
-At N=1 the line also carries `sweep`: the batched/served 2-D dendrite
+At N=1 the line also carries `full_runs_dba_vs_regular`: the dendrite workloads
+(512^2 FP64, 10 000 steps; 512^3 FP32, 20 000 steps) run to their end time in
+DBA and in regular mode, with total wall times (`--no-full-runs` skips it), and
+`sweep`: the batched/served 2-D dendrite
 parameter sweep (256 seeded requests, Poisson arrivals, admission by device
 memory, autotuned block edge and threads) against the same requests run one at
 a time -- runs/s of both and p50/p99 time to completion (`--no-sweep` skips it).
@@ -312,6 +315,8 @@ def run_ours(args, w):
             result["cpu_baseline"] = cpu_baseline(w, seconds=args.cpu_seconds)
         if world == 1 and not args.no_sweep:
             result["sweep"] = run_sweep(args)
+        if world == 1 and not args.no_full_runs:
+            result["full_runs_dba_vs_regular"] = run_full_runs(args)
     sim.close()
     if world > 1:
         dist.barrier()
@@ -413,6 +418,39 @@ def run_sweep(args):
     }
 
 
+def run_full_runs(args):
+    """DBA against the all-blocks regular mode over whole runs of the dendrite workloads:
+    each advanced from its initial state to its end time in both modes (captured graphs,
+    CUDA events on the engine's stream), with the tip and active fraction at the end."""
+    import torch
+    import dba_b200
+
+    out = {}
+    for name in ("dendrite_512_fp64", "dendrite3d_512_fp32"):
+        w = WORKLOADS[name]
+        row = {"steps": w["t_total"], "grid": [w["nx"], w["ny"], w["nz"]], "dtype": "f32" if w["precision"] else "f64"}
+        for mode, key in ((1, "dba"), (0, "regular")):
+            sim = dba_b200.Simulation(make_config(w)).init()
+            stream = torch.cuda.ExternalStream(sim.stream)
+            sim.step(48, mode)        # captures the step graph (every 48-step launch from step 0 reuses it)
+            sim.sync()
+            sim.init()                # back to the initial state; the graph stays valid
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            c0 = sim.cell_updates()
+            e0.record(stream)
+            sim.step(w["t_total"], mode)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            row[key + "_s"] = e0.elapsed_time(e1) / 1e3
+            row[key + "_mean_active_fraction"] = (sim.cell_updates() - c0) / (w["t_total"] * sim.n)
+            row[key + "_tip"] = sim.tip()
+            sim.close()
+        row["dba_speedup"] = row["regular_s"] / row["dba_s"] if row["dba_s"] else None
+        out[name] = row
+    return out
+
+
 def run_reference(args, w):
     world, rank, local = dist_setup()
     if rank != 0:
@@ -438,6 +476,18 @@ def run_reference(args, w):
     }
 
 
+def _finite(v):
+    """The JSON line with non-finite numbers (a tip past the domain, say) as null."""
+    import math
+    if isinstance(v, dict):
+        return {k: _finite(x) for k, x in v.items()}
+    if isinstance(v, (list, tuple)):
+        return [_finite(x) for x in v]
+    if isinstance(v, float) and not math.isfinite(v):
+        return None
+    return v
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -449,6 +499,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sweep", action="store_true", help="skip the batched dendrite sweep section")
+    ap.add_argument("--no-full-runs", action="store_true",
+                    help="skip the whole-run DBA-vs-regular comparison of the dendrite workloads")
     ap.add_argument("--sweep-requests", type=int, default=256)
     ap.add_argument("--sweep-rate", type=float, default=200.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--sweep-seed", type=int, default=0)
@@ -465,7 +517,7 @@ def main():
     else:
         res = run_ours(args, w)
     if res is not None:
-        print(json.dumps(res), flush=True)
+        print(json.dumps(_finite(res)), flush=True)
 
 
 if __name__ == "__main__":
