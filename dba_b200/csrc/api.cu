@@ -350,7 +350,7 @@ void ic_dendrite(const dba_config& k, std::vector<double>& out)
                     double cx = k.ic_corner ? 0.0 : k.nx / 2, cy = k.ic_corner ? 0.0 : k.ny / 2;
                     double cz = k.ic_corner ? 0.0 : k.nz / 2;
                     double r = std::sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy) + (k.nz > 1 ? (z - cz) * (z - cz) : 0.0));
-                    p[i] = 0.5 * (1.0 - std::tanh((r - k.ic_radius) / k.ic_width));
+                    p[i] = 0.5 * (1.0 - dba_tanh((r - k.ic_radius) / k.ic_width));
                 } else {   // reference cone seed (example_Dendritic_growth/kernel.cu:170-174)
                     int dx = x - k.nx / 2, dy = y - k.ny / 2, dz = z - k.nz / 2;
                     double dist = std::sqrt((double)(dx * dx + dy * dy + dz * dz));

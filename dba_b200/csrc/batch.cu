@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/dba.h"
+#include "fpmath.h"
 #include "launch.h"
 
 using namespace dba;
@@ -78,6 +79,41 @@ int cuda_status(cudaError_t e) { return e == cudaSuccess ? DBA_OK : (e == cudaEr
     } while (0)
 
 }  // namespace
+
+// seed of a new slot (dba_init's rules for a 2-D dendrite, api.cu ic_dendrite):
+// tanh seed or the reference cone (example_Dendritic_growth/kernel.cu:170-174),
+// T = -Delta.  This file is built with -fmad=false and tanh comes from the
+// shared fpmath.h, so the values equal the host's bit for bit.
+struct SeedP {
+    int nx, ny, tanh_seed;
+    double cx, cy, radius, width, Delta;
+};
+
+template <typename R>
+__global__ void slot_seed_kernel(R* p, R* T, SeedP s)
+{
+    const size_t n = (size_t)s.nx * s.ny;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % s.nx), y = (int)(i / s.nx);
+        double pv;
+        if (s.tanh_seed) {
+            const double r = sqrt((x - s.cx) * (x - s.cx) + (y - s.cy) * (y - s.cy));
+            pv = 0.5 * (1.0 - dba_tanh((r - s.radius) / s.width));
+        } else {
+            const int dx = x - s.nx / 2, dy = y - s.ny / 2;
+            const double dist = sqrt((double)(dx * dx + dy * dy));
+            pv = dist <= 5 ? (1. - 0.2 * dist) : 0;
+        }
+        p[i] = (R)pv;
+        T[i] = (R)(-s.Delta);
+    }
+}
+
+__global__ void fill_int_kernel(int* a, int n, int v)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
 
 struct dba_batch {
     dba_batch_config cfg;
@@ -234,27 +270,6 @@ int dba_batch_add(dba_batch* b, const dba_config* k, const double* ic, int* slot
         b->cells.give(coff, n);
         return DBA_ERR_NOMEM;
     }
-    // initial condition (FP64 host): the single-domain engine's dba_init rules
-    std::vector<double> p(n), T(n);
-    if (ic) {
-        std::memcpy(p.data(), ic, n * 8);
-        std::memcpy(T.data(), ic + n, n * 8);
-    } else {
-        for (int y = 0; y < k->ny; ++y)
-            for (int x = 0; x < k->nx; ++x) {
-                size_t i = (size_t)x + (size_t)k->nx * y;
-                if (k->ic == DBA_IC_TANH_SEED) {
-                    double cx = k->ic_corner ? 0.0 : k->nx / 2, cy = k->ic_corner ? 0.0 : k->ny / 2;
-                    double r = std::sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy));
-                    p[i] = 0.5 * (1.0 - std::tanh((r - k->ic_radius) / k->ic_width));
-                } else {
-                    int dx = x - k->nx / 2, dy = y - k->ny / 2, dz = 0 - k->nz / 2;
-                    double dist = std::sqrt((double)(dx * dx + dy * dy + dz * dz));
-                    p[i] = dist <= 5 ? (1. - 0.2 * dist) : 0;
-                }
-                T[i] = -k->Delta;
-            }
-    }
     const size_t cap = b->cfg.cell_capacity;
     unsigned char* base = (unsigned char*)b->arena;
     SlotRec r{};
@@ -267,18 +282,30 @@ int dba_batch_add(dba_batch* b, const dba_config* k, const double* ic, int* slot
     r.f0 = 1. / (2 * k->dx); r.f1 = 1. / k->dx / k->dx; r.f2 = -k->alpha / Pi; r.f3 = 1. / k->tau;
     r.dt = k->dt; r.delta = k->delta; r.eps2 = k->epsilon * k->epsilon; r.gamma = k->gamma;
     r.thr_p = k->metric_p; r.thr_p_hi = 1.0 - k->metric_p; r.thr_T = k->metric_T;
-    // upload fields (both buffers hold the initial state; parity 0 selects buffer 0)
-    std::vector<float> tmp;
-    auto put = [&](void* dst, const std::vector<double>& v) -> cudaError_t {
-        if (b->esz == 8) return cudaMemcpyAsync(dst, v.data(), n * 8, cudaMemcpyHostToDevice, b->st);
-        tmp.resize(n);
-        for (size_t i = 0; i < n; ++i) tmp[i] = (float)v[i];
-        cudaError_t e = cudaMemcpyAsync(dst, tmp.data(), n * 4, cudaMemcpyHostToDevice, b->st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);   // tmp is reused
-        return e;
-    };
-    BTRY(put(r.p[0], p));
-    BTRY(put(r.T[0], T));
+    // initial condition into buffer 0 (parity 0): from the caller's FP64 arrays, or
+    // generated on the device by the single-domain engine's dba_init rules
+    if (ic) {
+        std::vector<float> tmp;
+        for (int f = 0; f < 2; ++f) {
+            void* dst = f ? r.T[0] : r.p[0];
+            if (b->esz == 8) {
+                BTRY(cudaMemcpyAsync(dst, ic + f * n, n * 8, cudaMemcpyHostToDevice, b->st));
+                BTRY(cudaStreamSynchronize(b->st));
+            } else {
+                tmp.resize(n);
+                for (size_t i = 0; i < n; ++i) tmp[i] = (float)ic[f * n + i];
+                BTRY(cudaMemcpyAsync(dst, tmp.data(), n * 4, cudaMemcpyHostToDevice, b->st));
+                BTRY(cudaStreamSynchronize(b->st));
+            }
+        }
+    } else {
+        SeedP sp{k->nx, k->ny, k->ic == DBA_IC_TANH_SEED ? 1 : 0, k->ic_corner ? 0.0 : (double)(k->nx / 2),
+                 k->ic_corner ? 0.0 : (double)(k->ny / 2), k->ic_radius, k->ic_width, k->Delta};
+        const int grid = (int)std::min<size_t>((n + 255) / 256, 4096);
+        if (b->esz == 8) slot_seed_kernel<double><<<grid, 256, 0, b->st>>>((double*)r.p[0], (double*)r.T[0], sp);
+        else slot_seed_kernel<float><<<grid, 256, 0, b->st>>>((float*)r.p[0], (float*)r.T[0], sp);
+        BTRY(cudaGetLastError());
+    }
     // flags of its blocks: parity 0, all active for the next step, the rest cleared
     const size_t NB = b->cfg.block_capacity;
     const long s_next = b->step + 1;
@@ -288,8 +315,8 @@ int dba_batch_add(dba_batch* b, const dba_config* k, const double* ic, int* slot
             BTRY(cudaMemsetAsync(b->wake + (q * 2 + ch) * NB + boff, (q == s_next % 3) ? 1 : 0, nb, b->st));
         BTRY(cudaMemsetAsync(b->next + ch * NB + boff, 0, nb, b->st));
     }
-    std::vector<int> ids(nb, s);
-    BTRY(cudaMemcpyAsync(b->d_bslot + boff, ids.data(), nb * sizeof(int), cudaMemcpyHostToDevice, b->st));
+    fill_int_kernel<<<(nb + 255) / 256, 256, 0, b->st>>>(b->d_bslot + boff, nb, s);
+    BTRY(cudaGetLastError());
     BTRY(cudaMemcpyAsync(b->d_slots + s, &r, sizeof r, cudaMemcpyHostToDevice, b->st));
     BTRY(cudaStreamSynchronize(b->st));
     b->slots[s] = r;

@@ -131,3 +131,14 @@ static DBA_FM_HD double dba_atan(double x)
     }
     return x < 0.0 ? -r : r;
 }
+
+/* tanh from the shared exponential, sign(x) (1 - e^(-2|x|)) / (1 + e^(-2|x|)):
+   identical on host and device, absolute error ~1e-16 (used for seed profiles,
+   where an absolute error is what matters) */
+static DBA_FM_HD double dba_tanh(double x)
+{
+    const double a = x < 0.0 ? -x : x;
+    const double e = dba_exp(-2.0 * a);
+    const double t = (1.0 - e) / (1.0 + e);
+    return x < 0.0 ? -t : t;
+}
