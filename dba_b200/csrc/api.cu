@@ -48,7 +48,7 @@ struct dba_ctx {
     double* avg = nullptr;            // [nsum]
     unsigned int* ticket = nullptr;
     int* status = nullptr;
-    unsigned long long* stats = nullptr;   // [4]
+    unsigned long long* stats = nullptr;   // kStatWords striped counters
     int* list = nullptr;              // KH active list
     int* count = nullptr;             // KH list length
     double* staging = nullptr;        // n doubles
@@ -599,7 +599,7 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
         if (!err) c->ticket = (unsigned int*)dev_alloc(c, sizeof(unsigned int), &err);
     }
     if (!err) c->status = (int*)dev_alloc(c, sizeof(int), &err);
-    if (!err) c->stats = (unsigned long long*)dev_alloc(c, 4 * sizeof(unsigned long long), &err);
+    if (!err) c->stats = (unsigned long long*)dev_alloc(c, kStatWords * sizeof(unsigned long long), &err);
     if (!err) c->staging = (double*)dev_alloc(c, (c->n > 64 ? c->n : 64) * sizeof(double), &err);
     if (err) {
         dba_destroy(c);
@@ -883,8 +883,9 @@ int dba_observables(dba_ctx* c, dba_obs* o)
         for (int v : fl) cnt += v;
         o->active_blocks[ch] = cnt;
     }
-    unsigned long long stats[4];
-    DBA_TRY(cudaMemcpy(stats, c->stats, sizeof stats, cudaMemcpyDeviceToHost));
+    unsigned long long raw[kStatWords], stats[4];
+    DBA_TRY(cudaMemcpy(raw, c->stats, sizeof raw, cudaMemcpyDeviceToHost));
+    fold_stats(raw, stats);
     o->cell_updates = (long)(stats[2] * (unsigned long long)(c->n / c->g.nb));
     std::vector<double> f(c->n);
     const dba_config& k = c->cfg;
@@ -945,9 +946,10 @@ int dba_get_info(dba_ctx* c, dba_info* info)
     info->device_bytes = bytes;
     info->step = c->step;
     info->grid_ctas = c->grid;
-    unsigned long long stats[4] = {0, 0, 0, 0};
+    unsigned long long raw[kStatWords], stats[4];
     DBA_TRY(cudaStreamSynchronize(c->st));
-    DBA_TRY(cudaMemcpy(stats, c->stats, sizeof stats, cudaMemcpyDeviceToHost));
+    DBA_TRY(cudaMemcpy(raw, c->stats, sizeof raw, cudaMemcpyDeviceToHost));
+    fold_stats(raw, stats);
     info->active_block_steps = (long)stats[2];
     info->cells_per_block = (long)(c->n / c->g.nb);
     return DBA_OK;
@@ -970,8 +972,8 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
     const bool cons = c->nsum && c->cfg.conserved && dba_mode && !c->lazy;
     std::vector<cudaEvent_t> ev((size_t)nsteps * 4 + 2);
     for (auto& e : ev) DBA_TRY(cudaEventCreate(&e));
-    unsigned long long s0[4], s1[4];
-    DBA_TRY(cudaMemcpyAsync(s0, c->stats, sizeof s0, cudaMemcpyDeviceToHost, c->st));
+    unsigned long long r0[kStatWords], r1[kStatWords], s0[4], s1[4];
+    DBA_TRY(cudaMemcpyAsync(r0, c->stats, sizeof r0, cudaMemcpyDeviceToHost, c->st));
     DBA_TRY(cudaStreamSynchronize(c->st));
     int st = DBA_OK;
     DBA_TRY(cudaEventRecord(ev[0], c->st));
@@ -1022,9 +1024,11 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
     }
     cudaEvent_t& last = ev[ev.size() - 1];
     if (!st) st = cuda_status(cudaEventRecord(last, c->st));
-    if (!st) st = cuda_status(cudaMemcpyAsync(s1, c->stats, sizeof s1, cudaMemcpyDeviceToHost, c->st));
+    if (!st) st = cuda_status(cudaMemcpyAsync(r1, c->stats, sizeof r1, cudaMemcpyDeviceToHost, c->st));
     if (!st) st = cuda_status(cudaStreamSynchronize(c->st));
     if (!st) {
+        fold_stats(r0, s0);
+        fold_stats(r1, s1);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ev[0], last);
         out->step_ms = ms;

@@ -123,6 +123,7 @@ struct dba_batch {
     void* arena = nullptr;           // 4 arrays x cell_capacity x esz
     SlotRec* d_slots = nullptr;
     int* d_bslot = nullptr;
+    int* d_hi = nullptr;             // 1 + highest block id of a live slot
     uint8_t* par = nullptr;          // [2][2][NB]
     uint8_t* wake = nullptr;         // [3][2][NB]
     uint8_t* next = nullptr;         // [2][NB]
@@ -162,7 +163,19 @@ BatchP bparams(dba_batch* b)
     p.slots = b->d_slots;
     p.bslot = b->d_bslot;
     p.nbtot = b->cfg.block_capacity;
+    p.hi = b->d_hi;
     return p;
+}
+
+// publish 1 + the highest block id of any live slot (the step kernel's scan
+// bound), ordered on the batch stream before the next step
+cudaError_t update_hi(dba_batch* b)
+{
+    int hi = 0;
+    for (const SlotRec& r : b->slots)
+        if (r.live) hi = std::max(hi, r.boff + r.nb);
+    fill_int_kernel<<<1, 32, 0, b->st>>>(b->d_hi, 1, hi);
+    return cudaGetLastError();
 }
 
 cudaError_t enqueue(dba_batch* b, long s)
@@ -206,18 +219,20 @@ int dba_batch_create(const dba_batch_config* cfg, dba_batch** out)
     if (e == cudaSuccess) e = cudaMalloc(&b->arena, 4 * cells * b->esz);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_slots, sizeof(SlotRec) * cfg->max_slots);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_bslot, sizeof(int) * NB);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_hi, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(b->d_hi, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&b->par, 2 * 2 * NB);
     if (e == cudaSuccess) e = cudaMalloc(&b->wake, 3 * 2 * NB);
     if (e == cudaSuccess) e = cudaMalloc(&b->next, 2 * NB);
     if (e == cudaSuccess) e = cudaMalloc(&b->status, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&b->stats, 4 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&b->stats, kStatWords * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_tips, sizeof(double) * cfg->max_slots);
     if (e == cudaSuccess) e = cudaMemset(b->d_bslot, 0xff, sizeof(int) * NB);
     if (e == cudaSuccess) e = cudaMemset(b->par, 0, 2 * 2 * NB);
     if (e == cudaSuccess) e = cudaMemset(b->wake, 0, 3 * 2 * NB);
     if (e == cudaSuccess) e = cudaMemset(b->next, 0, 2 * NB);
     if (e == cudaSuccess) e = cudaMemset(b->status, 0, sizeof(int));
-    if (e == cudaSuccess) e = cudaMemset(b->stats, 0, 4 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(b->stats, 0, kStatWords * sizeof(unsigned long long));
     b->slots.assign(cfg->max_slots, SlotRec{});
     b->cell_off.assign(cfg->max_slots, 0);
     b->age.assign(cfg->max_slots, 0);
@@ -241,7 +256,7 @@ void dba_batch_destroy(dba_batch* b)
     if (b->st) cudaStreamSynchronize(b->st);
     for (auto& g : b->graphs)
         if (g) cudaGraphExecDestroy(g);
-    for (void* p : {(void*)b->arena, (void*)b->d_slots, (void*)b->d_bslot, (void*)b->par, (void*)b->wake,
+    for (void* p : {(void*)b->arena, (void*)b->d_slots, (void*)b->d_bslot, (void*)b->d_hi, (void*)b->par, (void*)b->wake,
                     (void*)b->next, (void*)b->status, (void*)b->stats, (void*)b->d_tips, (void*)b->staging})
         if (p) cudaFree(p);
     if (b->st) cudaStreamDestroy(b->st);
@@ -322,6 +337,7 @@ int dba_batch_add(dba_batch* b, const dba_config* k, const double* ic, int* slot
     b->slots[s] = r;
     b->cell_off[s] = coff;
     b->age[s] = 0;
+    BTRY(update_hi(b));
     *slot_out = s;
     return DBA_OK;
 }
@@ -338,6 +354,7 @@ int dba_batch_remove(dba_batch* b, int s)
     b->cells.give(b->cell_off[s], (size_t)r.nx * r.ny);
     b->blocks.give(r.boff, r.nb);
     r = SlotRec{};
+    BTRY(update_hi(b));
     return DBA_OK;
 }
 
@@ -432,9 +449,10 @@ int dba_batch_get_info(dba_batch* b, dba_batch_info* info)
     info->largest_free_blocks = (long)b->blocks.largest();
     for (auto& r : b->slots) info->live_slots += r.live ? 1 : 0;
     info->step = b->step;
-    unsigned long long st[4];
+    unsigned long long raw[kStatWords], st[4];
     BTRY(cudaStreamSynchronize(b->st));
-    BTRY(cudaMemcpy(st, b->stats, sizeof st, cudaMemcpyDeviceToHost));
+    BTRY(cudaMemcpy(raw, b->stats, sizeof raw, cudaMemcpyDeviceToHost));
+    fold_stats(raw, st);
     info->active_block_steps = (long)st[2];
     info->grid_ctas = b->grid;
     return DBA_OK;

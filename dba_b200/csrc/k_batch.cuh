@@ -5,10 +5,12 @@
 // blocks live in one global block index space: slot s owns blocks
 // [boff_s, boff_s + nb_s), and every per-block array (parity, wake flags,
 // next flags) is indexed by that global id.  One kernel per step scans the
-// whole space exactly as the single-domain kernel does (k_dendrite.cuh):
-// blocks whose slot is empty are skipped, the active ones of all slots are
-// merged into the CTAs' compact lists, and each listed block is advanced with
-// its own slot's grid, buffers and parameters, read from a device slot table.
+// space up to the highest live block (a device word the host updates on
+// admission and retirement) exactly as the single-domain kernel does
+// (k_dendrite.cuh): blocks whose slot is empty are skipped, the active ones of
+// all slots are merged into the CTAs' compact lists, and each listed block is
+// advanced with its own slot's grid, buffers and parameters, read from a device
+// slot table.
 // Because the kernel reads the table, CUDA graphs captured once stay valid
 // while simulations are admitted and retired between graph launches.
 #pragma once
@@ -29,6 +31,28 @@ struct BatchP {
     const SlotRec* slots;
     const int* bslot;      // global block -> slot (-1: free)
     int nbtot;             // size of the global block space
+    const int* hi;         // 1 + the highest block id of a live slot (0: none)
+};
+
+// Blocks one CTA stages and advances together: 1024 cells per group (32 blocks
+// at most, and never fewer cells than threads).  Staging a whole group before
+// any of it is computed puts that many blocks' loads in flight at once.
+template <int B, int NT>
+constexpr int batch_group()
+{
+    return NT / (B * B) > (1024 / (B * B) < 32 ? 1024 / (B * B) : 32) ? NT / (B * B)
+                                                                      : (1024 / (B * B) < 32 ? 1024 / (B * B) : 32);
+}
+
+// one listed block of a group: its slot, where its cells and the four halo
+// lines (west/east columns, south/north rows) start, and which blocks hold them
+struct BatchBlk {
+    SlotRec r;
+    long long gi0;      // first cell of the block in its slot's arrays
+    long long off[4];   // first halo cell west, east, south, north
+    int nbr[4];         // global ids of the blocks holding those halo lines
+    int meta;           // act | p parity << 2 | T parity << 3
+    int lb;             // block id within the slot
 };
 
 template <typename R, int B, int NT, bool DBA>
@@ -37,29 +61,40 @@ __global__ void __launch_bounds__(NT) batch_dendrite_step(BatchP bp, FlagP f)
     constexpr int V = B * B;
     constexpr int E = B + 2;
     constexpr int TV = E * E;
-    constexpr int K = V >= NT ? 1 : NT / V;
-    constexpr int CPT = V >= NT ? V / NT : 1;
-    constexpr int SY = E;
+    constexpr int K = batch_group<B, NT>();
+    constexpr int CPT = K * V / NT;
+    static_assert(K * V % NT == 0 && CPT >= 1, "group must give every thread whole cells");
 
     __shared__ R sp[K * TV];
     __shared__ R sT[K * TV];
     __shared__ int s_list[NT], s_lmeta[NT];
     __shared__ int s_cnt;
-    __shared__ int s_blk[K], s_meta[K], s_np[K], s_nT[K], s_slot[K];
-    __shared__ SlotRec s_rec[K];
+    __shared__ int s_np[K], s_nT[K];
+    __shared__ BatchBlk s_d[K];
 
     const int tid = threadIdx.x;
     const int G = gridDim.x;
     const int nb = bp.nbtot;
+    const int hi = min(*bp.hi, nb);   // every block at or above hi is free
 
-    for (long long j0 = 0; blockIdx.x + (long long)G * j0 < nb; j0 += NT) {
+    for (long long j0 = 0; blockIdx.x + (long long)G * j0 < hi; j0 += NT) {
+        // ---- scan: flags of the owned blocks (all loads of a thread issued together)
         const long long bl = blockIdx.x + (long long)G * (j0 + tid);
         const int b = (int)bl;
-        const bool valid = bl < nb && bp.bslot[b] >= 0;
+        int sl = -1, pp = 0, pT = 0, w0 = 1, w1 = 1;
+        if (bl < hi) {
+            sl = bp.bslot[b];
+            pp = f.par_cur[b];
+            pT = f.par_cur[nb + b];
+            if (DBA) {
+                w0 = f.wake_cur[b];
+                w1 = f.wake_cur[nb + b];
+            }
+        }
+        const bool valid = sl >= 0;
         int act = 0, meta = 0;
         if (valid) {
-            int pp = f.par_cur[b], pT = f.par_cur[nb + b];
-            act = DBA ? ((f.wake_cur[b] ? 1 : 0) | (f.wake_cur[nb + b] ? 2 : 0)) : 3;
+            act = (w0 ? 1 : 0) | (w1 ? 2 : 0);
             f.wake_clr[b] = 0;
             f.wake_clr[nb + b] = 0;
             if (!DBA) {
@@ -68,7 +103,7 @@ __global__ void __launch_bounds__(NT) batch_dendrite_step(BatchP bp, FlagP f)
             }
             f.par_nxt[b] = (uint8_t)(pp ^ (act & 1));
             f.par_nxt[nb + b] = (uint8_t)(pT ^ ((act >> 1) & 1));
-            meta = act | (pp << 2) | (pT << 3);
+            meta = act | (pp << 2) | (pT << 3) | (sl << 4);
         }
         count_stats(f.stats, act, valid);
         if (tid == 0) s_cnt = 0;
@@ -78,82 +113,109 @@ __global__ void __launch_bounds__(NT) batch_dendrite_step(BatchP bp, FlagP f)
         const int cnt = s_cnt;
 
         for (int q0 = 0; q0 < cnt; q0 += K) {
-            if (tid < K) {
-                int q = q0 + tid;
-                s_blk[tid] = q < cnt ? s_list[q] : -1;
-                s_meta[tid] = q < cnt ? s_lmeta[q] : 0;
-                s_slot[tid] = q < cnt ? bp.bslot[s_list[q]] : -1;
+            const int nk = min(K, cnt - q0);
+            // ---- group descriptors: one thread per listed block
+            if (tid < nk) {
+                const int blk = s_list[q0 + tid], m = s_lmeta[q0 + tid];
+                const SlotRec r = bp.slots[m >> 4];
+                const int lb = blk - r.boff;
+                const int by = lb / r.nbx, bx = lb - by * r.nbx;
+                const int x0 = bx * B, y0 = by * B;
+                const int xw = wrapc(x0 - 1, r.nx, r.bc), xe = wrapc(x0 + B, r.nx, r.bc);
+                const int ys = wrapc(y0 - 1, r.ny, r.bc), yn = wrapc(y0 + B, r.ny, r.bc);
+                BatchBlk& d = s_d[tid];
+                d.r = r;
+                d.meta = m & 15;
+                d.lb = lb;
+                d.gi0 = x0 + (long long)r.nx * y0;
+                d.off[0] = xw + (long long)r.nx * y0;
+                d.off[1] = xe + (long long)r.nx * y0;
+                d.off[2] = x0 + (long long)r.nx * ys;
+                d.off[3] = x0 + (long long)r.nx * yn;
+                d.nbr[0] = r.boff + xw / B + r.nbx * by;
+                d.nbr[1] = r.boff + xe / B + r.nbx * by;
+                d.nbr[2] = r.boff + bx + r.nbx * (ys / B);
+                d.nbr[3] = r.boff + bx + r.nbx * (yn / B);
                 s_np[tid] = 0;
                 s_nT[tid] = 0;
-                if (q < cnt) s_rec[tid] = bp.slots[s_slot[tid]];
             }
             __syncthreads();
-            for (int i = tid; i < K * TV; i += NT) {
+            // ---- stage the group: interiors from the block's current buffer; each
+            // halo line from both buffers of the block holding it, selected by that
+            // block's parity loaded alongside (one round trip); corners are never read
+            for (int i = tid; i < nk * TV; i += NT) {
                 const int k = i / TV;
-                const int blk = s_blk[k];
-                if (blk < 0) continue;
-                const SlotRec& r = s_rec[k];
-                const int lb = blk - r.boff;
                 const int j = i - k * TV;
                 const int ly = j / E, lx = j - ly * E;
-                const int bx = lb % r.nbx, by = lb / r.nbx;
-                const int gx = wrapc(bx * B + lx - 1, r.nx, r.bc);
-                const int gy = wrapc(by * B + ly - 1, r.ny, r.bc);
-                const int ob = r.boff + gx / B + r.nbx * (gy / B);
-                const size_t gi = (size_t)gx + (size_t)r.nx * gy;
-                sp[i] = (f.par_cur[ob] ? (const R*)r.p[1] : (const R*)r.p[0])[gi];
-                sT[i] = (f.par_cur[nb + ob] ? (const R*)r.T[1] : (const R*)r.T[0])[gi];
+                const bool ix = lx >= 1 && lx <= B, iy = ly >= 1 && ly <= B;
+                if (!ix && !iy) continue;
+                const BatchBlk& d = s_d[k];
+                const R* P0 = (const R*)d.r.p[0];
+                const R* P1 = (const R*)d.r.p[1];
+                const R* T0 = (const R*)d.r.T[0];
+                const R* T1 = (const R*)d.r.T[1];
+                R vp, vT;
+                if (ix && iy) {
+                    const long long o = d.gi0 + (lx - 1) + (long long)d.r.nx * (ly - 1);
+                    vp = ((d.meta & 4) ? P1 : P0)[o];
+                    vT = ((d.meta & 8) ? T1 : T0)[o];
+                } else {
+                    const int fc = ix ? (ly == 0 ? 2 : 3) : (lx == 0 ? 0 : 1);
+                    const long long o = d.off[fc] + (ix ? (long long)(lx - 1) : (long long)d.r.nx * (ly - 1));
+                    const int nbid = d.nbr[fc];
+                    const R a0 = P0[o], a1 = P1[o], c0 = T0[o], c1 = T1[o];
+                    vp = f.par_cur[nbid] ? a1 : a0;
+                    vT = f.par_cur[nb + nbid] ? c1 : c0;
+                }
+                sp[i] = vp;
+                sT[i] = vT;
             }
             __syncthreads();
+            // ---- advance: CPT cells per thread, cells of a block on consecutive threads
 #pragma unroll
             for (int c = 0; c < CPT; ++c) {
-                const int k = (V >= NT) ? 0 : tid / V;
-                const int v = (V >= NT) ? tid + c * NT : tid - k * V;
-                const int blk = s_blk[k];
-                if (blk < 0) continue;
-                const SlotRec& r = s_rec[k];
-                const int m = s_meta[k];
-                const int lb = blk - r.boff;
+                const int u = tid + c * NT;
+                const int k = u / V;
+                if (k >= nk) break;
+                const int v = u - k * V;
+                const BatchBlk& d = s_d[k];
+                const int m = d.meta;
                 const int ly = v / B, lx = v - ly * B;
-                const int ti = k * TV + (lx + 1) + SY * (ly + 1);
-                const int bx = lb % r.nbx, by = lb / r.nbx;
-                const size_t gi = (size_t)(bx * B + lx) + (size_t)r.nx * (size_t)(by * B + ly);
-                const R f0 = (R)r.f0, f1 = (R)r.f1, f2 = (R)r.f2, f3 = (R)r.f3, dt = (R)r.dt;
+                const int ti = k * TV + (lx + 1) + E * (ly + 1);
+                const long long gi = d.gi0 + lx + (long long)d.r.nx * ly;
+                const R f0 = (R)d.r.f0, f1 = (R)d.r.f1, f2 = (R)d.r.f2, f3 = (R)d.r.f3, dt = (R)d.r.dt;
                 const R pc = sp[ti], Tc = sT[ti];
                 R pn = pc;
                 if (m & 1) {
-                    pn = den_p_new<R>(pc, Tc, sp[ti + 1], sp[ti - 1], sp[ti + SY], sp[ti - SY], pc, pc, f0, f1, f2, f3,
-                                      dt, (R)r.delta, (R)r.eps2, (R)r.gamma);
-                    ((m & 4) ? (R*)r.p[0] : (R*)r.p[1])[gi] = pn;
-                    if (pn >= (R)r.thr_p && pn <= (R)r.thr_p_hi) s_np[k] = 1;
+                    pn = den_p_new<R>(pc, Tc, sp[ti + 1], sp[ti - 1], sp[ti + E], sp[ti - E], pc, pc, f0, f1, f2, f3,
+                                      dt, (R)d.r.delta, (R)d.r.eps2, (R)d.r.gamma);
+                    ((m & 4) ? (R*)d.r.p[0] : (R*)d.r.p[1])[gi] = pn;
+                    if (pn >= (R)d.r.thr_p && pn <= (R)d.r.thr_p_hi) s_np[k] = 1;
                     if (!isfinite(pn)) raise_status(f.status, 5);
                 }
                 if (m & 2) {
-                    const R Tn = den_T_new<R, DBA>(Tc, sT[ti + 1], sT[ti - 1], sT[ti + SY], sT[ti - SY], Tc, Tc,
+                    const R Tn = den_T_new<R, DBA>(Tc, sT[ti + 1], sT[ti - 1], sT[ti + E], sT[ti - E], Tc, Tc,
                                                    (m & 1) != 0, pn, pc, f1, dt);
-                    ((m & 8) ? (R*)r.T[0] : (R*)r.T[1])[gi] = Tn;
-                    if (fabs(Tn - Tc) >= (R)r.thr_T) s_nT[k] = 1;
+                    ((m & 8) ? (R*)d.r.T[0] : (R*)d.r.T[1])[gi] = Tn;
+                    if (fabs(Tn - Tc) >= (R)d.r.thr_T) s_nT[k] = 1;
                     if (!isfinite(Tn)) raise_status(f.status, 5);
                 }
             }
             __syncthreads();
-            if (DBA && tid < K) {
-                const int blk = s_blk[tid];
-                if (blk >= 0) {
-                    const SlotRec& r = s_rec[tid];
-                    GridP lg;
-                    lg.nx = r.nx; lg.ny = r.ny; lg.nz = 1;
-                    lg.nbx = r.nbx; lg.nby = r.nby; lg.nbz = 1; lg.nb = r.nb; lg.bc = r.bc;
-                    const int lb = blk - r.boff;
-                    const int m = s_meta[tid];
-                    if (m & 1) {
-                        f.next[blk] = (uint8_t)s_np[tid];
-                        if (s_np[tid]) wake_faces(lg, f.wake_nxt + r.boff, lb);
-                    }
-                    if (m & 2) {
-                        f.next[nb + blk] = (uint8_t)s_nT[tid];
-                        if (s_nT[tid]) wake_faces(lg, f.wake_nxt + nb + r.boff, lb);
-                    }
+            // ---- next flags and neighbour wake-up, one thread per block
+            if (DBA && tid < nk) {
+                const BatchBlk& d = s_d[tid];
+                GridP lg;
+                lg.nx = d.r.nx; lg.ny = d.r.ny; lg.nz = 1;
+                lg.nbx = d.r.nbx; lg.nby = d.r.nby; lg.nbz = 1; lg.nb = d.r.nb; lg.bc = d.r.bc;
+                const int blk = d.r.boff + d.lb;
+                if (d.meta & 1) {
+                    f.next[blk] = (uint8_t)s_np[tid];
+                    if (s_np[tid]) wake_faces(lg, f.wake_nxt + d.r.boff, d.lb);
+                }
+                if (d.meta & 2) {
+                    f.next[nb + blk] = (uint8_t)s_nT[tid];
+                    if (s_nT[tid]) wake_faces(lg, f.wake_nxt + nb + d.r.boff, d.lb);
                 }
             }
             __syncthreads();

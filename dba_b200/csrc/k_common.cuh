@@ -41,7 +41,7 @@ struct FlagP {
     uint8_t* next;
     double* bsum;
     int* status;
-    unsigned long long* stats;  // [0] ch0 active blocks, [1] ch1, [2] any, [3] ch0 && !ch1
+    unsigned long long* stats;  // kStatWords striped activity counters (count_stats)
 };
 
 __device__ __forceinline__ int wrapc(int v, int n, int bc)
@@ -141,6 +141,22 @@ __device__ __forceinline__ void list_append(bool take, int b, int meta, int* s_l
     }
 }
 
+// Activity counters ([0] ch0 active blocks, [1] ch1, [2] any, [3] ch0 && !ch1)
+// are striped: warp w of a launch adds into stripe w mod kStatStripes, whose
+// four counters sit at stats[stripe * kStatStride + k], one 128-byte line per
+// stripe, so the warps of a launch do not queue on one address.  Readers add
+// the stripes up (fold_stats).
+constexpr int kStatStripes = 32;
+constexpr int kStatStride = 16;
+constexpr int kStatWords = kStatStripes * kStatStride;
+
+inline __host__ __device__ void fold_stats(const unsigned long long* raw, unsigned long long out[4])
+{
+    for (int k = 0; k < 4; ++k) out[k] = 0;
+    for (int s = 0; s < kStatStripes; ++s)
+        for (int k = 0; k < 4; ++k) out[k] += raw[s * kStatStride + k];
+}
+
 __device__ __forceinline__ void count_stats(unsigned long long* stats, int act, bool valid)
 {
     unsigned m0 = __ballot_sync(0xffffffffu, valid && (act & 1));
@@ -148,10 +164,12 @@ __device__ __forceinline__ void count_stats(unsigned long long* stats, int act, 
     unsigned m2 = __ballot_sync(0xffffffffu, valid && (act & 3));
     unsigned m3 = __ballot_sync(0xffffffffu, valid && (act & 1) && !(act & 2));
     if ((threadIdx.x & 31) == 0 && m2) {
-        atomicAdd(&stats[0], (unsigned long long)__popc(m0));
-        atomicAdd(&stats[1], (unsigned long long)__popc(m1));
-        atomicAdd(&stats[2], (unsigned long long)__popc(m2));
-        atomicAdd(&stats[3], (unsigned long long)__popc(m3));
+        const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        unsigned long long* st = stats + kStatStride * (w & (kStatStripes - 1));
+        atomicAdd(&st[0], (unsigned long long)__popc(m0));
+        atomicAdd(&st[1], (unsigned long long)__popc(m1));
+        atomicAdd(&st[2], (unsigned long long)__popc(m2));
+        atomicAdd(&st[3], (unsigned long long)__popc(m3));
     }
 }
 

@@ -28,11 +28,11 @@ def _engine_sums_and_mean(sim, n, nb):
     in creation order, without the readback staging buffer.  For FP64 Model B:
     x,y,z x 2 buffers, 3 potentials, parity [2][nb], wake [3][nb], next [nb],
     block sums [3][nb] (FP64), run sums [3][ceil(nb/1024)], means [4] (FP64),
-    ticket, status, stats [4] (uint64)."""
+    ticket, status, striped activity counters [32 stripes x 16] (uint64)."""
     blob = np.empty(sim.state_size(), np.uint8)
     sim.save_state(blob)
     J = (nb + 1023) // 1024
-    sizes = [8, 8] + [n * 8] * 6 + [n * 8] * 3 + [2 * nb, 3 * nb, nb, 3 * nb * 8, 3 * J * 8, 4 * 8, 4, 4, 32]
+    sizes = [8, 8] + [n * 8] * 6 + [n * 8] * 3 + [2 * nb, 3 * nb, nb, 3 * nb * 8, 3 * J * 8, 4 * 8, 4, 4, 32 * 16 * 8]
     assert sum(sizes) == blob.size, "checkpoint layout changed; update this test"
     off = np.cumsum([0] + sizes)
     bsum = blob[off[14]:off[15]].view(np.float64).copy()
