@@ -63,11 +63,12 @@ int modelb_tile_grid(int B, int sms, int ntiles)
 cudaError_t launch_modelb_tiles(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
                                 const MBFastP& P, const MBFastBuf& Q, const LazyP& L)
 {
+    const MBPairP K = make_pair_params(P);
 #define XT(b)                                                                                         \
     if (B == b) {                                                                                     \
         const size_t sm = MBTile<b>::smem;                                                            \
-        if (dba_mode) modelb_tile_step<b, true><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, Q, L);      \
-        else modelb_tile_step<b, false><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, Q, L);              \
+        if (dba_mode) modelb_tile_step<b, true><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, K, Q, L);   \
+        else modelb_tile_step<b, false><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, K, Q, L);           \
         return cudaGetLastError();                                                                    \
     }
     XT(8) XT(16)

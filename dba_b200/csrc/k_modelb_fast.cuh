@@ -29,6 +29,7 @@
 
 #include "k_common.cuh"
 #include "k_modelb.cuh"
+#include "k_pair.cuh"
 
 namespace dba {
 
@@ -206,6 +207,98 @@ __device__ __forceinline__ void mb_changes(const MBFastP& P, float mx, float my,
     cx = __fmul_rn(P.dtvx, __fmaf_rn(P.Mx, lmx, -__fmul_rn(P.dn, Rr)));
     cy = __fmul_rn(P.dtvy, __fmaf_rn(P.My, lmy, -__fmul_rn(P.dm, Rr)));
     cz = __fmul_rn(P.dtvz, __fmaf_rn(P.Mz, lmz, Rr));
+}
+
+// ---- the same point formulas on pairs of cells (k_pair.cuh): lane by lane the
+// operations, their order and their rounding are those of the scalar helpers
+// above, so a pair kernel stores the bits a scalar kernel stores. ----
+
+// splatted constants of the pair formulas (negated where the scalar form negates
+// a product: (-a) * b rounds to exactly -(a * b))
+struct MBPairP {
+    f2 inv_dx2, cc, cf, cd, one, ln2, log2e, zero, nz;   // nz = (-0, -0): the addend of every product
+    f2 c0x, c0y, c0z, irx, iry, irz, chi_xy, chi_xz, chi_yz, chi_xb, chi_yb, chi_zb;
+    f2 nex, ney, nez, phi_logK;
+    f2 nvx, mvy, dvz, k0, dtvx, dtvy, dtvz, Mx, My, Mz, ndn, ndm;
+};
+
+inline MBPairP make_pair_params(const MBFastP& P)
+{
+    MBPairP q;
+    q.inv_dx2 = f2_splat_host(P.inv_dx2);
+    q.cc = f2_splat_host((float)(-10.0 / 3.0));
+    q.cf = f2_splat_host((float)(2.0 / 3.0));
+    q.cd = f2_splat_host((float)(1.0 / 6.0));
+    q.one = f2_splat_host(1.f);
+    q.ln2 = f2_splat_host(0.693147180559945309f);
+    q.log2e = f2_splat_host(1.442695040888963407f);
+    q.zero = f2_splat_host(0.f);
+    q.nz = f2_splat_host(-0.f);
+    q.c0x = f2_splat_host(P.c0x); q.c0y = f2_splat_host(P.c0y); q.c0z = f2_splat_host(P.c0z);
+    q.irx = f2_splat_host(P.irx); q.iry = f2_splat_host(P.iry); q.irz = f2_splat_host(P.irz);
+    q.chi_xy = f2_splat_host(P.chi_xy); q.chi_xz = f2_splat_host(P.chi_xz); q.chi_yz = f2_splat_host(P.chi_yz);
+    q.chi_xb = f2_splat_host(P.chi_xb); q.chi_yb = f2_splat_host(P.chi_yb); q.chi_zb = f2_splat_host(P.chi_zb);
+    q.nex = f2_splat_host(-P.ex); q.ney = f2_splat_host(-P.ey); q.nez = f2_splat_host(-P.ez);
+    q.phi_logK = f2_splat_host(P.phi_logK);
+    q.nvx = f2_splat_host(P.nvx); q.mvy = f2_splat_host(P.mvy); q.dvz = f2_splat_host(P.dvz);
+    q.k0 = f2_splat_host(P.k0);
+    q.dtvx = f2_splat_host(P.dtvx); q.dtvy = f2_splat_host(P.dtvy); q.dtvz = f2_splat_host(P.dtvz);
+    q.Mx = f2_splat_host(P.Mx); q.My = f2_splat_host(P.My); q.Mz = f2_splat_host(P.Mz);
+    q.ndn = f2_splat_host(-P.dn); q.ndm = f2_splat_host(-P.dm);
+    return q;
+}
+
+// lap9_rows on a pair
+__device__ __forceinline__ f2 lap9_rows2(const MBPairP& K, f2 hm, f2 cm, f2 h0, f2 c0, f2 hp, f2 cp)
+{
+    const f2 faces = add2(h0, add2(cp, cm));
+    const f2 diag = add2(hp, hm);
+    return mul2(K.inv_dx2, fma2(K.cd, diag, fma2(K.cf, faces, mul2(K.cc, c0, K.nz))), K.nz);
+}
+
+__device__ __forceinline__ f2 ln_approx2(const MBPairP& K, f2 x)
+{
+    float a, b;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(a) : "f"(f2_lo(x)));
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(b) : "f"(f2_hi(x)));
+    return mul2(f2_pack(a, b), K.ln2, K.nz);
+}
+
+__device__ __forceinline__ f2 exp_approx2(const MBPairP& K, f2 x)
+{
+    const f2 t = mul2(x, K.log2e, K.nz);
+    float a, b;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(a) : "f"(f2_lo(t)));
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(b) : "f"(f2_hi(t)));
+    return f2_pack(a, b);
+}
+
+// mb_potentials on a pair
+__device__ __forceinline__ void mb_potentials2(const MBPairP& K, f2 X, f2 Y, f2 Z, f2 lapx, f2 lapy, f2 lapz,
+                                               f2& ux, f2& uy, f2& uz)
+{
+    const f2 bb = sub2(sub2(sub2(K.one, X), Y), Z);
+    const f2 lb = ln_approx2(K, bb);
+    const f2 sumb = fma2(K.chi_zb, Z, fma2(K.chi_yb, Y, mul2(K.chi_xb, X, K.nz)));
+    f2 u = fma2(K.chi_xb, bb, fma2(K.chi_xz, Z, fma2(K.chi_xy, Y, K.c0x)));
+    u = sub2(fma2(ln_approx2(K, X), K.irx, sub2(u, sumb)), lb);
+    ux = fma2(K.nex, lapx, u);
+    u = fma2(K.chi_yb, bb, fma2(K.chi_yz, Z, fma2(K.chi_xy, X, K.c0y)));
+    u = sub2(fma2(ln_approx2(K, Y), K.iry, sub2(u, sumb)), lb);
+    uy = fma2(K.ney, lapy, u);
+    u = fma2(K.chi_zb, bb, fma2(K.chi_yz, Y, fma2(K.chi_xz, X, K.c0z)));
+    u = sub2(fma2(ln_approx2(K, Z), K.irz, sub2(u, sumb)), lb);
+    uz = sub2(fma2(K.nez, lapz, u), K.phi_logK);
+}
+
+// mb_changes on a pair
+__device__ __forceinline__ void mb_changes2(const MBPairP& K, f2 mx, f2 my, f2 mz, f2 lmx, f2 lmy, f2 lmz, f2& cx,
+                                            f2& cy, f2& cz)
+{
+    const f2 Rr = mul2(K.k0, sub2(exp_approx2(K, fma2(K.nvx, mx, mul2(K.mvy, my, K.nz))), exp_approx2(K, mul2(K.dvz, mz, K.nz))), K.nz);
+    cx = mul2(K.dtvx, fma2(K.Mx, lmx, mul2(K.ndn, Rr, K.nz)), K.nz);
+    cy = mul2(K.dtvy, fma2(K.My, lmy, mul2(K.ndm, Rr, K.nz)), K.nz);
+    cz = mul2(K.dtvz, fma2(K.Mz, lmz, Rr), K.nz);
 }
 
 template <int B, bool DBA>

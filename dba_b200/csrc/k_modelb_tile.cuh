@@ -11,10 +11,15 @@
 //   * the tile plus a 2-cell halo of x, y, z is staged with 16-byte cp.async
 //     copies, double-buffered: tile i+1 is in flight while tile i computes.
 //     Each 16-byte piece lies inside one block, whose parity picks the buffer;
-//   * each thread owns a 4-row strip of one column and slides a 3-row window
-//     down it, so the Laplacians reuse row sums instead of re-reading 9 cells;
-//   * the 1-cell potential ring around the tile is computed (active owner) or
-//     loaded from the persisted ring (inactive owner) by the first 132 threads;
+//   * each of the 128 threads owns a 4-column x 2-row patch.  A staged row of
+//     the patch is one 16-byte shared load plus its left and right neighbours;
+//     the row sums of the 9-point Laplacian are formed once per loaded row and
+//     the arithmetic runs on pairs of cells (k_pair.cuh: the two-lane FP32
+//     instructions of sm_100, rounded lane by lane like the scalar helpers), so
+//     the stored bits are those of the scalar kernels;
+//   * the 132-cell potential ring around the tile is computed (active owner)
+//     or loaded from the persisted ring (inactive owner) two cells per thread
+//     by the first 66 threads;
 //   * a block persists its ring potentials only when its own wake-up test is
 //     negative: a block whose test is positive is active next step (it wakes
 //     itself), so its ring from this step is never read as stale;
@@ -25,37 +30,79 @@
 
 #include "k_common.cuh"
 #include "k_modelb_fast.cuh"
+#include "k_pair.cuh"
 
 namespace dba {
 
 template <int B> struct MBTile {
-    static constexpr int NT = 256;
+    static constexpr int NT = 128;
     static constexpr int T = 32;              // tile edge in cells
     static constexpr int TB = T / B;          // blocks per tile edge
     static constexpr int NBT = TB * TB;       // blocks per tile
     static constexpr int RB = TB + 2;         // neighbourhood edge in blocks
     static constexpr int SR = T + 4;          // staged rows: 2-cell halo above and below
     static constexpr int SW = T + 8;          // staged row width: 4-cell (16-byte) halo left and right
-    static constexpr int SP = SW + 4;         // row pitch: rows shift by 12 banks, so column accesses
-                                              // of the ring spread over 8 banks
+    static constexpr int SP = SW + 4;         // staged row pitch (16-byte multiple)
     static constexpr int SV = SR * SP;        // one staged field
     static constexpr int NQ = SR * (SW / 4);  // 16-byte pieces per staged field
-    static constexpr int MP = T + 4;          // potential row pitch (T + 2 used)
-    static constexpr int MV = (T + 2) * MP;   // one potential field
+    static constexpr int NQT = (NQ + NT - 1) / NT;   // pieces per thread
+    static constexpr int MP = T + 8;          // potential row pitch: column lx at lx + 4 (aligned quads)
+    static constexpr int MV = (T + 2) * MP;   // one potential field (rows -1 .. T)
     static constexpr int RING = 4 * T + 4;    // potential cells around the tile
+    static constexpr int NPAIR = RING / 2;    // ring threads, two cells each
     static constexpr int TPP = NT / NBT;      // tiles per scan pass
-    static constexpr int ROWS = T * T / NT;   // rows per thread strip
+    static constexpr int ROWS = 2;            // rows per thread patch
+    static constexpr int QX = T / 4;          // patches per tile row
     static constexpr size_t smem = sizeof(float) * (2 * 3 * SV + 3 * MV);
-    static_assert(T % B == 0 && B % ROWS == 0 && NBT <= 16 && NQ <= 2 * NT && RING <= NT, "tile shape");
+    static_assert(QX * (T / ROWS) == NT, "one 4x2 patch per thread");
+    static_assert(T % B == 0 && B % 4 == 0 && B % ROWS == 0 && NBT <= 16 && NQT * NT >= NQ && NPAIR <= NT,
+                  "tile shape");
 };
 
+// one staged row of a 4-cell patch: centres as two pairs, and the row sums
+// right + left neighbour of each cell (the scalar kernels' h), as two pairs
+__device__ __forceinline__ void quad_row(const float* s, int i, f2& h01, f2& h23, f2& c01, f2& c23)
+{
+    const float4 v = *reinterpret_cast<const float4*>(s + i);
+    const float l = s[i - 1], r = s[i + 4];
+    h01 = f2_pack(__fadd_rn(v.y, l), __fadd_rn(v.z, v.x));
+    h23 = f2_pack(__fadd_rn(v.w, v.y), __fadd_rn(r, v.z));
+    c01 = f2_pack(v.x, v.y);
+    c23 = f2_pack(v.z, v.w);
+}
+
+// Laplacians and centres of the two patch rows of one field; i = patch column 0
+// of the row above the patch, PITCH = the array's row pitch
+template <int PITCH>
+__device__ __forceinline__ void quad_laps(const MBPairP& K, const float* s, int i, f2 lap[2][2], f2 cen[2][2])
+{
+    f2 h[3][2], c[3][2];
+    quad_row(s, i, h[0][0], h[0][1], c[0][0], c[0][1]);
+    quad_row(s, i + PITCH, h[1][0], h[1][1], c[1][0], c[1][1]);
+    quad_row(s, i + 2 * PITCH, h[2][0], h[2][1], c[2][0], c[2][1]);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        lap[0][k] = lap9_rows2(K, h[0][k], c[0][k], h[1][k], c[1][k], h[2][k], c[2][k]);
+        cen[0][k] = c[1][k];
+    }
+    quad_row(s, i + 3 * PITCH, h[0][0], h[0][1], c[0][0], c[0][1]);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        lap[1][k] = lap9_rows2(K, h[1][k], c[1][k], h[2][k], c[2][k], h[0][k], c[0][k]);
+        cen[1][k] = c[2][k];
+    }
+}
+
+__device__ __forceinline__ float4 f4_of(f2 a, f2 b) { return make_float4(f2_lo(a), f2_hi(a), f2_lo(b), f2_hi(b)); }
 
 template <int B, bool DBA>
-__global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBFastP P, MBFastBuf Q, LazyP L)
+__global__ void __launch_bounds__(128, 4)
+    modelb_tile_step(GridP g, FlagP f, MBFastP P, MBPairP K, MBFastBuf Q, LazyP L)
 {
     using S = MBTile<B>;
     constexpr int NT = S::NT, T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, SW = S::SW, SP = S::SP, SV = S::SV;
-    constexpr int NQ = S::NQ, MP = S::MP, MV = S::MV, RING = S::RING, TPP = S::TPP, ROWS = S::ROWS;
+    constexpr int NQ = S::NQ, NQT = S::NQT, MP = S::MP, MV = S::MV, RING = S::RING, NPAIR = S::NPAIR;
+    constexpr int TPP = S::TPP;
     extern __shared__ __align__(128) float smem_f[];
     float* stage = smem_f;               // [2][3][SV]
     float* mu = smem_f + 2 * 3 * SV;     // [3][MV]
@@ -71,38 +118,22 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
     const int G = gridDim.x;
     const int ntx = g.nx / T, nty = g.ny / T, ntiles = ntx * nty;
     const size_t nx = (size_t)g.nx;
-    const float inv_dx2 = P.inv_dx2;
     if (tid < 3) {
         s_Cf[tid] = lazy_offset(L, tid);
         s_fix[tid] = 0ull;
     }
 
-    // per-thread constants: staging pieces, strip position, ring cell
-    int q_soff[2], q_lx[2], q_ly[2], q_reg[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int p = tid + h * NT;
-        const int r = p / (SW / 4), c4 = p - r * (SW / 4);
-        q_soff[h] = r * SP + 4 * c4;
-        q_lx[h] = 4 * c4 - 4;
-        q_ly[h] = r - 2;
-        q_reg[h] = (q_lx[h] + B) / B + RB * ((q_ly[h] + B) / B);
-    }
-    const int tx = tid & 31, ly0 = (tid >> 5) * ROWS;
-    const int kb = tx / B + TB * (ly0 / B);     // tile block of this strip
-    // ring cell of this thread: the first RING threads, so whole warps carry the
-    // ring (measured faster than spreading it thinly over every warp)
-    const int rg_p = tid;
-    const bool rg_on = tid < RING;
-    int rg_lx = 0, rg_ly = 0;
-    if (rg_p < T + 2) { rg_ly = -1; rg_lx = rg_p - 1; }
-    else if (rg_p < 2 * (T + 2)) { rg_ly = T; rg_lx = rg_p - (T + 2) - 1; }
-    else if (rg_p < 2 * (T + 2) + T) { rg_lx = -1; rg_ly = rg_p - 2 * (T + 2); }
-    else { rg_lx = T; rg_ly = rg_p - 2 * (T + 2) - T; }
-    const int rg_reg = (rg_lx + B) / B + RB * ((rg_ly + B) / B);
+    // per-thread constants: patch position, ring cells
+    const int lx0 = 4 * (tid & 7), ly0 = 2 * (tid >> 3);
+    const int kb = lx0 / B + TB * (ly0 / B);     // tile block of this patch
+    // ring cells 2 tid and 2 tid + 1 (threads below NPAIR): the row above the
+    // tile, the row below (34 cells each, corners included), the left and the
+    // right column (32 each); consecutive cells are neighbours, so a pair never
+    // straddles two sides
+    const bool rg_on = tid < NPAIR;
     double fsum[3] = {0.0, 0.0, 0.0};   // this thread's stored changes (exact: see below)
     __syncthreads();
-    const float Cx = s_Cf[0], Cy = s_Cf[1], Cz = s_Cf[2];
+    const f2 C2x = f2_pack(s_Cf[0], s_Cf[0]), C2y = f2_pack(s_Cf[1], s_Cf[1]), C2z = f2_pack(s_Cf[2], s_Cf[2]);
 
     auto build_nbr = [&](int idx, int st) {
         if (tid < RB * RB) {
@@ -120,14 +151,18 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
         const int X0 = (tile % ntx) * T, Y0 = (tile / ntx) * T;
         float* dst = stage + st * 3 * SV;
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            if (h == 0 || tid + NT < NQ) {
-                const int gx = wrap_p(X0 + q_lx[h], g.nx), gy = wrap_p(Y0 + q_ly[h], g.ny);
+        for (int h = 0; h < NQT; ++h) {
+            const int p = tid + h * NT;          // piece p: staged row p / (SW/4), 4-cell column p % (SW/4)
+            if (p < NQ) {
+                const int r = p / (SW / 4), c4 = p - r * (SW / 4);
+                const int lx = 4 * c4 - 4, ly = r - 2;
+                const int soff = r * SP + 4 * c4;
+                const int gx = wrap_p(X0 + lx, g.nx), gy = wrap_p(Y0 + ly, g.ny);
                 const size_t gi = (size_t)gx + nx * gy;
-                const int par = s_npar[st][q_reg[h]];
-                cp_async16(dst + q_soff[h], (par ? Q.x[1] : Q.x[0]) + gi);
-                cp_async16(dst + SV + q_soff[h], (par ? Q.y[1] : Q.y[0]) + gi);
-                cp_async16(dst + 2 * SV + q_soff[h], (par ? Q.z[1] : Q.z[0]) + gi);
+                const int par = s_npar[st][(lx + B) / B + RB * ((ly + B) / B)];
+                cp_async16(dst + soff, (par ? Q.x[1] : Q.x[0]) + gi);
+                cp_async16(dst + SV + soff, (par ? Q.y[1] : Q.y[0]) + gi);
+                cp_async16(dst + 2 * SV + soff, (par ? Q.z[1] : Q.z[0]) + gi);
             }
         }
         cp_async_commit();
@@ -184,128 +219,154 @@ __global__ void __launch_bounds__(256, 4) modelb_tile_step(GridP g, FlagP f, MBF
             const float* sz = sy + SV;
             const bool own = (tm >> kb) & 1u;
 
-            // ---- potentials of this strip (Calc_mu, kernel.cu:371-388)
+            // ---- potentials of this patch (Calc_mu, kernel.cu:371-388)
             if (own) {
-                int si = (ly0 + 1) * SP + tx + 4;     // staged row ly0 - 1
-                float hxm = __fadd_rn(sx[si + 1], sx[si - 1]), cxm = sx[si];
-                float hym = __fadd_rn(sy[si + 1], sy[si - 1]), cym = sy[si];
-                float hzm = __fadd_rn(sz[si + 1], sz[si - 1]), czm = sz[si];
-                si += SP;
-                float hx0 = __fadd_rn(sx[si + 1], sx[si - 1]), cx0 = sx[si];
-                float hy0 = __fadd_rn(sy[si + 1], sy[si - 1]), cy0 = sy[si];
-                float hz0 = __fadd_rn(sz[si + 1], sz[si - 1]), cz0 = sz[si];
-                bool wake = false;
+                const int s0 = (ly0 + 1) * SP + lx0 + 4;     // staged row ly0 - 1, column lx0
+                f2 lx_[2][2], cx_[2][2], ly_[2][2], cy_[2][2], lz_[2][2], cz_[2][2];
+                quad_laps<SP>(K, sx, s0, lx_, cx_);
+                quad_laps<SP>(K, sy, s0, ly_, cy_);
+                quad_laps<SP>(K, sz, s0, lz_, cz_);
+                float wmax = -INFINITY;                      // largest |lap z| of the patch (wake test)
 #pragma unroll
-                for (int r = 0; r < ROWS; ++r) {
-                    si += SP;
-                    const float hxp = __fadd_rn(sx[si + 1], sx[si - 1]), cxp = sx[si];
-                    const float hyp = __fadd_rn(sy[si + 1], sy[si - 1]), cyp = sy[si];
-                    const float hzp = __fadd_rn(sz[si + 1], sz[si - 1]), czp = sz[si];
-                    const float lapx = lap9_rows(hxm, cxm, hx0, cx0, hxp, cxp, inv_dx2);
-                    const float lapy = lap9_rows(hym, cym, hy0, cy0, hyp, cyp, inv_dx2);
-                    const float lapz = lap9_rows(hzm, czm, hz0, cz0, hzp, czp, inv_dx2);
-                    float ux, uy, uz;
-                    mb_potentials(P, __fsub_rn(cx0, Cx), __fsub_rn(cy0, Cy), __fsub_rn(cz0, Cz), lapx, lapy, lapz,
-                                  ux, uy, uz);
-                    const int mi = (ly0 + r + 1) * MP + tx + 1;
-                    mu[mi] = ux;
-                    mu[MV + mi] = uy;
-                    mu[2 * MV + mi] = uz;
-                    wake |= fabsf(lapz) > P.thr;
-                    hxm = hx0; cxm = cx0; hx0 = hxp; cx0 = cxp;
-                    hym = hy0; cym = cy0; hy0 = hyp; cy0 = cyp;
-                    hzm = hz0; czm = cz0; hz0 = hzp; cz0 = czp;
+                for (int r = 0; r < 2; ++r) {
+                    f2 ux[2], uy[2], uz[2];
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        mb_potentials2(K, sub2(cx_[r][k], C2x), sub2(cy_[r][k], C2y), sub2(cz_[r][k], C2z),
+                                       lx_[r][k], ly_[r][k], lz_[r][k], ux[k], uy[k], uz[k]);
+                        wmax = fmaxf(wmax, fmaxf(fabsf(f2_lo(lz_[r][k])), fabsf(f2_hi(lz_[r][k]))));
+                    }
+                    const int mi = (ly0 + r + 1) * MP + lx0 + 4;
+                    *reinterpret_cast<float4*>(mu + mi) = f4_of(ux[0], ux[1]);
+                    *reinterpret_cast<float4*>(mu + MV + mi) = f4_of(uy[0], uy[1]);
+                    *reinterpret_cast<float4*>(mu + 2 * MV + mi) = f4_of(uz[0], uz[1]);
                 }
-                if (DBA && wake) s_nx[kb] = 1;
+                if (DBA && wmax > P.thr) s_nx[kb] = 1;
             } else {
                 // inactive block inside the tile: its persisted ring (stale potentials)
 #pragma unroll
-                for (int r = 0; r < ROWS; ++r) {
-                    const size_t gi = (size_t)(X0 + tx) + nx * (size_t)(Y0 + ly0 + r);
-                    const int mi = (ly0 + r + 1) * MP + tx + 1;
-                    mu[mi] = Q.mu[0][gi];
-                    mu[MV + mi] = Q.mu[1][gi];
-                    mu[2 * MV + mi] = Q.mu[2][gi];
+                for (int r = 0; r < 2; ++r) {
+                    const size_t gi = (size_t)(X0 + lx0) + nx * (size_t)(Y0 + ly0 + r);
+                    const int mi = (ly0 + r + 1) * MP + lx0 + 4;
+#pragma unroll
+                    for (int q = 0; q < 3; ++q)
+                        *reinterpret_cast<float4*>(mu + q * MV + mi) = *reinterpret_cast<const float4*>(Q.mu[q] + gi);
                 }
             }
             if (rg_on) {
-                const int mi = (rg_ly + 1) * MP + rg_lx + 1;
-                if (s_nact[st][rg_reg]) {
-                    const int si = (rg_ly + 2) * SP + rg_lx + 4;
-                    float ux, uy, uz;
-                    mb_potentials(P, __fsub_rn(sx[si], Cx), __fsub_rn(sy[si], Cy), __fsub_rn(sz[si], Cz),
-                                  lap9(sx, si, SP, inv_dx2), lap9(sy, si, SP, inv_dx2),
-                                  lap9(sz, si, SP, inv_dx2), ux, uy, uz);
-                    mu[mi] = ux;
-                    mu[MV + mi] = uy;
-                    mu[2 * MV + mi] = uz;
-                } else {
-                    const size_t gi = (size_t)wrap_p(X0 + rg_lx, g.nx) + nx * (size_t)wrap_p(Y0 + rg_ly, g.ny);
-                    mu[mi] = Q.mu[0][gi];
-                    mu[MV + mi] = Q.mu[1][gi];
-                    mu[2 * MV + mi] = Q.mu[2][gi];
+                int rg_lx[2], rg_ly[2], rg_reg[2];
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int p = 2 * tid + e;
+                    int lx, ly;
+                    if (p < T + 2) { ly = -1; lx = p - 1; }
+                    else if (p < 2 * (T + 2)) { ly = T; lx = p - (T + 2) - 1; }
+                    else if (p < 2 * (T + 2) + T) { lx = -1; ly = p - 2 * (T + 2); }
+                    else { lx = T; ly = p - 2 * (T + 2) - T; }
+                    rg_lx[e] = lx;
+                    rg_ly[e] = ly;
+                    rg_reg[e] = (lx + B) / B + RB * ((ly + B) / B);
+                }
+                const bool a0 = s_nact[st][rg_reg[0]] != 0, a1 = s_nact[st][rg_reg[1]] != 0;
+                const int si0 = (rg_ly[0] + 2) * SP + rg_lx[0] + 4, si1 = (rg_ly[1] + 2) * SP + rg_lx[1] + 4;
+                f2 ux = make_float2(0.f, 0.f), uy = ux, uz = ux;
+                if (a0 || a1) {
+                    const float Cx = f2_lo(C2x), Cy = f2_lo(C2y), Cz = f2_lo(C2z), inv_dx2 = P.inv_dx2;
+                    mb_potentials2(K, f2_pack(__fsub_rn(sx[si0], Cx), __fsub_rn(sx[si1], Cx)),
+                                   f2_pack(__fsub_rn(sy[si0], Cy), __fsub_rn(sy[si1], Cy)),
+                                   f2_pack(__fsub_rn(sz[si0], Cz), __fsub_rn(sz[si1], Cz)),
+                                   f2_pack(lap9(sx, si0, SP, inv_dx2), lap9(sx, si1, SP, inv_dx2)),
+                                   f2_pack(lap9(sy, si0, SP, inv_dx2), lap9(sy, si1, SP, inv_dx2)),
+                                   f2_pack(lap9(sz, si0, SP, inv_dx2), lap9(sz, si1, SP, inv_dx2)), ux, uy, uz);
+                }
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int mi = (rg_ly[e] + 1) * MP + rg_lx[e] + 4;
+                    if (e == 0 ? a0 : a1) {
+                        mu[mi] = e == 0 ? f2_lo(ux) : f2_hi(ux);
+                        mu[MV + mi] = e == 0 ? f2_lo(uy) : f2_hi(uy);
+                        mu[2 * MV + mi] = e == 0 ? f2_lo(uz) : f2_hi(uz);
+                    } else {
+                        const size_t gi =
+                            (size_t)wrap_p(X0 + rg_lx[e], g.nx) + nx * (size_t)wrap_p(Y0 + rg_ly[e], g.ny);
+                        mu[mi] = Q.mu[0][gi];
+                        mu[MV + mi] = Q.mu[1][gi];
+                        mu[2 * MV + mi] = Q.mu[2][gi];
+                    }
                 }
             }
             __syncthreads();                     // potentials and wake-up tests complete
 
-            // ---- update of this strip (Update, kernel.cu:419-434)
+            // ---- update of this patch (Update, kernel.cu:419-434)
             if (own) {
                 const int dst = (int)((tm >> (16 + kb)) & 1u) ^ 1;
                 float* ox = dst ? Q.x[1] : Q.x[0];
                 float* oy = dst ? Q.y[1] : Q.y[0];
                 float* oz = dst ? Q.z[1] : Q.z[0];
                 const bool persist = DBA && !s_nx[kb];
-                const bool edge_x = (tx % B) == 0 || (tx % B) == B - 1;
-                const bool ring_top = (ly0 % B) == 0, ring_bot = ((ly0 + ROWS - 1) % B) == B - 1;
-                int mi = ly0 * MP + tx + 1;           // potential row ly0 - 1
-                const float* m0 = mu;
-                const float* m1 = mu + MV;
-                const float* m2 = mu + 2 * MV;
-                float hxm = __fadd_rn(m0[mi + 1], m0[mi - 1]), cxm = m0[mi];
-                float hym = __fadd_rn(m1[mi + 1], m1[mi - 1]), cym = m1[mi];
-                float hzm = __fadd_rn(m2[mi + 1], m2[mi - 1]), czm = m2[mi];
-                mi += MP;
-                float hx0 = __fadd_rn(m0[mi + 1], m0[mi - 1]), cx0 = m0[mi];
-                float hy0 = __fadd_rn(m1[mi + 1], m1[mi - 1]), cy0 = m1[mi];
-                float hz0 = __fadd_rn(m2[mi + 1], m2[mi - 1]), cz0 = m2[mi];
-                bool bad = false;
+                const bool left = (lx0 % B) == 0, right = ((lx0 + 3) % B) == B - 1;
+                const bool ring_top = (ly0 % B) == 0, ring_bot = ((ly0 + 1) % B) == B - 1;
+                const int m0 = ly0 * MP + lx0 + 4;           // potential row ly0 - 1, column lx0
+                f2 lmx[2][2], mx[2][2], lmy[2][2], my[2][2], lmz[2][2], mz[2][2];
+                quad_laps<MP>(K, mu, m0, lmx, mx);
+                quad_laps<MP>(K, mu + MV, m0, lmy, my);
+                quad_laps<MP>(K, mu + 2 * MV, m0, lmz, mz);
+                f2 fin = K.zero;                             // NaN once any stored value is not finite
 #pragma unroll
-                for (int r = 0; r < ROWS; ++r) {
-                    mi += MP;
-                    const float hxp = __fadd_rn(m0[mi + 1], m0[mi - 1]), cxp = m0[mi];
-                    const float hyp = __fadd_rn(m1[mi + 1], m1[mi - 1]), cyp = m1[mi];
-                    const float hzp = __fadd_rn(m2[mi + 1], m2[mi - 1]), czp = m2[mi];
-                    float cx, cy, cz;
-                    mb_changes(P, cx0, cy0, cz0, lap9_rows(hxm, cxm, hx0, cx0, hxp, cxp, inv_dx2),
-                               lap9_rows(hym, cym, hy0, cy0, hyp, cyp, inv_dx2),
-                               lap9_rows(hzm, czm, hz0, cz0, hzp, czp, inv_dx2), cx, cy, cz);
-                    const int ly = ly0 + r;
-                    const int si = (ly + 2) * SP + tx + 4;
-                    const float x0 = sx[si], y0 = sy[si], z0 = sz[si];
-                    const float xn = __fadd_rn(x0, cx), yn = __fadd_rn(y0, cy), zn = __fadd_rn(z0, cz);
-                    const size_t gi = (size_t)(X0 + tx) + nx * (size_t)(Y0 + ly);
-                    ox[gi] = xn;
-                    oy[gi] = yn;
-                    oz[gi] = zn;
-                    bad |= !(fabsf(xn) < INFINITY && fabsf(yn) < INFINITY && fabsf(zn) < INFINITY);
-                    if (L.accumulate) {
-                        // the change actually stored (exact in FP32).  With stored values above
-                        // 2^-17 each is a multiple of 2^-40, so while a thread's partial sums stay
-                        // below 2^13 they are exact in FP64 and convert exactly to fixed point.
-                        fsum[0] += (double)__fsub_rn(xn, x0);
-                        fsum[1] += (double)__fsub_rn(yn, y0);
-                        fsum[2] += (double)__fsub_rn(zn, z0);
+                for (int r = 0; r < 2; ++r) {
+                    const int si = (ly0 + r + 2) * SP + lx0 + 4;
+                    const float4 x4 = *reinterpret_cast<const float4*>(sx + si);
+                    const float4 y4 = *reinterpret_cast<const float4*>(sy + si);
+                    const float4 z4 = *reinterpret_cast<const float4*>(sz + si);
+                    const f2 xo[2] = {f2_pack(x4.x, x4.y), f2_pack(x4.z, x4.w)};
+                    const f2 yo[2] = {f2_pack(y4.x, y4.y), f2_pack(y4.z, y4.w)};
+                    const f2 zo[2] = {f2_pack(z4.x, z4.y), f2_pack(z4.z, z4.w)};
+                    f2 xn[2], yn[2], zn[2];
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        f2 cx, cy, cz;
+                        mb_changes2(K, mx[r][k], my[r][k], mz[r][k], lmx[r][k], lmy[r][k], lmz[r][k], cx, cy, cz);
+                        xn[k] = add2(xo[k], cx);
+                        yn[k] = add2(yo[k], cy);
+                        zn[k] = add2(zo[k], cz);
+                        fin = add2(fin, fma2(xn[k], K.zero, fma2(yn[k], K.zero, mul2(zn[k], K.zero, K.nz))));
+                        if (L.accumulate) {
+                            // the change actually stored (exact in FP32).  With stored values above
+                            // 2^-17 each is a multiple of 2^-40, so while a thread's partial sums stay
+                            // below 2^13 they are exact in FP64 and convert exactly to fixed point.
+                            const f2 dx = sub2(xn[k], xo[k]), dy = sub2(yn[k], yo[k]), dz = sub2(zn[k], zo[k]);
+                            fsum[0] += (double)f2_lo(dx);
+                            fsum[0] += (double)f2_hi(dx);
+                            fsum[1] += (double)f2_lo(dy);
+                            fsum[1] += (double)f2_hi(dy);
+                            fsum[2] += (double)f2_lo(dz);
+                            fsum[2] += (double)f2_hi(dz);
+                        }
                     }
-                    if (persist && (edge_x || (r == 0 && ring_top) || (r == ROWS - 1 && ring_bot))) {
-                        Q.mu[0][gi] = cx0;
-                        Q.mu[1][gi] = cy0;
-                        Q.mu[2][gi] = cz0;
+                    const size_t gi = (size_t)(X0 + lx0) + nx * (size_t)(Y0 + ly0 + r);
+                    *reinterpret_cast<float4*>(ox + gi) = f4_of(xn[0], xn[1]);
+                    *reinterpret_cast<float4*>(oy + gi) = f4_of(yn[0], yn[1]);
+                    *reinterpret_cast<float4*>(oz + gi) = f4_of(zn[0], zn[1]);
+                    if (persist) {
+                        if ((r == 0 && ring_top) || (r == 1 && ring_bot)) {
+                            *reinterpret_cast<float4*>(Q.mu[0] + gi) = f4_of(mx[r][0], mx[r][1]);
+                            *reinterpret_cast<float4*>(Q.mu[1] + gi) = f4_of(my[r][0], my[r][1]);
+                            *reinterpret_cast<float4*>(Q.mu[2] + gi) = f4_of(mz[r][0], mz[r][1]);
+                        } else {
+                            if (left) {
+                                Q.mu[0][gi] = f2_lo(mx[r][0]);
+                                Q.mu[1][gi] = f2_lo(my[r][0]);
+                                Q.mu[2][gi] = f2_lo(mz[r][0]);
+                            }
+                            if (right) {
+                                Q.mu[0][gi + 3] = f2_hi(mx[r][1]);
+                                Q.mu[1][gi + 3] = f2_hi(my[r][1]);
+                                Q.mu[2][gi + 3] = f2_hi(mz[r][1]);
+                            }
+                        }
                     }
-                    hxm = hx0; cxm = cx0; hx0 = hxp; cx0 = cxp;
-                    hym = hy0; cym = cy0; hy0 = hyp; cy0 = cyp;
-                    hzm = hz0; czm = cz0; hz0 = hzp; cz0 = czp;
                 }
-                if (bad) raise_status(f.status, 5);
+                if (!(f2_lo(fin) == 0.f && f2_hi(fin) == 0.f)) raise_status(f.status, 5);
             }
             if (DBA && tid < NBT && ((tm >> tid) & 1u)) {
                 const int b = ((tile % ntx) * TB + tid % TB) + g.nbx * ((tile / ntx) * TB + tid / TB);
