@@ -11,8 +11,9 @@
 //   * the tile plus a 2-cell halo of x, y, z is staged with 16-byte cp.async
 //     copies, double-buffered: tile i+1 is in flight while tile i computes.
 //     Each 16-byte piece lies inside one block, whose parity picks the buffer;
-//   * each of the 128 threads owns a 4-column x 2-row patch.  A staged row of
-//     the patch is one 16-byte shared load plus its left and right neighbours;
+//   * each thread owns a 4-column x R-row patch (R = kMBTileRows; 256 / R
+//     threads per CTA).  A staged row of the patch is one 16-byte shared load
+//     plus its left and right neighbours;
 //     the row sums of the 9-point Laplacian are formed once per loaded row and
 //     the arithmetic runs on pairs of cells (k_pair.cuh: the two-lane FP32
 //     instructions of sm_100, rounded lane by lane like the scalar helpers), so
@@ -20,6 +21,8 @@
 //   * the 132-cell potential ring around the tile is computed (active owner)
 //     or loaded from the persisted ring (inactive owner) two cells per thread
 //     by the first 66 threads;
+//   * each listed tile's coordinates are derived once per tile and handed to
+//     the neighbour-table, staging and flag code;
 //   * a block persists its ring potentials only when its own wake-up test is
 //     negative: a block whose test is positive is active next step (it wakes
 //     itself), so its ring from this step is never read as stale;
@@ -34,8 +37,11 @@
 
 namespace dba {
 
-template <int B> struct MBTile {
-    static constexpr int NT = 128;
+// rows per thread patch of the tile kernel (1: 256 threads per CTA, 2: 128)
+constexpr int kMBTileRows = 2;
+
+template <int B, int R = kMBTileRows> struct MBTile {
+    static constexpr int NT = 256 / R;
     static constexpr int T = 32;              // tile edge in cells
     static constexpr int TB = T / B;          // blocks per tile edge
     static constexpr int NBT = TB * TB;       // blocks per tile
@@ -45,16 +51,19 @@ template <int B> struct MBTile {
     static constexpr int SP = SW + 4;         // staged row pitch (16-byte multiple)
     static constexpr int SV = SR * SP;        // one staged field
     static constexpr int NQ = SR * (SW / 4);  // 16-byte pieces per staged field
+    static constexpr int QC = SW / 4;         // 16-byte pieces per staged row
     static constexpr int NQT = (NQ + NT - 1) / NT;   // pieces per thread
+    static constexpr int QR = SR / NQT;       // row stride between a thread's pieces
     static constexpr int MP = T + 8;          // potential row pitch: column lx at lx + 4 (aligned quads)
     static constexpr int MV = (T + 2) * MP;   // one potential field (rows -1 .. T)
     static constexpr int RING = 4 * T + 4;    // potential cells around the tile
     static constexpr int NPAIR = RING / 2;    // ring threads, two cells each
     static constexpr int TPP = NT / NBT;      // tiles per scan pass
-    static constexpr int ROWS = 2;            // rows per thread patch
+    static constexpr int ROWS = R;            // rows per thread patch
     static constexpr int QX = T / 4;          // patches per tile row
     static constexpr size_t smem = sizeof(float) * (2 * 3 * SV + 3 * MV);
-    static_assert(QX * (T / ROWS) == NT, "one 4x2 patch per thread");
+    static_assert(QX * (T / ROWS) == NT, "one 4 x R patch per thread");
+    static_assert(SR % NQT == 0 && QR * QC <= NT, "each staging thread takes one column, NQT rows QR apart");
     static_assert(T % B == 0 && B % 4 == 0 && B % ROWS == 0 && NBT <= 16 && NQT * NT >= NQ && NPAIR <= NT,
                   "tile shape");
 };
@@ -71,35 +80,65 @@ __device__ __forceinline__ void quad_row(const float* s, int i, f2& h01, f2& h23
     c23 = f2_pack(v.z, v.w);
 }
 
-// Laplacians and centres of the two patch rows of one field; i = patch column 0
-// of the row above the patch, PITCH = the array's row pitch
-template <int PITCH>
-__device__ __forceinline__ void quad_laps(const MBPairP& K, const float* s, int i, f2 lap[2][2], f2 cen[2][2])
+// Laplacians and centres of the R patch rows of one field (a 3-row window slid
+// down the patch); i = patch column 0 of the row above the patch, PITCH = the
+// array's row pitch
+template <int PITCH, int R>
+__device__ __forceinline__ void quad_laps(const MBPairP& K, const float* s, int i, f2 lap[R][2], f2 cen[R][2])
 {
     f2 h[3][2], c[3][2];
     quad_row(s, i, h[0][0], h[0][1], c[0][0], c[0][1]);
     quad_row(s, i + PITCH, h[1][0], h[1][1], c[1][0], c[1][1]);
-    quad_row(s, i + 2 * PITCH, h[2][0], h[2][1], c[2][0], c[2][1]);
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        lap[0][k] = lap9_rows2(K, h[0][k], c[0][k], h[1][k], c[1][k], h[2][k], c[2][k]);
-        cen[0][k] = c[1][k];
-    }
-    quad_row(s, i + 3 * PITCH, h[0][0], h[0][1], c[0][0], c[0][1]);
+    for (int r = 0; r < R; ++r) {
+        const int m = r % 3, o = (r + 1) % 3, p = (r + 2) % 3;
+        quad_row(s, i + (r + 2) * PITCH, h[p][0], h[p][1], c[p][0], c[p][1]);
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        lap[1][k] = lap9_rows2(K, h[1][k], c[1][k], h[2][k], c[2][k], h[0][k], c[0][k]);
-        cen[1][k] = c[2][k];
+        for (int k = 0; k < 2; ++k) {
+            lap[r][k] = lap9_rows2(K, h[m][k], c[m][k], h[o][k], c[o][k], h[p][k], c[p][k]);
+            cen[r][k] = c[o][k];
+        }
     }
+}
+
+// Laplacians of one field at a ring pair: horizontal (cells i, i + 1 of one
+// row: three rows of four loads) or vertical (cells i, i + PITCH: four rows of
+// three loads); the same row sums and operations as the scalar lap9
+template <int PITCH>
+__device__ __forceinline__ f2 ring_lap_h(const MBPairP& K, const float* s, int i)
+{
+    f2 h[3], c[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        const float* q = s + i + (r - 1) * PITCH;
+        const float a0 = q[-1], a1 = q[0], a2 = q[1], a3 = q[2];
+        h[r] = f2_pack(__fadd_rn(a2, a0), __fadd_rn(a3, a1));
+        c[r] = f2_pack(a1, a2);
+    }
+    return lap9_rows2(K, h[0], c[0], h[1], c[1], h[2], c[2]);
+}
+
+template <int PITCH>
+__device__ __forceinline__ f2 ring_lap_v(const MBPairP& K, const float* s, int i)
+{
+    float h[4], c[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const float* q = s + i + (r - 1) * PITCH;
+        h[r] = __fadd_rn(q[1], q[-1]);
+        c[r] = q[0];
+    }
+    return lap9_rows2(K, f2_pack(h[0], h[1]), f2_pack(c[0], c[1]), f2_pack(h[1], h[2]), f2_pack(c[1], c[2]),
+                      f2_pack(h[2], h[3]), f2_pack(c[2], c[3]));
 }
 
 __device__ __forceinline__ float4 f4_of(f2 a, f2 b) { return make_float4(f2_lo(a), f2_hi(a), f2_lo(b), f2_hi(b)); }
 
-template <int B, bool DBA>
-__global__ void __launch_bounds__(128, 4)
+template <int B, int R, bool DBA>
+__global__ void __launch_bounds__(256 / R, 4)
     modelb_tile_step(GridP g, FlagP f, MBFastP P, MBPairP K, MBFastBuf Q, LazyP L)
 {
-    using S = MBTile<B>;
+    using S = MBTile<B, R>;
     constexpr int NT = S::NT, T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, SW = S::SW, SP = S::SP, SV = S::SV;
     constexpr int NQ = S::NQ, NQT = S::NQT, MP = S::MP, MV = S::MV, RING = S::RING, NPAIR = S::NPAIR;
     constexpr int TPP = S::TPP;
@@ -123,22 +162,27 @@ __global__ void __launch_bounds__(128, 4)
         s_fix[tid] = 0ull;
     }
 
-    // per-thread constants: patch position, ring cells
-    const int lx0 = 4 * (tid & 7), ly0 = 2 * (tid >> 3);
+    // per-thread constants: staging column and rows (thread q_c + QC q_r takes
+    // column q_c of staged rows q_r, q_r + QR, ...), patch position, ring cells
+    constexpr int QC = S::QC, QR = S::QR;
+    const bool q_on = tid < QR * QC;
+    const int q_r = tid / QC, q_c = tid - (tid / QC) * QC;
+    const int q_lx = 4 * q_c - 4;                               // tile column of the piece
+    const int q_soff = q_r * SP + 4 * q_c;                      // staged offset of the first piece
+    int q_yreg = 0;                                             // neighbourhood row of each piece (8 bits each)
+#pragma unroll
+    for (int h = 0; h < NQT; ++h) q_yreg |= (((q_r + h * QR - 2) + B) / B) << (8 * h);
+    const int q_xreg = (q_lx + B) / B;
+    const int lx0 = 4 * (tid & 7), ly0 = R * (tid >> 3);
     const int kb = lx0 / B + TB * (ly0 / B);     // tile block of this patch
-    // ring cells 2 tid and 2 tid + 1 (threads below NPAIR): the row above the
-    // tile, the row below (34 cells each, corners included), the left and the
-    // right column (32 each); consecutive cells are neighbours, so a pair never
-    // straddles two sides
+    // ring pairs: threads below NPAIR (66) take two neighbouring ring cells each
     const bool rg_on = tid < NPAIR;
     double fsum[3] = {0.0, 0.0, 0.0};   // this thread's stored changes (exact: see below)
     __syncthreads();
     const f2 C2x = f2_pack(s_Cf[0], s_Cf[0]), C2y = f2_pack(s_Cf[1], s_Cf[1]), C2z = f2_pack(s_Cf[2], s_Cf[2]);
 
-    auto build_nbr = [&](int idx, int st) {
+    auto build_nbr = [&](int tbx, int tby, int st) {
         if (tid < RB * RB) {
-            const int tile = s_tile[idx];
-            const int tbx = tile % ntx, tby = tile / ntx;
             const int rx = tid % RB, ry = tid / RB;
             const int bx = wrap_p(tbx * TB + rx - 1, g.nbx), by = wrap_p(tby * TB + ry - 1, g.nby);
             const int ob = bx + g.nbx * by;
@@ -146,23 +190,22 @@ __global__ void __launch_bounds__(128, 4)
             s_nact[st][tid] = DBA ? (f.wake_cur[ob] ? 1 : 0) : 1;
         }
     };
-    auto issue = [&](int idx, int st) {
-        const int tile = s_tile[idx];
-        const int X0 = (tile % ntx) * T, Y0 = (tile / ntx) * T;
-        float* dst = stage + st * 3 * SV;
+    auto issue = [&](int tbx, int tby, int st) {
+        if (q_on) {
+            const int X0 = tbx * T, Y0 = tby * T;
+            float* dst = stage + st * 3 * SV + q_soff;
+            // no piece of a tile away from the domain edge wraps
+            const bool inner = tbx > 0 && tbx < ntx - 1 && tby > 0 && tby < nty - 1;
+            const long long gi0 = (long long)(X0 + q_lx) + (long long)nx * (Y0 + q_r - 2);
 #pragma unroll
-        for (int h = 0; h < NQT; ++h) {
-            const int p = tid + h * NT;          // piece p: staged row p / (SW/4), 4-cell column p % (SW/4)
-            if (p < NQ) {
-                const int r = p / (SW / 4), c4 = p - r * (SW / 4);
-                const int lx = 4 * c4 - 4, ly = r - 2;
-                const int soff = r * SP + 4 * c4;
-                const int gx = wrap_p(X0 + lx, g.nx), gy = wrap_p(Y0 + ly, g.ny);
-                const size_t gi = (size_t)gx + nx * gy;
-                const int par = s_npar[st][(lx + B) / B + RB * ((ly + B) / B)];
-                cp_async16(dst + soff, (par ? Q.x[1] : Q.x[0]) + gi);
-                cp_async16(dst + SV + soff, (par ? Q.y[1] : Q.y[0]) + gi);
-                cp_async16(dst + 2 * SV + soff, (par ? Q.z[1] : Q.z[0]) + gi);
+            for (int h = 0; h < NQT; ++h) {
+                long long gi = gi0 + (long long)(h * QR) * (long long)nx;
+                if (!inner)
+                    gi = (long long)wrap_p(X0 + q_lx, g.nx) + (long long)nx * wrap_p(Y0 + q_r + h * QR - 2, g.ny);
+                const int par = s_npar[st][q_xreg + RB * ((q_yreg >> (8 * h)) & 0xff)];
+                cp_async16(dst + h * QR * SP, (par ? Q.x[1] : Q.x[0]) + gi);
+                cp_async16(dst + SV + h * QR * SP, (par ? Q.y[1] : Q.y[0]) + gi);
+                cp_async16(dst + 2 * SV + h * QR * SP, (par ? Q.z[1] : Q.z[0]) + gi);
             }
         }
         cp_async_commit();
@@ -197,23 +240,30 @@ __global__ void __launch_bounds__(128, 4)
             __syncthreads();
         }
         const int cnt = s_cnt;
+        int tbx_n = 0, tby_n = 0;                // tile coordinates of the next listed tile
         if (cnt > 0) {
-            build_nbr(0, 0);
+            tby_n = s_tile[0] / ntx;
+            tbx_n = s_tile[0] - tby_n * ntx;
+            build_nbr(tbx_n, tby_n, 0);
             __syncthreads();
-            issue(0, 0);
+            issue(tbx_n, tby_n, 0);
         }
         for (int i = 0; i < cnt; ++i) {
             const int st = i & 1;
-            if (i + 1 < cnt) build_nbr(i + 1, st ^ 1);
+            const int tbx = tbx_n, tby = tby_n;  // tile i
+            if (i + 1 < cnt) {
+                tby_n = s_tile[i + 1] / ntx;
+                tbx_n = s_tile[i + 1] - tby_n * ntx;
+                build_nbr(tbx_n, tby_n, st ^ 1);
+            }
             __syncthreads();                     // next table ready; stage st^1, mu and s_nx free
             if (tid < NBT) s_nx[tid] = 0;
-            if (i + 1 < cnt) issue(i + 1, st ^ 1);
+            if (i + 1 < cnt) issue(tbx_n, tby_n, st ^ 1);
             else cp_async_commit();
             cp_async_wait1();
             __syncthreads();                     // tile i staged
-            const int tile = s_tile[i];
             const unsigned tm = s_tmeta[i];
-            const int X0 = (tile % ntx) * T, Y0 = (tile / ntx) * T;
+            const int X0 = tbx * T, Y0 = tby * T;
             const float* sx = stage + st * 3 * SV;
             const float* sy = sx + SV;
             const float* sz = sy + SV;
@@ -222,13 +272,13 @@ __global__ void __launch_bounds__(128, 4)
             // ---- potentials of this patch (Calc_mu, kernel.cu:371-388)
             if (own) {
                 const int s0 = (ly0 + 1) * SP + lx0 + 4;     // staged row ly0 - 1, column lx0
-                f2 lx_[2][2], cx_[2][2], ly_[2][2], cy_[2][2], lz_[2][2], cz_[2][2];
-                quad_laps<SP>(K, sx, s0, lx_, cx_);
-                quad_laps<SP>(K, sy, s0, ly_, cy_);
-                quad_laps<SP>(K, sz, s0, lz_, cz_);
+                f2 lx_[R][2], cx_[R][2], ly_[R][2], cy_[R][2], lz_[R][2], cz_[R][2];
+                quad_laps<SP, R>(K, sx, s0, lx_, cx_);
+                quad_laps<SP, R>(K, sy, s0, ly_, cy_);
+                quad_laps<SP, R>(K, sz, s0, lz_, cz_);
                 float wmax = -INFINITY;                      // largest |lap z| of the patch (wake test)
 #pragma unroll
-                for (int r = 0; r < 2; ++r) {
+                for (int r = 0; r < R; ++r) {
                     f2 ux[2], uy[2], uz[2];
 #pragma unroll
                     for (int k = 0; k < 2; ++k) {
@@ -245,7 +295,7 @@ __global__ void __launch_bounds__(128, 4)
             } else {
                 // inactive block inside the tile: its persisted ring (stale potentials)
 #pragma unroll
-                for (int r = 0; r < 2; ++r) {
+                for (int r = 0; r < R; ++r) {
                     const size_t gi = (size_t)(X0 + lx0) + nx * (size_t)(Y0 + ly0 + r);
                     const int mi = (ly0 + r + 1) * MP + lx0 + 4;
 #pragma unroll
@@ -254,30 +304,35 @@ __global__ void __launch_bounds__(128, 4)
                 }
             }
             if (rg_on) {
+                // threads 0-31 and 64-65: horizontal pairs of the rows above and below
+                // the tile (17 each, corners included); threads 32-63: vertical pairs of
+                // the left and right columns (16 each), so no warp mixes the two shapes
+                const bool horiz = tid < 32 || tid >= 64;
                 int rg_lx[2], rg_ly[2], rg_reg[2];
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const int p = 2 * tid + e;
-                    int lx, ly;
-                    if (p < T + 2) { ly = -1; lx = p - 1; }
-                    else if (p < 2 * (T + 2)) { ly = T; lx = p - (T + 2) - 1; }
-                    else if (p < 2 * (T + 2) + T) { lx = -1; ly = p - 2 * (T + 2); }
-                    else { lx = T; ly = p - 2 * (T + 2) - T; }
-                    rg_lx[e] = lx;
-                    rg_ly[e] = ly;
-                    rg_reg[e] = (lx + B) / B + RB * ((ly + B) / B);
+                if (horiz) {
+                    const int hp = tid < 32 ? tid : tid - 32;
+                    const int ly = hp < T / 2 + 1 ? -1 : T;
+                    const int lx = 2 * (hp < T / 2 + 1 ? hp : hp - (T / 2 + 1)) - 1;
+                    rg_lx[0] = lx; rg_lx[1] = lx + 1; rg_ly[0] = ly; rg_ly[1] = ly;
+                } else {
+                    const int vp = tid - 32;
+                    const int lx = vp < T / 2 ? -1 : T;
+                    const int ly = 2 * (vp < T / 2 ? vp : vp - T / 2);
+                    rg_lx[0] = lx; rg_lx[1] = lx; rg_ly[0] = ly; rg_ly[1] = ly + 1;
                 }
+#pragma unroll
+                for (int e = 0; e < 2; ++e) rg_reg[e] = (rg_lx[e] + B) / B + RB * ((rg_ly[e] + B) / B);
                 const bool a0 = s_nact[st][rg_reg[0]] != 0, a1 = s_nact[st][rg_reg[1]] != 0;
                 const int si0 = (rg_ly[0] + 2) * SP + rg_lx[0] + 4, si1 = (rg_ly[1] + 2) * SP + rg_lx[1] + 4;
                 f2 ux = make_float2(0.f, 0.f), uy = ux, uz = ux;
                 if (a0 || a1) {
-                    const float Cx = f2_lo(C2x), Cy = f2_lo(C2y), Cz = f2_lo(C2z), inv_dx2 = P.inv_dx2;
+                    const float Cx = f2_lo(C2x), Cy = f2_lo(C2y), Cz = f2_lo(C2z);
+                    const f2 lpx = horiz ? ring_lap_h<SP>(K, sx, si0) : ring_lap_v<SP>(K, sx, si0);
+                    const f2 lpy = horiz ? ring_lap_h<SP>(K, sy, si0) : ring_lap_v<SP>(K, sy, si0);
+                    const f2 lpz = horiz ? ring_lap_h<SP>(K, sz, si0) : ring_lap_v<SP>(K, sz, si0);
                     mb_potentials2(K, f2_pack(__fsub_rn(sx[si0], Cx), __fsub_rn(sx[si1], Cx)),
                                    f2_pack(__fsub_rn(sy[si0], Cy), __fsub_rn(sy[si1], Cy)),
-                                   f2_pack(__fsub_rn(sz[si0], Cz), __fsub_rn(sz[si1], Cz)),
-                                   f2_pack(lap9(sx, si0, SP, inv_dx2), lap9(sx, si1, SP, inv_dx2)),
-                                   f2_pack(lap9(sy, si0, SP, inv_dx2), lap9(sy, si1, SP, inv_dx2)),
-                                   f2_pack(lap9(sz, si0, SP, inv_dx2), lap9(sz, si1, SP, inv_dx2)), ux, uy, uz);
+                                   f2_pack(__fsub_rn(sz[si0], Cz), __fsub_rn(sz[si1], Cz)), lpx, lpy, lpz, ux, uy, uz);
                 }
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
@@ -305,15 +360,15 @@ __global__ void __launch_bounds__(128, 4)
                 float* oz = dst ? Q.z[1] : Q.z[0];
                 const bool persist = DBA && !s_nx[kb];
                 const bool left = (lx0 % B) == 0, right = ((lx0 + 3) % B) == B - 1;
-                const bool ring_top = (ly0 % B) == 0, ring_bot = ((ly0 + 1) % B) == B - 1;
+                const bool ring_top = (ly0 % B) == 0, ring_bot = ((ly0 + R - 1) % B) == B - 1;
                 const int m0 = ly0 * MP + lx0 + 4;           // potential row ly0 - 1, column lx0
-                f2 lmx[2][2], mx[2][2], lmy[2][2], my[2][2], lmz[2][2], mz[2][2];
-                quad_laps<MP>(K, mu, m0, lmx, mx);
-                quad_laps<MP>(K, mu + MV, m0, lmy, my);
-                quad_laps<MP>(K, mu + 2 * MV, m0, lmz, mz);
+                f2 lmx[R][2], mx[R][2], lmy[R][2], my[R][2], lmz[R][2], mz[R][2];
+                quad_laps<MP, R>(K, mu, m0, lmx, mx);
+                quad_laps<MP, R>(K, mu + MV, m0, lmy, my);
+                quad_laps<MP, R>(K, mu + 2 * MV, m0, lmz, mz);
                 f2 fin = K.zero;                             // NaN once any stored value is not finite
 #pragma unroll
-                for (int r = 0; r < 2; ++r) {
+                for (int r = 0; r < R; ++r) {
                     const int si = (ly0 + r + 2) * SP + lx0 + 4;
                     const float4 x4 = *reinterpret_cast<const float4*>(sx + si);
                     const float4 y4 = *reinterpret_cast<const float4*>(sy + si);
@@ -348,7 +403,7 @@ __global__ void __launch_bounds__(128, 4)
                     *reinterpret_cast<float4*>(oy + gi) = f4_of(yn[0], yn[1]);
                     *reinterpret_cast<float4*>(oz + gi) = f4_of(zn[0], zn[1]);
                     if (persist) {
-                        if ((r == 0 && ring_top) || (r == 1 && ring_bot)) {
+                        if ((r == 0 && ring_top) || (r == R - 1 && ring_bot)) {
                             *reinterpret_cast<float4*>(Q.mu[0] + gi) = f4_of(mx[r][0], mx[r][1]);
                             *reinterpret_cast<float4*>(Q.mu[1] + gi) = f4_of(my[r][0], my[r][1]);
                             *reinterpret_cast<float4*>(Q.mu[2] + gi) = f4_of(mz[r][0], mz[r][1]);
@@ -369,10 +424,10 @@ __global__ void __launch_bounds__(128, 4)
                 if (!(f2_lo(fin) == 0.f && f2_hi(fin) == 0.f)) raise_status(f.status, 5);
             }
             if (DBA && tid < NBT && ((tm >> tid) & 1u)) {
-                const int b = ((tile % ntx) * TB + tid % TB) + g.nbx * ((tile / ntx) * TB + tid / TB);
+                const int bx = tbx * TB + tid % TB, by = tby * TB + tid / TB;
+                const int b = bx + g.nbx * by;
                 f.next[b] = (uint8_t)s_nx[tid];
-                if (s_nx[tid])
-                    wake_faces_2d(f.wake_nxt, (tile % ntx) * TB + tid % TB, (tile / ntx) * TB + tid / TB, g.nbx, g.nby);
+                if (s_nx[tid]) wake_faces_2d(f.wake_nxt, bx, by, g.nbx, g.nby);
             }
         }
         __syncthreads();                         // list and buffers reused by the next scan pass
