@@ -181,13 +181,23 @@ __global__ void __launch_bounds__(256 / R, 4)
     __syncthreads();
     const f2 C2x = f2_pack(s_Cf[0], s_Cf[0]), C2y = f2_pack(s_Cf[1], s_Cf[1]), C2z = f2_pack(s_Cf[2], s_Cf[2]);
 
-    auto build_nbr = [&](int tbx, int tby, int st) {
+    // neighbour table of a tile (parity and activity of the (TB+2)^2 blocks
+    // around it): loaded into registers one tile ahead, so the global loads
+    // overlap a tile's compute, and written to shared memory before its staging
+    int nb_par = 0, nb_act = 0;
+    auto nbr_load = [&](int tbx, int tby) {
         if (tid < RB * RB) {
             const int rx = tid % RB, ry = tid / RB;
             const int bx = wrap_p(tbx * TB + rx - 1, g.nbx), by = wrap_p(tby * TB + ry - 1, g.nby);
             const int ob = bx + g.nbx * by;
-            s_npar[st][tid] = f.par_cur[ob];
-            s_nact[st][tid] = DBA ? (f.wake_cur[ob] ? 1 : 0) : 1;
+            nb_par = f.par_cur[ob];
+            nb_act = DBA ? (f.wake_cur[ob] ? 1 : 0) : 1;
+        }
+    };
+    auto nbr_store = [&](int st) {
+        if (tid < RB * RB) {
+            s_npar[st][tid] = (uint8_t)nb_par;
+            s_nact[st][tid] = (uint8_t)nb_act;
         }
     };
     auto issue = [&](int tbx, int tby, int st) {
@@ -240,28 +250,36 @@ __global__ void __launch_bounds__(256 / R, 4)
             __syncthreads();
         }
         const int cnt = s_cnt;
-        int tbx_n = 0, tby_n = 0;                // tile coordinates of the next listed tile
+        // coordinates of tiles i (current), i + 1 (staged during i) and i + 2
+        // (neighbour table loaded during i)
+        int tbx = 0, tby = 0, tbx_n = 0, tby_n = 0, tbx_nn = 0, tby_nn = 0;
         if (cnt > 0) {
-            tby_n = s_tile[0] / ntx;
-            tbx_n = s_tile[0] - tby_n * ntx;
-            build_nbr(tbx_n, tby_n, 0);
+            tby = s_tile[0] / ntx;
+            tbx = s_tile[0] - tby * ntx;
+            nbr_load(tbx, tby);
+            nbr_store(0);
             __syncthreads();
-            issue(tbx_n, tby_n, 0);
+            issue(tbx, tby, 0);
+            if (cnt > 1) {
+                tby_n = s_tile[1] / ntx;
+                tbx_n = s_tile[1] - tby_n * ntx;
+                nbr_load(tbx_n, tby_n);
+            }
         }
         for (int i = 0; i < cnt; ++i) {
             const int st = i & 1;
-            const int tbx = tbx_n, tby = tby_n;  // tile i
-            if (i + 1 < cnt) {
-                tby_n = s_tile[i + 1] / ntx;
-                tbx_n = s_tile[i + 1] - tby_n * ntx;
-                build_nbr(tbx_n, tby_n, st ^ 1);
-            }
+            if (i + 1 < cnt) nbr_store(st ^ 1);  // table of tile i + 1, loaded one tile ago
             __syncthreads();                     // next table ready; stage st^1, mu and s_nx free
             if (tid < NBT) s_nx[tid] = 0;
             if (i + 1 < cnt) issue(tbx_n, tby_n, st ^ 1);
             else cp_async_commit();
             cp_async_wait1();
             __syncthreads();                     // tile i staged
+            if (i + 2 < cnt) {
+                tby_nn = s_tile[i + 2] / ntx;
+                tbx_nn = s_tile[i + 2] - tby_nn * ntx;
+                nbr_load(tbx_nn, tby_nn);
+            }
             const unsigned tm = s_tmeta[i];
             const int X0 = tbx * T, Y0 = tby * T;
             const float* sx = stage + st * 3 * SV;
@@ -429,6 +447,8 @@ __global__ void __launch_bounds__(256 / R, 4)
                 f.next[b] = (uint8_t)s_nx[tid];
                 if (s_nx[tid]) wake_faces_2d(f.wake_nxt, bx, by, g.nbx, g.nby);
             }
+            tbx = tbx_n; tby = tby_n;
+            tbx_n = tbx_nn; tby_n = tby_nn;
         }
         __syncthreads();                         // list and buffers reused by the next scan pass
     }
