@@ -12,8 +12,8 @@
 //     copies, double-buffered: tile i+1 is in flight while tile i computes.
 //     Each 16-byte piece lies inside one block, whose parity picks the buffer;
 //   * each thread owns a 4-column x R-row patch (R = kMBTileRows; 256 / R
-//     threads per CTA).  A staged row of the patch is one 16-byte shared load
-//     plus its left and right neighbours;
+//     threads per CTA).  A staged row of the patch is one 16-byte shared load,
+//     its left and right neighbours taken from the adjacent lanes;
 //     the row sums of the 9-point Laplacian are formed once per loaded row and
 //     the arithmetic runs on pairs of cells (k_pair.cuh: the two-lane FP32
 //     instructions of sm_100, rounded lane by lane like the scalar helpers), so
@@ -69,11 +69,22 @@ template <int B, int R = kMBTileRows> struct MBTile {
 };
 
 // one staged row of a 4-cell patch: centres as two pairs, and the row sums
-// right + left neighbour of each cell (the scalar kernels' h), as two pairs
+// right + left neighbour of each cell (the scalar kernels' h), as two pairs.
+// The eight patches of a tile row sit on eight consecutive lanes, so the left
+// and right neighbours come from the adjacent lanes' 16-byte loads; only the
+// two edge lanes read a halo word from shared memory.  (Loading both
+// neighbours from shared memory puts all 32 lanes on 8 banks: four-way
+// conflicts.)
 __device__ __forceinline__ void quad_row(const float* s, int i, f2& h01, f2& h23, f2& c01, f2& c23)
 {
     const float4 v = *reinterpret_cast<const float4*>(s + i);
-    const float l = s[i - 1], r = s[i + 4];
+    const int q = threadIdx.x & 7;
+    float l = __shfl_up_sync(0xffffffffu, v.w, 1, 8), r = __shfl_down_sync(0xffffffffu, v.x, 1, 8);
+    if (q == 0 || q == 7) {
+        const float e = s[i + (q == 0 ? -1 : 4)];
+        if (q == 0) l = e;
+        else r = e;
+    }
     h01 = f2_pack(__fadd_rn(v.y, l), __fadd_rn(v.z, v.x));
     h23 = f2_pack(__fadd_rn(v.w, v.y), __fadd_rn(r, v.z));
     c01 = f2_pack(v.x, v.y);
@@ -288,12 +299,15 @@ __global__ void __launch_bounds__(256 / R, 4)
             const bool own = (tm >> kb) & 1u;
 
             // ---- potentials of this patch (Calc_mu, kernel.cu:371-388)
+            // Laplacians of the patch: every lane of the warp takes part (the row
+            // loads exchange neighbours between lanes), whether or not its block is
+            // active; only active blocks use them
+            const int s0 = (ly0 + 1) * SP + lx0 + 4;         // staged row ly0 - 1, column lx0
+            f2 lx_[R][2], cx_[R][2], ly_[R][2], cy_[R][2], lz_[R][2], cz_[R][2];
+            quad_laps<SP, R>(K, sx, s0, lx_, cx_);
+            quad_laps<SP, R>(K, sy, s0, ly_, cy_);
+            quad_laps<SP, R>(K, sz, s0, lz_, cz_);
             if (own) {
-                const int s0 = (ly0 + 1) * SP + lx0 + 4;     // staged row ly0 - 1, column lx0
-                f2 lx_[R][2], cx_[R][2], ly_[R][2], cy_[R][2], lz_[R][2], cz_[R][2];
-                quad_laps<SP, R>(K, sx, s0, lx_, cx_);
-                quad_laps<SP, R>(K, sy, s0, ly_, cy_);
-                quad_laps<SP, R>(K, sz, s0, lz_, cz_);
                 float wmax = -INFINITY;                      // largest |lap z| of the patch (wake test)
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
@@ -371,6 +385,12 @@ __global__ void __launch_bounds__(256 / R, 4)
             __syncthreads();                     // potentials and wake-up tests complete
 
             // ---- update of this patch (Update, kernel.cu:419-434)
+            // Laplacians of the potentials: again every lane takes part
+            const int m0 = ly0 * MP + lx0 + 4;               // potential row ly0 - 1, column lx0
+            f2 lmx[R][2], mx[R][2], lmy[R][2], my[R][2], lmz[R][2], mz[R][2];
+            quad_laps<MP, R>(K, mu, m0, lmx, mx);
+            quad_laps<MP, R>(K, mu + MV, m0, lmy, my);
+            quad_laps<MP, R>(K, mu + 2 * MV, m0, lmz, mz);
             if (own) {
                 const int dst = (int)((tm >> (16 + kb)) & 1u) ^ 1;
                 float* ox = dst ? Q.x[1] : Q.x[0];
@@ -379,11 +399,6 @@ __global__ void __launch_bounds__(256 / R, 4)
                 const bool persist = DBA && !s_nx[kb];
                 const bool left = (lx0 % B) == 0, right = ((lx0 + 3) % B) == B - 1;
                 const bool ring_top = (ly0 % B) == 0, ring_bot = ((ly0 + R - 1) % B) == B - 1;
-                const int m0 = ly0 * MP + lx0 + 4;           // potential row ly0 - 1, column lx0
-                f2 lmx[R][2], mx[R][2], lmy[R][2], my[R][2], lmz[R][2], mz[R][2];
-                quad_laps<MP, R>(K, mu, m0, lmx, mx);
-                quad_laps<MP, R>(K, mu + MV, m0, lmy, my);
-                quad_laps<MP, R>(K, mu + 2 * MV, m0, lmz, mz);
                 f2 fin = K.zero;                             // NaN once any stored value is not finite
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
