@@ -83,12 +83,25 @@ __device__ __forceinline__ long long warp_sum_fix(long long v)
     return ((long long)shi << 24) + (long long)slo;
 }
 
-// all constants in float, computed once on the host (no conversions or divisions in the kernel)
+// All constants in float, computed once on the host (no conversions or
+// divisions in the kernel).  The point formulas below use them folded: the
+// Laplacian weights carry 1/dx^2; the logarithms stay in base 2 (their ln 2 is
+// folded into the coefficient that multiplies them); the exponents' log2(e) is
+// folded into the reaction coefficients; and the potentials are written as one
+// chain of fused multiply-adds per species, with the common subtrahend
+// chi_xb X + chi_yb Y + chi_zb Z (Calc_mu, kernel.cu:371-388) merged into the
+// per-species coefficients.  Mathematically these are the reference formulas;
+// only the FP32 rounding differs.
 struct MBFastP {
-    float inv_dx2, c0x, c0y, c0z, irx, iry, irz;
-    float chi_xy, chi_xz, chi_yz, chi_xb, chi_yb, chi_zb;
-    float ex, ey, ez, phi_logK;        // phi_logK = phi_term + log(K)/rz
-    float nvx, mvy, dvz, dtvx, dtvy, dtvz, dn, dm, Mx, My, Mz, k0, thr;
+    float Lc, Lf, Ld;                  // Laplacian weights -10/3, 2/3, 1/6 times 1/dx^2
+    float ax_y, ax_z, ax_x, bx, lx;    // mu_x = c0x + ax_y Y + ax_z Z + ax_x X + bx b + lx lg2 X - ln2 lg2 b - ex lap x
+    float ay_x, ay_z, ay_y, by, ly;
+    float az_x, az_y, az_z, bz, lz;
+    float c0x, c0y, c0z;               // c0z includes -(phi_term + log(K)/rz)
+    float mln2, nex, ney, nez;         // -ln 2, -ex, -ey, -ez
+    float ea, eb, ec;                  // exponents in base 2: (ea mx + eb my), ec mz
+    float Mxd, Myd, Mzd, Rx, Ry, Rz;   // change = Md lap(mu) + R (e^.. - e^..)
+    float thr;
     int conserved;
 };
 
@@ -101,18 +114,23 @@ struct MBFastBuf {
 
 inline MBFastP make_fast_params(const MBP<float>& P)
 {
+    const double ln2 = 0.693147180559945309417, log2e = 1.442695040888963407360;
     MBFastP q;
-    q.inv_dx2 = (float)P.inv_dx2;
-    q.c0x = (float)P.c0x; q.c0y = (float)P.c0y; q.c0z = (float)P.c0z;
-    q.irx = (float)(1.0 / P.rx); q.iry = (float)(1.0 / P.ry); q.irz = (float)(1.0 / P.rz);
-    q.chi_xy = (float)P.chi_xy; q.chi_xz = (float)P.chi_xz; q.chi_yz = (float)P.chi_yz;
-    q.chi_xb = (float)P.chi_xb; q.chi_yb = (float)P.chi_yb; q.chi_zb = (float)P.chi_zb;
-    q.ex = (float)P.ex; q.ey = (float)P.ey; q.ez = (float)P.ez;
-    q.phi_logK = (float)(P.phi_term + P.logK_rz);
-    q.nvx = (float)P.nvx; q.mvy = (float)P.mvy; q.dvz = (float)P.dvz;
-    q.dtvx = (float)P.dtvx; q.dtvy = (float)P.dtvy; q.dtvz = (float)P.dtvz;
-    q.dn = (float)P.dn; q.dm = (float)P.dm;
-    q.Mx = (float)P.Mx; q.My = (float)P.My; q.Mz = (float)P.Mz; q.k0 = (float)P.k0; q.thr = (float)P.thr;
+    q.Lc = (float)(-10.0 / 3.0 * P.inv_dx2);
+    q.Lf = (float)(2.0 / 3.0 * P.inv_dx2);
+    q.Ld = (float)(1.0 / 6.0 * P.inv_dx2);
+    q.ax_y = (float)(P.chi_xy - P.chi_yb); q.ax_z = (float)(P.chi_xz - P.chi_zb); q.ax_x = (float)(-P.chi_xb);
+    q.bx = (float)P.chi_xb; q.lx = (float)(ln2 / P.rx);
+    q.ay_x = (float)(P.chi_xy - P.chi_xb); q.ay_z = (float)(P.chi_yz - P.chi_zb); q.ay_y = (float)(-P.chi_yb);
+    q.by = (float)P.chi_yb; q.ly = (float)(ln2 / P.ry);
+    q.az_x = (float)(P.chi_xz - P.chi_xb); q.az_y = (float)(P.chi_yz - P.chi_yb); q.az_z = (float)(-P.chi_zb);
+    q.bz = (float)P.chi_zb; q.lz = (float)(ln2 / P.rz);
+    q.c0x = (float)P.c0x; q.c0y = (float)P.c0y; q.c0z = (float)(P.c0z - (P.phi_term + P.logK_rz));
+    q.mln2 = (float)(-ln2); q.nex = (float)(-P.ex); q.ney = (float)(-P.ey); q.nez = (float)(-P.ez);
+    q.ea = (float)(log2e * P.nvx); q.eb = (float)(log2e * P.mvy); q.ec = (float)(log2e * P.dvz);
+    q.Mxd = (float)(P.dtvx * P.Mx); q.Myd = (float)(P.dtvy * P.My); q.Mzd = (float)(P.dtvz * P.Mz);
+    q.Rx = (float)(-P.dtvx * P.dn * P.k0); q.Ry = (float)(-P.dtvy * P.dm * P.k0); q.Rz = (float)(P.dtvz * P.k0);
+    q.thr = (float)P.thr;
     q.conserved = P.conserved;
     return q;
 }
@@ -146,37 +164,37 @@ template <int B> struct MBFastShape {
 // kernels that use these helpers produce bit-identical values. ----
 
 // 2-D form of the 27-point Laplacian (kernel.cu:332-344 with z wrapped onto the
-// cell) from row data: h = right + left neighbour of a row, c = its centre,
-// m / 0 / p = rows y-1, y, y+1
-__device__ __forceinline__ float lap9_rows(float hm, float cm, float h0, float c0, float hp, float cp, float inv_dx2)
+// cell: weights -10/3, 2/3, 1/6 on centre, faces, diagonals, times 1/dx^2) from
+// row data: h = right + left neighbour of a row, c = its centre, m / 0 / p =
+// rows y-1, y, y+1
+__device__ __forceinline__ float lap9_rows(const MBFastP& P, float hm, float cm, float h0, float c0, float hp, float cp)
 {
-    const float cc = (float)(-10.0 / 3.0), cf = (float)(2.0 / 3.0), cd = (float)(1.0 / 6.0);
     const float faces = __fadd_rn(h0, __fadd_rn(cp, cm));
     const float diag = __fadd_rn(hp, hm);
-    return __fmul_rn(inv_dx2, __fmaf_rn(cd, diag, __fmaf_rn(cf, faces, __fmul_rn(cc, c0))));
+    return __fmaf_rn(P.Ld, diag, __fmaf_rn(P.Lf, faces, __fmul_rn(P.Lc, c0)));
 }
 
-__device__ __forceinline__ float lap9(const float* c, int i, int sy, float inv_dx2)
+__device__ __forceinline__ float lap9(const MBFastP& P, const float* c, int i, int sy)
 {
-    return lap9_rows(__fadd_rn(c[i + 1 - sy], c[i - 1 - sy]), c[i - sy], __fadd_rn(c[i + 1], c[i - 1]), c[i],
-                     __fadd_rn(c[i + 1 + sy], c[i - 1 + sy]), c[i + sy], inv_dx2);
+    return lap9_rows(P, __fadd_rn(c[i + 1 - sy], c[i - 1 - sy]), c[i - sy], __fadd_rn(c[i + 1], c[i - 1]), c[i],
+                     __fadd_rn(c[i + 1 + sy], c[i - 1 + sy]), c[i + sy]);
 }
 
-// Natural log and exponential by change of base onto the hardware base-2
-// approximations (PTX lg2.approx / ex2.approx, flush-to-zero forms):
-// ln x = log2(x) ln 2,  e^x = 2^(x log2 e).  Relative error ~2^-22; the fields
-// never approach the denormal range.
-__device__ __forceinline__ float ln_approx(float x)
+// Hardware base-2 approximations (PTX lg2.approx / ex2.approx, flush-to-zero
+// forms; relative error ~2^-22, and the fields never approach the denormal
+// range): ln x = ln 2 log2 x and e^x = 2^(x log2 e), with ln 2 and log2 e
+// folded into the constants.
+__device__ __forceinline__ float lg2_approx(float x)
 {
     float r;
     asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return __fmul_rn(r, 0.693147180559945309f);
+    return r;
 }
 
-__device__ __forceinline__ float exp_approx(float x)
+__device__ __forceinline__ float ex2_approx(float x)
 {
     float r;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(__fmul_rn(x, 1.442695040888963407f)));
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
 
@@ -185,66 +203,60 @@ __device__ __forceinline__ void mb_potentials(const MBFastP& P, float X, float Y
                                               float lapz, float& ux, float& uy, float& uz)
 {
     const float bb = __fsub_rn(__fsub_rn(__fsub_rn(1.f, X), Y), Z);
-    const float lb = ln_approx(bb);
-    const float sumb = __fmaf_rn(P.chi_zb, Z, __fmaf_rn(P.chi_yb, Y, __fmul_rn(P.chi_xb, X)));   // common subtrahend
-    float u = __fmaf_rn(P.chi_xb, bb, __fmaf_rn(P.chi_xz, Z, __fmaf_rn(P.chi_xy, Y, P.c0x)));
-    u = __fsub_rn(__fmaf_rn(ln_approx(X), P.irx, __fsub_rn(u, sumb)), lb);
-    ux = __fmaf_rn(-P.ex, lapx, u);
-    u = __fmaf_rn(P.chi_yb, bb, __fmaf_rn(P.chi_yz, Z, __fmaf_rn(P.chi_xy, X, P.c0y)));
-    u = __fsub_rn(__fmaf_rn(ln_approx(Y), P.iry, __fsub_rn(u, sumb)), lb);
-    uy = __fmaf_rn(-P.ey, lapy, u);
-    u = __fmaf_rn(P.chi_zb, bb, __fmaf_rn(P.chi_yz, Y, __fmaf_rn(P.chi_xz, X, P.c0z)));
-    u = __fsub_rn(__fmaf_rn(ln_approx(Z), P.irz, __fsub_rn(u, sumb)), lb);
-    uz = __fsub_rn(__fmaf_rn(-P.ez, lapz, u), P.phi_logK);
+    const float lb = lg2_approx(bb);
+    float u = __fmaf_rn(P.ax_z, Z, __fmaf_rn(P.ax_y, Y, P.c0x));
+    u = __fmaf_rn(P.bx, bb, __fmaf_rn(P.ax_x, X, u));
+    u = __fmaf_rn(P.mln2, lb, __fmaf_rn(P.lx, lg2_approx(X), u));
+    ux = __fmaf_rn(P.nex, lapx, u);
+    u = __fmaf_rn(P.ay_z, Z, __fmaf_rn(P.ay_x, X, P.c0y));
+    u = __fmaf_rn(P.by, bb, __fmaf_rn(P.ay_y, Y, u));
+    u = __fmaf_rn(P.mln2, lb, __fmaf_rn(P.ly, lg2_approx(Y), u));
+    uy = __fmaf_rn(P.ney, lapy, u);
+    u = __fmaf_rn(P.az_y, Y, __fmaf_rn(P.az_x, X, P.c0z));
+    u = __fmaf_rn(P.bz, bb, __fmaf_rn(P.az_z, Z, u));
+    u = __fmaf_rn(P.mln2, lb, __fmaf_rn(P.lz, lg2_approx(Z), u));
+    uz = __fmaf_rn(P.nez, lapz, u);
 }
 
 // per-step changes (Update, kernel.cu:419-434) from the potentials at the cell and their Laplacians
 __device__ __forceinline__ void mb_changes(const MBFastP& P, float mx, float my, float mz, float lmx, float lmy,
                                            float lmz, float& cx, float& cy, float& cz)
 {
-    const float Rr = __fmul_rn(P.k0, __fsub_rn(exp_approx(__fmaf_rn(P.nvx, mx, __fmul_rn(P.mvy, my))),
-                                               exp_approx(__fmul_rn(P.dvz, mz))));
-    cx = __fmul_rn(P.dtvx, __fmaf_rn(P.Mx, lmx, -__fmul_rn(P.dn, Rr)));
-    cy = __fmul_rn(P.dtvy, __fmaf_rn(P.My, lmy, -__fmul_rn(P.dm, Rr)));
-    cz = __fmul_rn(P.dtvz, __fmaf_rn(P.Mz, lmz, Rr));
+    const float D = __fsub_rn(ex2_approx(__fmaf_rn(P.ea, mx, __fmul_rn(P.eb, my))), ex2_approx(__fmul_rn(P.ec, mz)));
+    cx = __fmaf_rn(P.Mxd, lmx, __fmul_rn(P.Rx, D));
+    cy = __fmaf_rn(P.Myd, lmy, __fmul_rn(P.Ry, D));
+    cz = __fmaf_rn(P.Mzd, lmz, __fmul_rn(P.Rz, D));
 }
 
 // ---- the same point formulas on pairs of cells (k_pair.cuh): lane by lane the
 // operations, their order and their rounding are those of the scalar helpers
 // above, so a pair kernel stores the bits a scalar kernel stores. ----
 
-// splatted constants of the pair formulas (negated where the scalar form negates
-// a product: (-a) * b rounds to exactly -(a * b))
+// splatted constants of the pair formulas (those of MBFastP, both lanes equal)
 struct MBPairP {
-    f2 inv_dx2, cc, cf, cd, one, ln2, log2e, zero, nz;   // nz = (-0, -0): the addend of every product
-    f2 c0x, c0y, c0z, irx, iry, irz, chi_xy, chi_xz, chi_yz, chi_xb, chi_yb, chi_zb;
-    f2 nex, ney, nez, phi_logK;
-    f2 nvx, mvy, dvz, k0, dtvx, dtvy, dtvz, Mx, My, Mz, ndn, ndm;
+    f2 Lc, Lf, Ld, one, zero, nz;      // nz = (-0, -0): the addend of every product
+    f2 ax_y, ax_z, ax_x, bx, lx, ay_x, ay_z, ay_y, by, ly, az_x, az_y, az_z, bz, lz;
+    f2 c0x, c0y, c0z, mln2, nex, ney, nez;
+    f2 ea, eb, ec, Mxd, Myd, Mzd, Rx, Ry, Rz;
 };
 
 inline MBPairP make_pair_params(const MBFastP& P)
 {
     MBPairP q;
-    q.inv_dx2 = f2_splat_host(P.inv_dx2);
-    q.cc = f2_splat_host((float)(-10.0 / 3.0));
-    q.cf = f2_splat_host((float)(2.0 / 3.0));
-    q.cd = f2_splat_host((float)(1.0 / 6.0));
-    q.one = f2_splat_host(1.f);
-    q.ln2 = f2_splat_host(0.693147180559945309f);
-    q.log2e = f2_splat_host(1.442695040888963407f);
-    q.zero = f2_splat_host(0.f);
-    q.nz = f2_splat_host(-0.f);
+    q.Lc = f2_splat_host(P.Lc); q.Lf = f2_splat_host(P.Lf); q.Ld = f2_splat_host(P.Ld);
+    q.one = f2_splat_host(1.f); q.zero = f2_splat_host(0.f); q.nz = f2_splat_host(-0.f);
+    q.ax_y = f2_splat_host(P.ax_y); q.ax_z = f2_splat_host(P.ax_z); q.ax_x = f2_splat_host(P.ax_x);
+    q.bx = f2_splat_host(P.bx); q.lx = f2_splat_host(P.lx);
+    q.ay_x = f2_splat_host(P.ay_x); q.ay_z = f2_splat_host(P.ay_z); q.ay_y = f2_splat_host(P.ay_y);
+    q.by = f2_splat_host(P.by); q.ly = f2_splat_host(P.ly);
+    q.az_x = f2_splat_host(P.az_x); q.az_y = f2_splat_host(P.az_y); q.az_z = f2_splat_host(P.az_z);
+    q.bz = f2_splat_host(P.bz); q.lz = f2_splat_host(P.lz);
     q.c0x = f2_splat_host(P.c0x); q.c0y = f2_splat_host(P.c0y); q.c0z = f2_splat_host(P.c0z);
-    q.irx = f2_splat_host(P.irx); q.iry = f2_splat_host(P.iry); q.irz = f2_splat_host(P.irz);
-    q.chi_xy = f2_splat_host(P.chi_xy); q.chi_xz = f2_splat_host(P.chi_xz); q.chi_yz = f2_splat_host(P.chi_yz);
-    q.chi_xb = f2_splat_host(P.chi_xb); q.chi_yb = f2_splat_host(P.chi_yb); q.chi_zb = f2_splat_host(P.chi_zb);
-    q.nex = f2_splat_host(-P.ex); q.ney = f2_splat_host(-P.ey); q.nez = f2_splat_host(-P.ez);
-    q.phi_logK = f2_splat_host(P.phi_logK);
-    q.nvx = f2_splat_host(P.nvx); q.mvy = f2_splat_host(P.mvy); q.dvz = f2_splat_host(P.dvz);
-    q.k0 = f2_splat_host(P.k0);
-    q.dtvx = f2_splat_host(P.dtvx); q.dtvy = f2_splat_host(P.dtvy); q.dtvz = f2_splat_host(P.dtvz);
-    q.Mx = f2_splat_host(P.Mx); q.My = f2_splat_host(P.My); q.Mz = f2_splat_host(P.Mz);
-    q.ndn = f2_splat_host(-P.dn); q.ndm = f2_splat_host(-P.dm);
+    q.mln2 = f2_splat_host(P.mln2); q.nex = f2_splat_host(P.nex); q.ney = f2_splat_host(P.ney);
+    q.nez = f2_splat_host(P.nez);
+    q.ea = f2_splat_host(P.ea); q.eb = f2_splat_host(P.eb); q.ec = f2_splat_host(P.ec);
+    q.Mxd = f2_splat_host(P.Mxd); q.Myd = f2_splat_host(P.Myd); q.Mzd = f2_splat_host(P.Mzd);
+    q.Rx = f2_splat_host(P.Rx); q.Ry = f2_splat_host(P.Ry); q.Rz = f2_splat_host(P.Rz);
     return q;
 }
 
@@ -253,52 +265,40 @@ __device__ __forceinline__ f2 lap9_rows2(const MBPairP& K, f2 hm, f2 cm, f2 h0, 
 {
     const f2 faces = add2(h0, add2(cp, cm));
     const f2 diag = add2(hp, hm);
-    return mul2(K.inv_dx2, fma2(K.cd, diag, fma2(K.cf, faces, mul2(K.cc, c0, K.nz))), K.nz);
+    return fma2(K.Ld, diag, fma2(K.Lf, faces, mul2(K.Lc, c0, K.nz)));
 }
 
-__device__ __forceinline__ f2 ln_approx2(const MBPairP& K, f2 x)
-{
-    float a, b;
-    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(a) : "f"(f2_lo(x)));
-    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(b) : "f"(f2_hi(x)));
-    return mul2(f2_pack(a, b), K.ln2, K.nz);
-}
-
-__device__ __forceinline__ f2 exp_approx2(const MBPairP& K, f2 x)
-{
-    const f2 t = mul2(x, K.log2e, K.nz);
-    float a, b;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(a) : "f"(f2_lo(t)));
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(b) : "f"(f2_hi(t)));
-    return f2_pack(a, b);
-}
+__device__ __forceinline__ f2 lg2_approx2(f2 x) { return f2_pack(lg2_approx(f2_lo(x)), lg2_approx(f2_hi(x))); }
+__device__ __forceinline__ f2 ex2_approx2(f2 x) { return f2_pack(ex2_approx(f2_lo(x)), ex2_approx(f2_hi(x))); }
 
 // mb_potentials on a pair
 __device__ __forceinline__ void mb_potentials2(const MBPairP& K, f2 X, f2 Y, f2 Z, f2 lapx, f2 lapy, f2 lapz,
                                                f2& ux, f2& uy, f2& uz)
 {
     const f2 bb = sub2(sub2(sub2(K.one, X), Y), Z);
-    const f2 lb = ln_approx2(K, bb);
-    const f2 sumb = fma2(K.chi_zb, Z, fma2(K.chi_yb, Y, mul2(K.chi_xb, X, K.nz)));
-    f2 u = fma2(K.chi_xb, bb, fma2(K.chi_xz, Z, fma2(K.chi_xy, Y, K.c0x)));
-    u = sub2(fma2(ln_approx2(K, X), K.irx, sub2(u, sumb)), lb);
+    const f2 lb = lg2_approx2(bb);
+    f2 u = fma2(K.ax_z, Z, fma2(K.ax_y, Y, K.c0x));
+    u = fma2(K.bx, bb, fma2(K.ax_x, X, u));
+    u = fma2(K.mln2, lb, fma2(K.lx, lg2_approx2(X), u));
     ux = fma2(K.nex, lapx, u);
-    u = fma2(K.chi_yb, bb, fma2(K.chi_yz, Z, fma2(K.chi_xy, X, K.c0y)));
-    u = sub2(fma2(ln_approx2(K, Y), K.iry, sub2(u, sumb)), lb);
+    u = fma2(K.ay_z, Z, fma2(K.ay_x, X, K.c0y));
+    u = fma2(K.by, bb, fma2(K.ay_y, Y, u));
+    u = fma2(K.mln2, lb, fma2(K.ly, lg2_approx2(Y), u));
     uy = fma2(K.ney, lapy, u);
-    u = fma2(K.chi_zb, bb, fma2(K.chi_yz, Y, fma2(K.chi_xz, X, K.c0z)));
-    u = sub2(fma2(ln_approx2(K, Z), K.irz, sub2(u, sumb)), lb);
-    uz = sub2(fma2(K.nez, lapz, u), K.phi_logK);
+    u = fma2(K.az_y, Y, fma2(K.az_x, X, K.c0z));
+    u = fma2(K.bz, bb, fma2(K.az_z, Z, u));
+    u = fma2(K.mln2, lb, fma2(K.lz, lg2_approx2(Z), u));
+    uz = fma2(K.nez, lapz, u);
 }
 
 // mb_changes on a pair
 __device__ __forceinline__ void mb_changes2(const MBPairP& K, f2 mx, f2 my, f2 mz, f2 lmx, f2 lmy, f2 lmz, f2& cx,
                                             f2& cy, f2& cz)
 {
-    const f2 Rr = mul2(K.k0, sub2(exp_approx2(K, fma2(K.nvx, mx, mul2(K.mvy, my, K.nz))), exp_approx2(K, mul2(K.dvz, mz, K.nz))), K.nz);
-    cx = mul2(K.dtvx, fma2(K.Mx, lmx, mul2(K.ndn, Rr, K.nz)), K.nz);
-    cy = mul2(K.dtvy, fma2(K.My, lmy, mul2(K.ndm, Rr, K.nz)), K.nz);
-    cz = mul2(K.dtvz, fma2(K.Mz, lmz, Rr), K.nz);
+    const f2 D = sub2(ex2_approx2(fma2(K.ea, mx, mul2(K.eb, my, K.nz))), ex2_approx2(mul2(K.ec, mz, K.nz)));
+    cx = fma2(K.Mxd, lmx, mul2(K.Rx, D, K.nz));
+    cy = fma2(K.Myd, lmy, mul2(K.Ry, D, K.nz));
+    cz = fma2(K.Mzd, lmz, mul2(K.Rz, D, K.nz));
 }
 
 template <int B, bool DBA>
@@ -326,7 +326,6 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
     const int tid = threadIdx.x;
     const int G = gridDim.x;
     const int nb = g.nb;
-    const float inv_dx2 = P.inv_dx2;
     if (tid < 3) {
         s_Cf[tid] = lazy_offset(L, tid);
         s_fix[tid] = 0ull;
@@ -415,9 +414,9 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 if (r == 4 || s_ra[k][r]) {
                     const int ti = k * TV + (fx + 1) + SE * (fy + 1);
                     const float X = __fsub_rn(sx[ti], Cx), Y = __fsub_rn(sy[ti], Cy), Z = __fsub_rn(sz[ti], Cz);
-                    const float lapx = lap9(sx, ti, SE, inv_dx2);
-                    const float lapy = lap9(sy, ti, SE, inv_dx2);
-                    const float lapz = lap9(sz, ti, SE, inv_dx2);
+                    const float lapx = lap9(P, sx, ti, SE);
+                    const float lapy = lap9(P, sy, ti, SE);
+                    const float lapz = lap9(P, sz, ti, SE);
                     float ux, uy, uz;
                     mb_potentials(P, X, Y, Z, lapx, lapy, lapz, ux, uy, uz);
                     mx[mi] = ux;
@@ -454,8 +453,8 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
                 const int bx = blk % g.nbx, by = blk / g.nbx;
                 const size_t gi = (size_t)(bx * B + lx) + (size_t)g.nx * (size_t)(by * B + ly);
                 float cx, cy, cz;
-                mb_changes(P, mx[fi], my[fi], mz[fi], lap9(mx, fi, SF, inv_dx2), lap9(my, fi, SF, inv_dx2),
-                           lap9(mz, fi, SF, inv_dx2), cx, cy, cz);
+                mb_changes(P, mx[fi], my[fi], mz[fi], lap9(P, mx, fi, SF), lap9(P, my, fi, SF),
+                           lap9(P, mz, fi, SF), cx, cy, cz);
                 // stored values carry raw changes (value = stored - C)
                 const float x0 = sx[ti], y0 = sy[ti], z0 = sz[ti];
                 const float xn = __fadd_rn(x0, cx), yn = __fadd_rn(y0, cy), zn = __fadd_rn(z0, cz);
