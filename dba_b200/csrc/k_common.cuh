@@ -59,6 +59,7 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // periodic wrap of an index at most one period outside [0, n)
 __device__ __forceinline__ int wrap_p(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }

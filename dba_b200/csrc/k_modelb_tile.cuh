@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256 / R, 4)
     __shared__ unsigned s_tmeta[TPP];    // bits 0..15 active blocks, 16..31 their parity
     __shared__ int s_cnt;
     __shared__ uint8_t s_npar[2][RB * RB], s_nact[2][RB * RB];
-    __shared__ int s_nx[NBT];
+    __shared__ int s_nx[2][NBT];         // wake tests of the blocks of tiles with parity 0 / 1
     __shared__ float s_Cf[3];
     __shared__ unsigned long long s_fix[3];
 
@@ -269,6 +269,7 @@ __global__ void __launch_bounds__(256 / R, 4)
             tbx = s_tile[0] - tby * ntx;
             nbr_load(tbx, tby);
             nbr_store(0);
+            if (tid < NBT) s_nx[0][tid] = 0;
             __syncthreads();
             issue(tbx, tby, 0);
             if (cnt > 1) {
@@ -280,12 +281,13 @@ __global__ void __launch_bounds__(256 / R, 4)
         for (int i = 0; i < cnt; ++i) {
             const int st = i & 1;
             if (i + 1 < cnt) nbr_store(st ^ 1);  // table of tile i + 1, loaded one tile ago
-            __syncthreads();                     // next table ready; stage st^1, mu and s_nx free
-            if (tid < NBT) s_nx[tid] = 0;
+            cp_async_wait0();
+            __syncthreads();                     // tile i staged, table i + 1 stored; tile i - 1 done
+            // tile i - 1 has been read by every thread, so its stage buffer, the
+            // potentials and the wake tests of parity st ^ 1 are free: stage tile i + 1
+            // now, while tile i computes
+            if (tid < NBT) s_nx[st ^ 1][tid] = 0;
             if (i + 1 < cnt) issue(tbx_n, tby_n, st ^ 1);
-            else cp_async_commit();
-            cp_async_wait1();
-            __syncthreads();                     // tile i staged
             if (i + 2 < cnt) {
                 tby_nn = s_tile[i + 2] / ntx;
                 tbx_nn = s_tile[i + 2] - tby_nn * ntx;
@@ -323,7 +325,7 @@ __global__ void __launch_bounds__(256 / R, 4)
                     *reinterpret_cast<float4*>(mu + MV + mi) = f4_of(uy[0], uy[1]);
                     *reinterpret_cast<float4*>(mu + 2 * MV + mi) = f4_of(uz[0], uz[1]);
                 }
-                if (DBA && wmax > P.thr) s_nx[kb] = 1;
+                if (DBA && wmax > P.thr) s_nx[st][kb] = 1;
             } else {
                 // inactive block inside the tile: its persisted ring (stale potentials)
 #pragma unroll
@@ -396,7 +398,7 @@ __global__ void __launch_bounds__(256 / R, 4)
                 float* ox = dst ? Q.x[1] : Q.x[0];
                 float* oy = dst ? Q.y[1] : Q.y[0];
                 float* oz = dst ? Q.z[1] : Q.z[0];
-                const bool persist = DBA && !s_nx[kb];
+                const bool persist = DBA && !s_nx[st][kb];
                 const bool left = (lx0 % B) == 0, right = ((lx0 + 3) % B) == B - 1;
                 const bool ring_top = (ly0 % B) == 0, ring_bot = ((ly0 + R - 1) % B) == B - 1;
                 f2 fin = K.zero;                             // NaN once any stored value is not finite
@@ -459,8 +461,8 @@ __global__ void __launch_bounds__(256 / R, 4)
             if (DBA && tid < NBT && ((tm >> tid) & 1u)) {
                 const int bx = tbx * TB + tid % TB, by = tby * TB + tid / TB;
                 const int b = bx + g.nbx * by;
-                f.next[b] = (uint8_t)s_nx[tid];
-                if (s_nx[tid]) wake_faces_2d(f.wake_nxt, bx, by, g.nbx, g.nby);
+                f.next[b] = (uint8_t)s_nx[st][tid];
+                if (s_nx[st][tid]) wake_faces_2d(f.wake_nxt, bx, by, g.nbx, g.nby);
             }
             tbx = tbx_n; tby = tby_n;
             tbx_n = tbx_nn; tby_n = tby_nn;
