@@ -216,9 +216,16 @@ class Simulation:
     def _fid(self, name):
         return self.fields.index(name) if isinstance(name, str) else int(name)
 
-    def field(self, name):
+    def field(self, name, out=None):
+        """Current values of a field as float64, shape (nz, ny, nx).  `out`, if given,
+        is a C-contiguous float64 array of nx*ny*nz elements that receives them (for
+        instance page-locked host memory, which the device copies into at full link
+        speed) and is returned reshaped."""
         fid = self._fid(name)
-        out = np.empty(self.n, np.float64)
+        if out is None:
+            out = np.empty(self.n, np.float64)
+        elif out.dtype != np.float64 or out.size != self.n or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float64 array of %d elements" % self.n)
         _check(self._L.dba_read_field(self._h, fid, out.ctypes.data_as(ctypes.POINTER(_d))), "dba_read_field")
         return out.reshape(self.shape)
 

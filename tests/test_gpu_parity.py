@@ -229,3 +229,21 @@ def test_modelb_fp32_fast_path_block_edges(B):
         assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-4, f
     agree = np.mean(s.flags(0) == o.flags()[0])
     assert agree >= 0.98
+
+
+def test_field_into_caller_buffer():
+    """field(name, out=...) fills a caller-provided (here page-locked) float64 array with
+    the same values field(name) returns, and rejects a buffer of the wrong size or type."""
+    import torch
+
+    prm = dict(MODELB_REF, metric_eps=1e-3)
+    s = dba_b200.Simulation(modelb_cfg(prm, 64, 64, 1, 16, precision=1, conserved=1)).init()
+    s.step(20, 1)
+    buf = torch.empty(64 * 64, dtype=torch.float64, pin_memory=True).numpy()
+    for f in ("x", "y", "z", "b"):
+        got = s.field(f, out=buf)
+        assert np.array_equal(got, s.field(f)), f
+    with pytest.raises(ValueError):
+        s.field("x", out=np.empty(10))
+    with pytest.raises(ValueError):
+        s.field("x", out=np.empty(64 * 64, np.float32))
