@@ -23,8 +23,9 @@ memory, autotuned block edge and threads) against the same requests run one at
 a time -- runs/s of both and p50/p99 time to completion (`--no-sweep` skips it).
 
 `--impl reference` times the reference's own serial CPU program for the same
-model (its functions driven step by step by oracle/_ref/*_cpu_steps, built from
-the reference sources) on this host; rank 0 only.
+model, built from the reference sources under oracle/_ref (Model B and KH: its
+functions driven step by step by *_cpu_steps; dendrite: the program itself,
+an n-step run minus a 0-step run) on this host; rank 0 only.
 """
 import argparse
 import json
@@ -355,11 +356,26 @@ def time_reference_cpu(w, nsteps):
                              check=True).stdout
         secs = float([ln for ln in out.splitlines() if ln.startswith("LOOP_SECONDS")][-1].split()[1])
         return secs, "reference", f"{binary} (reference CPU_version functions, regular mode, FP64)"
-    # the reference's dendrite CPU program is single precision with fixed ghosts; time the FP64 restatement
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from cases import DENDRITE_REF
-    from oracle_lib import OracleDendrite
     prm = dict(DENDRITE_REF, **{k: v for k, v in w["params"].items() if k in DENDRITE_REF})
+    den = os.path.join(ROOT, "oracle", "_ref", "dendrite_cpu")
+    if w["model"] == "dendrite" and os.path.exists(den):
+        # the reference's own dendrite CPU program (CPU_version/Base.cpp, single precision, regular
+        # mode): it reads ./Input.txt and writes no output while t_freq > t_total; the loop time is
+        # the wall time of an nsteps run minus that of a 0-step run (setup, allocation, seed)
+        def run(k):
+            d = tempfile.mkdtemp()
+            with open(os.path.join(d, "Input.txt"), "w") as f:
+                f.write(f"{w['nx']} {w['ny']} {w['nz']}\n{k} {k + 1} {prm['dt']}\n{prm['dx']} {prm['dx']} {prm['dx']}\n"
+                        f"{prm['delta']} {prm['tau']} {prm['epsilon']} {prm['alpha']} {prm['gamma']}\n{prm['Delta']}\n")
+            t0 = time.perf_counter()
+            subprocess.run([den], cwd=d, check=True, stdout=subprocess.DEVNULL)
+            return time.perf_counter() - t0
+        secs = max(run(nsteps) - run(0), 1e-9)
+        return secs, "reference", "dendrite_cpu (reference CPU_version/Base.cpp, regular mode, float; n-step minus 0-step run)"
+    # no reference program built: time the FP64 restatement
+    from oracle_lib import OracleDendrite
     o = OracleDendrite(w["nx"], w["ny"], w["nz"], w["block"], prm, bc=w["params"].get("bc", 0))
     o.init_cone()
     t0 = time.perf_counter()

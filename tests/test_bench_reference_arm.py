@@ -25,3 +25,15 @@ def test_reference_arm_json_line():
     assert d["e2e"] == {"value": d["value"], "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
     assert d["config"]["workload"] == "modelb_2048_fp32_conserved"
+
+
+def test_reference_arm_dendrite_program():
+    """The dendrite workloads time the reference's own CPU_version program when it is built."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload",
+                          "dendrite_512_fp64", "--steps", "4", "--warmup", "0"], capture_output=True, text=True,
+                         timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    d = json.loads([l for l in out.stdout.splitlines() if l.startswith("{")][-1])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["config"]["workload"] == "dendrite_512_fp64"
+    built = os.path.exists(os.path.join(ROOT, "oracle", "_ref", "dendrite_cpu"))
+    assert d["cpu_baseline"]["kind"] == ("reference" if built else "port")
