@@ -57,6 +57,14 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+// cp.async of one 4- or 8-byte element (L1-allocating form, any naturally aligned address)
+template <int N>
+__device__ __forceinline__ void cp_async_elem(void* smem, const void* gmem)
+{
+    static_assert(N == 4 || N == 8, "element size");
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(N) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
@@ -180,7 +188,9 @@ __device__ __forceinline__ void count_stats(unsigned long long* stats, int act, 
 // run sums are reduced with strides R/2..1.  Cell v of block k lives in thread
 // k*V + v (V < kThreads) or thread v % kThreads, pass v / kThreads (V >= kThreads).
 // `val[c]` is this thread's value for pass c.  Writes the block sums to out[k]
-// (thread 0 of each block) via the scratch s_run[kThreads / 32 * CPT].
+// (thread 0 of each block) via the scratch s_run[kThreads / 32 * CPT].  A
+// launch wider than kThreads calls it with all its threads (it holds barriers);
+// threads from kThreads on carry no cells and write nothing.
 template <int V, int CPT>
 __device__ __forceinline__ void block_tree_sums(const double* val, double* s_run, double* out_k, int k_of_thread)
 {
@@ -191,7 +201,8 @@ __device__ __forceinline__ void block_tree_sums(const double* val, double* s_run
         double v = val[c];
 #pragma unroll
         for (int h = SEG / 2; h >= 1; h /= 2) v += __shfl_down_sync(0xffffffffu, v, h, SEG);
-        if (V < 32) {
+        if (threadIdx.x >= kThreads) {
+        } else if (V < 32) {
             if ((lane % SEG) == 0) out_k[threadIdx.x / V] = v;
         } else {
             // run index within the block

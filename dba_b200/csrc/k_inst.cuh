@@ -216,11 +216,11 @@ __global__ void __launch_bounds__(kThreads) kh_prim_blocks(GridP g, int B, KHP<R
         const int x = (int)(i % g.nx), y = (int)(i / g.nx);
         const int ob = x / B + g.nbx * (y / B);
         if (only && !only[ob]) continue;
-        const R vol = (R)P.vol, gm1 = (R)(P.gamma - 1.0);
+        const KHK<R> K = kh_consts<R>(P.dt, P.dx, P.dy, P.vol, P.gamma);
         const bool alt = P.upar && P.upar[ob];
         R r, pp, u, v;
         kh_prim_of<R>((alt ? P.U1 : P.U)[0][i], (alt ? P.U1 : P.U)[1][i], (alt ? P.U1 : P.U)[2][i],
-                      (alt ? P.U1 : P.U)[3][i], vol, gm1, r, pp, u, v);
+                      (alt ? P.U1 : P.U)[3][i], K, r, pp, u, v);
         P.W[0][i] = r;
         P.W[1][i] = pp;
         P.W[2][i] = u;

@@ -63,28 +63,98 @@ __device__ __forceinline__ float kq(float a)
 }
 __device__ __forceinline__ double kq(double a) { return __dsqrt_rn(a); }
 
-// getPrimitive (KH_DBA.cu:461-475): rho, p, vx, vy from Mass, Momx, Momy, Energy
-template <typename R>
-__device__ __forceinline__ void kh_prim_of(R U0, R U1, R U2, R U3, R vol, R gm1, R& r, R& p, R& u, R& v)
+__device__ __forceinline__ float krcp(float a)
 {
-    r = kd(U0, vol);
-    u = kd(kd(U1, r), vol);
-    v = kd(kd(U2, r), vol);
-    p = km(ks(kd(U3, vol), km(km((R)0.5, r), ka(km(u, u), km(v, v)))), gm1);
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
 }
 
-// central gradient (Grad_x / Grad_y, KH_DBA.cu:249-275)
+// Per-launch constants of the point formulas.  FP64 evaluates the reference's
+// expressions in its order (divisions by 2 become exact multiplications by 0.5,
+// which round identically); FP32 evaluates the same quantities around
+// reciprocals and FMAs, so hx / hy and ex / ey mean different things per precision.
 template <typename R>
-__device__ __forceinline__ R kh_grad(R wp, R wm, R h) { return kd(kd(ks(wp, wm), (R)2.0), h); }
+struct KHK {
+    R vol, gm1, gam, hdt, dtdx;
+    R hx, hy;       // FP64: dx, dy (gradient (w+ - w-) * 0.5 / h).  FP32: 0.5 / dx, 0.5 / dy
+    R ex, ey;       // FP64: dx, dy (face state w -+ g h * 0.5).       FP32: 0.5 * dx, 0.5 * dy
+    R ivol, ig1;    // FP32: 1 / vol, 1 / (gamma - 1)
+};
+
+template <typename R>
+__device__ __forceinline__ KHK<R> kh_consts(double dt, double dx, double dy, double vol, double gamma)
+{
+    KHK<R> K;
+    K.vol = (R)vol;
+    K.gm1 = (R)(gamma - 1.0);
+    K.gam = (R)gamma;
+    K.hdt = (R)(0.5 * dt);
+    K.dtdx = (R)(dt * dx);
+    if constexpr (sizeof(R) == 4) {
+        K.hx = (R)(0.5 / dx);
+        K.hy = (R)(0.5 / dy);
+        K.ex = (R)(0.5 * dx);
+        K.ey = (R)(0.5 * dy);
+        K.ivol = (R)(1.0 / vol);
+        K.ig1 = (R)(1.0 / (gamma - 1.0));
+    } else {
+        K.hx = K.ex = (R)dx;
+        K.hy = K.ey = (R)dy;
+        K.ivol = (R)(1.0 / vol);
+        K.ig1 = (R)(1.0 / (gamma - 1.0));
+    }
+    return K;
+}
+
+// getPrimitive (KH_DBA.cu:461-475): rho, p, vx, vy from Mass, Momx, Momy, Energy
+template <typename R>
+__device__ __forceinline__ void kh_prim_of(R U0, R U1, R U2, R U3, const KHK<R>& K, R& r, R& p, R& u, R& v)
+{
+    if constexpr (sizeof(R) == 4) {          // U1 / r / vol = U1 / U0
+        const float iU0 = krcp(U0);
+        r = __fmul_rn(U0, K.ivol);
+        u = __fmul_rn(U1, iU0);
+        v = __fmul_rn(U2, iU0);
+        const float ke = __fmaf_rn(u, u, __fmul_rn(v, v));
+        p = __fmul_rn(K.gm1, __fmaf_rn(__fmul_rn(-0.5f, r), ke, __fmul_rn(U3, K.ivol)));
+    } else {
+        r = kd(U0, K.vol);
+        u = kd(kd(U1, r), K.vol);
+        v = kd(kd(U2, r), K.vol);
+        p = km(ks(kd(U3, K.vol), km(km((R)0.5, r), ka(km(u, u), km(v, v)))), K.gm1);
+    }
+}
+
+// central gradient (Grad_x / Grad_y, KH_DBA.cu:249-275); h = K.hx or K.hy
+template <typename R>
+__device__ __forceinline__ R kh_grad(R wp, R wm, R h)
+{
+    if constexpr (sizeof(R) == 4)
+        return __fmul_rn(__fsub_rn(wp, wm), h);
+    else
+        return kd(km(ks(wp, wm), (R)0.5), h);
+}
 
 // half-step states (extrap_in_time, KH_DBA.cu:524-531); gr = rho_dx rho_dy p_dx p_dy vx_dx vx_dy vy_dx vy_dy
 template <typename R>
-__device__ __forceinline__ void kh_prime_of(R r, R pp, R u, R v, const R* gr, R hdt, R gam, R& rp, R& ppp, R& up, R& vp)
+__device__ __forceinline__ void kh_prime_of(R r, R pp, R u, R v, const R* gr, const KHK<R>& K, R& rp, R& ppp, R& up,
+                                            R& vp)
 {
-    rp = ks(r, km(hdt, ka(ka(ka(km(u, gr[0]), km(r, gr[4])), km(v, gr[1])), km(r, gr[7]))));
-    up = ks(u, km(hdt, ka(ka(km(u, gr[4]), km(v, gr[5])), km(kd((R)1.0, r), gr[2]))));
-    vp = ks(v, km(hdt, ka(ka(km(u, gr[6]), km(v, gr[7])), km(kd((R)1.0, r), gr[3]))));
-    ppp = ks(pp, km(hdt, ka(ka(km(km(gam, pp), ka(gr[4], gr[7])), km(u, gr[2])), km(v, gr[3]))));
+    const R hdt = K.hdt;
+    if constexpr (sizeof(R) == 4) {
+        const float dv = __fadd_rn(gr[4], gr[7]), ir = krcp(r), mh = -hdt;
+        rp = __fmaf_rn(mh, __fmaf_rn(u, gr[0], __fmaf_rn(v, gr[1], __fmul_rn(r, dv))), r);
+        up = __fmaf_rn(mh, __fmaf_rn(u, gr[4], __fmaf_rn(v, gr[5], __fmul_rn(ir, gr[2]))), u);
+        vp = __fmaf_rn(mh, __fmaf_rn(u, gr[6], __fmaf_rn(v, gr[7], __fmul_rn(ir, gr[3]))), v);
+        ppp = __fmaf_rn(mh, __fmaf_rn(__fmul_rn(K.gam, pp), dv, __fmaf_rn(u, gr[2], __fmul_rn(v, gr[3]))), pp);
+    } else {
+        const R ir = kd((R)1.0, r);
+        rp = ks(r, km(hdt, ka(ka(ka(km(u, gr[0]), km(r, gr[4])), km(v, gr[1])), km(r, gr[7]))));
+        up = ks(u, km(hdt, ka(ka(km(u, gr[4]), km(v, gr[5])), km(ir, gr[2]))));
+        vp = ks(v, km(hdt, ka(ka(km(u, gr[6]), km(v, gr[7])), km(ir, gr[3]))));
+        ppp = ks(pp, km(hdt, ka(ka(km(km(K.gam, pp), ka(gr[4], gr[7])), km(u, gr[2])), km(v, gr[3]))));
+    }
 }
 
 // wake-up metric (KH_DBA.cu:614-617): sum of |gradients| in order
@@ -98,9 +168,21 @@ __device__ __forceinline__ R kh_metric(const R* gr)
 }
 
 // face state extrapolated from a cell (extrapolateInSpaceToFace, KH_DBA.cu:630-660):
-// towards the -side face w - g h / 2, towards the +side face w + g h / 2
-template <typename R> __device__ __forceinline__ R kh_face_m(R w, R g, R h) { return ks(w, kd(km(g, h), (R)2.0)); }
-template <typename R> __device__ __forceinline__ R kh_face_p(R w, R g, R h) { return ka(w, kd(km(g, h), (R)2.0)); }
+// towards the -side face w - g h / 2, towards the +side face w + g h / 2; e = K.ex or K.ey
+template <typename R> __device__ __forceinline__ R kh_face_m(R w, R g, R e)
+{
+    if constexpr (sizeof(R) == 4)
+        return __fmaf_rn(-g, e, w);
+    else
+        return ks(w, km(km(g, e), (R)0.5));
+}
+template <typename R> __device__ __forceinline__ R kh_face_p(R w, R g, R e)
+{
+    if constexpr (sizeof(R) == 4)
+        return __fmaf_rn(g, e, w);
+    else
+        return ka(w, km(km(g, e), (R)0.5));
+}
 
 // conserved-field change of one cell (applyFluxes, KH_DBA.cu:818-841)
 template <typename R>
@@ -153,9 +235,9 @@ __global__ void __launch_bounds__(kThreads) kh_prim(GridP g, KHP<R> P)
         int X, Y;
         kh_cell(g, B, P.list[it / V], (int)(it % V), X, Y);
         const size_t i = (size_t)X + (size_t)g.nx * Y;
-        const R vol = (R)P.vol, gm1 = (R)(P.gamma - 1.0);
+        const KHK<R> K = kh_consts<R>(P.dt, P.dx, P.dy, P.vol, P.gamma);
         R r, pp, u, v;
-        kh_prim_of<R>(P.U[0][i], P.U[1][i], P.U[2][i], P.U[3][i], vol, gm1, r, pp, u, v);
+        kh_prim_of<R>(P.U[0][i], P.U[1][i], P.U[2][i], P.U[3][i], K, r, pp, u, v);
         P.W[0][i] = r;
         P.W[1][i] = pp;
         P.W[2][i] = u;
@@ -185,20 +267,20 @@ __global__ void __launch_bounds__(kThreads) kh_extrap(GridP g, FlagP f, KHP<R> P
             const size_t i = (size_t)X + (size_t)g.nx * Y;
             const size_t ixm = (size_t)xm + (size_t)g.nx * Y, ixp = (size_t)xp + (size_t)g.nx * Y;
             const size_t iym = (size_t)X + (size_t)g.nx * ym, iyp = (size_t)X + (size_t)g.nx * yp;
-            const R dx = (R)P.dx, dy = (R)P.dy, hdt = (R)(0.5 * P.dt), gam = (R)P.gamma;
+            const KHK<R> K = kh_consts<R>(P.dt, P.dx, P.dy, P.vol, P.gamma);
             R gr[8];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const R* w = P.W[q == 0 ? 0 : (q == 1 ? 1 : (q == 2 ? 2 : 3))];
-                gr[2 * q] = kh_grad<R>(w[ixp], w[ixm], dx);
-                gr[2 * q + 1] = kh_grad<R>(w[iyp], w[iym], dy);
+                gr[2 * q] = kh_grad<R>(w[ixp], w[ixm], K.hx);
+                gr[2 * q + 1] = kh_grad<R>(w[iyp], w[iym], K.hy);
             }
             // gr: rho_dx rho_dy p_dx p_dy vx_dx vx_dy vy_dx vy_dy
 #pragma unroll
             for (int q = 0; q < 8; ++q) P.Gd[q][i] = gr[q];
             const R r = P.W[0][i], pp = P.W[1][i], u = P.W[2][i], v = P.W[3][i];
             R rp, ppp, up, vp;
-            kh_prime_of<R>(r, pp, u, v, gr, hdt, gam, rp, ppp, up, vp);
+            kh_prime_of<R>(r, pp, u, v, gr, K, rp, ppp, up, vp);
             P.Wp[0][i] = rp;
             P.Wp[2][i] = up;
             P.Wp[3][i] = vp;
@@ -219,29 +301,57 @@ __global__ void __launch_bounds__(kThreads) kh_extrap(GridP g, FlagP f, KHP<R> P
 // Rusanov flux across one face (getFlux, KH_DBA.cu:662-697); outputs in the
 // order Mass, Energy, normal momentum, tangential momentum
 template <typename R>
-__device__ __forceinline__ void kh_getflux(R gam, R rho_L, R rho_R, R p_L, R p_R, R vx_L, R vx_R, R vy_L, R vy_R,
-                                           R& fM, R& fE, R& fX, R& fY)
+__device__ __forceinline__ void kh_getflux(const KHK<R>& K, R rho_L, R rho_R, R p_L, R p_R, R vx_L, R vx_R, R vy_L,
+                                           R vy_R, R& fM, R& fE, R& fX, R& fY)
 {
-    const R g1 = ks(gam, (R)1.0), h = (R)0.5;
-    const R en_L = ka(kd(p_L, g1), km(km(h, rho_L), ka(km(vx_L, vx_L), km(vy_L, vy_L))));
-    const R en_R = ka(kd(p_R, g1), km(km(h, rho_R), ka(km(vx_R, vx_R), km(vy_R, vy_R))));
-    const R rho_star = km(h, ka(rho_L, rho_R));
-    const R momx_star = km(h, ka(km(rho_L, vx_L), km(rho_R, vx_R)));
-    const R momy_star = km(h, ka(km(rho_L, vy_L), km(rho_R, vy_R)));
-    const R en_star = km(h, ka(en_L, en_R));
-    const R p_star = km(g1, ks(en_star, kd(km(h, ka(km(momx_star, momx_star), km(momy_star, momy_star))), rho_star)));
-    const R fMv = momx_star;
-    const R fXv = ka(kd(km(momx_star, momx_star), rho_star), p_star);
-    const R fYv = kd(km(momx_star, momy_star), rho_star);
-    const R fEv = kd(km(ka(en_star, p_star), momx_star), rho_star);
-    const R C_L = ka(kq(kd(km(gam, p_L), rho_L)), (R)fabs(vx_L));
-    const R C_R = ka(kq(kd(km(gam, p_R), rho_R)), (R)fabs(vx_R));
-    const R C = (C_L >= C_R) ? C_L : C_R;
-    const R Ch = km(C, h);
-    fM = ks(fMv, km(Ch, ks(rho_L, rho_R)));
-    fX = ks(fXv, km(Ch, ks(km(rho_L, vx_L), km(rho_R, vx_R))));
-    fY = ks(fYv, km(Ch, ks(km(rho_L, vy_L), km(rho_R, vy_R))));
-    fE = ks(fEv, km(Ch, ks(en_L, en_R)));
+    if constexpr (sizeof(R) == 4) {
+        // the same Rusanov flux around one reciprocal of rho_star and one per side for the sound speed
+        const float h = 0.5f, g1 = K.gm1;
+        const float en_L = __fmaf_rn(__fmul_rn(h, rho_L), __fmaf_rn(vx_L, vx_L, __fmul_rn(vy_L, vy_L)), __fmul_rn(p_L, K.ig1));
+        const float en_R = __fmaf_rn(__fmul_rn(h, rho_R), __fmaf_rn(vx_R, vx_R, __fmul_rn(vy_R, vy_R)), __fmul_rn(p_R, K.ig1));
+        const float mx_L = __fmul_rn(rho_L, vx_L), mx_R = __fmul_rn(rho_R, vx_R);
+        const float my_L = __fmul_rn(rho_L, vy_L), my_R = __fmul_rn(rho_R, vy_R);
+        const float rho_star = __fmul_rn(h, __fadd_rn(rho_L, rho_R));
+        const float momx_star = __fmul_rn(h, __fadd_rn(mx_L, mx_R));
+        const float momy_star = __fmul_rn(h, __fadd_rn(my_L, my_R));
+        const float en_star = __fmul_rn(h, __fadd_rn(en_L, en_R));
+        const float irs = krcp(rho_star);
+        const float vxs = __fmul_rn(momx_star, irs);
+        const float p_star = __fmul_rn(g1, __fmaf_rn(__fmul_rn(-h, irs),
+                                                     __fmaf_rn(momx_star, momx_star, __fmul_rn(momy_star, momy_star)), en_star));
+        const float fXv = __fmaf_rn(momx_star, vxs, p_star);
+        const float fYv = __fmul_rn(momy_star, vxs);
+        const float fEv = __fmul_rn(__fadd_rn(en_star, p_star), vxs);
+        const float C_L = __fadd_rn(kq(__fmul_rn(__fmul_rn(K.gam, p_L), krcp(rho_L))), fabsf(vx_L));
+        const float C_R = __fadd_rn(kq(__fmul_rn(__fmul_rn(K.gam, p_R), krcp(rho_R))), fabsf(vx_R));
+        const float mCh = __fmul_rn(-h, fmaxf(C_L, C_R));
+        fM = __fmaf_rn(mCh, __fsub_rn(rho_L, rho_R), momx_star);
+        fX = __fmaf_rn(mCh, __fsub_rn(mx_L, mx_R), fXv);
+        fY = __fmaf_rn(mCh, __fsub_rn(my_L, my_R), fYv);
+        fE = __fmaf_rn(mCh, __fsub_rn(en_L, en_R), fEv);
+    } else {
+        const R gam = K.gam;
+        const R g1 = ks(gam, (R)1.0), h = (R)0.5;
+        const R en_L = ka(kd(p_L, g1), km(km(h, rho_L), ka(km(vx_L, vx_L), km(vy_L, vy_L))));
+        const R en_R = ka(kd(p_R, g1), km(km(h, rho_R), ka(km(vx_R, vx_R), km(vy_R, vy_R))));
+        const R rho_star = km(h, ka(rho_L, rho_R));
+        const R momx_star = km(h, ka(km(rho_L, vx_L), km(rho_R, vx_R)));
+        const R momy_star = km(h, ka(km(rho_L, vy_L), km(rho_R, vy_R)));
+        const R en_star = km(h, ka(en_L, en_R));
+        const R p_star = km(g1, ks(en_star, kd(km(h, ka(km(momx_star, momx_star), km(momy_star, momy_star))), rho_star)));
+        const R fMv = momx_star;
+        const R fXv = ka(kd(km(momx_star, momx_star), rho_star), p_star);
+        const R fYv = kd(km(momx_star, momy_star), rho_star);
+        const R fEv = kd(km(ka(en_star, p_star), momx_star), rho_star);
+        const R C_L = ka(kq(kd(km(gam, p_L), rho_L)), (R)fabs(vx_L));
+        const R C_R = ka(kq(kd(km(gam, p_R), rho_R)), (R)fabs(vx_R));
+        const R C = (C_L >= C_R) ? C_L : C_R;
+        const R Ch = km(C, h);
+        fM = ks(fMv, km(Ch, ks(rho_L, rho_R)));
+        fX = ks(fXv, km(Ch, ks(km(rho_L, vx_L), km(rho_R, vx_R))));
+        fY = ks(fYv, km(Ch, ks(km(rho_L, vy_L), km(rho_R, vy_R))));
+        fE = ks(fEv, km(Ch, ks(en_L, en_R)));
+    }
 }
 
 // --- stage 3: face states and fluxes (:630-660, :792-810) -----------------
@@ -256,7 +366,7 @@ __global__ void __launch_bounds__(kThreads) kh_flux(GridP g, KHP<R> P)
         const int xp = wrapc(X + 1, g.nx, 0), yp = wrapc(Y + 1, g.ny, 0);
         const size_t i = (size_t)X + (size_t)g.nx * Y;
         const size_t ixp = (size_t)xp + (size_t)g.nx * Y, iyp = (size_t)X + (size_t)g.nx * yp;
-        const R dx = (R)P.dx, dy = (R)P.dy;
+        const KHK<R> K = kh_consts<R>(P.dt, P.dx, P.dy, P.vol, P.gamma);
         R fc[4][4];   // [rho, vx, vy, p][face 0..3]
         const int wi[4] = {0, 2, 3, 1};      // prime / gradient slot of rho, vx, vy, p
 #pragma unroll
@@ -264,17 +374,16 @@ __global__ void __launch_bounds__(kThreads) kh_flux(GridP g, KHP<R> P)
             const R* w = P.Wp[wi[q]];
             const R* gx = P.Gd[2 * (q == 0 ? 0 : (q == 1 ? 2 : (q == 2 ? 3 : 1)))];
             const R* gy = P.Gd[2 * (q == 0 ? 0 : (q == 1 ? 2 : (q == 2 ? 3 : 1))) + 1];
-            fc[q][0] = kh_face_m<R>(w[ixp], gx[ixp], dx);
-            fc[q][1] = kh_face_p<R>(w[i], gx[i], dx);
-            fc[q][2] = kh_face_m<R>(w[iyp], gy[iyp], dy);
-            fc[q][3] = kh_face_p<R>(w[i], gy[i], dy);
+            fc[q][0] = kh_face_m<R>(w[ixp], gx[ixp], K.ex);
+            fc[q][1] = kh_face_p<R>(w[i], gx[i], K.ex);
+            fc[q][2] = kh_face_m<R>(w[iyp], gy[iyp], K.ey);
+            fc[q][3] = kh_face_p<R>(w[i], gy[i], K.ey);
         }
-        const R gam = (R)P.gamma;
         R fM, fE, fX, fY;
-        kh_getflux<R>(gam, fc[0][0], fc[0][1], fc[3][0], fc[3][1], fc[1][0], fc[1][1], fc[2][0], fc[2][1], fM, fE, fX, fY);
+        kh_getflux<R>(K, fc[0][0], fc[0][1], fc[3][0], fc[3][1], fc[1][0], fc[1][1], fc[2][0], fc[2][1], fM, fE, fX, fY);
         P.Fl[0][i] = fM; P.Fl[1][i] = fE; P.Fl[2][i] = fX; P.Fl[3][i] = fY;
         // y faces: normal velocity vy, outputs land in Momy_y (normal) and Momx_y (tangential)
-        kh_getflux<R>(gam, fc[0][2], fc[0][3], fc[3][2], fc[3][3], fc[2][2], fc[2][3], fc[1][2], fc[1][3], fM, fE, fX, fY);
+        kh_getflux<R>(K, fc[0][2], fc[0][3], fc[3][2], fc[3][3], fc[2][2], fc[2][3], fc[1][2], fc[1][3], fM, fE, fX, fY);
         P.Fl[4][i] = fM; P.Fl[5][i] = fE; P.Fl[7][i] = fX; P.Fl[6][i] = fY;
     }
 }

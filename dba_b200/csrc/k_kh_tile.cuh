@@ -59,40 +59,96 @@ __device__ __forceinline__ float kh_speed(R r, R p, R u, R v, R gam)
     return (float)ka(kq(kd(km(gam, p), r)), kq(ka(km(u, u), km(v, v))));
 }
 
+// one cell's four staged quantities, moved as one vector: primitives (rho, p, vx, vy),
+// half-step states (same order), gradients along one axis (same order), face fluxes
+// (Mass, Energy, Momx, Momy), conserved fields (Mass, Momx, Momy, Energy)
+template <typename R>
+struct Q4 {
+    R a, b, c, d;
+};
+
+// An array of n Q4s in shared memory, laid out so that consecutive lanes move
+// consecutive 16-byte words: FP32 as float4[n]; FP64 as two planes double2[n]
+// (a, b) and double2[n] (c, d).
+template <typename R>
+struct QA {
+    R* base;
+    int n;
+    __device__ __forceinline__ Q4<R> operator()(int i) const
+    {
+        if constexpr (sizeof(R) == 4) {
+            const float4 v = reinterpret_cast<const float4*>(base)[i];
+            return Q4<R>{v.x, v.y, v.z, v.w};
+        } else {
+            const double2 lo = reinterpret_cast<const double2*>(base)[i];
+            const double2 hi = reinterpret_cast<const double2*>(base)[n + i];
+            return Q4<R>{lo.x, lo.y, hi.x, hi.y};
+        }
+    }
+    __device__ __forceinline__ void put(int i, const Q4<R>& q) const
+    {
+        if constexpr (sizeof(R) == 4) {
+            reinterpret_cast<float4*>(base)[i] = make_float4(q.a, q.b, q.c, q.d);
+        } else {
+            reinterpret_cast<double2*>(base)[i] = make_double2(q.a, q.b);
+            reinterpret_cast<double2*>(base)[n + i] = make_double2(q.c, q.d);
+        }
+    }
+};
+
 template <typename R, int B> struct KHTile {
-    static constexpr int NT = 256;
+    // 13 warps: every staging phase below is one item per thread (400 primitive
+    // cells, 320 gradient cells, 288 face pairs, 256 updates), so no warp runs a
+    // second round while the others wait at the phase's barrier
+    static constexpr int NT = 416;
+    static constexpr int MINB = sizeof(R) == 4 ? 3 : 2;   // resident CTAs per SM
     static constexpr int T = 16;               // tile edge in cells
     static constexpr int TB = T / B;           // blocks per tile edge
     static constexpr int NBT = TB * TB;
     static constexpr int RB = TB + 2;          // neighbourhood edge in blocks
-    static constexpr int E2 = T + 4, P2 = E2 + 1;   // primitives: tile + 2, row pitch
-    static constexpr int E1 = T + 2, P1 = E1 + 1;   // gradients / half-step states: tile + 1
-    static constexpr int FXW = T + 1;               // x-face fluxes: columns -1 .. T-1
-    static constexpr int NW = 4 * E2 * P2, NP = 4 * E1 * P1, NG = 8 * E1 * P1;
-    static constexpr int NFX = 4 * T * FXW, NFY = 4 * (T + 1) * T, NU = 4 * T * T;
+    static constexpr int E2 = T + 4, P2 = E2;  // primitives: tile + 2, row pitch
+    static constexpr int E1 = T + 2, P1 = E1;  // gradients / half-step states: tile + 1
+    static constexpr int FXW = T + 1;          // x-face fluxes: columns -1 .. T-1
+    static constexpr int N1 = E2 * E2;                  // primitive cells
+    static constexpr int N2 = E1 * E1 - 4;              // gradient cells (the ring's corners feed no face)
+    static constexpr int N3 = (T + 1) * (T + 1) - 1;    // face-owning cells (cell (-1, -1) owns none needed)
+    // staged in units of Q4<R> (one cell's four quantities): primitives, half-step states,
+    // x and y gradients, x and y face fluxes, own conserved fields
+    static constexpr int NW = E2 * P2, NP = E1 * P1, NG = 2 * E1 * P1;
+    static constexpr int NFX = T * FXW, NFY = (T + 1) * T, NU = T * T;
     static constexpr int TPP = NT / NBT;       // tiles per scan pass
-    static constexpr size_t smem = sizeof(R) * (size_t)(NW + NP + NG + NFX + NFY + NU);
+    static constexpr int NS = 4 * N1;                 // staged next-tile inputs, R elements
+    static constexpr size_t smem = sizeof(R) * ((size_t)4 * (NW + NP + NG + NFX + NFY + NU) + NS);
     static_assert(T % B == 0 && B >= 2 && NBT <= 16, "tile shape");
+    static_assert(N1 <= NT && N2 <= NT && N3 <= NT && T * T <= NT, "one item per thread and phase");
 };
 
+// region (block of the 3x3 neighbourhood of blocks around the tile) of tile-local cell (lx, ly)
+template <int B, int RB>
+__device__ __forceinline__ int kh_region(int lx, int ly) { return (lx + B) / B + RB * ((ly + B) / B); }
+
 template <typename R, int B, bool DBA>
-__global__ void __launch_bounds__(256) kh_tile_step(GridP g, FlagP f, KHTileP<R> P)
+__global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_step(GridP g, FlagP f, KHTileP<R> P)
 {
     using S = KHTile<R, B>;
     constexpr int NT = S::NT, T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, TPP = S::TPP;
     constexpr int E2 = S::E2, P2 = S::P2, E1 = S::E1, P1 = S::P1, FXW = S::FXW;
     constexpr int V = B * B;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* sW = reinterpret_cast<R*>(smem_raw);    // [4][E2][P2]  cell (x, y) at (y + 2) * P2 + x + 2
-    R* sP = sW + S::NW;                         // [4][E1][P1]  cell (x, y) at (y + 1) * P1 + x + 1
-    R* sG = sP + S::NP;                         // [8][E1][P1]
-    R* sFx = sG + S::NG;                        // [4][T][FXW]  face right of (x, y) at y * FXW + x + 1
-    R* sFy = sFx + S::NFX;                      // [4][T+1][T]  face above (x, y) at (y + 1) * T + x
-    R* sU = sFy + S::NFY;                       // [4][T][T]    own cells' conserved fields
-    __shared__ int s_tile[TPP];
+    using Q = Q4<R>;
+    R* sm0 = reinterpret_cast<R*>(smem_raw);
+    const QA<R> sW{sm0, S::NW};                                  // [E2][P2]  primitives of cell (x, y) at (y + 2) * P2 + x + 2
+    const QA<R> sP{sW.base + 4 * S::NW, S::NP};                  // [E1][P1]  half-step states of (x, y) at (y + 1) * P1 + x + 1
+    const QA<R> sGx{sP.base + 4 * S::NP, E1 * P1};               // [E1][P1]  x gradients
+    const QA<R> sGy{sGx.base + 4 * E1 * P1, E1 * P1};            // [E1][P1]  y gradients
+    const QA<R> sFx{sGx.base + 4 * S::NG, S::NFX};               // [T][FXW]  flux through the face right of (x, y) at y * FXW + x + 1
+    const QA<R> sFy{sFx.base + 4 * S::NFX, S::NFY};              // [T+1][T]  flux through the face above (x, y) at (y + 1) * T + x
+    const QA<R> sU{sFy.base + 4 * S::NFY, S::NU};                // [T][T]    own cells' conserved fields
+    R* sStage = sU.base + 4 * S::NU;            // [4][N1] phase-1 inputs of the next tile, copied ahead
+    __shared__ int s_tile[TPP];                 // listed tiles: tbx | tby << 15 | halo-inside-domain << 30
     __shared__ unsigned s_tmeta[TPP];           // bits 0..15 active blocks, 16..31 their parity
     __shared__ int s_cnt;
-    __shared__ uint8_t s_npar[RB * RB], s_nact[RB * RB];
+    __shared__ uint8_t s_npar[2][RB * RB], s_nact[2][RB * RB];   // neighbourhood of this tile and the next
     __shared__ int s_nx[NBT];
     __shared__ double s_run[4][NT / 32];
     __shared__ double s_bsum[4][NBT];
@@ -119,12 +175,42 @@ __global__ void __launch_bounds__(256) kh_tile_step(GridP g, FlagP f, KHTileP<R>
     }
     __syncthreads();
     const double dtc = s_dt;
-    const R vol = (R)P.vol, gm1 = (R)(P.gamma - 1.0), gam = (R)P.gamma;
-    const R dx = (R)P.dx, dy = (R)P.dy, hdt = (R)(0.5 * dtc), dtdx = (R)(dtc * P.dx);
-    // this thread's own cell in the update phase: cell v of tile block kb (the
-    // layout block_tree_sums expects)
+    const KHK<R> K = kh_consts<R>(dtc, P.dx, P.dy, P.vol, P.gamma);
+
+    // This thread's item in each phase; the same tile-local cells for every tile.
+    // phase 1: primitive cell (x1, y1) of the tile + 2
+    const bool h1 = tid < S::N1;
+    const int x1 = tid % E2 - 2, y1 = tid / E2 - 2;
+    const int r1 = kh_region<B, RB>(x1, y1), s1 = (y1 + 2) * P2 + x1 + 2;
+    const bool in1 = x1 >= 0 && x1 < T && y1 >= 0 && y1 < T;
+    const int o1 = x1 + g.nx * y1;
+    // phase 2: gradient cell (x2, y2): row -1 (columns 0 .. T-1), rows 0 .. T-1 (columns -1 .. T), row T
+    const bool h2 = tid < S::N2;
+    int x2, y2;
+    if (tid < T) {
+        x2 = tid;
+        y2 = -1;
+    } else if (tid < T + T * E1) {
+        x2 = (tid - T) % E1 - 1;
+        y2 = (tid - T) / E1;
+    } else {
+        x2 = tid - T - T * E1;
+        y2 = T;
+    }
+    const int r2 = kh_region<B, RB>(x2, y2), p2 = (y2 + 1) * P1 + x2 + 1, s2 = (y2 + 2) * P2 + x2 + 2;
+    const bool in2 = x2 >= 0 && x2 < T && y2 >= 0 && y2 < T;
+    const int o2 = x2 + g.nx * y2;
+    // phase 3: face-owning cell (x3, y3) of columns and rows -1 .. T-1, skipping (-1, -1)
+    const bool h3 = tid < S::N3;
+    const int x3 = (tid + 1) % (T + 1) - 1, y3 = (tid + 1) / (T + 1) - 1;
+    const int r3 = kh_region<B, RB>(x3, y3), p3 = (y3 + 1) * P1 + x3 + 1;
+    const bool xf3 = y3 >= 0, yf3 = x3 >= 0;
+    const int o3 = x3 + g.nx * y3;
+    // phase 4: own cell v of tile block kb (the layout block_tree_sums expects)
+    const bool h4 = tid < T * T;
     const int ukb = tid / V, uv = tid % V;
     const int ux = (ukb % TB) * B + uv % B, uy = (ukb / TB) * B + uv / B;
+    const int o4 = ux + g.nx * uy;
 
     for (long long j0 = 0; blockIdx.x + (long long)G * j0 < ntiles; j0 += TPP) {
         // ---- scan: per-block bookkeeping, one list entry per tile with an active block
@@ -133,9 +219,13 @@ __global__ void __launch_bounds__(256) kh_tile_step(GridP g, FlagP f, KHTileP<R>
             const int kq = tid % NBT;
             const bool valid = tl < ntiles;
             const int tile = (int)tl;
-            int act = 0, pp = 0;
+            int act = 0, pp = 0, entry = 0;
             if (valid) {
-                const int b = ((tile % ntx) * TB + kq % TB) + g.nbx * ((tile / ntx) * TB + kq / TB);
+                const int tby = tile / ntx, tbx = tile - tby * ntx;
+                const int b = (tbx * TB + kq % TB) + g.nbx * (tby * TB + kq / TB);
+                const int X0 = tbx * T, Y0 = tby * T;
+                const bool inner = X0 >= 2 && X0 + T + 2 <= g.nx && Y0 >= 2 && Y0 + T + 2 <= g.ny;
+                entry = tbx | (tby << 15) | ((int)inner << 30);
                 pp = f.par_cur[b];
                 act = DBA ? (f.wake_cur[b] ? 1 : 0) : 1;
                 f.wake_clr[b] = 0;
@@ -153,185 +243,202 @@ __global__ void __launch_bounds__(256) kh_tile_step(GridP g, FlagP f, KHTileP<R>
             const unsigned abits = (ma >> g0) & gm, pbits = (mp >> g0) & gm;
             if (tid == 0) s_cnt = 0;
             __syncthreads();
-            list_append(valid && kq == 0 && abits != 0, tile, (int)(abits | (pbits << 16)), s_tile,
+            list_append(valid && kq == 0 && abits != 0, entry, (int)(abits | (pbits << 16)), s_tile,
                         reinterpret_cast<int*>(s_tmeta), &s_cnt);
             __syncthreads();
         }
         const int cnt = s_cnt;
-        for (int i = 0; i < cnt; ++i) {
-            const int tile = s_tile[i];
-            const unsigned tm = s_tmeta[i];
-            const int tbx = tile % ntx, tby = tile / ntx;
-            const int X0 = tbx * T, Y0 = tby * T;
+        // Tile i's phase-1 inputs (conserved fields where the owning block is active,
+        // persisted primitives where it is not) are copied into sStage while tile i-1
+        // computes; each thread copies and later reads only its own phase-1 cell.  Within
+        // a step nothing writes what is copied: updates go to the other buffer and only
+        // active blocks persist.
+        auto neighbourhood = [&](int entry, int buf) {
             if (tid < RB * RB) {
+                const int tbx = entry & 0x7fff, tby = (entry >> 15) & 0x7fff;
                 const int bx = wrap_p(tbx * TB + tid % RB - 1, g.nbx), by = wrap_p(tby * TB + tid / RB - 1, g.nby);
                 const int ob = bx + g.nbx * by;
-                s_npar[tid] = f.par_cur[ob];
-                s_nact[tid] = DBA ? (f.wake_cur[ob] ? 1 : 0) : 1;
+                s_npar[buf][tid] = f.par_cur[ob];
+                s_nact[buf][tid] = DBA ? (f.wake_cur[ob] ? 1 : 0) : 1;
             }
+        };
+        struct TileAt {
+            int X0, Y0;
+            bool inner;       // the 2-cell halo stays inside the domain: no periodic wrap
+            long long base;   // index of the tile's first cell
+        };
+        auto tile_at = [&](int entry) -> TileAt {
+            const int X0 = (entry & 0x7fff) * T, Y0 = ((entry >> 15) & 0x7fff) * T;
+            return TileAt{X0, Y0, ((entry >> 30) & 1) != 0, (long long)X0 + (long long)nx * Y0};
+        };
+        auto cell_index = [&](const TileAt& t, int lx, int ly, int off) -> size_t {
+            return t.inner ? (size_t)(t.base + off)
+                           : (size_t)wrap_p(t.X0 + lx, g.nx) + nx * (size_t)wrap_p(t.Y0 + ly, g.ny);
+        };
+        auto prefetch = [&](const TileAt& t, int buf) {
+            if (h1) {
+                const size_t gi = cell_index(t, x1, y1, o1);
+                const bool act = s_nact[buf][r1];
+                const int par = s_npar[buf][r1];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    cp_async_elem<sizeof(R)>(sStage + q * S::N1 + tid, (act ? P.U[q][par] : P.W[q]) + gi);
+            }
+            cp_async_commit();
+        };
+        if (cnt > 0) {
+            neighbourhood(s_tile[0], 0);
+            __syncthreads();
+            prefetch(tile_at(s_tile[0]), 0);
+        }
+        for (int i = 0; i < cnt; ++i) {
+            const int entry = s_tile[i];
+            const unsigned tm = s_tmeta[i];
+            const int nb = i & 1;                 // this tile's neighbourhood tables
+            const TileAt cur = tile_at(entry);
+            const int tbx = entry & 0x7fff, tby = (entry >> 15) & 0x7fff;
+            const long long base = cur.base;
             if (tid < NBT) {
                 s_nx[tid] = 0;
                 s_vblk[tid] = 0u;
             }
-            __syncthreads();
+            if (i + 1 < cnt) neighbourhood(s_tile[i + 1], nb ^ 1);
 
-            // 1. primitives on tile + 2
-            for (int c = tid; c < E2 * E2; c += NT) {
-                const int ly = c / E2 - 2, lx = c % E2 - 2;
-                const int reg = (lx + B) / B + RB * ((ly + B) / B);
-                const size_t gi = (size_t)wrap_p(X0 + lx, g.nx) + nx * (size_t)wrap_p(Y0 + ly, g.ny);
-                const int si = (ly + 2) * P2 + lx + 2;
-                R r, pp, u, v;
-                if (s_nact[reg]) {
-                    const int par = s_npar[reg];
-                    const R U0 = P.U[0][par][gi], U1 = P.U[1][par][gi], U2 = P.U[2][par][gi], U3 = P.U[3][par][gi];
-                    kh_prim_of<R>(U0, U1, U2, U3, vol, gm1, r, pp, u, v);
-                    if (lx >= 0 && lx < T && ly >= 0 && ly < T) {
-                        const int ui = ly * T + lx;
-                        sU[ui] = U0;
-                        sU[T * T + ui] = U1;
-                        sU[2 * T * T + ui] = U2;
-                        sU[3 * T * T + ui] = U3;
-                    }
+            // 1. primitives on tile + 2, from the staged inputs
+            cp_async_wait0();
+            if (h1) {
+                const R v0 = sStage[tid], v1 = sStage[S::N1 + tid], v2 = sStage[2 * S::N1 + tid],
+                        v3 = sStage[3 * S::N1 + tid];
+                if (s_nact[nb][r1]) {
+                    R r, pp, u, v;
+                    kh_prim_of<R>(v0, v1, v2, v3, K, r, pp, u, v);
+                    if (in1) sU.put(y1 * T + x1, Q{v0, v1, v2, v3});
+                    sW.put(s1, Q{r, pp, u, v});
                 } else {
-                    r = P.W[0][gi];
-                    pp = P.W[1][gi];
-                    u = P.W[2][gi];
-                    v = P.W[3][gi];
+                    sW.put(s1, Q{v0, v1, v2, v3});
                 }
-                sW[si] = r;
-                sW[E2 * P2 + si] = pp;
-                sW[2 * E2 * P2 + si] = u;
-                sW[3 * E2 * P2 + si] = v;
             }
             __syncthreads();
+            if (i + 1 < cnt) prefetch(tile_at(s_tile[i + 1]), nb ^ 1);
 
             // 2. gradients and half-step states on tile + 1; wake-up metric of own cells
-            for (int c = tid; c < E1 * E1; c += NT) {
-                const int ly = c / E1 - 1, lx = c % E1 - 1;
-                const int reg = (lx + B) / B + RB * ((ly + B) / B);
-                const int pi = (ly + 1) * P1 + lx + 1;
-                if (s_nact[reg]) {
-                    const int si = (ly + 2) * P2 + lx + 2;
-                    R gr[8];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {   // rho, p, vx, vy
-                        const R* w = sW + q * E2 * P2;
-                        gr[2 * q] = kh_grad<R>(w[si + 1], w[si - 1], dx);
-                        gr[2 * q + 1] = kh_grad<R>(w[si + P2], w[si - P2], dy);
-                    }
+            if (h2) {
+                if (s_nact[nb][r2]) {
+                    const Q c = sW(s2), xp = sW(s2 + 1), xm = sW(s2 - 1), yp = sW(s2 + P2), ym = sW(s2 - P2);
+                    // rho_dx rho_dy p_dx p_dy vx_dx vx_dy vy_dx vy_dy
+                    R gr[8] = {kh_grad<R>(xp.a, xm.a, K.hx), kh_grad<R>(yp.a, ym.a, K.hy),
+                               kh_grad<R>(xp.b, xm.b, K.hx), kh_grad<R>(yp.b, ym.b, K.hy),
+                               kh_grad<R>(xp.c, xm.c, K.hx), kh_grad<R>(yp.c, ym.c, K.hy),
+                               kh_grad<R>(xp.d, xm.d, K.hx), kh_grad<R>(yp.d, ym.d, K.hy)};
                     R rp, ppp, up, vp;
-                    kh_prime_of<R>(sW[si], sW[E2 * P2 + si], sW[2 * E2 * P2 + si], sW[3 * E2 * P2 + si], gr, hdt, gam,
-                                   rp, ppp, up, vp);
-                    sP[pi] = rp;
-                    sP[E1 * P1 + pi] = ppp;
-                    sP[2 * E1 * P1 + pi] = up;
-                    sP[3 * E1 * P1 + pi] = vp;
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) sG[q * E1 * P1 + pi] = gr[q];
-                    if (DBA && lx >= 0 && lx < T && ly >= 0 && ly < T && kh_metric<R>(gr) > (R)P.thr)
-                        s_nx[lx / B + TB * (ly / B)] = 1;
+                    kh_prime_of<R>(c.a, c.b, c.c, c.d, gr, K, rp, ppp, up, vp);
+                    sP.put(p2, Q{rp, ppp, up, vp});
+                    sGx.put(p2, Q{gr[0], gr[2], gr[4], gr[6]});
+                    sGy.put(p2, Q{gr[1], gr[3], gr[5], gr[7]});
+                    if (DBA && in2 && kh_metric<R>(gr) > (R)P.thr) s_nx[x2 / B + TB * (y2 / B)] = 1;
                 } else {
-                    const size_t gi = (size_t)wrap_p(X0 + lx, g.nx) + nx * (size_t)wrap_p(Y0 + ly, g.ny);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) sP[q * E1 * P1 + pi] = P.Wp[q][gi];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) sG[q * E1 * P1 + pi] = P.Gd[q][gi];
+                    const size_t gi = cell_index(cur, x2, y2, o2);
+                    sP.put(p2, Q{P.Wp[0][gi], P.Wp[1][gi], P.Wp[2][gi], P.Wp[3][gi]});
+                    sGx.put(p2, Q{P.Gd[0][gi], P.Gd[2][gi], P.Gd[4][gi], P.Gd[6][gi]});
+                    sGy.put(p2, Q{P.Gd[1][gi], P.Gd[3][gi], P.Gd[5][gi], P.Gd[7][gi]});
                 }
             }
             __syncthreads();
 
-            // 3. face fluxes: x faces of columns -1 .. T-1, y faces of rows -1 .. T-1
-            for (int c = tid; c < 2 * T * FXW; c += NT) {
-                const bool xf = c < T * FXW;
-                const int c2 = xf ? c : c - T * FXW;
-                const int lx = xf ? c2 % FXW - 1 : c2 % T, ly = xf ? c2 / FXW : c2 / T - 1;
-                const int reg = (lx + B) / B + RB * ((ly + B) / B);
-                R* dst = xf ? sFx + ly * FXW + lx + 1 : sFy + (ly + 1) * T + lx;
-                constexpr int FS = T * FXW;          // stride between flux fields (same for x and y)
-                static_assert(T * FXW == (T + 1) * T, "flux tiles share a stride");
-                if (s_nact[reg]) {
-                    const int pi = (ly + 1) * P1 + lx + 1;
-                    const int pn = xf ? pi + 1 : pi + P1;      // the face's other cell
-                    const int gd = xf ? 0 : 1;                 // x or y gradient slot
-                    const R h = xf ? dx : dy;
-                    // face states [rho, vx, vy, p]: fc[.][0] from the +side cell, fc[.][1] from this cell
-                    const int wi[4] = {0, 2, 3, 1};
-                    R fc[4][2];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const R* w = sP + wi[q] * E1 * P1;
-                        const R* gq = sG + (2 * wi[q] + gd) * E1 * P1;
-                        fc[q][0] = kh_face_m<R>(w[pn], gq[pn], h);
-                        fc[q][1] = kh_face_p<R>(w[pi], gq[pi], h);
+            // 3. face fluxes.  Cell (x3, y3) owns the x face on its right (needed for rows
+            //    0 .. T-1) and the y face above it (columns 0 .. T-1); both are computed where
+            //    the cell's block is active and read back where it is not.
+            if (h3) {
+                if (s_nact[nb][r3]) {
+                    // face states from the +side cell (m) and this cell (p); getflux takes
+                    // rho, p, normal velocity, tangential velocity of both sides
+                    const Q w0 = sP(p3);
+                    if (xf3) {
+                        const Q w1 = sP(p3 + 1), g0 = sGx(p3), g1 = sGx(p3 + 1);
+                        R fM, fE, fX, fY;
+                        kh_getflux<R>(K, kh_face_m<R>(w1.a, g1.a, K.ex), kh_face_p<R>(w0.a, g0.a, K.ex),
+                                      kh_face_m<R>(w1.b, g1.b, K.ex), kh_face_p<R>(w0.b, g0.b, K.ex),
+                                      kh_face_m<R>(w1.c, g1.c, K.ex), kh_face_p<R>(w0.c, g0.c, K.ex),
+                                      kh_face_m<R>(w1.d, g1.d, K.ex), kh_face_p<R>(w0.d, g0.d, K.ex), fM, fE, fX, fY);
+                        sFx.put(y3 * FXW + x3 + 1, Q{fM, fE, fX, fY});
                     }
-                    R fM, fE, fX, fY;
-                    if (xf) {
-                        kh_getflux<R>(gam, fc[0][0], fc[0][1], fc[3][0], fc[3][1], fc[1][0], fc[1][1], fc[2][0],
-                                      fc[2][1], fM, fE, fX, fY);
-                        dst[0] = fM; dst[FS] = fE; dst[2 * FS] = fX; dst[3 * FS] = fY;   // Mass Energy Momx Momy
-                    } else {
-                        kh_getflux<R>(gam, fc[0][0], fc[0][1], fc[3][0], fc[3][1], fc[2][0], fc[2][1], fc[1][0],
-                                      fc[1][1], fM, fE, fX, fY);
-                        dst[0] = fM; dst[FS] = fE; dst[2 * FS] = fY; dst[3 * FS] = fX;   // Mass Energy Momx Momy
+                    if (yf3) {
+                        const Q w1 = sP(p3 + P1), g0 = sGy(p3), g1 = sGy(p3 + P1);
+                        R fM, fE, fX, fY;
+                        kh_getflux<R>(K, kh_face_m<R>(w1.a, g1.a, K.ey), kh_face_p<R>(w0.a, g0.a, K.ey),
+                                      kh_face_m<R>(w1.b, g1.b, K.ey), kh_face_p<R>(w0.b, g0.b, K.ey),
+                                      kh_face_m<R>(w1.d, g1.d, K.ey), kh_face_p<R>(w0.d, g0.d, K.ey),
+                                      kh_face_m<R>(w1.c, g1.c, K.ey), kh_face_p<R>(w0.c, g0.c, K.ey), fM, fE, fX, fY);
+                        sFy.put((y3 + 1) * T + x3, Q{fM, fE, fY, fX});   // normal momentum is Momy here
                     }
                 } else {
-                    const size_t gi = (size_t)wrap_p(X0 + lx, g.nx) + nx * (size_t)wrap_p(Y0 + ly, g.ny);
-                    const int o = xf ? 0 : 4;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) dst[q * FS] = P.Fl[o + q][gi];
+                    const size_t gi = cell_index(cur, x3, y3, o3);
+                    if (xf3) sFx.put(y3 * FXW + x3 + 1, Q{P.Fl[0][gi], P.Fl[1][gi], P.Fl[2][gi], P.Fl[3][gi]});
+                    if (yf3) sFy.put((y3 + 1) * T + x3, Q{P.Fl[4][gi], P.Fl[5][gi], P.Fl[6][gi], P.Fl[7][gi]});
                 }
             }
             __syncthreads();
 
             // 4. update of own active cells; persistence for blocks that may sleep
-            const bool own = (tm >> ukb) & 1u;
+            const bool own = h4 && ((tm >> ukb) & 1u);
             double ch[4] = {0.0, 0.0, 0.0, 0.0};
             if (own) {
                 const int dst = (int)((tm >> (16 + ukb)) & 1u) ^ 1;
-                const size_t gi = (size_t)(X0 + ux) + nx * (size_t)(Y0 + uy);
+                const size_t gi = (size_t)(base + o4);
                 const int ui = uy * T + ux;
-                // field q: Mass, Momx, Momy, Energy; flux slot in the shared tiles: Mass 0, Energy 1, Momx 2, Momy 3
-                const int fs[4] = {0, 2, 3, 1};
-                bool bad = false;
+                // fluxes (Mass, Energy, Momx, Momy) through the right, left, upper and lower faces
+                const Q fr = sFx(uy * FXW + ux + 1), fl = sFx(uy * FXW + ux);
+                const Q fu = sFy((uy + 1) * T + ux), fd = sFy(uy * T + ux);
+                const Q u0 = sU(ui);
+                const R c[4] = {kh_change<R>(K.dtdx, fr.a, fl.a, fu.a, fd.a), kh_change<R>(K.dtdx, fr.c, fl.c, fu.c, fd.c),
+                                kh_change<R>(K.dtdx, fr.d, fl.d, fu.d, fd.d), kh_change<R>(K.dtdx, fr.b, fl.b, fu.b, fd.b)};
+                const Q un{ka(u0.a, c[0]), ka(u0.b, c[1]), ka(u0.c, c[2]), ka(u0.d, c[3])};   // Mass Momx Momy Energy
+                P.U[0][dst][gi] = un.a;
+                P.U[1][dst][gi] = un.b;
+                P.U[2][dst][gi] = un.c;
+                P.U[3][dst][gi] = un.d;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const R* Fx = sFx + fs[q] * (T * FXW);
-                    const R* Fy = sFy + fs[q] * (T * FXW);
-                    const R c = kh_change<R>(dtdx, Fx[uy * FXW + ux + 1], Fx[uy * FXW + ux], Fy[(uy + 1) * T + ux],
-                                             Fy[uy * T + ux]);
-                    const R un = ka(sU[q * T * T + ui], c);
-                    P.U[q][dst][gi] = un;
-                    bad |= !isfinite(un);
-                    ch[q] = (double)c;
-                    if (cfl) sU[q * T * T + ui] = un;   // own cell only: new state for the speed below
-                }
-                if (bad) raise_status(f.status, 5);
+                for (int q = 0; q < 4; ++q) ch[q] = (double)c[q];
+                if (!(isfinite(un.a) && isfinite(un.b) && isfinite(un.c) && isfinite(un.d))) raise_status(f.status, 5);
                 if (cfl) {
-                    R r, pp, u, v;
-                    kh_prim_of<R>(sU[ui], sU[T * T + ui], sU[2 * T * T + ui], sU[3 * T * T + ui], vol, gm1, r, pp, u, v);
-                    atomicMax(&s_vblk[ukb], __float_as_uint(kh_speed<R>(r, pp, u, v, gam)));
+                    R r, pp, uu, vv;
+                    kh_prim_of<R>(un.a, un.b, un.c, un.d, K, r, pp, uu, vv);
+                    atomicMax(&s_vblk[ukb], __float_as_uint(kh_speed<R>(r, pp, uu, vv, K.gam)));
                 }
                 if (DBA && !s_nx[ukb]) {
                     const int si = (uy + 2) * P2 + ux + 2, pi = (uy + 1) * P1 + ux + 1;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) P.W[q][gi] = sW[q * E2 * P2 + si];
+                    const Q w = sW(si);
+                    P.W[0][gi] = w.a;
+                    P.W[1][gi] = w.b;
+                    P.W[2][gi] = w.c;
+                    P.W[3][gi] = w.d;
                     const int bxl = ux % B, byl = uy % B;
                     if (bxl == 0 || bxl == B - 1 || byl == 0 || byl == B - 1) {
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) P.Wp[q][gi] = sP[q * E1 * P1 + pi];
-#pragma unroll
-                        for (int q = 0; q < 8; ++q) P.Gd[q][gi] = sG[q * E1 * P1 + pi];
+                        const Q hp = sP(pi), gx = sGx(pi), gy = sGy(pi);
+                        P.Wp[0][gi] = hp.a;
+                        P.Wp[1][gi] = hp.b;
+                        P.Wp[2][gi] = hp.c;
+                        P.Wp[3][gi] = hp.d;
+                        P.Gd[0][gi] = gx.a;
+                        P.Gd[1][gi] = gy.a;
+                        P.Gd[2][gi] = gx.b;
+                        P.Gd[3][gi] = gy.b;
+                        P.Gd[4][gi] = gx.c;
+                        P.Gd[5][gi] = gy.c;
+                        P.Gd[6][gi] = gx.d;
+                        P.Gd[7][gi] = gy.d;
                     }
                     if (bxl == B - 1) {
-                        const R* Fx = sFx + uy * FXW + ux + 1;
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) P.Fl[q][gi] = Fx[q * (T * FXW)];
+                        P.Fl[0][gi] = fr.a;
+                        P.Fl[1][gi] = fr.b;
+                        P.Fl[2][gi] = fr.c;
+                        P.Fl[3][gi] = fr.d;
                     }
                     if (byl == B - 1) {
-                        const R* Fy = sFy + (uy + 1) * T + ux;
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) P.Fl[4 + q][gi] = Fy[q * (T * FXW)];
+                        P.Fl[4][gi] = fu.a;
+                        P.Fl[5][gi] = fu.b;
+                        P.Fl[6][gi] = fu.c;
+                        P.Fl[7][gi] = fu.d;
                     }
                 }
             }
