@@ -70,6 +70,11 @@ WORKLOADS = {
         model="kh", nx=4096, ny=4096, nz=1, block=16, precision=1, conserved=0, mode=1, t_total=49000,
         params=dict(dt=1.0 / 4096 * 0.4 / 3.0, dx=1.0 / 4096, dy=1.0 / 4096, kh_gamma=1.4, metric_eps=1.0, ic=2,
                     noise_amp=1e-4, cfl=0.4)),
+    # the same flow on a 2048^2 grid (512 MB of state, above L2): the size kernel profiles are taken on
+    "kh_2048_fp32": dict(
+        model="kh", nx=2048, ny=2048, nz=1, block=16, precision=1, conserved=0, mode=1, t_total=24500,
+        params=dict(dt=1.0 / 2048 * 0.4 / 3.0, dx=1.0 / 2048, dy=1.0 / 2048, kh_gamma=1.4, metric_eps=1.0, ic=2,
+                    noise_amp=1e-4, cfl=0.4)),
 }
 
 

@@ -397,8 +397,10 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                 P.U[1][dst][gi] = un.b;
                 P.U[2][dst][gi] = un.c;
                 P.U[3][dst][gi] = un.d;
+                if (P.conserved) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) ch[q] = (double)c[q];
+                    for (int q = 0; q < 4; ++q) ch[q] = (double)c[q];
+                }
                 if (!(isfinite(un.a) && isfinite(un.b) && isfinite(un.c) && isfinite(un.d))) raise_status(f.status, 5);
                 if (cfl) {
                     R r, pp, uu, vv;
