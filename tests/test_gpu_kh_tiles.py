@@ -65,6 +65,32 @@ def test_kh_tiles_bitexact_vs_stage_kernels(prec, B, conserved):
 
 
 @pytest.mark.parametrize("prec", [1, 0])
+@pytest.mark.parametrize("B", [8, 16])
+def test_kh_tiles_many_tiles_per_cta(prec, B):
+    """A 1024x512 grid has 2048 tiles, several per CTA, so each CTA stages the next
+    listed tile's inputs while it computes the current one; the results must still
+    equal the stage kernels' bit for bit."""
+    nx, ny = 1024, 512
+
+    def sim(tiles):
+        prm = dict(KH_REF, metric_eps=20.0)
+        s = dba_b200.Simulation(kh_cfg(prm, nx, ny, B, precision=prec, conserved=0, tiles=tiles))
+        return s.init([a[None] for a in sharp_bands(nx, ny, seed=5)])
+
+    t, k = sim(1), sim(0)
+    act = []
+    for n in (1, 2, 7, 30, 60):
+        t.step(n, 1)
+        k.step(n, 1)
+        _same(t, k)
+        act.append(float(np.mean(t.flags(0))))
+    assert 0.0 < min(act) < 0.8
+    t.step(10, 0)
+    k.step(10, 0)
+    _same(t, k)
+
+
+@pytest.mark.parametrize("prec", [1, 0])
 def test_kh_tiles_regular_then_dba(prec):
     t, k = _sim(prec, 8, 0, 1), _sim(prec, 8, 0, 0)
     for n, mode in ((10, 0), (30, 1), (10, 0), (20, 1)):
