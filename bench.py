@@ -21,6 +21,11 @@ DBA and in regular mode, with total wall times (`--no-full-runs` skips it), and
 parameter sweep (256 seeded requests, Poisson arrivals, admission by device
 memory, autotuned block edge and threads) against the same requests run one at
 a time -- runs/s of both and p50/p99 time to completion (`--no-sweep` skips it).
+`--full-runs-kh 1,20` adds the KH flow (4096^2, 62 880 steps: simulated time 2)
+with those wake-up thresholds to the whole runs.
+For FP32 workloads, `fp32_error_vs_fp64` gives the relative L2 error and the
+largest difference of each state field after `--error-steps` steps (default
+1000) on the full grid, against the FP64 engine from the same initial state.
 
 `--impl reference` times the reference's own serial CPU program for the same
 model, built from the reference sources under oracle/_ref (Model B and KH: its
@@ -64,10 +69,10 @@ WORKLOADS = {
         model="dendrite", nx=512, ny=512, nz=512, block=8, precision=1, conserved=0, mode=1, t_total=20000,
         params=dict(Delta=1.15, delta=0.2, metric_p=1e-3, metric_T=1e-5, ic=1, ic_radius=10.0, ic_width=2.0, bc=1,
                     ic_corner=1)),
-    # C2: KH 4096^2 FP32, 16x16 blocks, gamma 1.4, sharp bands + seeded noise, CFL 0.4 chosen on the device
-    # (t = 2 is ~49 000 steps at the layer's ~2.4 maximum signal speed)
+    # C2: KH 4096^2 FP32, 16x16 blocks, gamma 1.4, sharp bands + seeded noise, CFL 0.4 chosen on the device;
+    # simulated time 2 is reached after 62 880 steps (measured in both modes)
     "kh_4096_fp32": dict(
-        model="kh", nx=4096, ny=4096, nz=1, block=16, precision=1, conserved=0, mode=1, t_total=49000,
+        model="kh", nx=4096, ny=4096, nz=1, block=16, precision=1, conserved=0, mode=1, t_total=62880,
         params=dict(dt=1.0 / 4096 * 0.4 / 3.0, dx=1.0 / 4096, dy=1.0 / 4096, kh_gamma=1.4, metric_eps=1.0, ic=2,
                     noise_amp=1e-4, cfl=0.4)),
     # the same flow on a 2048^2 grid (512 MB of state, above L2): the size kernel profiles are taken on
@@ -327,6 +332,8 @@ def run_ours(args, w):
             result["sweep"] = run_sweep(args)
         if world == 1 and not args.no_full_runs:
             result["full_runs_dba_vs_regular"] = run_full_runs(args)
+        if world == 1 and w["precision"] == 1 and args.error_steps > 0:
+            result["fp32_error_vs_fp64"] = run_fp32_error(w, args.error_steps)
     sim.close()
     if world > 1:
         dist.barrier()
@@ -443,17 +450,58 @@ def run_sweep(args):
     }
 
 
+STATE_FIELDS = {"dendrite": ("p", "T"), "modelb": ("x", "y", "z"), "kh": ("Mass", "Momx", "Momy", "Energy")}
+
+
+def run_fp32_error(w, nsteps):
+    """Error of the FP32 engine on the workload's full grid against the FP64 engine (whose
+    fields equal the CPU restatement bit for bit at every step, in the parity tests): both
+    advanced nsteps in the workload's mode from the same initial state; per state field the
+    relative L2 error and the largest absolute difference."""
+    import numpy as np
+    import dba_b200
+
+    ref, act, status = {}, [], []
+    out = {"steps": nsteps, "mode": "DBA" if w["mode"] else "regular",
+           "against": "FP64 engine (bit-identical to the FP64 CPU restatement)", "fields": {}}
+    for prec in (0, 1):
+        sim = dba_b200.Simulation(make_config(dict(w, precision=prec))).init()
+        sim.step(nsteps, w["mode"])
+        status.append(sim._L.dba_sync(sim._h))
+        act.append(float(np.mean(sim.flags(0) != 0)))
+        for f in STATE_FIELDS[w["model"]]:
+            a = sim.field(f)
+            if prec == 0:
+                ref[f] = a
+            else:
+                d = a - ref[f]
+                nrm = float(np.linalg.norm(ref[f]))
+                out["fields"][f] = {"rel_l2": float(np.linalg.norm(d)) / nrm if nrm else None,
+                                    "max_abs": float(np.max(np.abs(d)))}
+        sim.close()
+    out["active_fraction_fp64_fp32"] = act
+    out["status"] = status
+    return out
+
+
 def run_full_runs(args):
-    """DBA against the all-blocks regular mode over whole runs of the dendrite workloads:
-    each advanced from its initial state to its end time in both modes (captured graphs,
-    CUDA events on the engine's stream), with the tip and active fraction at the end."""
+    """DBA against the all-blocks regular mode over whole runs of the dendrite workloads
+    (and, with --full-runs-kh EPS[,EPS..], of the KH flow with those wake-up thresholds):
+    each advanced from its initial state to its end in both modes (captured graphs, CUDA
+    events on the engine's stream), with the active fraction and the tip or simulated time
+    at the end (the KH step count is the one that reaches simulated time 2)."""
     import torch
     import dba_b200
 
     out = {}
-    for name in ("dendrite_512_fp64", "dendrite3d_512_fp32"):
-        w = WORKLOADS[name]
+    runs = [(n, WORKLOADS[n]) for n in ("dendrite_512_fp64", "dendrite3d_512_fp32")]
+    for eps in (args.full_runs_kh.split(",") if args.full_runs_kh else []):
+        w = WORKLOADS["kh_4096_fp32"]
+        runs.append((f"kh_4096_fp32_eps{float(eps):g}", dict(w, params=dict(w["params"], metric_eps=float(eps)))))
+    for name, w in runs:
         row = {"steps": w["t_total"], "grid": [w["nx"], w["ny"], w["nz"]], "dtype": "f32" if w["precision"] else "f64"}
+        if w["model"] == "kh":
+            row["metric_eps"] = w["params"]["metric_eps"]
         for mode, key in ((1, "dba"), (0, "regular")):
             sim = dba_b200.Simulation(make_config(w)).init()
             stream = torch.cuda.ExternalStream(sim.stream)
@@ -464,12 +512,16 @@ def run_full_runs(args):
             e1 = torch.cuda.Event(enable_timing=True)
             c0 = sim.cell_updates()
             e0.record(stream)
-            sim.step(w["t_total"], mode)
+            nsteps = w["t_total"]
+            sim.step(nsteps, mode)
             e1.record(stream)
             torch.cuda.synchronize()
             row[key + "_s"] = e0.elapsed_time(e1) / 1e3
-            row[key + "_mean_active_fraction"] = (sim.cell_updates() - c0) / (w["t_total"] * sim.n)
-            row[key + "_tip"] = sim.tip()
+            row[key + "_mean_active_fraction"] = (sim.cell_updates() - c0) / (nsteps * sim.n)
+            if w["model"] == "dendrite":
+                row[key + "_tip"] = sim.tip()
+            else:
+                row[key + "_time"] = sim.observables()["time"]
             sim.close()
         row["dba_speedup"] = row["regular_s"] / row["dba_s"] if row["dba_s"] else None
         out[name] = row
@@ -526,6 +578,10 @@ def main():
     ap.add_argument("--no-sweep", action="store_true", help="skip the batched dendrite sweep section")
     ap.add_argument("--no-full-runs", action="store_true",
                     help="skip the whole-run DBA-vs-regular comparison of the dendrite workloads")
+    ap.add_argument("--full-runs-kh", default="", metavar="EPS[,EPS..]",
+                    help="add the KH flow (4096^2, to simulated time 2) with these wake-up thresholds to the whole runs")
+    ap.add_argument("--error-steps", type=int, default=1000,
+                    help="steps of the FP32-against-FP64 error check on the full grid (0: skip)")
     ap.add_argument("--sweep-requests", type=int, default=256)
     ap.add_argument("--sweep-rate", type=float, default=200.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--sweep-seed", type=int, default=0)
