@@ -150,8 +150,8 @@ __global__ void __launch_bounds__(256 / R, 4)
     modelb_tile_step(GridP g, FlagP f, MBFastP P, MBPairP K, MBFastBuf Q, LazyP L)
 {
     using S = MBTile<B, R>;
-    constexpr int NT = S::NT, T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, SW = S::SW, SP = S::SP, SV = S::SV;
-    constexpr int NQ = S::NQ, NQT = S::NQT, MP = S::MP, MV = S::MV, RING = S::RING, NPAIR = S::NPAIR;
+    constexpr int T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, SP = S::SP, SV = S::SV;
+    constexpr int NQT = S::NQT, MP = S::MP, MV = S::MV, NPAIR = S::NPAIR;
     constexpr int TPP = S::TPP;
     extern __shared__ __align__(128) float smem_f[];
     float* stage = smem_f;               // [2][3][SV]
