@@ -14,7 +14,10 @@
 //     computes; pieces that fall outside a zero-flux wall are clamped cell by
 //     cell instead;
 //   * each thread owns one (x, y) column of the tile and slides a 3-plane
-//     window along z, so the z neighbours come from registers.
+//     window along z, so the z neighbours come from registers.  A warp holds
+//     8 x 4 columns of one block, so the warps of a listed tile's inactive
+//     blocks skip the update; with a 40-float row pitch its four row segments
+//     fall on distinct banks.
 #pragma once
 
 #include "k_common.cuh"
@@ -28,7 +31,7 @@ struct DenTile {
     static constexpr int TX = 32;                // tile x extent (4 blocks)
     static constexpr int TBX = TX / B;
     static constexpr int SW = TX + 8;            // staged row: 4-cell (16-byte) halo each side
-    static constexpr int SP = SW + 4;            // row pitch
+    static constexpr int SP = SW;                // row pitch (16-byte multiple)
     static constexpr int SR = B + 2;             // staged rows per plane (y) and planes (z)
     static constexpr int PL = SR * SP;           // one staged plane
     static constexpr int SV = SR * PL;           // one staged field
@@ -62,8 +65,8 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
     const float f0 = (float)P.f0, f1 = (float)P.f1, f2 = (float)P.f2, f3 = (float)P.f3;
     const float dt = (float)P.dt, delta = (float)P.delta, eps2 = (float)P.eps2, gam = (float)P.gamma;
     const float thr_p = (float)P.thr_p, thr_p_hi = (float)P.thr_p_hi, thr_T = (float)P.thr_T;
-    const int cx = tid % TX, cy = tid / TX;       // this thread's column
-    const int kb = cx / B;                        // its block within the tile
+    const int kb = tid / (B * B);                 // this thread's block within the tile
+    const int cx = kb * B + tid % B, cy = (tid / B) % B;   // and its column
 
     auto tile_xyz = [&](int tile, int& X0, int& Y0, int& Z0) {
         X0 = (tile % ntx) * TX;
