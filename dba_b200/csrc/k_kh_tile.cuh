@@ -22,6 +22,13 @@
 // of its 1-cell ring, and the fluxes of its right column and top row -- only
 // when its own wake-up test is negative: a block whose test is positive is
 // active next step (it wakes itself), so nothing it computes now is read stale.
+//
+// Launch shape: 416 threads (13 warps), so that each phase is one item per
+// thread (400, 320, 288 and 256 items) and no warp runs a second round while
+// the others wait at the phase's barrier.  Each thread's tile-local cells are
+// fixed for the whole launch; the list entries carry the tiles' coordinates.
+// Cells are staged as 16-byte vectors (Q4 / QA), and the next listed tile's
+// phase-1 inputs are copied with cp.async while the current tile computes.
 #pragma once
 
 #include "k_common.cuh"
