@@ -21,8 +21,9 @@
 //   * the 132-cell potential ring around the tile is computed (active owner)
 //     or loaded from the persisted ring (inactive owner) two cells per thread
 //     by the first 66 threads;
-//   * each listed tile's coordinates are derived once per tile and handed to
-//     the neighbour-table, staging and flag code;
+//   * each listed tile's coordinates are packed into its list entry by the
+//     scan (no division in the tile loop) and handed to the neighbour-table,
+//     staging and flag code;
 //   * a block persists its ring potentials only when its own wake-up test is
 //     negative: a block whose test is positive is active next step (it wakes
 //     itself), so its ring from this step is never read as stale;
@@ -156,7 +157,7 @@ __global__ void __launch_bounds__(256 / R, 4)
     extern __shared__ __align__(128) float smem_f[];
     float* stage = smem_f;               // [2][3][SV]
     float* mu = smem_f + 2 * 3 * SV;     // [3][MV]
-    __shared__ int s_tile[TPP];
+    __shared__ int s_tile[TPP];          // listed tiles: tbx | tby << 16
     __shared__ unsigned s_tmeta[TPP];    // bits 0..15 active blocks, 16..31 their parity
     __shared__ int s_cnt;
     __shared__ uint8_t s_npar[2][RB * RB], s_nact[2][RB * RB];
@@ -239,9 +240,11 @@ __global__ void __launch_bounds__(256 / R, 4)
             const int kq = tid % NBT;
             const bool valid = tl < ntiles;
             const int tile = (int)tl;
-            int act = 0, pp = 0;
+            int act = 0, pp = 0, entry = 0;
             if (valid) {
-                const int b = ((tile % ntx) * TB + kq % TB) + g.nbx * ((tile / ntx) * TB + kq / TB);
+                const int tby = tile / ntx, tbx = tile - tby * ntx;
+                const int b = (tbx * TB + kq % TB) + g.nbx * (tby * TB + kq / TB);
+                entry = tbx | (tby << 16);
                 pp = f.par_cur[b];
                 act = DBA ? (f.wake_cur[b] ? 1 : 0) : 1;
                 f.wake_clr[b] = 0;
@@ -256,7 +259,7 @@ __global__ void __launch_bounds__(256 / R, 4)
             const unsigned abits = (ma >> g0) & gm, pbits = (mp >> g0) & gm;
             if (tid == 0) s_cnt = 0;
             __syncthreads();
-            list_append(valid && kq == 0 && abits != 0, tile, (int)(abits | (pbits << 16)), s_tile,
+            list_append(valid && kq == 0 && abits != 0, entry, (int)(abits | (pbits << 16)), s_tile,
                         reinterpret_cast<int*>(s_tmeta), &s_cnt);
             __syncthreads();
         }
@@ -265,16 +268,16 @@ __global__ void __launch_bounds__(256 / R, 4)
         // (neighbour table loaded during i)
         int tbx = 0, tby = 0, tbx_n = 0, tby_n = 0, tbx_nn = 0, tby_nn = 0;
         if (cnt > 0) {
-            tby = s_tile[0] / ntx;
-            tbx = s_tile[0] - tby * ntx;
+            tby = s_tile[0] >> 16;
+            tbx = s_tile[0] & 0xffff;
             nbr_load(tbx, tby);
             nbr_store(0);
             if (tid < NBT) s_nx[0][tid] = 0;
             __syncthreads();
             issue(tbx, tby, 0);
             if (cnt > 1) {
-                tby_n = s_tile[1] / ntx;
-                tbx_n = s_tile[1] - tby_n * ntx;
+                tby_n = s_tile[1] >> 16;
+                tbx_n = s_tile[1] & 0xffff;
                 nbr_load(tbx_n, tby_n);
             }
         }
@@ -289,8 +292,8 @@ __global__ void __launch_bounds__(256 / R, 4)
             if (tid < NBT) s_nx[st ^ 1][tid] = 0;
             if (i + 1 < cnt) issue(tbx_n, tby_n, st ^ 1);
             if (i + 2 < cnt) {
-                tby_nn = s_tile[i + 2] / ntx;
-                tbx_nn = s_tile[i + 2] - tby_nn * ntx;
+                tby_nn = s_tile[i + 2] >> 16;
+                tbx_nn = s_tile[i + 2] & 0xffff;
                 nbr_load(tbx_nn, tby_nn);
             }
             const unsigned tm = s_tmeta[i];
