@@ -66,9 +66,13 @@ def _done(tip, edge, target):
 
 class SweepServer:
     def __init__(self, precision=1, block=8, max_slots=128, block_capacity=1 << 17, cell_capacity=0, chunk=96,
-                 target=0.8, max_steps=200000, threads=256):
-        self.batch = engine.Batch(precision=precision, block=block, max_slots=max_slots,
-                                  block_capacity=block_capacity, cell_capacity=cell_capacity, threads=threads)
+                 target=0.8, max_steps=200000, threads=256, batch=None):
+        """`batch`: an object with the engine.Batch methods add / remove / step / tips /
+        field / sync / close to serve from (default: a new engine.Batch on the current device)."""
+        if batch is None:
+            batch = engine.Batch(precision=precision, block=block, max_slots=max_slots,
+                                 block_capacity=block_capacity, cell_capacity=cell_capacity, threads=threads)
+        self.batch = batch
         self.precision, self.block, self.chunk = precision, block, chunk
         self.target, self.max_steps = target, max_steps
 
