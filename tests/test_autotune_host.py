@@ -1,0 +1,41 @@
+"""Host logic of the batch autotuner (dba_b200/autotune.py) on the CPU: the
+fastest (block edge, threads) pair is chosen, the chunk keeps the mean overshoot
+past a stop within 5 % of the shortest sweep run, and the choice is cached per
+device and precision.  The timing of each candidate is replaced by known scores."""
+import json
+
+from dba_b200 import autotune
+
+
+def test_tune_picks_fastest_and_caches(tmp_path, monkeypatch):
+    cache = tmp_path / "autotune.json"
+    monkeypatch.setenv("DBA_AUTOTUNE_CACHE", str(cache))
+    scores = {(8, 128): 1.0, (8, 256): 3.0, (8, 512): 2.0, (16, 128): 0.5, (16, 256): 2.5, (16, 512): 2.9}
+    calls = []
+
+    def fake_time(block, threads=256, precision=1, **kw):
+        calls.append((block, threads, precision))
+        return scores[(block, threads)]
+
+    monkeypatch.setattr(autotune, "time_candidate", fake_time)
+    c = autotune.tune(precision=1, use_cache=True)
+    assert (c["block"], c["threads"]) == (8, 256)
+    assert c["chunk"] == 96 and c["chunk"] / 2 <= 0.05 * autotune.SHORTEST_RUN_STEPS
+    assert len(calls) == len(scores)
+    stored = json.load(open(cache))
+    assert list(stored.values())[0]["block"] == 8
+    # cached: no new timing runs
+    c2 = autotune.tune(precision=1, use_cache=True)
+    assert len(calls) == len(scores) and (c2["block"], c2["threads"]) == (8, 256)
+    # other precision: a separate entry
+    autotune.tune(precision=0, use_cache=True)
+    assert len(calls) == 2 * len(scores) and len(json.load(open(cache))) == 2
+
+
+def test_tune_without_cache_leaves_no_file(tmp_path, monkeypatch):
+    cache = tmp_path / "none.json"
+    monkeypatch.setenv("DBA_AUTOTUNE_CACHE", str(cache))
+    monkeypatch.setattr(autotune, "time_candidate", lambda block, threads=256, precision=1, **kw: block * threads)
+    c = autotune.tune(precision=1, use_cache=False)
+    assert (c["block"], c["threads"]) == (16, 512)
+    assert not cache.exists()
