@@ -4,6 +4,7 @@ import math
 import random
 
 import mpmath as mp
+import numpy as np
 import pytest
 
 from oracle_lib import lib
@@ -50,3 +51,21 @@ def test_special_values():
     assert L.oracle_fm(2, math.inf) == pytest.approx(math.pi / 2, rel=0, abs=1e-16)
     assert L.oracle_fm(2, -math.inf) == pytest.approx(-math.pi / 2, rel=0, abs=1e-16)
     assert L.oracle_fm(2, 1.0) == pytest.approx(math.pi / 4, rel=2e-16)
+
+
+def test_halving_by_multiplication_rounds_like_division():
+    """The FP64 KH formulas write the reference's divisions by 2 as multiplications by
+    0.5: both are correctly rounded results of the same real number, so every double
+    (subnormals, extremes, infinities, signed zeros) gives the same bits either way."""
+    rng = np.random.default_rng(11)
+    bits = rng.integers(0, 2**64, size=1 << 20, dtype=np.uint64)
+    x = bits.view(np.float64)
+    x = x[np.isfinite(x)]
+    edge = np.array([0.0, -0.0, 5e-324, -5e-324, 2.2250738585072014e-308, 4.450147717014403e-308,
+                     1.7976931348623157e308, -1.7976931348623157e308, np.inf, -np.inf, 1.0, 3.0, 1e-300])
+    for v in (x, edge, x * 0.37, x * 1e-300):
+        with np.errstate(all="ignore"):
+            a, b = v / 2.0, v * 0.5
+        assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    nan = np.array([np.nan])
+    assert np.isnan(nan / 2.0) and np.isnan(nan * 0.5)
