@@ -29,12 +29,13 @@ def _cache_path():
 
 
 def _device_key(precision):
-    try:
-        import torch
-        name = torch.cuda.get_device_name(0)
-    except Exception:
-        name = "cuda"
-    return f"{name}|prec{precision}"
+    """Cache key of the current CUDA device: its name, compute capability and SM
+    count (so different GPUs on one host, or a non-zero current device, each get
+    their own entry), and the precision."""
+    import torch
+    dev = torch.cuda.current_device()
+    p = torch.cuda.get_device_properties(dev)
+    return f"{p.name}|sm{p.major}{p.minor}|{p.multi_processor_count}sms|prec{precision}"
 
 
 def time_candidate(block, threads=256, precision=1, nslots=24, steps=480, seed=5):

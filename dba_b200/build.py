@@ -28,7 +28,7 @@ UNITS = [
     ("batch.cu", ["-fmad=false"]),
 ]
 HEADERS = ["fpmath.h", "fpmath_coeffs.h", "k_common.cuh", "k_dendrite.cuh", "k_modelb.cuh", "k_kh.cuh",
-           "k_reduce.cuh", "k_inst.cuh", "launch.h", "k_modelb_fast.cuh", "k_modelb_tile.cuh", "k_kh_tile.cuh", "k_dendrite_tile.cuh", "k_batch.cuh", "k_post.cuh", "k_pair.cuh"]
+           "k_reduce.cuh", "k_inst.cuh", "launch.h", "k_modelb_fast.cuh", "k_modelb_tile.cuh", "k_modelb_strip.cuh", "k_kh_tile.cuh", "k_dendrite_tile.cuh", "k_batch.cuh", "k_post.cuh", "k_pair.cuh"]
 
 
 def _newer(target, deps):
@@ -68,7 +68,7 @@ def build(verbose=False, jobs=4):
     if bad:
         raise RuntimeError("compilation failed")
     if _newer(LIB, objs):
-        _run([NVCC] + GENCODE + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"], verbose)
+        _run([NVCC] + GENCODE + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcurand", "-lpthread"], verbose)
     run_src = os.path.join(CSRC, "dba_run.cpp")
     if os.path.exists(run_src) and _newer(BIN, [run_src, LIB]):
         _run([CXX, "-O2", "-std=c++17", run_src, "-o", BIN, "-L" + HERE, "-ldba_b200",

@@ -2,6 +2,7 @@
 // the per-step launch sequence (captured into CUDA graphs), readback,
 // observables and checkpoints.
 #include <cuda_runtime.h>
+#include <curand.h>
 
 #include <algorithm>
 #include <cmath>
@@ -21,7 +22,9 @@ using namespace dba;
 
 namespace {
 
-constexpr int kGraphSteps = 48;   // steps per captured graph (multiple of 6)
+// steps per captured graph, longest first; each a multiple of 6, the period of the
+// flag, parity and rotating-total indices, so one graph per start phase serves every run
+constexpr int kGraphSteps[2] = {48, 6};
 
 struct Alloc {
     void* p = nullptr;
@@ -58,14 +61,14 @@ struct dba_ctx {
     bool initialized = false;
     // FP32 2-D Model B conserved: lazy correction state (k_modelb_fast.cuh)
     bool lazy = false;
-    bool tiles = false;               // FP32 2-D Model B on 32x32-cell tiles (k_modelb_tile.cuh)
+    int mb_kernel = MB_KERNEL_BLOCK;  // FP32 2-D Model B: strip (k_modelb_strip.cuh), 32x32 tile or one-block kernel
     bool kh_tiles = false;            // KH one-kernel step on 16x16-cell tiles (k_kh_tile.cuh)
     bool den_tiles = false;           // FP32 3-D dendrite on 32x8x8-cell tiles (k_dendrite_tile.cuh)
     float* kvmax = nullptr;           // KH tiles: per-block largest signal speed (CFL)
     unsigned* kgmax = nullptr;        // KH tiles: rotating maxima of the CFL speed, float bits [3]
     double* ktime = nullptr;          // KH tiles: simulated time accumulated on the device (CFL)
     long long* lz = nullptr;          // tot[2][3] then chg[3][3]: rotating fixed-point totals (LazyP)
-    cudaGraphExec_t graphs[6][2] = {};
+    cudaGraphExec_t graphs[2][6][2] = {};   // [length tier][start phase][mode]
     bool use_graphs = true;
     int last_error = DBA_OK;
 };
@@ -281,7 +284,7 @@ cudaError_t enqueue_step_t(dba_ctx* c, long s, bool dba_mode)
     case DBA_MODEL_MODELB: {
         MBP<R> P = mb_params<R>(c, dba_mode);
         LazyP L = lazy_params(c, s, P.conserved != 0);
-        e = launch_modelb<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
+        e = launch_modelb<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->mb_kernel);
         if (e != cudaSuccess || !P.conserved || c->lazy) return e;
         break;
     }
@@ -327,6 +330,8 @@ int validate(const dba_config* k)
     if (k->cfl < 0 || (k->cfl > 0 && !(k->model == DBA_MODEL_KH && k->tiles && kh_tiles_ok(k->nz == 1 ? 2 : 3, B, k->nx, k->ny))))
         return DBA_ERR_CONFIG;   // the CFL step lives in the KH tile kernel
     if (k->precision != DBA_PREC_F64 && k->precision != DBA_PREC_F32) return DBA_ERR_CONFIG;
+    if (k->ic < DBA_IC_REFERENCE || k->ic > DBA_IC_CURAND || (k->ic == DBA_IC_CURAND && k->model != DBA_MODEL_MODELB))
+        return DBA_ERR_CONFIG;
     if (k->dt <= 0 || k->dx <= 0) return DBA_ERR_CONFIG;
     size_t nb = (size_t)(k->nx / B) * (k->ny / B) * (k->nz == 1 ? 1 : k->nz / B);
     if (nb > (size_t)1024 * 1024) return DBA_ERR_CONFIG;
@@ -360,12 +365,51 @@ void ic_dendrite(const dba_config& k, std::vector<double>& out)
             }
 }
 
-void ic_modelb(const dba_config& k, std::vector<double>& out)
+// The reference GPU program's draw (example_Reactive_ModelB/kernel.cu:1032-1042):
+// the cuRAND host API's default pseudo-random generator (XORWOW) seeded with
+// `seed`, three curandGenerateUniformDouble passes of n values (x, then y, then z)
+// into device memory; read back for Initialize, which runs on the host here.
+int curand_uniform_passes(const dba_config& k, std::vector<double>& u)
 {
+    const size_t n = (size_t)k.nx * k.ny * k.nz;
+    u.assign(3 * n, 0.0);
+    double* d = nullptr;
+    if (cudaMalloc(&d, 3 * n * sizeof(double)) != cudaSuccess) return DBA_ERR_NOMEM;
+    curandGenerator_t gen = nullptr;
+    int st = DBA_OK;
+    if (curandCreateGenerator(&gen, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS ||
+        curandSetPseudoRandomGeneratorSeed(gen, k.seed) != CURAND_STATUS_SUCCESS)
+        st = DBA_ERR_CUDA;
+    for (int q = 0; q < 3 && !st; ++q)
+        if (curandGenerateUniformDouble(gen, d + q * n, n) != CURAND_STATUS_SUCCESS) st = DBA_ERR_CUDA;
+    if (!st && cudaMemcpy(u.data(), d, 3 * n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = DBA_ERR_CUDA;
+    if (gen) curandDestroyGenerator(gen);
+    cudaFree(d);
+    return st;
+}
+
+int ic_modelb(const dba_config& k, std::vector<double>& out)
+{
+    size_t n = (size_t)k.nx * k.ny * k.nz;
+    if (k.ic == DBA_IC_CURAND) {
+        // Initialize (example_Reactive_ModelB/kernel.cu:209-211) on the three passes, in FP64
+        // with the product and the sum rounded separately (the host code is built without
+        // contraction), as the kernel computes them when built without FMA contraction
+        std::vector<double> u;
+        int st = curand_uniform_passes(k, u);
+        if (st) return st;
+        out.assign(3 * n, 0.0);
+        for (size_t i = 0; i < n; ++i) {
+            out[i] = k.x0 + k.noise_amp * (u[i] - 0.5);
+            out[n + i] = k.y0 + k.noise_amp * (u[n + i] - 0.5);
+            out[2 * n + i] = k.z0 + k.noise_amp_z * (u[2 * n + i] - 0.5);
+        }
+        return DBA_OK;
+    }
     // mt19937_64 draws x, y, z interleaved per cell as the reference CPU program
     // (example_Reactive_ModelB/CPU_version/base_CPU.cpp:540-549), then
     // Initialize (example_Reactive_ModelB/kernel.cu:209-211)
-    size_t n = (size_t)k.nx * k.ny * k.nz;
     out.assign(3 * n, 0.0);
     std::mt19937_64 rng(k.seed);
     std::uniform_real_distribution<double> u(0.0, 1.0);
@@ -375,6 +419,7 @@ void ic_modelb(const dba_config& k, std::vector<double>& out)
         out[n + i] = k.y0 + k.noise_amp * (uy - 0.5);
         out[2 * n + i] = k.z0 + k.noise_amp_z * (uz - 0.5);
     }
+    return DBA_OK;
 }
 
 void ic_kh(const dba_config& k, std::vector<double>& out)
@@ -615,8 +660,12 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
         const int nt = (cfg->nx / 16) * (cfg->ny / 16);
         c->grid = c->esz == 8 ? kh_tile_grid<double>(c->B, c->sms, nt) : kh_tile_grid<float>(c->B, c->sms, nt);
     }
-    if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->tiles && modelb_tiles_ok(c->D, c->B, cfg->nx, cfg->ny)) {
-        c->tiles = true;
+    if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->tiles == 1 &&
+        modelb_strip_ok(c->D, c->B, cfg->nx, cfg->ny, kMBStripRows)) {
+        c->mb_kernel = MB_KERNEL_STRIP;
+        c->grid = modelb_strip_grid(c->B, c->sms, (cfg->nx / 64) * (cfg->ny / kMBStripRows));
+    } else if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->tiles && modelb_tiles_ok(c->D, c->B, cfg->nx, cfg->ny)) {
+        c->mb_kernel = MB_KERNEL_TILE;
         c->grid = modelb_tile_grid(c->B, c->sms, (cfg->nx / 32) * (cfg->ny / 32));
     }
     if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->conserved && modelb_uses_fast<float>(c->D, c->B)) {
@@ -641,9 +690,10 @@ void dba_destroy(dba_ctx* c)
     if (!c) return;
     dba_wait_io(c);   // background VTR writers hold only snapshots, but report into this context's status
     if (c->st) cudaStreamSynchronize(c->st);
-    for (auto& row : c->graphs)
-        for (auto& gexec : row)
-            if (gexec) cudaGraphExecDestroy(gexec);
+    for (auto& tier : c->graphs)
+        for (auto& row : tier)
+            for (auto& gexec : row)
+                if (gexec) cudaGraphExecDestroy(gexec);
     for (auto& a : c->allocs) cudaFree(a.p);
     if (c->host_staging) cudaFreeHost(c->host_staging);
     if (c->st) cudaStreamDestroy(c->st);
@@ -658,7 +708,10 @@ int dba_init(dba_ctx* c, const double* ic)
     const double* src = ic;
     if (!src) {
         if (k.model == DBA_MODEL_DENDRITE) ic_dendrite(k, buf);
-        else if (k.model == DBA_MODEL_MODELB) ic_modelb(k, buf);
+        else if (k.model == DBA_MODEL_MODELB) {
+            const int st = ic_modelb(k, buf);
+            if (st) return st;
+        }
         else ic_kh(k, buf);
         src = buf.data();
     }
@@ -719,13 +772,15 @@ int dba_step(dba_ctx* c, int nsteps, int mode)
     const bool dba_mode = mode == DBA_MODE_DBA;
     while (nsteps > 0) {
         const int r = (int)((c->step + 1) % 6);
-        if (c->use_graphs && nsteps >= kGraphSteps) {
-            cudaGraphExec_t& ge = c->graphs[r][mode];
+        const int tier = nsteps >= kGraphSteps[0] ? 0 : (nsteps >= kGraphSteps[1] ? 1 : -1);
+        if (c->use_graphs && tier >= 0) {
+            const int len = kGraphSteps[tier];
+            cudaGraphExec_t& ge = c->graphs[tier][r][mode];
             if (!ge) {
                 cudaGraph_t graph;
                 DBA_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
                 cudaError_t e = cudaSuccess;
-                for (int q = 0; q < kGraphSteps && e == cudaSuccess; ++q) e = enqueue_step(c, c->step + 1 + q, dba_mode);
+                for (int q = 0; q < len && e == cudaSuccess; ++q) e = enqueue_step(c, c->step + 1 + q, dba_mode);
                 cudaError_t e2 = cudaStreamEndCapture(c->st, &graph);
                 if (e != cudaSuccess) return cuda_status(e);
                 if (e2 != cudaSuccess) return cuda_status(e2);
@@ -734,9 +789,9 @@ int dba_step(dba_ctx* c, int nsteps, int mode)
                 if (e != cudaSuccess) return cuda_status(e);
             }
             DBA_TRY(cudaGraphLaunch(ge, c->st));
-            c->step += kGraphSteps;
-            nsteps -= kGraphSteps;
-            c->time += kGraphSteps * host_dt(c);
+            c->step += len;
+            nsteps -= len;
+            c->time += len * host_dt(c);
         } else {
             DBA_TRY(enqueue_step(c, c->step + 1, dba_mode));
             c->step += 1;
@@ -988,7 +1043,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 else if (c->cfg.model == DBA_MODEL_MODELB) {
                     MBP<double> P = mb_params<double>(c, dba_mode);
                     LazyP L = lazy_params(c, s, P.conserved != 0);
-                    r = launch_modelb<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
+                    r = launch_modelb<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->mb_kernel);
                 }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
@@ -1002,7 +1057,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 else if (c->cfg.model == DBA_MODEL_MODELB) {
                     MBP<float> P = mb_params<float>(c, dba_mode);
                     LazyP L = lazy_params(c, s, P.conserved != 0);
-                    r = launch_modelb<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
+                    r = launch_modelb<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->mb_kernel);
                 }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);

@@ -26,7 +26,12 @@ void apply_option(dba_config* c, const std::string& key, const std::string& val)
     else if (key == "precision") c->precision = (val == "fp32" || val == "f32" || val == "1") ? DBA_PREC_F32 : DBA_PREC_F64;
     else if (key == "bc") c->bc = (val == "zeroflux" || val == "1") ? DBA_BC_ZEROFLUX : DBA_BC_PERIODIC;
     else if (key == "conserved") c->conserved = i();
-    else if (key == "ic") c->ic = (val == "tanh") ? DBA_IC_TANH_SEED : (val == "sharp" ? DBA_IC_SHARP_BANDS : (val == "reference" ? DBA_IC_REFERENCE : i()));
+    else if (key == "ic")
+        c->ic = val == "tanh"        ? DBA_IC_TANH_SEED
+                : val == "sharp"     ? DBA_IC_SHARP_BANDS
+                : val == "curand"    ? DBA_IC_CURAND
+                : val == "reference" ? DBA_IC_REFERENCE
+                                     : i();
     else if (key == "seed") c->seed = std::stoull(val);
     else if (key == "ic_radius") c->ic_radius = d();
     else if (key == "ic_width") c->ic_width = d();

@@ -63,13 +63,15 @@ static __global__ void post_minmax_kernel(const double* f, size_t n, unsigned lo
 }
 
 // root of x, halving the path on the way (only non-roots are rewritten, and
-// always to one of their ancestors, so concurrent unions stay correct)
+// always to one of their ancestors, so concurrent unions stay correct).  Labels
+// are read from L2 (ld.global.cg), never from a possibly stale L1 line: a retry
+// after a failed atomicCAS must see the link another thread just made.
 __device__ __forceinline__ long long uf_find(long long* lab, long long x)
 {
     for (;;) {
-        const long long p = lab[x];
+        const long long p = __ldcg(lab + x);
         if (p == x) return x;
-        const long long gp = lab[p];
+        const long long gp = __ldcg(lab + p);
         if (gp != p) lab[x] = gp;
         x = p;
     }

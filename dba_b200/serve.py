@@ -12,6 +12,10 @@ blocks of every admitted simulation, fields resident on the GPU) and loops:
   * read all tips with one small kernel; retire the finished simulations,
     freeing their memory for the next admissions.
 
+A request that does not fit even in an empty batch (more cells, blocks or slots
+than the batch was created with) is returned at once with completed=False and
+a `rejected` reason, so the requests behind it are still served.
+
 Requests that arrive while others are on the GPU join at the next chunk
 boundary, so their work overlaps on the device.  Latency is completion time
 minus arrival time.
@@ -90,7 +94,16 @@ class SweepServer:
                 req = waiting[0]
                 slot = self.batch.add(request_config(req, self.precision, self.block))
                 if slot is None:
-                    break                       # no room: wait for retirements
+                    if running:
+                        break                   # no room: wait for retirements
+                    # nothing is running, so nothing will free room: this request can
+                    # never be admitted (larger than the batch's arena, block space or
+                    # slot table); reject it and serve the ones behind it
+                    waiting.popleft()
+                    now = clock() - t0
+                    results.append(dict(req, t_done=now, latency=now - req["t_arrive"], tip=float("nan"), steps=0,
+                                        completed=False, rejected="does not fit in an empty batch"))
+                    continue
                 waiting.popleft()
                 running[slot] = dict(req, t_admit=clock() - t0)
             if not running:

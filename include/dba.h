@@ -53,6 +53,11 @@ extern "C" {
 #define DBA_IC_REFERENCE 0    /* the reference program's own initial condition */
 #define DBA_IC_TANH_SEED 1    /* dendrite: tanh-profile solid seed of radius ic_radius */
 #define DBA_IC_SHARP_BANDS 2  /* KH: sharp |y-0.5|<0.25 bands plus seeded white noise */
+#define DBA_IC_CURAND 3       /* Model B: the reference GPU program's draw (example_Reactive_ModelB/kernel.cu:
+                                 1032-1042): cuRAND's default generator (XORWOW) seeded with `seed`, three
+                                 uniform-double passes for x, y, z, then Initialize (:209-211) in FP64 with
+                                 separately rounded product and sum.  DBA_IC_REFERENCE for Model B is the
+                                 reference CPU program's mt19937_64 stream (CPU_version/base_CPU.cpp:540-549). */
 
 /* ---- configuration: the reference's Input.txt values plus engine options ---- */
 typedef struct dba_config {
@@ -82,10 +87,12 @@ typedef struct dba_config {
     double ic_radius, ic_width;/* dendrite tanh seed */
     int ic_corner;             /* dendrite tanh seed at cell (0,0,0) instead of the centre */
     double noise_amp, noise_amp_z; /* Model B: x,y and z uniform-noise amplitudes (0.05, 0.001) */
-    int tiles;                 /* 1 (default): tile kernels where the shape allows -- FP32 2-D Model B on 32x32
-                                  cells (nx, ny multiples of 32, block 8 or 16), KH on 16x16 cells (nx, ny
-                                  multiples of 16, block 8 or 16), FP32 3-D dendrite on 32x8x8 cells (block 8,
-                                  nx a multiple of 32); 0: the one-block kernels and the four-stage KH kernels */
+    int tiles;                 /* 1 (default): tile kernels where the shape allows -- FP32 2-D Model B on
+                                  64-column x 32-row strips marched by one warp each (block 16, nx a multiple
+                                  of 64, ny of 32), else on 32x32 cells (nx, ny multiples of 32, block 8 or 16),
+                                  KH on 16x16 cells (nx, ny multiples of 16, block 8 or 16), FP32 3-D dendrite
+                                  on 32x8x8 cells (block 8, nx a multiple of 32); 2: as 1 but FP32 2-D Model B
+                                  always on 32x32 cells; 0: the one-block kernels and the four-stage KH kernels */
     double cfl;                /* KH: > 0 picks each step's dt = cfl * min(dx, dy) / max(c + |v|) on the device
                                   (tile kernel only); 0 (default): the fixed dt */
 } dba_config;
@@ -273,22 +280,6 @@ int dba_batch_get_info(dba_batch* b, dba_batch_info* info);
 int dba_batch_get_stream(dba_batch* b, void** stream);
 void dba_batch_destroy(dba_batch* b);
 
-/* No counterpart in the reference.  For callers that cannot call cudaMalloc
- * -- work enqueued while a stream is captured into a CUDA graph, latency-critical
- * loops that must not take an allocation's implicit device synchronisation, or
- * hosts whose device memory belongs to another allocator: the conserved-DBA
- * mean change, computed with the same fixed-order reduction dba_step uses,
- * allocating nothing.  Its scratch is a fixed array inside the library
- * (32 KiB + 256 B on every GPU that loads it, held until exit).
- *   block_sums: device pointer, nfields x nb FP64 per-block sums of the change
- *   mean_out:   device pointer, nfields FP64 results: sum / ncells
- *   stream:     cudaStream_t to enqueue on (NULL = legacy default stream)
- * Limits: nb <= DBA_NOALLOC_MAX_BLOCKS, 1 <= nfields <= DBA_NOALLOC_MAX_FIELDS;
- * larger sizes return DBA_ERR_ARG.  The first call on a device looks up the
- * array's device address (make it before any stream capture).  All calls share
- * the array: calls that overlap on the GPU race.  Asynchronous on `stream`. */
-#define DBA_NOALLOC_MAX_BLOCKS (1 << 20)
-#define DBA_NOALLOC_MAX_FIELDS 4
 /* ---- VTK XML RectilinearGrid output (the reference's CUDA-MPI write_output_vtr /
    write_output_pvtr, example_Dendritic_growth/CUDA-MPI/dendrite_kernels.cu:875-1060) ----
    Writes <base>.vtr, or with pieces > 1 <base>_<r>.vtr for r < pieces (y slabs that
@@ -322,6 +313,24 @@ int dba_tip_profile(dba_ctx* ctx, int field, int dz, int* tip_x, int* tip_x_max)
 int dba_size_distribution(dba_ctx* ctx, int field, double* avg, long* volume, long* islands, long* sizes,
                           long max_sizes);
 
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * -- work enqueued while a stream is captured into a CUDA graph, latency-critical
+ * loops that must not take an allocation's implicit device synchronisation, or
+ * hosts whose device memory belongs to another allocator: the conserved-DBA
+ * mean change, computed with the same fixed-order reduction dba_step uses,
+ * allocating nothing.  Its scratch is a fixed array inside the library
+ * (32 KiB + 256 B on every GPU that loads it, held until exit).
+ *   block_sums: device pointer, nfields x nb FP64 per-block sums of the change
+ *   mean_out:   device pointer, nfields FP64 results: sum / ncells
+ *   stream:     cudaStream_t to enqueue on (NULL = legacy default stream)
+ * Limits: nb <= DBA_NOALLOC_MAX_BLOCKS, 1 <= nfields <= DBA_NOALLOC_MAX_FIELDS;
+ * larger sizes return DBA_ERR_ARG.  The first call on a device looks up the
+ * array's device address (make it before any stream capture); that address is
+ * cached per device index for the life of the process, so it belongs to the
+ * device's primary context and does not survive cudaDeviceReset.  All calls share
+ * the array: calls that overlap on the GPU race.  Asynchronous on `stream`. */
+#define DBA_NOALLOC_MAX_BLOCKS (1 << 20)
+#define DBA_NOALLOC_MAX_FIELDS 4
 int dba_mean_change_noalloc(const double* block_sums, int nb, int nfields, double ncells, double* mean_out,
                             void* stream);
 

@@ -27,18 +27,55 @@
  * bit.  The conserved-DBA mass sums use the engine's fixed tree order
  * (dba_tree_sum below) instead of Thrust's unspecified order.
  *
- * Build: see oracle/Makefile (g++ -O2 -ffp-contract=off).
+ * Build: see oracle/Makefile (g++ -O2 -ffp-contract=off -pthread).
  */
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <random>
+#include <thread>
 #include <vector>
 
 #include "../dba_b200/csrc/fpmath.h"
 
 namespace {
+
+// ---------------------------------------------------------------------------
+// host threads for the large grids
+// ---------------------------------------------------------------------------
+
+// Runs f(i) for i in [0, n) on the host's hardware threads, in chunks handed out
+// dynamically, when the grid holds at least 2^18 cells (smaller grids run
+// serially).  Every loop this serves writes only the cells or per-block slots of
+// its own index, so results do not depend on the thread count or the schedule.
+// ORACLE_THREADS caps the thread count (1 = serial).
+template <class F> void par_for(int n, size_t cells, F f)
+{
+    static const int hw = [] {
+        int t = (int)std::thread::hardware_concurrency();
+        if (const char* e = std::getenv("ORACLE_THREADS")) t = std::atoi(e);
+        return std::max(1, std::min(t, 64));
+    }();
+    const int nt = std::min(hw, n);
+    if (nt <= 1 || cells < ((size_t)1 << 18)) {
+        for (int i = 0; i < n; ++i) f(i);
+        return;
+    }
+    const int chunk = std::max(1, n / (nt * 8));
+    std::atomic<int> next{0};
+    auto work = [&] {
+        for (int a; (a = next.fetch_add(chunk)) < n;)
+            for (int i = a, e = std::min(n, a + chunk); i < e; ++i) f(i);
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) th.emplace_back(work);
+    work();
+    for (auto& t : th) t.join();
+}
 
 // ---------------------------------------------------------------------------
 // deterministic sums (mirrors the engine's warp-shuffle trees)
@@ -400,11 +437,13 @@ struct ModelB {
         ch_x[i] = cx; ch_y[i] = cy; ch_z[i] = cz;
         b[i] = 1.0 - x_new[i] - y_new[i] - z_new[i];
     }
+    // every cell writes only its own outputs, so rows run in parallel (par_for)
     template <class F> void all_cells(F f)
     {
-        for (int Z = 0; Z < g.nz; ++Z)
-            for (int Y = 0; Y < g.ny; ++Y)
-                for (int X = 0; X < g.nx; ++X) f(X, Y, Z, g.idx(X, Y, Z));
+        par_for(g.nz * g.ny, g.n(), [&](int r) {
+            const int Z = r / g.ny, Y = r % g.ny;
+            for (int X = 0; X < g.nx; ++X) f(X, Y, Z, g.idx(X, Y, Z));
+        });
     }
     void step_regular()                                        // kernel.cu:1060-1090
     {
@@ -424,22 +463,24 @@ struct ModelB {
     void step_dba()
     {
         int nb = g.nb();
-        for (int bb = 0; bb < nb; ++bb)                        // Calc_mu_wakeup
+        par_for(nb, g.n(), [&](int bb) {                       // Calc_mu_wakeup
             if (wake[bb]) g.for_block(bb, [&](int X, int Y, int Z, size_t i) { calc_mu_cell(X, Y, Z, i); });
-        for (int bb = 0; bb < nb; ++bb) {                      // Update_wakeup
+        });
+        par_for(nb, g.n(), [&](int bb) {                       // Update_wakeup
             if (wake[bb])
                 g.for_block(bb, [&](int X, int Y, int Z, size_t i) { update_cell(X, Y, Z, i); });
             else if (conserved)
                 g.for_block(bb, [&](int, int, int, size_t i) { ch_x[i] = 0; ch_y[i] = 0; ch_z[i] = 0; });
-        }
+        });
         if (conserved) {                                       // Conserved/kernel.cu:1152-1176
             std::vector<double> sx(nb, 0.0), sy(nb, 0.0), sz(nb, 0.0);
-            for (int bb = 0; bb < nb; ++bb)
+            par_for(nb, g.n(), [&](int bb) {
                 if (wake[bb]) {
                     sx[bb] = block_sum(ch_x, bb);
                     sy[bb] = block_sum(ch_y, bb);
                     sz[bb] = block_sum(ch_z, bb);
                 }
+            });
             double N = (double)(g.nx * g.ny * g.nz);
             double ax = dba_tree_sum(sx) / N, ay = dba_tree_sum(sy) / N, az = dba_tree_sum(sz) / N;
             last_avg[0] = ax; last_avg[1] = ay; last_avg[2] = az;
@@ -451,9 +492,10 @@ struct ModelB {
             });
             x = x_new; y = y_new; z = z_new;                   // Swap_regular
         } else {
-            for (int bb = 0; bb < nb; ++bb)                    // Swap_wakeup :469-517
+            par_for(nb, g.n(), [&](int bb) {                   // Swap_wakeup :469-517
                 if (wake[bb])
                     g.for_block(bb, [&](int, int, int, size_t i) { x[i] = x_new[i]; y[i] = y_new[i]; z[i] = z_new[i]; });
+            });
         }
         for (int bb = 0; bb < nb; ++bb) {                      // Wakeup_Next :657-713
             int s = wake[bb];
@@ -618,8 +660,9 @@ struct KH {
     }
     template <class F> void all_cells(F f)
     {
-        for (int Y = 0; Y < g.ny; ++Y)
+        par_for(g.ny, g.n(), [&](int Y) {
             for (int X = 0; X < g.nx; ++X) f(X, Y, g.idx(X, Y, 0));
+        });
     }
     void step_regular()                                        // KH_DBA.cu:1389-1436
     {
@@ -639,25 +682,29 @@ struct KH {
     void step_dba()                                            // KH_DBA.cu:1437-1497
     {
         int nb = g.nb();
-        for (int bb = 0; bb < nb; ++bb)
+        par_for(nb, g.n(), [&](int bb) {
             if (wake[bb]) g.for_block(bb, [&](int, int, int, size_t i) { prim_cell(i); });
-        for (int bb = 0; bb < nb; ++bb)
+        });
+        par_for(nb, g.n(), [&](int bb) {
             if (wake[bb]) g.for_block(bb, [&](int X, int Y, int, size_t i) { extrap_cell(X, Y, i); });
-        for (int bb = 0; bb < nb; ++bb)
+        });
+        par_for(nb, g.n(), [&](int bb) {
             if (wake[bb]) g.for_block(bb, [&](int X, int Y, int, size_t i) { flux_cell(X, Y, i); });
-        for (int bb = 0; bb < nb; ++bb) {
+        });
+        par_for(nb, g.n(), [&](int bb) {
             if (wake[bb])
                 g.for_block(bb, [&](int X, int Y, int, size_t i) { apply_cell(X, Y, i); });
             else if (conserved)
                 g.for_block(bb, [&](int, int, int, size_t i) { chM[i] = 0; chE[i] = 0; chX[i] = 0; chY[i] = 0; });
-        }
+        });
         if (conserved) {                                       // Conserved/KH_DBA.cu:1553-1575
             std::vector<double> sM(nb, 0.0), sE(nb, 0.0), sX(nb, 0.0), sY(nb, 0.0);
-            for (int bb = 0; bb < nb; ++bb)
+            par_for(nb, g.n(), [&](int bb) {
                 if (wake[bb]) {
                     sM[bb] = block_sum(chM, bb); sE[bb] = block_sum(chE, bb);
                     sX[bb] = block_sum(chX, bb); sY[bb] = block_sum(chY, bb);
                 }
+            });
             double N = (double)(g.nx * g.ny);
             double aM = dba_tree_sum(sM) / N, aE = dba_tree_sum(sE) / N;
             double aX = dba_tree_sum(sX) / N, aY = dba_tree_sum(sY) / N;

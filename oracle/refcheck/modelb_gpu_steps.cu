@@ -7,7 +7,10 @@
 // :1152-1165, Swap_regular) -- and records every step's block flags plus
 // periodic FP64 field dumps.  The initial uniforms come from mt19937_64(1234)
 // interleaved per cell (the reference CPU program's stream, base_CPU.cpp:540-549)
-// instead of cuRAND so the checker can start from the same state.
+// instead of cuRAND so the checker can start from the same state; with a fifth
+// argument `curand` they come from the reference GPU program's own draw instead
+// (kernel.cu:1032-1042: cuRAND's default generator, seed 1234, three
+// curandGenerateUniformDouble passes for x, y, z).
 //
 // Launch shape: 4x4x1 CTAs (one warp) on an 8x8x1 grid; Nx, Ny multiples of
 // 32 keep every block index in bounds and one-warp CTAs rule out the
@@ -21,7 +24,7 @@
 int main(int argc, char** argv)
 {
     if (argc < 5) {
-        std::fprintf(stderr, "usage: %s <Input.txt> <nsteps> <dump_every> <out_prefix>\n", argv[0]);
+        std::fprintf(stderr, "usage: %s <Input.txt> <nsteps> <dump_every> <out_prefix> [curand]\n", argv[0]);
         return 2;
     }
     dimGrid3D = dim3(8, 8, 1);
@@ -38,12 +41,23 @@ int main(int argc, char** argv)
     std::string pre = argv[4];
     size_t n = (size_t)P.Nx * P.Ny * P.Nz;
     int nb = P.blockNum_x * P.blockNum_y * P.blockNum_z;
-    std::mt19937_64 rng(1234ULL);
-    std::uniform_real_distribution<double> u(0.0, 1.0);
-    for (size_t i = 0; i < n; ++i) {
-        V.x_old[i] = u(rng);
-        V.y_old[i] = u(rng);
-        V.z_old[i] = u(rng);
+    if (argc > 5 && std::string(argv[5]) == "curand") {
+        curandGenerator_t gen;
+        CURAND_CALL(curandCreateGenerator(&gen, CURAND_RNG_PSEUDO_DEFAULT));
+        CURAND_CALL(curandSetPseudoRandomGeneratorSeed(gen, 1234ULL));
+        CURAND_CALL(curandGenerateUniformDouble(gen, V.x_old, n));
+        CURAND_CALL(curandGenerateUniformDouble(gen, V.y_old, n));
+        CURAND_CALL(curandGenerateUniformDouble(gen, V.z_old, n));
+        CURAND_CALL(curandDestroyGenerator(gen));
+        CUDACHECK(cudaDeviceSynchronize());
+    } else {
+        std::mt19937_64 rng(1234ULL);
+        std::uniform_real_distribution<double> u(0.0, 1.0);
+        for (size_t i = 0; i < n; ++i) {
+            V.x_old[i] = u(rng);
+            V.y_old[i] = u(rng);
+            V.z_old[i] = u(rng);
+        }
     }
     Initialize<<<dimGrid3D, dimBlock3D>>>(V.x_old, V.y_old, V.z_old, V.b, V.phi_old, V.wake_up, V.wake_up_next, P);
     CUDACHECK(cudaDeviceSynchronize());

@@ -7,7 +7,8 @@ step, every block-flag array, plus FP64 field snapshots.  Harness launch shape
 (one-warp 4x4x1 CTAs, grid sizes that keep every block index in bounds) is
 described in oracle/refcheck/*.cu.
 
-Usage (on a B200):  python tests/golden/make_gpu_golden.py <out_dir>
+Usage (on a B200):  python tests/golden/make_gpu_golden.py <out_dir> [curand]
+(`curand`: only the cuRAND initial-condition fixture, ref_gpu_modelb_curand.npz)
 """
 import os
 import subprocess
@@ -26,18 +27,35 @@ MB_INPUT = ("{nx} {ny} 1\n{steps} {steps} {dt}\n1 1 1\n0 0 0 0 0 4\n1 1 2\n1 1 2
 KH_INPUT = "{nx} {ny} 1\n{steps} {steps} {dt}\n{dx} {dx} {dx}\n1\n{eps}\n"
 
 
-def run(binary, text, steps, every, nflag, nb, nf, n, d, ic_fields=None):
+def run(binary, text, steps, every, nflag, nb, nf, n, d, ic_fields=None, extra=()):
     open(f"{d}/Input.txt", "w").write(text)
-    subprocess.check_call([f"{REF}/{binary}", f"{d}/Input.txt", str(steps), str(every), f"{d}/o"],
+    subprocess.check_call([f"{REF}/{binary}", f"{d}/Input.txt", str(steps), str(every), f"{d}/o", *extra],
                           stdout=subprocess.DEVNULL)
     flags = np.fromfile(f"{d}/o_flags.bin", dtype=np.int32).reshape(steps, nflag, nb).astype(np.uint8)
     raw = np.fromfile(f"{d}/o_fields.bin", dtype=np.float64)
     return flags, raw
 
 
-def main(out):
+def curand_fixture(out, d, nx=64, ny=64):
+    """ref_gpu_modelb_curand.npz: the reference GPU program's own initial condition
+    (cuRAND XORWOW, seed 1234, three uniform passes, Initialize) and 60 DBA steps
+    from it, plain Model B, Metric_eps 1e-3."""
+    n, nb = nx * ny, (nx // 4) * (ny // 4)
+    steps, every = 60, 30
+    flags, raw = run("modelb_gpu_steps", MB_INPUT.format(nx=nx, ny=ny, steps=steps, dt=0.001, eps=1e-3), steps, every,
+                     2, nb, 3, n, d, extra=("curand",))
+    fields = raw.reshape(-1, 3, ny, nx)
+    np.savez_compressed(f"{out}/ref_gpu_modelb_curand.npz", nx=nx, ny=ny, steps=steps, every=every, mode=1,
+                        dt=0.001, metric_eps=1e-3, flags=flags, fields=fields)
+
+
+def main(out, only=None):
     os.makedirs(out, exist_ok=True)
     d = tempfile.mkdtemp()
+    if only == "curand":
+        curand_fixture(out, d)
+        print("wrote ref_gpu_modelb_curand.npz")
+        return
     nx = ny = 64
     n, nb = nx * ny, (nx // 4) * (ny // 4)
     # dendrite: 200 DBA steps, snapshots every 100
@@ -63,8 +81,10 @@ def main(out):
         fields = np.concatenate([np.zeros((1, 4, ny, nx)), dumps])
         np.savez_compressed(f"{out}/{name}", nx=nx, ny=ny, steps=steps, every=every, mode=1, dt=0.0002, dx=0.002,
                             metric_eps=10.0, flags=flags, fields=fields, ic=ic)
+    curand_fixture(out, d)
     print("wrote", sorted(os.listdir(out)))
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else HERE)
+    # python tests/golden/make_gpu_golden.py [out_dir] [curand]
+    main(sys.argv[1] if len(sys.argv) > 1 else HERE, sys.argv[2] if len(sys.argv) > 2 else None)

@@ -126,3 +126,22 @@ def test_sweep_requests_are_seeded_and_in_range():
     c = serve.request_config(a[0])
     assert c.Delta == pytest.approx(0.6 + a[0]["u"]) and c.delta == pytest.approx(4 * a[0]["eps4"])
     assert (c.nx, c.ny, c.nz, c.bc, c.ic) == (a[0]["edge"], a[0]["edge"], 1, 1, 1)
+
+
+def test_request_larger_than_the_batch_is_rejected_not_waited_on():
+    # the 512^2 request needs more cells than the whole arena holds: once nothing is
+    # running it is returned as rejected, and the requests behind it are still served
+    fb = FakeBatch(cell_capacity=2 * 128 * 128)
+    srv = serve.SweepServer(chunk=10, target=0.8, batch=fb)
+    res = {r["id"]: r for r in srv.run(reqs([128, 512, 128]), clock=fake_clock())}
+    assert len(res) == 3
+    assert not res[1]["completed"] and res[1]["steps"] == 0 and "rejected" in res[1]
+    assert res[0]["completed"] and res[2]["completed"]
+    assert [e for e, _ in fb.admitted] == [128, 128]
+
+
+def test_batch_without_slots_rejects_every_request():
+    fb = FakeBatch(cell_capacity=1 << 20, max_slots=0)
+    srv = serve.SweepServer(chunk=10, target=0.8, batch=fb)
+    res = srv.run(reqs([128, 256]), clock=fake_clock())
+    assert len(res) == 2 and not any(r["completed"] for r in res) and all("rejected" in r for r in res)
