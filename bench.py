@@ -14,15 +14,20 @@ Multi-GPU: the path does not shard in this build (one domain per GPU), so
 `--gpus N` runs N independent replicas, one process per GPU, and `value` is the
 sum of their active cell-updates divided by the slowest rank's time.
 
-At N=1 the line also carries `full_runs_dba_vs_regular`: the dendrite workloads
-(512^2 FP64, 10 000 steps; 512^3 FP32, 20 000 steps) run to their end time in
-DBA and in regular mode, with total wall times (`--no-full-runs` skips it), and
-`sweep`: the batched/served 2-D dendrite
-parameter sweep (256 seeded requests, Poisson arrivals, admission by device
-memory, autotuned block edge and threads) against the same requests run one at
-a time -- runs/s of both and p50/p99 time to completion (`--no-sweep` skips it).
-`--full-runs-kh 1,20` adds the KH flow (4096^2, 62 880 steps: simulated time 2)
-with those wake-up thresholds to the whole runs.
+At N=1 the line also carries:
+  * `workloads`: the other workloads measured the same way (value, roofline,
+    vs_dense, e2e, cpu_baseline) -- the 512^2 FP64 dendrite, the 512^3 FP32
+    dendrite and the 4096^2 FP32 KH flow, each pre-rolled to mid-run
+    (`--no-side-workloads` skips them);
+  * `full_runs_dba_vs_regular`: whole runs to the same end time in DBA and in
+    regular mode with total wall times -- the dendrite workloads (512^2 FP64,
+    10 000 steps; 512^3 FP32, 20 000 steps), the Model B workload (50 000 steps)
+    and the KH flow to simulated time 2 (62 880 steps) at the wake-up thresholds
+    of `--full-runs-kh` (default 1, the workload's) (`--no-full-runs` skips them);
+  * `sweep`: the batched/served 2-D dendrite parameter sweep (256 seeded
+    requests, Poisson arrivals, admission by device memory, autotuned block edge
+    and threads) against the same requests run one at a time -- runs/s of both
+    and p50/p99 time to completion (`--no-sweep` skips it).
 For FP32 workloads, `fp32_error_vs_fp64` gives the relative L2 error and the
 largest difference of each state field after `--error-steps` steps (default
 1000) on the full grid, against the FP64 engine from the same initial state.
@@ -174,40 +179,36 @@ def dist_setup():
     return world, rank, local
 
 
-def run_ours(args, w):
-    import datetime
-
+def measure(args, name, w, steps, warmup, preroll, world=1, rank=0, local=0, cpu_seconds=None):
+    """One workload: `preroll` untimed steps, `warmup` more, then `steps` timed steps on the
+    engine's stream (CUDA events; the max over ranks when world > 1), the dominant kernel's
+    roofline, the same state in regular (dense) mode, and the end-to-end leg through the
+    public API with host buffers.  Returns the JSON fields of the workload (rank 0)."""
     import numpy as np
     import torch
-    import torch.distributed as dist
 
     import dba_b200
 
-    world, rank, local = dist_setup()
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     cfg = make_config(w)
     sim = dba_b200.Simulation(cfg).init()
     stream = torch.cuda.ExternalStream(sim.stream)
-    # pre-roll to mid-run (untimed), then warm-up
-    preroll = w["t_total"] // 2 if args.preroll < 0 else args.preroll
     if preroll:
         sim.step(preroll, w["mode"])
-    sim.step(args.warmup, w["mode"])
+    sim.step(warmup, w["mode"])
     sim.sync()
     # host copy of this state: the end-to-end run below starts from it
     blob = torch.empty(sim.state_size(), dtype=torch.uint8, pin_memory=True)
     sim.save_state(blob)
-    prof0 = sim.step_profiled(1, w["mode"])   # also a final warm-up of the direct-launch path
+    sim.step_profiled(1, w["mode"])           # also a final warm-up of the direct-launch path
     sim.load_state(blob)
-    # runs of 48 steps or more go through a CUDA graph per start phase (step mod 6) and mode,
-    # captured on first use: capture the one the timed steps use now, outside the timed region
-    sim.step(min(args.steps, 48), w["mode"])
+    # runs of 6 steps or more go through CUDA graphs (48- and 6-step, per start phase and mode),
+    # captured on first use: capture the ones the timed steps use now, outside the timed region
+    sim.step(steps, w["mode"])
     sim.load_state(blob)
     sim.sync()
 
     if world > 1:
+        import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
     st0 = sim.cell_updates()
@@ -215,7 +216,7 @@ def run_ours(args, w):
     ev1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         ev0.record(stream)
-        sim.step(args.steps, w["mode"])
+        sim.step(steps, w["mode"])
         ev1.record(stream)
         torch.cuda.synchronize()
     status = sim._L.dba_sync(sim._h)
@@ -225,7 +226,7 @@ def run_ours(args, w):
 
     # dominant kernel: the fused stencil kernel, timed per launch with CUDA events on the same stream
     sim.load_state(blob)
-    nprof = min(args.steps, 200)
+    nprof = min(steps, 200)
     prof = sim.step_profiled(nprof, w["mode"])
     esz = 8 if w["precision"] == 0 else 4
     per_cell = ALG_BYTES[w["model"]] * esz
@@ -237,16 +238,15 @@ def run_ours(args, w):
     # average launch duration of the dominant kernel: when a step is that one kernel, the timed
     # region itself (K launches between two events); otherwise its per-launch events
     if launches_per_step(w) == 1:
-        kernel_ms = ms / max(1, args.steps)
-        # bytes of the timed launches themselves (dendrite: per-channel activity of the profiled steps)
-        alg_per_launch = cells * per_cell / max(1, args.steps) if w["model"] != "dendrite" else alg / nprof
+        kernel_ms = ms / max(1, steps)
+        alg_per_launch = cells * per_cell / max(1, steps) if w["model"] != "dendrite" else alg / nprof
     else:
         kernel_ms = prof["stencil_ms"] / nprof
         alg_per_launch = alg / nprof
     achieved = alg_per_launch / (kernel_ms * 1e-3) / 1e9 if kernel_ms > 0 else 0.0
     peak, peak_kind = hbm_peak()
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", f"{args.workload}.traffic.json")
+    tfile = os.path.join(ROOT, "profiles", f"{name}.traffic.json")
     if os.path.exists(tfile) and prof["active_blocks"]:
         try:
             tj = json.load(open(tfile))
@@ -258,7 +258,7 @@ def run_ours(args, w):
     # through the captured-graph path and timed with CUDA events, for the DBA-vs-dense comparison
     def graph_ms(mode):
         sim.load_state(blob)
-        sim.step(3, mode)
+        sim.step(ncmp, mode)
         sim.load_state(blob)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -269,7 +269,7 @@ def run_ours(args, w):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / ncmp, (sim.cell_updates() - c0) / ncmp
 
-    ncmp = min(args.steps, 1000)
+    ncmp = min(max(steps, 48), 1000)
     dense_ms, dense_cells = graph_ms(0)
     dba_ms, _ = graph_ms(w["mode"])
 
@@ -283,7 +283,7 @@ def run_ours(args, w):
     t0 = time.perf_counter()
     sim.load_state(blob)
     st_e0 = sim.cell_updates()
-    sim.step(args.steps, w["mode"])
+    sim.step(steps, w["mode"])
     for q in range(nf):
         sim.field(q, out=out_host[q])
     t_e2e = (time.perf_counter() - t0) * 1e3
@@ -292,23 +292,22 @@ def run_ours(args, w):
     d2h = out_host.nbytes
     t_e2e, cells_e2e = aggregate(t_e2e, cells_e2e, world)
 
-    result = None
+    res = None
     if rank == 0:
-        value = cells_all / (t_max * 1e-3)
         total_blocks = sim.info.nb
-        active_frac = cells / max(1, args.steps) / (total_blocks * prof["cells_per_block"])
-        result = {
-            "metric": "active cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if w["precision"] else "f64",
-            "data": "synthetic (seeded initial condition)",
-            "config": {"workload": args.workload, "model": w["model"], "grid": [cfg.nx, cfg.ny, cfg.nz],
+        res = {
+            "value": cells_all / (t_max * 1e-3), "unit": "cell-updates/s", "steps": steps, "warmup": warmup,
+            "ms_per_step": t_max / steps, "dtype": "f32" if w["precision"] else "f64",
+            "config": {"workload": name, "model": w["model"], "grid": [cfg.nx, cfg.ny, cfg.nz],
                        "block": cfg.block, "conserved": bool(cfg.conserved), "mode": "DBA" if w["mode"] else "regular",
-                       "preroll_steps": preroll, "active_fraction": active_frac,
-                       "l2": "state larger than L2 (%.0f MB resident), no flush" % (sim.info.device_bytes / 1e6),
+                       "preroll_steps": preroll,
+                       "active_fraction": cells / max(1, steps) / (total_blocks * prof["cells_per_block"]),
+                       "l2": ("state larger than L2 (%.0f MB resident), no flush" if sim.info.device_bytes > 126e6
+                              else "state of %.0f MB fits in L2; no flush (the workload itself is L2-resident)")
+                       % (sim.info.device_bytes / 1e6),
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": cells_e2e / (t_e2e * 1e-3), "unit": "cell-updates/s",
-                    "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps},
+                    "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
                          "kernel": f"{w['model']}_step", "peak_kind": peak_kind,
@@ -322,19 +321,55 @@ def run_ours(args, w):
                          "dense_over_dba_time": dense_ms / dba_ms if dba_ms else None,
                          "dense_cell_updates_per_s": dense_cells / (dense_ms * 1e-3) if dense_ms else None,
                          "steps": ncmp, "timing": "captured graphs, CUDA events, same starting state"},
-            "gpu_launches": args.steps * launches_per_step(w),
+            "gpu_launches": steps * launches_per_step(w),
             "clocks": clk.summary(),
             "status": status,
         }
-        if world == 1 and not args.no_cpu_baseline:
-            result["cpu_baseline"] = cpu_baseline(w, seconds=args.cpu_seconds)
+        if world == 1 and cpu_seconds:
+            res["cpu_baseline"] = cpu_baseline(w, seconds=cpu_seconds)
+    sim.close()
+    return res
+
+
+# the other workloads measured beside the headline (N = 1): untimed steps before the
+# measurement, at least 48 timed steps
+SIDE_WORKLOADS = {"dendrite_512_fp64": 5000, "dendrite3d_512_fp32": 10000, "kh_4096_fp32": 31440}
+
+
+def run_ours(args, w):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    preroll = w["t_total"] // 2 if args.preroll < 0 else args.preroll
+    m = measure(args, args.workload, w, args.steps, args.warmup, preroll, world, rank, local,
+                cpu_seconds=None if args.no_cpu_baseline else args.cpu_seconds)
+    result = None
+    if rank == 0:
+        result = {"metric": "active cell-updates/s", "value": m["value"], "unit": "cell-updates/s", "n_gpus": world,
+                  "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_per_step"],
+                  "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": m["dtype"],
+                  "data": "synthetic (seeded initial condition)"}
+        result.update({k: v for k, v in m.items() if k not in result and k not in ("steps", "warmup")})
+        if world == 1 and not args.no_side_workloads:
+            side = {}
+            for name, pre in SIDE_WORKLOADS.items():
+                if name == args.workload:
+                    continue
+                side[name] = measure(args, name, WORKLOADS[name], max(args.steps, 48), args.warmup, pre,
+                                     cpu_seconds=None if args.no_cpu_baseline else args.side_cpu_seconds)
+            result["workloads"] = side
         if world == 1 and not args.no_sweep:
             result["sweep"] = run_sweep(args)
         if world == 1 and not args.no_full_runs:
             result["full_runs_dba_vs_regular"] = run_full_runs(args)
         if world == 1 and w["precision"] == 1 and args.error_steps > 0:
             result["fp32_error_vs_fp64"] = run_fp32_error(w, args.error_steps)
-    sim.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -485,8 +520,8 @@ def run_fp32_error(w, nsteps):
 
 
 def run_full_runs(args):
-    """DBA against the all-blocks regular mode over whole runs of the dendrite workloads
-    (and, with --full-runs-kh EPS[,EPS..], of the KH flow with those wake-up thresholds):
+    """DBA against the all-blocks regular mode over whole runs of the dendrite workloads and
+    the Model B workload (and of the KH flow with the wake-up thresholds of --full-runs-kh):
     each advanced from its initial state to its end in both modes (captured graphs, CUDA
     events on the engine's stream), with the active fraction and the tip or simulated time
     at the end (the KH step count is the one that reaches simulated time 2)."""
@@ -494,7 +529,7 @@ def run_full_runs(args):
     import dba_b200
 
     out = {}
-    runs = [(n, WORKLOADS[n]) for n in ("dendrite_512_fp64", "dendrite3d_512_fp32")]
+    runs = [(n, WORKLOADS[n]) for n in ("dendrite_512_fp64", "dendrite3d_512_fp32", "modelb_2048_fp32_conserved")]
     for eps in (args.full_runs_kh.split(",") if args.full_runs_kh else []):
         w = WORKLOADS["kh_4096_fp32"]
         runs.append((f"kh_4096_fp32_eps{float(eps):g}", dict(w, params=dict(w["params"], metric_eps=float(eps)))))
@@ -574,12 +609,17 @@ def main():
     ap.add_argument("--workload", default="modelb_2048_fp32_conserved", choices=sorted(WORKLOADS))
     ap.add_argument("--preroll", type=int, default=-1, help="untimed steps before warm-up (default: half the run)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--side-cpu-seconds", type=float, default=6.0,
+                    help="CPU time of each side workload's reference CPU sample")
+    ap.add_argument("--no-side-workloads", action="store_true",
+                    help="skip the other workloads (512^2 dendrite, 512^3 dendrite, KH 4096^2) measured beside the headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sweep", action="store_true", help="skip the batched dendrite sweep section")
     ap.add_argument("--no-full-runs", action="store_true",
                     help="skip the whole-run DBA-vs-regular comparison of the dendrite workloads")
-    ap.add_argument("--full-runs-kh", default="", metavar="EPS[,EPS..]",
-                    help="add the KH flow (4096^2, to simulated time 2) with these wake-up thresholds to the whole runs")
+    ap.add_argument("--full-runs-kh", default="1", metavar="EPS[,EPS..]",
+                    help="KH flow (4096^2, to simulated time 2) whole runs with these wake-up thresholds "
+                         "(default: the workload's, 1; empty: none)")
     ap.add_argument("--error-steps", type=int, default=1000,
                     help="steps of the FP32-against-FP64 error check on the full grid (0: skip)")
     ap.add_argument("--sweep-requests", type=int, default=256)

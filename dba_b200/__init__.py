@@ -6,8 +6,9 @@ fallback: importing works without a GPU, but creating a Simulation needs the
 compiled library and a CUDA device.
 """
 from .engine import (  # noqa: F401
-    DBA_ERR, FIELDS, MODELS, Batch, Config, DBAError, Simulation, config, lib_path, load_library, parse_input,
+    BATCH_PERSISTENT, BATCH_WAIT_LIMIT, DBA_ERR, FIELDS, MODELS, OPT_WAIT_LIMIT, Batch, Config, DBAError, Simulation,
+    config, lib_path, load_library, parse_input,
 )
 
 __all__ = ["Batch", "Config", "DBAError", "Simulation", "config", "parse_input", "load_library", "lib_path", "FIELDS",
-           "MODELS", "DBA_ERR"]
+           "MODELS", "DBA_ERR", "OPT_WAIT_LIMIT", "BATCH_PERSISTENT", "BATCH_WAIT_LIMIT"]

@@ -28,7 +28,7 @@ UNITS = [
     ("batch.cu", ["-fmad=false"]),
 ]
 HEADERS = ["fpmath.h", "fpmath_coeffs.h", "k_common.cuh", "k_dendrite.cuh", "k_modelb.cuh", "k_kh.cuh",
-           "k_reduce.cuh", "k_inst.cuh", "launch.h", "k_modelb_fast.cuh", "k_modelb_tile.cuh", "k_modelb_strip.cuh", "k_kh_tile.cuh", "k_dendrite_tile.cuh", "k_batch.cuh", "k_post.cuh", "k_pair.cuh"]
+           "k_reduce.cuh", "k_inst.cuh", "launch.h", "k_modelb_fast.cuh", "k_modelb_tile.cuh", "k_kh_tile.cuh", "k_dendrite_tile.cuh", "k_batch.cuh", "k_post.cuh", "k_pair.cuh"]
 
 
 def _newer(target, deps):

@@ -61,7 +61,8 @@ struct dba_ctx {
     bool initialized = false;
     // FP32 2-D Model B conserved: lazy correction state (k_modelb_fast.cuh)
     bool lazy = false;
-    int mb_kernel = MB_KERNEL_BLOCK;  // FP32 2-D Model B: strip (k_modelb_strip.cuh), 32x32 tile or one-block kernel
+    long long wait_limit = 1LL << 20;  // attempts of a bounded device retry loop (DBA_OPT_WAIT_LIMIT)
+    bool tiles = false;               // FP32 2-D Model B on 32x32-cell tiles (k_modelb_tile.cuh)
     bool kh_tiles = false;            // KH one-kernel step on 16x16-cell tiles (k_kh_tile.cuh)
     bool den_tiles = false;           // FP32 3-D dendrite on 32x8x8-cell tiles (k_dendrite_tile.cuh)
     float* kvmax = nullptr;           // KH tiles: per-block largest signal speed (CFL)
@@ -284,7 +285,7 @@ cudaError_t enqueue_step_t(dba_ctx* c, long s, bool dba_mode)
     case DBA_MODEL_MODELB: {
         MBP<R> P = mb_params<R>(c, dba_mode);
         LazyP L = lazy_params(c, s, P.conserved != 0);
-        e = launch_modelb<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->mb_kernel);
+        e = launch_modelb<R>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
         if (e != cudaSuccess || !P.conserved || c->lazy) return e;
         break;
     }
@@ -660,12 +661,8 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
         const int nt = (cfg->nx / 16) * (cfg->ny / 16);
         c->grid = c->esz == 8 ? kh_tile_grid<double>(c->B, c->sms, nt) : kh_tile_grid<float>(c->B, c->sms, nt);
     }
-    if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->tiles == 1 &&
-        modelb_strip_ok(c->D, c->B, cfg->nx, cfg->ny, kMBStripRows)) {
-        c->mb_kernel = MB_KERNEL_STRIP;
-        c->grid = modelb_strip_grid(c->B, c->sms, (cfg->nx / 64) * (cfg->ny / kMBStripRows));
-    } else if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->tiles && modelb_tiles_ok(c->D, c->B, cfg->nx, cfg->ny)) {
-        c->mb_kernel = MB_KERNEL_TILE;
+    if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->tiles && modelb_tiles_ok(c->D, c->B, cfg->nx, cfg->ny)) {
+        c->tiles = true;
         c->grid = modelb_tile_grid(c->B, c->sms, (cfg->nx / 32) * (cfg->ny / 32));
     }
     if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->conserved && modelb_uses_fast<float>(c->D, c->B)) {
@@ -800,6 +797,17 @@ int dba_step(dba_ctx* c, int nsteps, int mode)
         }
     }
     return DBA_OK;
+}
+
+int dba_set_option(dba_ctx* c, int option, long long value)
+{
+    if (!c) return DBA_ERR_ARG;
+    if (option == DBA_OPT_WAIT_LIMIT) {
+        if (value < 0) return DBA_ERR_ARG;
+        c->wait_limit = value;
+        return DBA_OK;
+    }
+    return DBA_ERR_ARG;
 }
 
 int dba_sync(dba_ctx* c)
@@ -1043,7 +1051,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 else if (c->cfg.model == DBA_MODEL_MODELB) {
                     MBP<double> P = mb_params<double>(c, dba_mode);
                     LazyP L = lazy_params(c, s, P.conserved != 0);
-                    r = launch_modelb<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->mb_kernel);
+                    r = launch_modelb<double>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
                 }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
@@ -1057,7 +1065,7 @@ int dba_step_profiled(dba_ctx* c, int nsteps, int mode, dba_prof* out)
                 else if (c->cfg.model == DBA_MODEL_MODELB) {
                     MBP<float> P = mb_params<float>(c, dba_mode);
                     LazyP L = lazy_params(c, s, P.conserved != 0);
-                    r = launch_modelb<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->mb_kernel);
+                    r = launch_modelb<float>(c->D, c->B, dba_mode, c->grid, c->st, c->g, f, P, &L, c->tiles);
                 }
                 else {
                     r = cudaMemsetAsync(c->count, 0, sizeof(int), c->st);
@@ -1297,7 +1305,7 @@ int dba_size_distribution(dba_ctx* c, int field, double* avg_out, long* volume_o
     if (e == cudaSuccess) e = cudaMemsetAsync(first, 0xff, n * sizeof(unsigned long long), c->st);
     if (e == cudaSuccess) {
         post_init_kernel<<<grid, 256, 0, c->st>>>(c->staging, pg, avg, lab, small + 2);
-        post_union_kernel<<<grid, 256, 0, c->st>>>(pg, lab, c->status);
+        post_union_kernel<<<grid, 256, 0, c->st>>>(pg, lab, c->status, c->wait_limit);
         post_count_kernel<<<grid, 256, 0, c->st>>>(c->staging, pg, avg, lab, size, first);
         post_collect_kernel<<<grid, 256, 0, c->st>>>(pg, lab, size, first, small + 4, small + 3, cap);
         e = cudaGetLastError();

@@ -4,9 +4,11 @@
 // of four arrays (p and T, two ping-pong buffers each) and nb consecutive ids
 // of the global block space.  Both are first-fit allocated when a slot is
 // added and returned when it is removed, so admission is by free device
-// memory.  One kernel per step advances every live slot (k_batch.cuh); steps
-// are captured into CUDA graphs that stay valid across admissions because the
-// kernel reads the slot table from device memory.
+// memory.  By default one persistent cooperative launch advances every live
+// slot many steps, with a bounded grid barrier between steps (k_batch.cuh,
+// batch_dendrite_steps); with DBA_BATCH_PERSISTENT off, one kernel per step.
+// Either is captured into CUDA graphs that stay valid across admissions because
+// the kernels read the slot table from device memory.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -137,6 +139,14 @@ struct dba_batch {
     FreeList cells, blocks;
     long step = 0;
     cudaGraphExec_t graphs[6] = {};
+    // persistent form (batch_dendrite_steps): grid, barrier words (count, generation),
+    // polls per barrier wait before DBA_ERR_TIMEOUT, graphs of one 48-step launch per phase
+    int persistent = 1;
+    int grid_p = 0;
+    unsigned* bar = nullptr;
+    long long wait_limit = 1LL << 24;
+    cudaGraphExec_t pgraphs[6] = {};
+    bool pgraph_ok = true;
 };
 
 namespace {
@@ -155,6 +165,18 @@ FlagP bflags(dba_batch* b, long s)
     f.status = b->status;
     f.stats = b->stats;
     return f;
+}
+
+BatchFlagBase bflag_base(dba_batch* b)
+{
+    BatchFlagBase fb;
+    fb.par = b->par;
+    fb.wake = b->wake;
+    fb.next = b->next;
+    fb.status = b->status;
+    fb.stats = b->stats;
+    fb.L = 2 * (size_t)b->cfg.block_capacity;
+    return fb;
 }
 
 BatchP bparams(dba_batch* b)
@@ -184,6 +206,26 @@ cudaError_t enqueue(dba_batch* b, long s)
     BatchP p = bparams(b);
     return b->esz == 8 ? launch_batch_step<double>(b->cfg.block, b->cfg.threads, b->grid, b->st, p, f)
                        : launch_batch_step<float>(b->cfg.block, b->cfg.threads, b->grid, b->st, p, f);
+}
+
+// nsteps steps from step s0 in one persistent launch
+cudaError_t enqueue_steps(dba_batch* b, long long s0, int nsteps)
+{
+    const BatchP p = bparams(b);
+    const BatchFlagBase fb = bflag_base(b);
+    const GridBar gb{b->bar, b->bar + 1, b->wait_limit};
+    return b->esz == 8 ? launch_batch_steps<double>(b->cfg.block, b->cfg.threads, b->grid_p, b->st, p, fb, s0, nsteps, gb)
+                       : launch_batch_steps<float>(b->cfg.block, b->cfg.threads, b->grid_p, b->st, p, fb, s0, nsteps, gb);
+}
+
+void drop_graphs(dba_batch* b)
+{
+    for (auto* set : {b->graphs, b->pgraphs})
+        for (int r = 0; r < 6; ++r)
+            if (set[r]) {
+                cudaGraphExecDestroy(set[r]);
+                set[r] = nullptr;
+            }
 }
 
 }  // namespace
@@ -227,6 +269,8 @@ int dba_batch_create(const dba_batch_config* cfg, dba_batch** out)
     if (e == cudaSuccess) e = cudaMalloc(&b->status, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&b->stats, kStatWords * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&b->d_tips, sizeof(double) * cfg->max_slots);
+    if (e == cudaSuccess) e = cudaMalloc(&b->bar, 2 * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(b->bar, 0, 2 * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemset(b->d_bslot, 0xff, sizeof(int) * NB);
     if (e == cudaSuccess) e = cudaMemset(b->par, 0, 2 * 2 * NB);
     if (e == cudaSuccess) e = cudaMemset(b->wake, 0, 3 * 2 * NB);
@@ -246,6 +290,8 @@ int dba_batch_create(const dba_batch_config* cfg, dba_batch** out)
     b->blocks.init(NB);
     b->grid = b->esz == 8 ? batch_grid<double>(b->cfg.block, b->cfg.threads, b->sms)
                           : batch_grid<float>(b->cfg.block, b->cfg.threads, b->sms);
+    b->grid_p = b->esz == 8 ? batch_steps_grid<double>(b->cfg.block, b->cfg.threads, b->sms)
+                            : batch_steps_grid<float>(b->cfg.block, b->cfg.threads, b->sms);
     *out = b;
     return DBA_OK;
 }
@@ -254,10 +300,10 @@ void dba_batch_destroy(dba_batch* b)
 {
     if (!b) return;
     if (b->st) cudaStreamSynchronize(b->st);
-    for (auto& g : b->graphs)
-        if (g) cudaGraphExecDestroy(g);
+    drop_graphs(b);
     for (void* p : {(void*)b->arena, (void*)b->d_slots, (void*)b->d_bslot, (void*)b->d_hi, (void*)b->par, (void*)b->wake,
-                    (void*)b->next, (void*)b->status, (void*)b->stats, (void*)b->d_tips, (void*)b->staging})
+                    (void*)b->next, (void*)b->status, (void*)b->stats, (void*)b->d_tips, (void*)b->staging,
+                    (void*)b->bar})
         if (p) cudaFree(p);
     if (b->st) cudaStreamDestroy(b->st);
     delete b;
@@ -358,9 +404,55 @@ int dba_batch_remove(dba_batch* b, int s)
     return DBA_OK;
 }
 
+static void age_slots(dba_batch* b, int n)
+{
+    for (int s = 0; s < b->cfg.max_slots; ++s)
+        if (b->slots[s].live) b->age[s] += n;
+}
+
+// persistent form: runs of 48 steps replay a graph holding one 48-step launch
+// (captured per start phase on first use); a shorter remainder is one direct launch
+static int step_persistent(dba_batch* b, int nsteps)
+{
+    while (nsteps > 0) {
+        const int res = (int)((b->step + 1) % 6);
+        const int len = nsteps >= kGraphSteps ? kGraphSteps : nsteps;
+        bool done = false;
+        if (len == kGraphSteps && b->pgraph_ok) {
+            cudaGraphExec_t& ge = b->pgraphs[res];
+            if (!ge) {
+                cudaGraph_t graph = nullptr;
+                BTRY(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+                // only s0 mod 6 matters to the flag rotation, so the phase stands for the step
+                const cudaError_t e = enqueue_steps(b, res, len);
+                const cudaError_t e2 = cudaStreamEndCapture(b->st, &graph);
+                cudaError_t e3 = cudaErrorUnknown;
+                if (e == cudaSuccess && e2 == cudaSuccess) e3 = cudaGraphInstantiate(&ge, graph, 0);
+                if (graph) cudaGraphDestroy(graph);
+                if (e3 != cudaSuccess) {
+                    // this runtime does not capture cooperative launches: launch them directly
+                    cudaGetLastError();
+                    ge = nullptr;
+                    b->pgraph_ok = false;
+                }
+            }
+            if (ge) {
+                BTRY(cudaGraphLaunch(ge, b->st));
+                done = true;
+            }
+        }
+        if (!done) BTRY(enqueue_steps(b, b->step + 1, len));
+        b->step += len;
+        nsteps -= len;
+        age_slots(b, len);
+    }
+    return DBA_OK;
+}
+
 int dba_batch_step(dba_batch* b, int nsteps)
 {
     if (!b || nsteps < 0) return DBA_ERR_ARG;
+    if (b->persistent) return step_persistent(b, nsteps);
     while (nsteps > 0) {
         const int res = (int)((b->step + 1) % 6);
         if (nsteps >= kGraphSteps) {
@@ -380,16 +472,32 @@ int dba_batch_step(dba_batch* b, int nsteps)
             BTRY(cudaGraphLaunch(ge, b->st));
             b->step += kGraphSteps;
             nsteps -= kGraphSteps;
-            for (int s = 0; s < b->cfg.max_slots; ++s)
-                if (b->slots[s].live) b->age[s] += kGraphSteps;
+            age_slots(b, kGraphSteps);
         } else {
             BTRY(enqueue(b, b->step + 1));
             b->step += 1;
             nsteps -= 1;
-            for (int s = 0; s < b->cfg.max_slots; ++s)
-                if (b->slots[s].live) b->age[s] += 1;
+            age_slots(b, 1);
         }
     }
+    return DBA_OK;
+}
+
+int dba_batch_set_option(dba_batch* b, int option, long long value)
+{
+    if (!b) return DBA_ERR_ARG;
+    if (option == DBA_BATCH_PERSISTENT) {
+        if (value != 0 && value != 1) return DBA_ERR_ARG;
+        b->persistent = (int)value;
+    } else if (option == DBA_BATCH_WAIT_LIMIT) {
+        if (value < 0) return DBA_ERR_ARG;
+        b->wait_limit = value;
+    } else {
+        return DBA_ERR_ARG;
+    }
+    // captured launches hold the old values
+    BTRY(cudaStreamSynchronize(b->st));
+    drop_graphs(b);
     return DBA_OK;
 }
 
@@ -399,6 +507,8 @@ int dba_batch_sync(dba_batch* b)
     BTRY(cudaStreamSynchronize(b->st));
     int s = 0;
     BTRY(cudaMemcpy(&s, b->status, sizeof(int), cudaMemcpyDeviceToHost));
+    // a barrier that timed out leaves arrivals counted: start the next launch from zero
+    if (s == DBA_ERR_TIMEOUT) BTRY(cudaMemset(b->bar, 0, 2 * sizeof(unsigned)));
     return s;
 }
 

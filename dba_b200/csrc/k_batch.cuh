@@ -13,6 +13,8 @@
 // slot table.
 // Because the kernel reads the table, CUDA graphs captured once stay valid
 // while simulations are admitted and retired between graph launches.
+// batch_dendrite_steps is the persistent form: one cooperative launch advances
+// many steps, separated by a grid barrier whose waits are bounded.
 #pragma once
 
 #include "k_common.cuh"
@@ -55,8 +57,31 @@ struct BatchBlk {
     int lb;             // block id within the slot
 };
 
-template <typename R, int B, int NT, bool DBA>
-__global__ void __launch_bounds__(NT) batch_dendrite_step(BatchP bp, FlagP f)
+// shared memory of one step of the batch kernels
+template <typename R, int B, int NT> struct BatchSmem {
+    static constexpr int TV = (B + 2) * (B + 2);
+    static constexpr int K = batch_group<B, NT>();
+    R sp[K * TV];
+    R sT[K * TV];
+    int s_list[NT], s_lmeta[NT];
+    int s_cnt;
+    int s_np[K], s_nT[K];
+    BatchBlk s_d[K];
+};
+
+// Loads of data that other CTAs of the same launch write (flags, parities, field
+// values): through L2 in the persistent kernel, since L1 is not coherent across
+// SMs within a launch; plain loads in the one-step kernel, whose launch boundary
+// orders them.
+template <bool COHERENT, typename T> __device__ __forceinline__ T ldx(const T* p)
+{
+    if constexpr (COHERENT) return __ldcg(p);
+    else return *p;
+}
+
+// One time step of every live slot (the body of both batch kernels).
+template <typename R, int B, int NT, bool DBA, bool COHERENT>
+__device__ __forceinline__ void batch_step_body(const BatchP& bp, const FlagP& f, BatchSmem<R, B, NT>& S)
 {
     constexpr int V = B * B;
     constexpr int E = B + 2;
@@ -64,13 +89,14 @@ __global__ void __launch_bounds__(NT) batch_dendrite_step(BatchP bp, FlagP f)
     constexpr int K = batch_group<B, NT>();
     constexpr int CPT = K * V / NT;
     static_assert(K * V % NT == 0 && CPT >= 1, "group must give every thread whole cells");
-
-    __shared__ R sp[K * TV];
-    __shared__ R sT[K * TV];
-    __shared__ int s_list[NT], s_lmeta[NT];
-    __shared__ int s_cnt;
-    __shared__ int s_np[K], s_nT[K];
-    __shared__ BatchBlk s_d[K];
+    R* const sp = S.sp;
+    R* const sT = S.sT;
+    int* const s_list = S.s_list;
+    int* const s_lmeta = S.s_lmeta;
+    int& s_cnt = S.s_cnt;
+    int* const s_np = S.s_np;
+    int* const s_nT = S.s_nT;
+    BatchBlk* const s_d = S.s_d;
 
     const int tid = threadIdx.x;
     const int G = gridDim.x;
@@ -84,11 +110,11 @@ __global__ void __launch_bounds__(NT) batch_dendrite_step(BatchP bp, FlagP f)
         int sl = -1, pp = 0, pT = 0, w0 = 1, w1 = 1;
         if (bl < hi) {
             sl = bp.bslot[b];
-            pp = f.par_cur[b];
-            pT = f.par_cur[nb + b];
+            pp = ldx<COHERENT>(f.par_cur + b);
+            pT = ldx<COHERENT>(f.par_cur + nb + b);
             if (DBA) {
-                w0 = f.wake_cur[b];
-                w1 = f.wake_cur[nb + b];
+                w0 = ldx<COHERENT>(f.wake_cur + b);
+                w1 = ldx<COHERENT>(f.wake_cur + nb + b);
             }
         }
         const bool valid = sl >= 0;
@@ -157,15 +183,16 @@ __global__ void __launch_bounds__(NT) batch_dendrite_step(BatchP bp, FlagP f)
                 R vp, vT;
                 if (ix && iy) {
                     const long long o = d.gi0 + (lx - 1) + (long long)d.r.nx * (ly - 1);
-                    vp = ((d.meta & 4) ? P1 : P0)[o];
-                    vT = ((d.meta & 8) ? T1 : T0)[o];
+                    vp = ldx<COHERENT>(((d.meta & 4) ? P1 : P0) + o);
+                    vT = ldx<COHERENT>(((d.meta & 8) ? T1 : T0) + o);
                 } else {
                     const int fc = ix ? (ly == 0 ? 2 : 3) : (lx == 0 ? 0 : 1);
                     const long long o = d.off[fc] + (ix ? (long long)(lx - 1) : (long long)d.r.nx * (ly - 1));
                     const int nbid = d.nbr[fc];
-                    const R a0 = P0[o], a1 = P1[o], c0 = T0[o], c1 = T1[o];
-                    vp = f.par_cur[nbid] ? a1 : a0;
-                    vT = f.par_cur[nb + nbid] ? c1 : c0;
+                    const R a0 = ldx<COHERENT>(P0 + o), a1 = ldx<COHERENT>(P1 + o);
+                    const R c0 = ldx<COHERENT>(T0 + o), c1 = ldx<COHERENT>(T1 + o);
+                    vp = ldx<COHERENT>(f.par_cur + nbid) ? a1 : a0;
+                    vT = ldx<COHERENT>(f.par_cur + nb + nbid) ? c1 : c0;
                 }
                 sp[i] = vp;
                 sT[i] = vT;
@@ -220,6 +247,96 @@ __global__ void __launch_bounds__(NT) batch_dendrite_step(BatchP bp, FlagP f)
             }
             __syncthreads();
         }
+    }
+}
+
+template <typename R, int B, int NT, bool DBA>
+__global__ void __launch_bounds__(NT) batch_dendrite_step(BatchP bp, FlagP f)
+{
+    __shared__ BatchSmem<R, B, NT> S;
+    batch_step_body<R, B, NT, DBA, false>(bp, f, S);
+}
+
+// Flag arrays of a batch, from which each step's rotation (FlagP) is derived:
+// par [2][2][L/2], wake [3][2][L/2], L = 2 x block capacity.
+struct BatchFlagBase {
+    uint8_t* par;
+    uint8_t* wake;
+    uint8_t* next;
+    int* status;
+    unsigned long long* stats;
+    size_t L;
+};
+
+__device__ __forceinline__ FlagP batch_flags(const BatchFlagBase& b, long long s)
+{
+    FlagP f;
+    f.par_cur = b.par + (s % 2) * b.L;
+    f.par_nxt = b.par + ((s + 1) % 2) * b.L;
+    f.wake_cur = b.wake + (s % 3) * b.L;
+    f.wake_nxt = b.wake + ((s + 1) % 3) * b.L;
+    f.wake_clr = b.wake + ((s + 2) % 3) * b.L;
+    f.next = b.next;
+    f.bsum = nullptr;
+    f.status = b.status;
+    f.stats = b.stats;
+    return f;
+}
+
+// Grid barrier of the persistent kernel (all CTAs co-resident: a cooperative
+// launch).  count: arrivals of the current barrier; gen: barrier generation.
+// A CTA that waits more than `limit` polls writes DBA_ERR_TIMEOUT (6) to the
+// status word and returns false; its caller then leaves the kernel, so every
+// CTA ends after a bounded wait even when one of them never arrives.
+struct GridBar {
+    unsigned* count;
+    unsigned* gen;
+    long long limit;
+};
+
+__device__ __forceinline__ bool grid_sync(const GridBar& gb, int* status)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile unsigned* vgen = gb.gen;
+        const unsigned g = *vgen;            // cannot advance before this CTA arrives
+        __threadfence();                     // this CTA's writes before its arrival
+        if (atomicAdd(gb.count, 1u) == gridDim.x - 1) {
+            atomicExch(gb.count, 0u);
+            __threadfence();
+            atomicAdd(gb.gen, 1u);
+        } else {
+            long long it = 0;
+            while (*vgen == g) {
+                if (++it > gb.limit) {
+                    ok = 0;
+                    raise_status(status, 6);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();                     // the other CTAs' writes before this CTA's next reads
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Persistent form: one launch advances every live slot `nsteps` steps from step
+// s0 (only s0 mod 6 matters: the flag rotation's period), with a grid barrier
+// between steps.  The body is the one-step kernel's, with the loads of data
+// other CTAs write taken through L2.
+template <typename R, int B, int NT, bool DBA>
+__global__ void __launch_bounds__(NT) batch_dendrite_steps(BatchP bp, BatchFlagBase fb, long long s0, int nsteps,
+                                                           GridBar gb)
+{
+    __shared__ BatchSmem<R, B, NT> S;
+    for (int q = 0; q < nsteps; ++q) {
+        batch_step_body<R, B, NT, DBA, true>(bp, batch_flags(fb, s0 + q), S);
+        if (q + 1 < nsteps && !grid_sync(gb, fb.status)) return;
     }
 }
 

@@ -12,7 +12,8 @@
 //     for ten values.  16-byte cp.async pieces, each inside one block (whose
 //     parity picks the buffer), double-buffered so tile i+1 loads while tile i
 //     computes; pieces that fall outside a zero-flux wall are clamped cell by
-//     cell instead;
+//     cell instead.  Only the pieces an active block of the tile reads are
+//     copied (a tile listed for one active block stages 16 of its 40 columns);
 //   * each thread owns one (x, y) column of the tile and slides a 3-plane
 //     window along z, so the z neighbours come from registers.  A warp holds
 //     8 x 4 columns of one block, so the warps of a listed tile's inactive
@@ -92,8 +93,16 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
         int X0, Y0, Z0;
         tile_xyz(s_tile[idx], X0, Y0, Z0);
         float* dst = smem_f + st * 2 * SV;
+        // 16-byte pieces an active block reads: block k (cells 8k .. 8k+7 and one halo cell
+        // each side) reads pieces 2k .. 2k+3 of every staged row; the others are not copied
+        const unsigned am = (s_tmeta[idx] | (s_tmeta[idx] >> 4)) & 0xfu;
+        unsigned need = 0;
+#pragma unroll
+        for (int k = 0; k < TBX; ++k)
+            if ((am >> k) & 1u) need |= 0xfu << (2 * k);
         for (int q = tid; q < NQ; q += NT) {
             const int c4 = q % (SW / 4), ry = (q / (SW / 4)) % SR, rz = q / ((SW / 4) * SR);
+            if (!((need >> c4) & 1u)) continue;
             const int lx = 4 * c4 - 4, ly = ry - 1, lz = rz - 1;
             const int reg = (lx + B) / B + RX * ((ly + B) / B + 3 * ((lz + B) / B));
             const int gy = wrapc(Y0 + ly, g.ny, g.bc), gz = wrapc(Z0 + lz, g.nz, g.bc);

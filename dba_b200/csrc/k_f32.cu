@@ -3,8 +3,6 @@
 #define REAL_T float
 #include "k_inst.cuh"
 
-#include <type_traits>
-
 namespace dba {
 
 cudaError_t launch_gather_lazy(cudaStream_t st, const GridP& g, int B, const float* b0, const float* b1,
@@ -60,34 +58,6 @@ cudaError_t launch_dendrite3_tiles(bool dba_mode, int grid, cudaStream_t st, con
 int modelb_tile_grid(int B, int sms, int ntiles)
 {
     return B == 8 ? tile_grid_b<8>(sms, ntiles) : tile_grid_b<16>(sms, ntiles);
-}
-
-int modelb_strip_grid(int B, int sms, int nunits)
-{
-    if (B != 16) return 0;
-    using S = MBStrip<16, kMBStripRows>;
-    cudaFuncSetAttribute(modelb_strip_step<16, kMBStripRows, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem);
-    cudaFuncSetAttribute(modelb_strip_step<16, kMBStripRows, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem);
-    int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, modelb_strip_step<16, kMBStripRows, true>, S::NT, S::smem) !=
-            cudaSuccess ||
-        occ < 1)
-        occ = 1;
-    // one unit per warp when the units fit in one wave of resident warps
-    const int need = (nunits + S::NW - 1) / S::NW;
-    const int g = occ * sms;
-    return g < need ? g : need;
-}
-
-cudaError_t launch_modelb_strip(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
-                                const MBFastP& P, const MBFastBuf& Q, const LazyP& L)
-{
-    if (B != 16) return cudaErrorInvalidValue;
-    using S = MBStrip<16, kMBStripRows>;
-    const MBPairP K = make_pair_params(P);
-    if (dba_mode) modelb_strip_step<16, kMBStripRows, true><<<grid, S::NT, S::smem, st>>>(g, f, P, K, Q, L);
-    else modelb_strip_step<16, kMBStripRows, false><<<grid, S::NT, S::smem, st>>>(g, f, P, K, Q, L);
-    return cudaGetLastError();
 }
 
 cudaError_t launch_modelb_tiles(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,

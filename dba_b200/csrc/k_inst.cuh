@@ -84,7 +84,7 @@ bool modelb_uses_fast(int D, int B)
 
 template <typename R>
 cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
-                          const MBP<R>& P, const LazyP* lz, int kernel)
+                          const MBP<R>& P, const LazyP* lz, bool tiles)
 {
     if constexpr (sizeof(R) == 4) {
         if (modelb_uses_fast<R>(D, B)) {
@@ -92,8 +92,7 @@ cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st
             if (lz) L = *lz;
             const MBFastP FP = make_fast_params(P);
             const MBFastBuf FB = make_fast_buf(P);
-            if (kernel == MB_KERNEL_STRIP) return launch_modelb_strip(B, dba_mode, grid, st, g, f, FP, FB, L);
-            if (kernel == MB_KERNEL_TILE) return launch_modelb_tiles(B, dba_mode, grid, st, g, f, FP, FB, L);
+            if (tiles) return launch_modelb_tiles(B, dba_mode, grid, st, g, f, FP, FB, L);
 #define XF(b)                                                                                   \
     if (B == b) {                                                                               \
         const size_t sm = MBFastShape<b>::smem;                                                 \
@@ -116,7 +115,7 @@ cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st
     DBA_MB_SHAPES(XM)
 #undef XM
     (void)lz;
-    (void)kernel;
+    (void)tiles;
     return cudaErrorInvalidValue;
 }
 
@@ -274,6 +273,60 @@ cudaError_t launch_batch_step(int B, int threads, int grid, cudaStream_t st, con
     return cudaGetLastError();
 }
 
+template <typename R, int NT>
+static const void* batch_steps_kernel(int B)
+{
+    return B == 4 ? (const void*)batch_dendrite_steps<R, 4, NT, true>
+                  : (B == 8 ? (const void*)batch_dendrite_steps<R, 8, NT, true> : (const void*)batch_dendrite_steps<R, 16, NT, true>);
+}
+
+template <typename R>
+int batch_steps_grid(int B, int threads, int sms)
+{
+    const void* k = threads == 128 ? batch_steps_kernel<R, 128>(B)
+                                   : (threads == 512 ? batch_steps_kernel<R, 512>(B) : batch_steps_kernel<R, 256>(B));
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, 0) != cudaSuccess || occ < 1) occ = 1;
+    return occ * sms;   // every CTA resident at once (the grid barrier needs it)
+}
+
+template <typename R, int B, int NT>
+static cudaError_t batch_coop(int grid, cudaStream_t st, const BatchP& p, const BatchFlagBase& fb, long long s0,
+                              int nsteps, const GridBar& gb)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, batch_dendrite_steps<R, B, NT, true>, p, fb, s0, nsteps, gb);
+}
+
+template <typename R, int NT>
+static cudaError_t batch_steps_nt(int B, int grid, cudaStream_t st, const BatchP& p, const BatchFlagBase& fb,
+                                  long long s0, int nsteps, const GridBar& gb)
+{
+    if (B == 4) return batch_coop<R, 4, NT>(grid, st, p, fb, s0, nsteps, gb);
+    if (B == 8) return batch_coop<R, 8, NT>(grid, st, p, fb, s0, nsteps, gb);
+    return batch_coop<R, 16, NT>(grid, st, p, fb, s0, nsteps, gb);
+}
+
+template <typename R>
+cudaError_t launch_batch_steps(int B, int threads, int grid, cudaStream_t st, const BatchP& p, const BatchFlagBase& fb,
+                               long long s0, int nsteps, const GridBar& gb)
+{
+    if (B != 4 && B != 8 && B != 16) return cudaErrorInvalidValue;
+    if (threads == 128) return batch_steps_nt<R, 128>(B, grid, st, p, fb, s0, nsteps, gb);
+    if (threads == 256) return batch_steps_nt<R, 256>(B, grid, st, p, fb, s0, nsteps, gb);
+    if (threads == 512) return batch_steps_nt<R, 512>(B, grid, st, p, fb, s0, nsteps, gb);
+    return cudaErrorInvalidValue;
+}
+
 template <typename R>
 cudaError_t launch_batch_tips(cudaStream_t st, const BatchP& p, const uint8_t* par_cur, int nslots, double* tips)
 {
@@ -282,12 +335,15 @@ cudaError_t launch_batch_tips(cudaStream_t st, const BatchP& p, const uint8_t* p
 }
 
 template int batch_grid<REAL_T>(int, int, int);
+template int batch_steps_grid<REAL_T>(int, int, int);
+template cudaError_t launch_batch_steps<REAL_T>(int, int, int, cudaStream_t, const BatchP&, const BatchFlagBase&,
+                                                long long, int, const GridBar&);
 template cudaError_t launch_batch_step<REAL_T>(int, int, int, cudaStream_t, const BatchP&, const FlagP&);
 template cudaError_t launch_batch_tips<REAL_T>(cudaStream_t, const BatchP&, const uint8_t*, int, double*);
 template bool shape_supported<REAL_T>(int, int, int);
 template int step_grid<REAL_T>(int, int, int, int);
 template cudaError_t launch_dendrite<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const DenP<REAL_T>&);
-template cudaError_t launch_modelb<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const MBP<REAL_T>&, const LazyP*, int);
+template cudaError_t launch_modelb<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const MBP<REAL_T>&, const LazyP*, bool);
 template bool modelb_uses_fast<REAL_T>(int, int);
 template cudaError_t launch_kh<REAL_T>(int, bool, int, cudaStream_t, const GridP&, const FlagP&, const KHP<REAL_T>&);
 template cudaError_t launch_correct<REAL_T>(int, cudaStream_t, const GridP&, const CorrP<REAL_T>&);

@@ -78,10 +78,10 @@ __device__ __forceinline__ long long uf_find(long long* lab, long long x)
 }
 
 // link the roots of a and b (the larger index under the smaller); returns false
-// if the bounded retry loop gave up
-__device__ __forceinline__ bool uf_union(long long* lab, long long a, long long b)
+// if the retry loop gave up after `limit` attempts
+__device__ __forceinline__ bool uf_union(long long* lab, long long a, long long b, long long limit)
 {
-    for (int guard = 0; guard < (1 << 20); ++guard) {
+    for (long long guard = 0; guard < limit; ++guard) {
         a = uf_find(lab, a);
         b = uf_find(lab, b);
         if (a == b) return true;
@@ -115,7 +115,7 @@ static __global__ void post_init_kernel(const double* f, PostGrid g, double avg,
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(volume, v);
 }
 
-static __global__ void post_union_kernel(PostGrid g, long long* lab, int* status)
+static __global__ void post_union_kernel(PostGrid g, long long* lab, int* status, long long limit)
 {
     const size_t plane = (size_t)g.nx * g.ny;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += (size_t)gridDim.x * blockDim.x) {
@@ -125,9 +125,9 @@ static __global__ void post_union_kernel(PostGrid g, long long* lab, int* status
         const size_t jy = (size_t)x + (size_t)g.nx * (y + 1 == g.ny ? 0 : y + 1) + plane * z;
         const size_t jz = (size_t)x + (size_t)g.nx * y + plane * (z + 1 == g.nz ? 0 : z + 1);
         bool ok = true;
-        if (lab[jx] >= 0) ok &= uf_union(lab, (long long)i, (long long)jx);
-        if (lab[jy] >= 0) ok &= uf_union(lab, (long long)i, (long long)jy);
-        if (lab[jz] >= 0) ok &= uf_union(lab, (long long)i, (long long)jz);
+        if (lab[jx] >= 0) ok &= uf_union(lab, (long long)i, (long long)jx, limit);
+        if (lab[jy] >= 0) ok &= uf_union(lab, (long long)i, (long long)jy, limit);
+        if (lab[jz] >= 0) ok &= uf_union(lab, (long long)i, (long long)jz, limit);
         if (!ok) atomicCAS(status, 0, 6);   // DBA_ERR_TIMEOUT
     }
 }

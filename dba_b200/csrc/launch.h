@@ -13,7 +13,6 @@
 #include "k_modelb.cuh"
 #include "k_modelb_fast.cuh"
 #include "k_modelb_tile.cuh"
-#include "k_modelb_strip.cuh"
 #include "k_reduce.cuh"
 #include "k_batch.cuh"
 #include "k_post.cuh"
@@ -33,22 +32,15 @@ int dendrite3_tile_grid(int sms, int ntiles);
 cudaError_t launch_dendrite3_tiles(bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
                                    const DenP<float>& P);
 // FP32 2-D uses the fast kernels (lazy conserved correction, reduction fused):
-// kernel 2 = the strip kernel (see modelb_strip_ok), 1 = the 32x32-cell tile
-// kernel (see modelb_tiles_ok), 0 = one block at a time.  `lz` may be null for FP64.
-enum { MB_KERNEL_BLOCK = 0, MB_KERNEL_TILE = 1, MB_KERNEL_STRIP = 2 };
+// the 32x32-cell tile kernel when `tiles` (see modelb_tiles_ok), else one block
+// at a time.  `lz` may be null for FP64.
 template <typename R>
 cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
-                          const MBP<R>& P, const LazyP* lz, int kernel);
+                          const MBP<R>& P, const LazyP* lz, bool tiles);
 template <typename R> bool modelb_uses_fast(int D, int B);
 bool modelb_tiles_ok(int D, int B, int nx, int ny);
 // persistent grid of the tile kernel (also sets its shared-memory limit on the current device)
 int modelb_tile_grid(int B, int sms, int ntiles);
-// FP32 2-D Model B, one warp per 64 x kMBStripRows unit (k_modelb_strip.cuh): rows per unit,
-// grid for a step (also sets the kernel's shared-memory limit on the current device), launch
-constexpr int kMBStripRows = 32;
-int modelb_strip_grid(int B, int sms, int nunits);
-cudaError_t launch_modelb_strip(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
-                                const MBFastP& P, const MBFastBuf& Q, const LazyP& L);
 cudaError_t launch_modelb_tiles(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
                                 const MBFastP& P, const MBFastBuf& Q, const LazyP& L);
 cudaError_t launch_gather_lazy(cudaStream_t st, const GridP& g, int B, const float* b0, const float* b1,
@@ -78,6 +70,11 @@ cudaError_t launch_kh_prim_blocks(cudaStream_t st, const GridP& g, int B, const 
 template <typename R> int batch_grid(int B, int threads, int sms);
 template <typename R>
 cudaError_t launch_batch_step(int B, int threads, int grid, cudaStream_t st, const BatchP& p, const FlagP& f);
+// persistent form: `nsteps` steps from step s0 in one cooperative launch (grid from batch_steps_grid)
+template <typename R> int batch_steps_grid(int B, int threads, int sms);
+template <typename R>
+cudaError_t launch_batch_steps(int B, int threads, int grid, cudaStream_t st, const BatchP& p, const BatchFlagBase& fb,
+                               long long s0, int nsteps, const GridBar& gb);
 template <typename R>
 cudaError_t launch_batch_tips(cudaStream_t st, const BatchP& p, const uint8_t* par_cur, int nslots, double* tips);
 

@@ -17,6 +17,9 @@ FIELDS = {
     1: ["x", "y", "z", "b", "mu_x", "mu_y", "mu_z"],
     2: ["Mass", "Momx", "Momy", "Energy", "rho", "p", "vx", "vy"],
 }
+OPT_WAIT_LIMIT = 1          # dba_set_option
+BATCH_PERSISTENT = 1        # dba_batch_set_option
+BATCH_WAIT_LIMIT = 2
 DBA_ERR = {0: "ok", 1: "config", 2: "cuda", 3: "nomem", 4: "io", 5: "nonfinite", 6: "timeout", 7: "state", 8: "arg"}
 
 
@@ -135,6 +138,8 @@ def load_library():
             "dba_batch_get_info": (_i, [V, P(BatchInfo)]),
             "dba_batch_get_stream": (_i, [V, P(V)]),
             "dba_batch_destroy": (None, [V]),
+            "dba_batch_set_option": (_i, [V, _i, ctypes.c_longlong]),
+            "dba_set_option": (_i, [V, _i, ctypes.c_longlong]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -281,6 +286,10 @@ class Simulation:
         _check(st, "dba_size_distribution")
         return avg.value, vol.value, sizes[:nis.value].copy()
 
+    def set_option(self, option, value):
+        """dba_set_option: OPT_WAIT_LIMIT bounds the device retry loops (post-processing)."""
+        _check(self._L.dba_set_option(self._h, int(option), int(value)), "dba_set_option")
+
     def step_profiled(self, n, mode=1):
         p = Prof()
         _check(self._L.dba_step_profiled(self._h, int(n), int(mode), ctypes.byref(p)), "dba_step_profiled")
@@ -372,6 +381,11 @@ class Batch:
 
     def sync(self):
         _check(self._L.dba_batch_sync(self._h), "dba_batch_sync")
+
+    def set_option(self, option, value):
+        """dba_batch_set_option: BATCH_PERSISTENT (1 persistent launches, 0 one launch per
+        step) or BATCH_WAIT_LIMIT (polls per grid-barrier wait before DBA_ERR_TIMEOUT)."""
+        _check(self._L.dba_batch_set_option(self._h, int(option), int(value)), "dba_batch_set_option")
 
     def tips(self):
         t = np.empty(self.max_slots, np.float64)

@@ -87,12 +87,10 @@ typedef struct dba_config {
     double ic_radius, ic_width;/* dendrite tanh seed */
     int ic_corner;             /* dendrite tanh seed at cell (0,0,0) instead of the centre */
     double noise_amp, noise_amp_z; /* Model B: x,y and z uniform-noise amplitudes (0.05, 0.001) */
-    int tiles;                 /* 1 (default): tile kernels where the shape allows -- FP32 2-D Model B on
-                                  64-column x 32-row strips marched by one warp each (block 16, nx a multiple
-                                  of 64, ny of 32), else on 32x32 cells (nx, ny multiples of 32, block 8 or 16),
-                                  KH on 16x16 cells (nx, ny multiples of 16, block 8 or 16), FP32 3-D dendrite
-                                  on 32x8x8 cells (block 8, nx a multiple of 32); 2: as 1 but FP32 2-D Model B
-                                  always on 32x32 cells; 0: the one-block kernels and the four-stage KH kernels */
+    int tiles;                 /* 1 (default): tile kernels where the shape allows -- FP32 2-D Model B on 32x32
+                                  cells (nx, ny multiples of 32, block 8 or 16), KH on 16x16 cells (nx, ny
+                                  multiples of 16, block 8 or 16), FP32 3-D dendrite on 32x8x8 cells (block 8,
+                                  nx a multiple of 32); 0: the one-block kernels and the four-stage KH kernels */
     double cfl;                /* KH: > 0 picks each step's dt = cfl * min(dx, dy) / max(c + |v|) on the device
                                   (tile kernel only); 0 (default): the fixed dt */
 } dba_config;
@@ -280,6 +278,20 @@ int dba_batch_get_info(dba_batch* b, dba_batch_info* info);
 int dba_batch_get_stream(dba_batch* b, void** stream);
 void dba_batch_destroy(dba_batch* b);
 
+/* Batch options (no counterpart in the reference).
+ *   DBA_BATCH_PERSISTENT  1 (default): dba_batch_step advances its steps in persistent
+ *                         launches -- one cooperative launch of up to 48 steps, all CTAs
+ *                         resident, a grid barrier between steps; 0: one launch per step.
+ *                         Both give the same fields, bit for bit.
+ *   DBA_BATCH_WAIT_LIMIT  polls a CTA makes at one grid barrier before it gives up (default
+ *                         1 << 24, about a second): the launch then ends early, dba_batch_sync
+ *                         returns DBA_ERR_TIMEOUT and the slots' fields are undefined (remove
+ *                         and re-add them).  0 gives up at once (a test of the error path).
+ * Changing an option waits for the batch's stream and drops its captured graphs. */
+#define DBA_BATCH_PERSISTENT 1
+#define DBA_BATCH_WAIT_LIMIT 2
+int dba_batch_set_option(dba_batch* b, int option, long long value);
+
 /* ---- VTK XML RectilinearGrid output (the reference's CUDA-MPI write_output_vtr /
    write_output_pvtr, example_Dendritic_growth/CUDA-MPI/dendrite_kernels.cu:875-1060) ----
    Writes <base>.vtr, or with pieces > 1 <base>_<r>.vtr for r < pieces (y slabs that
@@ -312,6 +324,14 @@ int dba_tip_profile(dba_ctx* ctx, int field, int dz, int* tip_x, int* tip_x_max)
    DBA_ERR_TIMEOUT through dba_sync if the bounded union loop ever gives up. */
 int dba_size_distribution(dba_ctx* ctx, int field, double* avg, long* volume, long* islands, long* sizes,
                           long max_sizes);
+
+/* Context options (no counterpart in the reference).
+ *   DBA_OPT_WAIT_LIMIT  attempts a bounded device retry loop makes before it gives up
+ *                       (default 1 << 20): the union step of dba_size_distribution, whose
+ *                       compare-and-swap retries end with DBA_ERR_TIMEOUT through dba_sync.
+ *                       0 gives up at once (a test of the error path). */
+#define DBA_OPT_WAIT_LIMIT 1
+int dba_set_option(dba_ctx* ctx, int option, long long value);
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * -- work enqueued while a stream is captured into a CUDA graph, latency-critical

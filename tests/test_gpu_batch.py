@@ -109,3 +109,51 @@ def test_sweep_fp32_error_vs_fp64():
     assert abs(f32["v"] - f64["v"]) <= 0.01 * abs(f64["v"])
     for k in ("p", "T"):
         assert np.linalg.norm(f32[k] - f64[k]) / np.linalg.norm(f64[k]) <= 1e-4, k
+
+
+def _mixed_batch(persistent, precision=1):
+    b = dba_b200.Batch(precision=precision, block=8, max_slots=8, block_capacity=1 << 14, cell_capacity=1 << 21)
+    b.set_option(dba_b200.BATCH_PERSISTENT, persistent)
+    slots = [b.add(serve.request_config(_req(e, u, k, i), precision=precision))
+             for i, (e, u, k) in enumerate(((256, 0.6, 0.05), (128, 0.3, 0.02), (512, 0.45, 0.04)))]
+    return b, slots
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_persistent_launch_equals_one_launch_per_step(precision):
+    """The persistent form (one cooperative launch of up to 48 steps, grid barrier
+    between steps) gives the same fields bit for bit as one launch per step, over
+    graph-sized runs, direct remainders and an admission between launches."""
+    a, sa = _mixed_batch(1, precision)
+    b, sb = _mixed_batch(0, precision)
+    for n in (5, 48, 96, 7):
+        a.step(n)
+        b.step(n)
+        for x, y in zip(sa, sb):
+            assert np.array_equal(a.field(x, "p"), b.field(y, "p")), n
+            assert np.array_equal(a.field(x, "T"), b.field(y, "T")), n
+    ta = a.add(serve.request_config(_req(128, 0.5, 0.03, 9), precision=precision))
+    tb = b.add(serve.request_config(_req(128, 0.5, 0.03, 9), precision=precision))
+    a.step(60)
+    b.step(60)
+    assert np.array_equal(a.field(ta, "p"), b.field(tb, "p"))
+    assert np.array_equal(a.tips()[0], b.tips()[0], equal_nan=True)
+    a.sync()
+    b.sync()
+
+
+def test_grid_barrier_wait_limit_reports_timeout():
+    """With a wait limit of 0 polls, every CTA that reaches a grid barrier before the
+    last one gives up at once: the launch ends early and dba_batch_sync reports
+    DBA_ERR_TIMEOUT (a host-visible status; the context stays usable)."""
+    b, _ = _mixed_batch(1)
+    b.set_option(dba_b200.BATCH_WAIT_LIMIT, 0)
+    b.step(10)
+    with pytest.raises(dba_b200.DBAError) as e:
+        b.sync()
+    assert e.value.code == 6
+    # the device is still fine: a new batch runs normally
+    c, sc = _mixed_batch(1)
+    c.step(10)
+    c.sync()
+    assert np.all(np.isfinite(c.field(sc[0], "p")))

@@ -1,8 +1,6 @@
-"""FP32 2-D Model B: the strip kernel (tiles = 1 with block 16: one warp per
-64-column x 32-row unit) and the 32x32-cell tile kernel (tiles = 2, and tiles = 1
-with block 8) against the one-block-at-a-time kernel (tiles = 0).
+"""FP32 2-D Model B: the 32x32-cell tile kernel against the one-block-at-a-time kernel.
 
-All kernels evaluate every point formula with the same explicitly rounded
+Both kernels evaluate every point formula with the same explicitly rounded
 operations, so with the same DBA flags they must produce bit-identical fields,
 wake-up flags and conserved totals.  The initial condition is noisy only inside
 a disc, so most blocks go inactive after the first step: listed tiles then hold
@@ -30,11 +28,11 @@ def patch_ic(nx, ny, cx, cy, radius, seed=7):
     return [a[None] for a in (x, y, z)]
 
 
-def _pair(B, conserved, nx=128, ny=96, kernel=1):
+def _pair(B, conserved, nx=128, ny=96):
     prm = dict(MODELB_REF, metric_eps=3e-4, k_0=0.3)
     ic = patch_ic(nx, ny, cx=8, cy=40, radius=22)
     sims = []
-    for tiles in (kernel, 0):
+    for tiles in (1, 0):
         cfg = modelb_cfg(prm, nx, ny, 1, B, precision=1, conserved=conserved, tiles=tiles)
         sims.append(dba_b200.Simulation(cfg).init(ic))
     return sims
@@ -48,10 +46,10 @@ def _same(a, b):
     assert np.array_equal(a.flags(0), b.flags(0))
 
 
-@pytest.mark.parametrize("B,kernel", [(8, 1), (16, 1), (16, 2)])
+@pytest.mark.parametrize("B", [8, 16])
 @pytest.mark.parametrize("conserved", [0, 1])
-def test_tiles_bitexact_vs_block_kernel_dba(B, kernel, conserved):
-    t, k = _pair(B, conserved, kernel=kernel)
+def test_tiles_bitexact_vs_block_kernel_dba(B, conserved):
+    t, k = _pair(B, conserved)
     assert t.info.grid_ctas <= (128 // 32) * (96 // 32)      # tile grid: at most one CTA per tile
     seen = set()
     for _ in range(12):          # single steps through the first wake-up transients
@@ -69,9 +67,9 @@ def test_tiles_bitexact_vs_block_kernel_dba(B, kernel, conserved):
     k.sync()
 
 
-@pytest.mark.parametrize("B,kernel", [(8, 1), (16, 1), (16, 2)])
-def test_tiles_bitexact_vs_block_kernel_regular_then_dba(B, kernel):
-    t, k = _pair(B, 1, kernel=kernel)
+@pytest.mark.parametrize("B", [8, 16])
+def test_tiles_bitexact_vs_block_kernel_regular_then_dba(B):
+    t, k = _pair(B, 1)
     t.step(30, 0)
     k.step(30, 0)
     _same(t, k)
@@ -80,10 +78,9 @@ def test_tiles_bitexact_vs_block_kernel_regular_then_dba(B, kernel):
     _same(t, k)
 
 
-@pytest.mark.parametrize("kernel", [1, 2])
-def test_tiles_conserved_mass_exact(kernel):
-    """Lazy conserved DBA on strips / tiles: species totals stay at their initial values."""
-    t, _ = _pair(16, 1, kernel=kernel)
+def test_tiles_conserved_mass_exact():
+    """Lazy conserved DBA on tiles: species totals stay at their initial values."""
+    t, _ = _pair(16, 1)
     m0 = [t.field(f).sum() for f in ("x", "y", "z")]
     t.step(500, 1)
     m1 = [t.field(f).sum() for f in ("x", "y", "z")]
@@ -91,18 +88,17 @@ def test_tiles_conserved_mass_exact(kernel):
         assert abs(b - a) / abs(a) <= 1e-10, (a, b)
 
 
-@pytest.mark.parametrize("B,kernel", [(8, 1), (16, 1), (16, 2)])
-def test_tiles_many_tiles_per_cta(B, kernel):
+@pytest.mark.parametrize("B", [8, 16])
+def test_tiles_many_tiles_per_cta(B):
     """2048x1024 has 2048 tiles, several per CTA, so each CTA stages the next listed
     tile while it computes the current one (and loads the neighbour table of the one
-    after), and 1024 strip units; the results must still equal the block kernel's
-    bit for bit, in regular steps (every tile listed) and in DBA steps with a large
-    noisy disc."""
+    after); the results must still equal the block kernel's bit for bit, in regular
+    steps (every tile listed) and in DBA steps with a large noisy disc."""
     nx, ny = 2048, 1024
     prm = dict(MODELB_REF, metric_eps=3e-4, k_0=0.3)
     ic = patch_ic(nx, ny, cx=700, cy=500, radius=380, seed=11)
     t, k = (dba_b200.Simulation(modelb_cfg(prm, nx, ny, 1, B, precision=1, conserved=1, tiles=tl)).init(ic)
-            for tl in (kernel, 0))
+            for tl in (1, 0))
     assert t.info.grid_ctas < (nx // 32) * (ny // 32)
     t.step(5, 0)
     k.step(5, 0)

@@ -6,9 +6,8 @@
    512^2 workload itself: tanh seed, 8x8 blocks, zero-flux walls), conserved
    Model B at 2048^2 with 16x16 blocks and the 2048^2 workload's parameters,
    KH at 1024^2 with 8x8 blocks and partial activity.
-2. The FP32 Model B throughput kernels -- the strip kernel (one warp per 64 x 32
-   unit) and the 32x32 tile kernel (several tiles per CTA, next-tile copies
-   live) -- against the FP64 restatement at 2048^2 with partial activity, and on
+2. The FP32 Model B tile kernel (several 32x32 tiles per CTA, next-tile copies
+   live) against the FP64 restatement at 2048^2 with partial activity, and on
    the 2048^2 workload itself from its initial condition: relative L2 <= 1e-4
    per field, species totals conserved to 1e-10.
 3. The FP64 engine started from the initial state of each reference GPU run
@@ -146,37 +145,41 @@ def test_kh_1024_fp64_bitexact_every_step(conserved):
 # 2. FP32 tile kernel against the FP64 restatement at 2048^2
 # ---------------------------------------------------------------------------
 
-@pytest.mark.parametrize("tiles", [1, 2])
-def test_modelb_fp32_tiles_2048_partial_activity_vs_oracle(tiles):
-    """FP32 strip kernel (tiles = 1: 2048 units) and tile kernel (tiles = 2: 4096 tiles,
-    several per CTA) with activity falling from 100 % to a few per cent over 120 conserved
-    DBA steps (reference parameters, threshold 1e-3): relative L2 <= 1e-4 per field every
-    40 steps, at least 98 % of the wake flags equal."""
-    prm = dict(MODELB_REF, metric_eps=1e-3)
+def test_modelb_fp32_tiles_2048_partial_activity_vs_oracle():
+    """FP32 tile kernel (4096 tiles, several per CTA) against the FP64 restatement while
+    activity falls from every block to none: the reference's parameters with the
+    workload's reaction rate k_0 = 1e-4 and wake-up threshold 1e-3, conserved DBA, 60
+    steps.  Relative L2 <= 1e-4 per field every 10 steps and at least 99 % of the wake
+    flags equal at every step.  (With k_0 = 1 the FP32 rounding moves some blocks'
+    metrics across the threshold and those blocks then differ by whole updates: a third
+    of the blocks have differed once by step 120, which bounds nothing about the
+    arithmetic, so that case is not a tolerance test.)"""
+    prm = dict(MODELB_REF, metric_eps=1e-3, k_0=1e-4)
     o = OracleModelB(2048, 2048, 1, 16, prm, conserved=1)
     o.init_mt()
-    s = dba_b200.Simulation(modelb_cfg(prm, 2048, 2048, 1, 16, precision=1, conserved=1, tiles=tiles)).init()
+    s = dba_b200.Simulation(modelb_cfg(prm, 2048, 2048, 1, 16, precision=1, conserved=1, tiles=1)).init()
+    assert s.info.grid_ctas < (2048 // 32) ** 2
     fr = []
-    for _ in range(3):
-        o.step(40, 1)
-        s.step(40, 1)
-        for f in ("x", "y", "z"):
-            assert _rel_l2(s.field(f), o.field(f)) <= 1e-4, f
+    for t in range(1, 61):
+        o.step(1, 1)
+        s.step(1, 1)
         w = o.flags()[0]
-        assert np.mean(s.flags(0) == w) >= 0.98
+        assert np.mean(s.flags(0) == w) >= 0.99, t
         fr.append(float(w.mean()))
-    assert min(fr) < 0.9, fr          # partial activity was reached
+        if t % 10 == 0:
+            for f in ("x", "y", "z"):
+                assert _rel_l2(s.field(f), o.field(f)) <= 1e-4, (f, t)
+    assert min(fr) < 0.9 and max(fr) > 0.5, fr          # partial activity was exercised
     s.sync()
 
 
-@pytest.mark.parametrize("tiles", [1, 2])
-def test_modelb_fp32_workload_2048_vs_oracle(tiles):
+def test_modelb_fp32_workload_2048_vs_oracle():
     """The 2048^2 FP32 conserved workload from its initial condition, 50 DBA steps: relative
     L2 <= 1e-4 per field against the FP64 restatement, species totals conserved to 1e-10."""
     o = OracleModelB(2048, 2048, 1, 16, MODELB_2048, conserved=1)
     o.init_mt(amp=0.02, z_amp=0.02)
     s = dba_b200.Simulation(modelb_cfg(MODELB_2048, 2048, 2048, 1, 16, precision=1, conserved=1, noise_amp=0.02,
-                                       noise_amp_z=0.02, tiles=tiles)).init()
+                                       noise_amp_z=0.02)).init()
     m0 = [s.field(f).sum() for f in ("x", "y", "z")]
     o.step(50, 1)
     s.step(50, 1)

@@ -59,3 +59,15 @@ def test_tip_profile_matches_tool(prec):
     otip, om = ol.tip_profile(p, dz=40)
     assert np.array_equal(tip, otip) and m == om
     assert m > 32                              # the seed (centre x = 32) has grown along +x
+
+
+def test_union_retry_limit_reports_timeout():
+    """The union step of dba_size_distribution retries its compare-and-swap at most
+    DBA_OPT_WAIT_LIMIT times; with a limit of 0 every union gives up and dba_sync
+    reports DBA_ERR_TIMEOUT instead of a wrong answer passing silently."""
+    s = dba_b200.Simulation(modelb_cfg(MB, 32, 32, 32, 8, precision=0)).init(smooth_z((32, 32, 32), 5, width=1.5, skew=2.0))
+    s.set_option(dba_b200.OPT_WAIT_LIMIT, 0)
+    s.size_distribution("z")
+    with pytest.raises(dba_b200.DBAError) as e:
+        s.sync()
+    assert e.value.code == 6
