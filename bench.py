@@ -179,7 +179,8 @@ def dist_setup():
     return world, rank, local
 
 
-def measure(args, name, w, steps, warmup, preroll, world=1, rank=0, local=0, cpu_seconds=None):
+def measure(args, name, w, steps, warmup, preroll, world=1, rank=0, local=0, cpu_seconds=None,
+            e2e_from="snapshot"):
     """One workload: `preroll` untimed steps, `warmup` more, then `steps` timed steps on the
     engine's stream (CUDA events; the max over ranks when world > 1), the dominant kernel's
     roofline, the same state in regular (dense) mode, and the end-to-end leg through the
@@ -273,22 +274,47 @@ def measure(args, name, w, steps, warmup, preroll, world=1, rank=0, local=0, cpu
     dense_ms, dense_cells = graph_ms(0)
     dba_ms, _ = graph_ms(w["mode"])
 
-    # end to end through the public API: host state in pinned memory -> device, K steps, fields -> host
+    # end to end through the public API, host buffers in page-locked memory.  e2e_from ==
+    # "initial fields": the workload's initial state fields go host -> device (dba_init_f32 for
+    # FP32, dba_init for FP64), K steps, the state fields come back in the context's precision
+    # (dba_read_field_f32 / dba_read_field) -- a whole run of K steps.  "snapshot": the mid-run
+    # state is resumed from a host snapshot (dba_load_state), K steps, fields back.
     n = cfg.nx * cfg.ny * cfg.nz
     nf = {"dendrite": 2, "modelb": 3, "kh": 4}[w["model"]]
-    out_host = torch.empty((nf, n), dtype=torch.float64, pin_memory=True).numpy()   # page-locked result buffer
+    f32 = w["precision"] == 1
+    hdt = torch.float32 if f32 else torch.float64
+    out_host = torch.empty((nf, n), dtype=hdt, pin_memory=True).numpy()   # page-locked result buffer
+    read = (lambda q: sim.field_f32(q, out=out_host[q])) if f32 else (lambda q: sim.field(q, out=out_host[q]))
+    ic_host = None
+    if e2e_from == "initial fields":
+        # the workload's own initial condition, as the caller would hold it
+        sim.init()
+        names = ["rho", "p", "vx", "vy"] if w["model"] == "kh" else list(range(nf))
+        ic_host = torch.empty(nf * n, dtype=hdt, pin_memory=True).numpy()
+        for q, nm in enumerate(names):
+            ic_host[q * n:(q + 1) * n] = (sim.field_f32(nm) if f32 else sim.field(nm)).ravel()
+        ic_list = None if f32 else [ic_host[q * n:(q + 1) * n] for q in range(nf)]
+
+        def start():
+            return sim.init_f32(ic_host) if f32 else sim.init(ic_list)
+        start()
+        sim.step(steps, w["mode"])   # graphs of this start phase, outside the timed region
+        torch.cuda.synchronize()
+    else:
+        def start():
+            sim.load_state(blob)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    sim.load_state(blob)
+    start()
     st_e0 = sim.cell_updates()
     sim.step(steps, w["mode"])
     for q in range(nf):
-        sim.field(q, out=out_host[q])
+        read(q)
     t_e2e = (time.perf_counter() - t0) * 1e3
     cells_e2e = sim.cell_updates() - st_e0
-    h2d = blob.numel()
+    h2d = ic_host.nbytes if ic_host is not None else blob.numel()
     d2h = out_host.nbytes
     t_e2e, cells_e2e = aggregate(t_e2e, cells_e2e, world)
 
@@ -307,7 +333,8 @@ def measure(args, name, w, steps, warmup, preroll, world=1, rank=0, local=0, cpu
                        % (sim.info.device_bytes / 1e6),
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": cells_e2e / (t_e2e * 1e-3), "unit": "cell-updates/s",
-                    "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps},
+                    "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
+                    "from": e2e_from, "ms": t_e2e, "host_dtype": "f32" if f32 else "f64"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak if peak else None, "traffic": traffic,
                          "kernel": f"{w['model']}_step", "peak_kind": peak_kind,
@@ -347,8 +374,11 @@ def run_ours(args, w):
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     preroll = w["t_total"] // 2 if args.preroll < 0 else args.preroll
+    # the headline's e2e is a whole run from host initial fields (every block of the Model B
+    # workload is active from its first step to its last, so the active set is the timed one)
     m = measure(args, args.workload, w, args.steps, args.warmup, preroll, world, rank, local,
-                cpu_seconds=None if args.no_cpu_baseline else args.cpu_seconds)
+                cpu_seconds=None if args.no_cpu_baseline else args.cpu_seconds,
+                e2e_from="initial fields" if w["model"] == "modelb" else "snapshot")
     result = None
     if rank == 0:
         result = {"metric": "active cell-updates/s", "value": m["value"], "unit": "cell-updates/s", "n_gpus": world,
@@ -460,7 +490,8 @@ def run_sweep(args):
 
     choice = autotune.tune(precision=1, use_cache=False)
     reqs = serve.sweep_requests(n=args.sweep_requests, rate=args.sweep_rate, seed=args.sweep_seed)
-    srv = serve.SweepServer(precision=1, block=choice["block"], threads=choice["threads"], chunk=choice["chunk"])
+    srv = serve.SweepServer(precision=1, block=choice["block"], threads=choice["threads"], chunk=choice["chunk"],
+                            persistent=choice.get("persistent", 1))
     t0 = time.perf_counter()
     res = srv.run(reqs)
     t_batched = time.perf_counter() - t0
@@ -474,7 +505,9 @@ def run_sweep(args):
     same_steps = sum(r["steps"] == by_id[r["id"]]["steps"] for r in res)
     return {
         "requests": len(reqs), "arrival_rate_per_s": args.sweep_rate, "seed": args.sweep_seed,
-        "autotune": {"block": choice["block"], "threads": choice["threads"], "chunk": choice["chunk"]},
+        "autotune": {"block": choice["block"], "threads": choice["threads"], "chunk": choice["chunk"],
+                     "launch": "persistent" if choice.get("persistent", 1) else "one per step",
+                     "scores": choice.get("scores")},
         "batched_runs_per_s": summ["runs_per_s"], "sequential_runs_per_s": len(seq) / t_seq,
         "speedup": (summ["runs_per_s"] * t_seq / len(seq)) if summ["runs_per_s"] else None,
         "p50_latency_s": summ.get("p50_latency_s"), "p99_latency_s": summ.get("p99_latency_s"),

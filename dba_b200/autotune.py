@@ -2,13 +2,16 @@
 
 The batch kernel's DBA block edge (8 or 16 cells) trades halo overhead and
 per-block work against activity granularity; its threads per CTA (128, 256 or
-512) trade blocks processed per pass against occupancy; and the number of steps
-advanced between tip checks (`chunk`) trades host synchronisation against
-overshoot past each run's stopping point.  `tune()` times every (block edge,
-threads) pair on a short seeded mixed workload (the sweep's grid sizes and
-parameter ranges, every slot admitted at once, a fixed number of steps) and
-returns the fastest by active cell-updates per second, caching the choice per
-GPU and precision in a JSON file (DBA_AUTOTUNE_CACHE, default
+512) trade blocks processed per pass against occupancy; its launch form
+(persistent: one cooperative launch of up to 48 steps with a grid barrier
+between steps; or one launch per step, both replayed from CUDA graphs) trades
+the barrier's cost against launch gaps; and the number of steps advanced
+between tip checks (`chunk`) trades host synchronisation against overshoot past
+each run's stopping point.  `tune()` times every (block edge, threads, launch
+form) on a short seeded mixed workload (the sweep's grid sizes and parameter
+ranges, every slot admitted at once, a fixed number of steps) and returns the
+fastest by active cell-updates per second, caching the choice per GPU and
+precision in a JSON file (DBA_AUTOTUNE_CACHE, default
 ~/.cache/dba_b200/autotune.json).
 """
 import json
@@ -19,6 +22,7 @@ from . import engine, serve
 
 CANDIDATE_BLOCKS = (8, 16)
 CANDIDATE_THREADS = (128, 256, 512)
+CANDIDATE_PERSISTENT = (1, 0)
 CANDIDATE_CHUNKS = (48, 96, 192)
 SHORTEST_RUN_STEPS = 960
 
@@ -38,11 +42,12 @@ def _device_key(precision):
     return f"{p.name}|sm{p.major}{p.minor}|{p.multi_processor_count}sms|prec{precision}"
 
 
-def time_candidate(block, threads=256, precision=1, nslots=24, steps=480, seed=5):
-    """Active cell-updates per second of one (block edge, threads) pair on a mixed batch."""
+def time_candidate(block, threads=256, precision=1, persistent=1, nslots=24, steps=480, seed=5):
+    """Active cell-updates per second of one (block edge, threads, launch form) on a mixed batch."""
     reqs = serve.sweep_requests(n=nslots, rate=0.0, seed=seed, edges=(128, 256, 512))
     b = engine.Batch(precision=precision, block=block, max_slots=nslots, block_capacity=1 << 17, threads=threads)
     try:
+        b.set_option(engine.BATCH_PERSISTENT, persistent)
         for r in reqs:
             if b.add(serve.request_config(r, precision, block)) is None:
                 break
@@ -73,15 +78,17 @@ def tune(precision=1, use_cache=True, verbose=False):
     scores = {}
     for blk in CANDIDATE_BLOCKS:
         for nt in CANDIDATE_THREADS:
-            scores[(blk, nt)] = time_candidate(blk, nt, precision)
-            if verbose:
-                print(f"block {blk} threads {nt}: {scores[(blk, nt)]:.3e} cell-updates/s", flush=True)
-    best_block, best_threads = max(scores, key=scores.get)
+            for pers in CANDIDATE_PERSISTENT:
+                scores[(blk, nt, pers)] = time_candidate(blk, nt, precision, persistent=pers)
+                if verbose:
+                    print(f"block {blk} threads {nt} persistent {pers}: {scores[(blk, nt, pers)]:.3e} cell-updates/s",
+                          flush=True)
+    best_block, best_threads, best_pers = max(scores, key=scores.get)
     # chunk: the largest (fewest host syncs) whose mean overshoot past the stop, chunk / 2,
     # stays within 5 % of the shortest runs of the sweep (a 128^2 grid stops after ~960 steps)
     best_chunk = max(c for c in CANDIDATE_CHUNKS if c / 2 <= 0.05 * SHORTEST_RUN_STEPS)
-    choice = {"block": int(best_block), "threads": int(best_threads), "chunk": int(best_chunk),
-              "scores": {f"{b}x{t}": v for (b, t), v in scores.items()}}
+    choice = {"block": int(best_block), "threads": int(best_threads), "persistent": int(best_pers),
+              "chunk": int(best_chunk), "scores": {f"{b}x{t}x{'p' if q else 's'}": v for (b, t, q), v in scores.items()}}
     if use_cache:
         os.makedirs(os.path.dirname(path), exist_ok=True)
         cache[key] = choice

@@ -63,6 +63,7 @@ struct dba_ctx {
     bool lazy = false;
     long long wait_limit = 1LL << 20;  // attempts of a bounded device retry loop (DBA_OPT_WAIT_LIMIT)
     bool tiles = false;               // FP32 2-D Model B on 32x32-cell tiles (k_modelb_tile.cuh)
+    float* fstaging = nullptr;        // dba_read_field_f32: a field as floats (allocated on first use)
     bool kh_tiles = false;            // KH one-kernel step on 16x16-cell tiles (k_kh_tile.cuh)
     bool den_tiles = false;           // FP32 3-D dendrite on 32x8x8-cell tiles (k_dendrite_tile.cuh)
     float* kvmax = nullptr;           // KH tiles: per-block largest signal speed (CFL)
@@ -491,6 +492,12 @@ int gather(dba_ctx* c, const void* b0, const void* b1, const uint8_t* par, size_
     return cuda_status(cudaStreamSynchronize(c->st));
 }
 
+__global__ void to_float_kernel(const double* src, float* dst, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+
 // a state field's current values, as doubles, into c->staging (device only)
 int field_on_device(dba_ctx* c, int field)
 {
@@ -692,6 +699,7 @@ void dba_destroy(dba_ctx* c)
             for (auto& gexec : row)
                 if (gexec) cudaGraphExecDestroy(gexec);
     for (auto& a : c->allocs) cudaFree(a.p);
+    if (c->fstaging) cudaFree(c->fstaging);
     if (c->host_staging) cudaFreeHost(c->host_staging);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -755,6 +763,31 @@ int dba_init(dba_ctx* c, const double* ic)
     // step 1 reads wake[1 % 3]: every block starts active (kernel.cu:157-160)
     DBA_TRY(cudaMemset(c->wake + 1 * (size_t)c->nch * c->g.nb, 1, (size_t)c->nch * c->g.nb));
     DBA_TRY(cudaDeviceSynchronize());
+    c->step = 0;
+    c->time = 0.0;
+    c->initialized = true;
+    return DBA_OK;
+}
+
+int dba_init_f32(dba_ctx* c, const float* ic)
+{
+    if (!c || !ic) return DBA_ERR_ARG;
+    const dba_config& k = c->cfg;
+    if (c->esz != 4 || k.model == DBA_MODEL_KH) {
+        // FP64 contexts and KH (its primitives become conserved fields in FP64 on the host)
+        const size_t m = (size_t)c->nstate * c->n;
+        std::vector<double> tmp(m);
+        for (size_t i = 0; i < m; ++i) tmp[i] = ic[i];
+        return dba_init(c, tmp.data());
+    }
+    // FP32 dendrite and Model B: the state fields go to the device as they are
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    for (auto& a : c->allocs) DBA_TRY(cudaMemset(a.p, 0, a.bytes));
+    for (int q = 0; q < c->nstate; ++q)
+        DBA_TRY(cudaMemcpyAsync(c->state[q][0], ic + q * c->n, c->n * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    // step 1 reads wake[1 % 3]: every block starts active (as dba_init)
+    DBA_TRY(cudaMemsetAsync(c->wake + 1 * (size_t)c->nch * c->g.nb, 1, (size_t)c->nch * c->g.nb, c->st));
+    DBA_TRY(cudaStreamSynchronize(c->st));
     c->step = 0;
     c->time = 0.0;
     c->initialized = true;
@@ -876,6 +909,30 @@ int dba_read_field(dba_ctx* c, int field, double* host)
     }
     const int w = field - 4;   // rho, p, vx, vy
     return gather(c, c->aux[w], c->aux[w], nullptr, 0, 1, c->n, host);
+}
+
+int dba_read_field_f32(dba_ctx* c, int field, float* host)
+{
+    if (!c || !host) return DBA_ERR_ARG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    if (field < 0 || field >= nfields_of(c->cfg.model)) return DBA_ERR_ARG;
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    int st = field_on_device(c, field);
+    if (st == DBA_ERR_ARG) {
+        // fields without a device-side gather (derived and intermediate fields): the FP64 path
+        std::vector<double> tmp(c->n);
+        st = dba_read_field(c, field, tmp.data());
+        for (size_t i = 0; !st && i < c->n; ++i) host[i] = (float)tmp[i];
+        return st;
+    }
+    if (st) return st;
+    if (!c->fstaging) DBA_TRY(cudaMalloc(&c->fstaging, c->n * sizeof(float)));
+    const int grid = (int)std::min<size_t>((c->n + 255) / 256, 4096);
+    to_float_kernel<<<grid, 256, 0, c->st>>>(c->staging, c->fstaging, c->n);
+    DBA_TRY(cudaGetLastError());
+    DBA_TRY(cudaMemcpyAsync(host, c->fstaging, c->n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    return DBA_OK;
 }
 
 int dba_read_flags(dba_ctx* c, int which, int32_t* host)

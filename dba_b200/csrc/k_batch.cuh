@@ -315,7 +315,7 @@ __device__ __forceinline__ bool grid_sync(const GridBar& gb, int* status)
                     raise_status(status, 6);
                     break;
                 }
-                __nanosleep(64);
+                if (it > 256) __nanosleep(32);   // spin first: a step's barrier usually opens within microseconds
             }
         }
         __threadfence();                     // the other CTAs' writes before this CTA's next reads

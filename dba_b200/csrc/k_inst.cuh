@@ -215,9 +215,12 @@ __global__ void __launch_bounds__(kThreads) kh_prim_blocks(GridP g, int B, KHP<R
     for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (size_t)gridDim.x * kThreads) {
         const int x = (int)(i % g.nx), y = (int)(i / g.nx);
         const int ob = x / B + g.nbx * (y / B);
-        if (only && !only[ob]) continue;
+        // tile contexts (upar set) keep no stale primitives: a block not in `only` takes
+        // them from its other buffer, the state its last active step started from
+        const bool fresh = !only || only[ob];
+        if (!fresh && !P.upar) continue;
         const KHK<R> K = kh_consts<R>(P.dt, P.dx, P.dy, P.vol, P.gamma);
-        const bool alt = P.upar && P.upar[ob];
+        const bool alt = P.upar && (P.upar[ob] != 0) == fresh;
         R r, pp, u, v;
         kh_prim_of<R>((alt ? P.U1 : P.U)[0][i], (alt ? P.U1 : P.U)[1][i], (alt ? P.U1 : P.U)[2][i],
                       (alt ? P.U1 : P.U)[3][i], K, r, pp, u, v);
@@ -280,6 +283,10 @@ static const void* batch_steps_kernel(int B)
                   : (B == 8 ? (const void*)batch_dendrite_steps<R, 8, NT, true> : (const void*)batch_dendrite_steps<R, 16, NT, true>);
 }
 
+#ifndef BATCH_PERSIST_THREADS_PER_SM
+#define BATCH_PERSIST_THREADS_PER_SM 1024   // resident threads per SM of the persistent batch kernel
+#endif
+
 template <typename R>
 int batch_steps_grid(int B, int threads, int sms)
 {
@@ -287,7 +294,11 @@ int batch_steps_grid(int B, int threads, int sms)
                                    : (threads == 512 ? batch_steps_kernel<R, 512>(B) : batch_steps_kernel<R, 256>(B));
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, 0) != cudaSuccess || occ < 1) occ = 1;
-    return occ * sms;   // every CTA resident at once (the grid barrier needs it)
+    // every CTA resident at once (the grid barrier needs it), and few of them: each grid
+    // barrier costs one arrival per CTA on one counter
+    const int cap = BATCH_PERSIST_THREADS_PER_SM / threads;
+    if (occ > cap) occ = cap > 0 ? cap : 1;
+    return occ * sms;
 }
 
 template <typename R, int B, int NT>

@@ -5,9 +5,14 @@
 // apply_flux), but the intermediates live in shared memory instead of
 // full-grid arrays.  Per listed tile (one block of 16, or 2x2 blocks of 8):
 //
-//   1. primitives on the tile + 2-cell halo: recomputed from the conserved
-//      fields where the owning block is active this step, read from the
-//      persisted primitive arrays where it is not (the reference's stale reads);
+//   1. primitives on the tile + 2-cell halo: computed from the conserved
+//      fields -- the current buffer where the owning block is active this step,
+//      its other buffer where it is not.  A sleeping block's other buffer still
+//      holds the state its last active step started from (that step wrote the
+//      new state to the current buffer, and nothing writes the other one until
+//      the block is active again), so this gives, bit for bit, the primitives the
+//      reference reads stale (KH_DBA.cu:418-482 recomputes them only for active
+//      blocks) without storing them;
 //   2. gradients and half-step states on the tile + 1-cell halo: computed where
 //      the owner is active (from the staged primitives), persisted values where
 //      it is not; the wake-up metric of the tile's own cells;
@@ -17,11 +22,12 @@
 //      fields ping-pong per block, so neighbours staging this step still read
 //      the old values), FP64 per-block change sums for conserved DBA.
 //
-// A block persists what neighbours could later read as stale -- its primitives
-// (all cells: readback and the 2-cell halo), the gradients and half-step states
-// of its 1-cell ring, and the fluxes of its right column and top row -- only
-// when its own wake-up test is negative: a block whose test is positive is
-// active next step (it wakes itself), so nothing it computes now is read stale.
+// A block persists what neighbours could later read as stale and cannot be
+// recomputed from its buffers -- the gradients and half-step states of its
+// 1-cell ring (they depend on neighbours' primitives as of that step) and the
+// fluxes of its right column and top row -- only when its own wake-up test is
+// negative: a block whose test is positive is active next step (it wakes
+// itself), so nothing it computes now is read stale.
 //
 // Launch shape: 416 threads (13 warps), so that each phase is one item per
 // thread (400, 320, 288 and 256 items) and no warp runs a second round while
@@ -103,12 +109,18 @@ struct QA {
     }
 };
 
+#ifndef KH_TILE_MINB_DBA_F32
+#define KH_TILE_MINB_DBA_F32 3   // resident CTAs per SM of the FP32 DBA variant
+#endif
+
 template <typename R, int B> struct KHTile {
     // 13 warps: every staging phase below is one item per thread (400 primitive
     // cells, 320 gradient cells, 288 face pairs, 256 updates), so no warp runs a
     // second round while the others wait at the phase's barrier
     static constexpr int NT = 416;
     static constexpr int MINB = sizeof(R) == 4 ? 3 : 2;   // resident CTAs per SM
+    // the DBA variant (wake-up metric, persistence) under its own occupancy target
+    static constexpr int MINB_DBA = sizeof(R) == 4 ? KH_TILE_MINB_DBA_F32 : 2;
     static constexpr int T = 16;               // tile edge in cells
     static constexpr int TB = T / B;           // blocks per tile edge
     static constexpr int NBT = TB * TB;
@@ -135,7 +147,8 @@ template <int B, int RB>
 __device__ __forceinline__ int kh_region(int lx, int ly) { return (lx + B) / B + RB * ((ly + B) / B); }
 
 template <typename R, int B, bool DBA>
-__global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_step(GridP g, FlagP f, KHTileP<R> P)
+__global__ void __launch_bounds__(KHTile<R, B>::NT, DBA ? KHTile<R, B>::MINB_DBA : KHTile<R, B>::MINB)
+    kh_tile_step(GridP g, FlagP f, KHTileP<R> P)
 {
     using S = KHTile<R, B>;
     constexpr int NT = S::NT, T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, TPP = S::TPP;
@@ -151,7 +164,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
     const QA<R> sFx{sGx.base + 4 * S::NG, S::NFX};               // [T][FXW]  flux through the face right of (x, y) at y * FXW + x + 1
     const QA<R> sFy{sFx.base + 4 * S::NFX, S::NFY};              // [T+1][T]  flux through the face above (x, y) at (y + 1) * T + x
     const QA<R> sU{sFy.base + 4 * S::NFY, S::NU};                // [T][T]    own cells' conserved fields
-    R* sStage = sU.base + 4 * S::NU;            // [4][N1] phase-1 inputs of the next tile, copied ahead
+    R* sStage = sU.base + 4 * S::NU;            // [4][N1] phase-1 conserved inputs of the next tile, copied ahead
     __shared__ int s_tile[TPP];                 // listed tiles: tbx | tby << 15 | halo-inside-domain << 30
     __shared__ unsigned s_tmeta[TPP];           // bits 0..15 active blocks, 16..31 their parity
     __shared__ int s_cnt;
@@ -255,11 +268,12 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
             __syncthreads();
         }
         const int cnt = s_cnt;
-        // Tile i's phase-1 inputs (conserved fields where the owning block is active,
-        // persisted primitives where it is not) are copied into sStage while tile i-1
-        // computes; each thread copies and later reads only its own phase-1 cell.  Within
-        // a step nothing writes what is copied: updates go to the other buffer and only
-        // active blocks persist.
+        // Tile i's phase-1 inputs (the conserved fields of the owning block's current
+        // buffer where it is active, of its other buffer where it is not) are copied
+        // into sStage while tile i-1 computes; each thread copies and later reads only
+        // its own phase-1 cell.  Within a step nothing writes what is copied: active
+        // blocks write their other buffer, which no neighbour reads this step (a
+        // neighbour reads an active block's current buffer).
         auto neighbourhood = [&](int entry, int buf) {
             if (tid < RB * RB) {
                 const int tbx = entry & 0x7fff, tby = (entry >> 15) & 0x7fff;
@@ -289,7 +303,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                 const int par = s_npar[buf][r1];
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
-                    cp_async_elem<sizeof(R)>(sStage + q * S::N1 + tid, (act ? P.U[q][par] : P.W[q]) + gi);
+                    cp_async_elem<sizeof(R)>(sStage + q * S::N1 + tid, P.U[q][act ? par : par ^ 1] + gi);
             }
             cp_async_commit();
         };
@@ -316,14 +330,10 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
             if (h1) {
                 const R v0 = sStage[tid], v1 = sStage[S::N1 + tid], v2 = sStage[2 * S::N1 + tid],
                         v3 = sStage[3 * S::N1 + tid];
-                if (s_nact[nb][r1]) {
-                    R r, pp, u, v;
-                    kh_prim_of<R>(v0, v1, v2, v3, K, r, pp, u, v);
-                    if (in1) sU.put(y1 * T + x1, Q{v0, v1, v2, v3});
-                    sW.put(s1, Q{r, pp, u, v});
-                } else {
-                    sW.put(s1, Q{v0, v1, v2, v3});
-                }
+                R r, pp, u, v;
+                kh_prim_of<R>(v0, v1, v2, v3, K, r, pp, u, v);
+                if (in1 && s_nact[nb][r1]) sU.put(y1 * T + x1, Q{v0, v1, v2, v3});
+                sW.put(s1, Q{r, pp, u, v});
             }
             __syncthreads();
             if (i + 1 < cnt) prefetch(tile_at(s_tile[i + 1]), nb ^ 1);
@@ -415,12 +425,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                     atomicMax(&s_vblk[ukb], __float_as_uint(kh_speed<R>(r, pp, uu, vv, K.gam)));
                 }
                 if (DBA && !s_nx[ukb]) {
-                    const int si = (uy + 2) * P2 + ux + 2, pi = (uy + 1) * P1 + ux + 1;
-                    const Q w = sW(si);
-                    P.W[0][gi] = w.a;
-                    P.W[1][gi] = w.b;
-                    P.W[2][gi] = w.c;
-                    P.W[3][gi] = w.d;
+                    const int pi = (uy + 1) * P1 + ux + 1;
                     const int bxl = ux % B, byl = uy % B;
                     if (bxl == 0 || bxl == B - 1 || byl == 0 || byl == B - 1) {
                         const Q hp = sP(pi), gx = sGx(pi), gy = sGy(pi);

@@ -106,6 +106,8 @@ def load_library():
             "dba_step": (_i, [V, _i, _i]),
             "dba_sync": (_i, [V]),
             "dba_read_field": (_i, [V, _i, P(_d)]),
+            "dba_read_field_f32": (_i, [V, _i, P(ctypes.c_float)]),
+            "dba_init_f32": (_i, [V, P(ctypes.c_float)]),
             "dba_read_flags": (_i, [V, _i, P(ctypes.c_int32)]),
             "dba_observables": (_i, [V, P(Obs)]),
             "dba_tip": (_i, [V, P(_d)]),
@@ -211,6 +213,28 @@ class Simulation:
             a = np.ascontiguousarray(np.concatenate([np.asarray(f, np.float64).ravel() for f in ic]))
             _check(self._L.dba_init(self._h, a.ctypes.data_as(ctypes.POINTER(_d))), "dba_init")
         return self
+
+    def init_f32(self, ic):
+        """dba_init from FP32 host fields: `ic` is a C-contiguous float32 array holding the
+        initial fields one after another (dendrite p, T; Model B x, y, z; KH rho, p, vx, vy),
+        for instance page-locked memory, which the device copies from at full link speed."""
+        nic = {0: 2, 1: 3, 2: 4}[self.cfg.model]
+        if ic.dtype != np.float32 or not ic.flags.c_contiguous or ic.size != nic * self.n:
+            raise ValueError("ic must be a C-contiguous float32 array of the initial fields")
+        _check(self._L.dba_init_f32(self._h, ic.ctypes.data_as(ctypes.POINTER(ctypes.c_float))), "dba_init_f32")
+        return self
+
+    def field_f32(self, name, out=None):
+        """Current values of a field rounded to float32 (dba_read_field_f32), shape (nz, ny, nx);
+        `out` as in field() but float32."""
+        fid = self._fid(name)
+        if out is None:
+            out = np.empty(self.n, np.float32)
+        elif out.dtype != np.float32 or out.size != self.n or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of %d elements" % self.n)
+        _check(self._L.dba_read_field_f32(self._h, fid, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))),
+               "dba_read_field_f32")
+        return out.reshape(self.shape)
 
     def step(self, n=1, mode=1):
         _check(self._L.dba_step(self._h, int(n), int(mode)), "dba_step")

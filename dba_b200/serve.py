@@ -70,12 +70,14 @@ def _done(tip, edge, target):
 
 class SweepServer:
     def __init__(self, precision=1, block=8, max_slots=128, block_capacity=1 << 17, cell_capacity=0, chunk=96,
-                 target=0.8, max_steps=200000, threads=256, batch=None):
+                 target=0.8, max_steps=200000, threads=256, batch=None, persistent=1):
         """`batch`: an object with the engine.Batch methods add / remove / step / tips /
-        field / sync / close to serve from (default: a new engine.Batch on the current device)."""
+        field / sync / close to serve from (default: a new engine.Batch on the current device,
+        with persistent (1) or per-step (0) launches)."""
         if batch is None:
             batch = engine.Batch(precision=precision, block=block, max_slots=max_slots,
                                  block_capacity=block_capacity, cell_capacity=cell_capacity, threads=threads)
+            batch.set_option(engine.BATCH_PERSISTENT, persistent)
         self.batch = batch
         self.precision, self.block, self.chunk = precision, block, chunk
         self.target, self.max_steps = target, max_steps
@@ -180,8 +182,9 @@ def main(argv=None):
     ap.add_argument("--block", type=int, default=8)
     ap.add_argument("--threads", type=int, default=256)
     ap.add_argument("--chunk", type=int, default=96)
+    ap.add_argument("--persistent", type=int, default=1, help="1 persistent batch launches, 0 one launch per step")
     a = ap.parse_args(argv)
-    srv = SweepServer(precision=a.precision, block=a.block, threads=a.threads, chunk=a.chunk)
+    srv = SweepServer(precision=a.precision, block=a.block, threads=a.threads, chunk=a.chunk, persistent=a.persistent)
     res = srv.run(sweep_requests(n=a.requests, rate=a.rate, seed=a.seed))
     srv.close()
     print(json.dumps(summarize(res)))

@@ -152,6 +152,11 @@ int dba_create(const dba_config* cfg, dba_ctx** out);
  * fields, each nx*ny*nz x-fastest: dendrite p,T; Model B x,y,z; KH rho,p,vx,vy.
  * All blocks start active; the step counter is reset. */
 int dba_init(dba_ctx* ctx, const double* ic);
+/* dba_init from FP32 host fields (no counterpart in the reference: its fields are FP64).
+ * Same layout and meaning as dba_init's `ic` (non-null).  An FP32 context copies them to
+ * the device as they are (page-locked host memory moves at full link speed); an FP64 context
+ * or a KH context converts them to FP64 first. */
+int dba_init_f32(dba_ctx* ctx, const float* ic);
 
 /* Replaces the body of the time loop of main()
  * (example_Dendritic_growth/kernel.cu:913-990, example_Reactive_ModelB/kernel.cu:1057-1161,
@@ -170,6 +175,10 @@ int dba_sync(dba_ctx* ctx);
  * 4 mu_x, 5 mu_y, 6 mu_z; KH 0 Mass, 1 Momx, 2 Momy, 3 Energy, 4 rho, 5 p,
  * 6 vx, 7 vy (primitives recomputed from the conserved fields). */
 int dba_read_field(dba_ctx* ctx, int field, double* host);
+/* dba_read_field into an FP32 host array of nx*ny*nz values (no counterpart in the
+ * reference): the values dba_read_field returns, rounded to float.  For the state fields of
+ * an FP32 context this moves half the bytes over the host link. */
+int dba_read_field_f32(dba_ctx* ctx, int field, float* host);
 
 /* Replaces the host reads of wake_up / wake_up_next (Output_wakeup,
  * example_Dendritic_growth/kernel.cu:711-757): which = 2*channel + 0 for the

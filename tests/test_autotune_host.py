@@ -38,23 +38,24 @@ def test_tune_picks_fastest_and_caches(tmp_path, monkeypatch):
     scores = {(8, 128): 1.0, (8, 256): 3.0, (8, 512): 2.0, (16, 128): 0.5, (16, 256): 2.5, (16, 512): 2.9}
     calls = []
 
-    def fake_time(block, threads=256, precision=1, **kw):
-        calls.append((block, threads, precision))
-        return scores[(block, threads)]
+    def fake_time(block, threads=256, precision=1, persistent=1, **kw):
+        calls.append((block, threads, precision, persistent))
+        # the per-step form wins for block 8 threads 256 only
+        return scores[(block, threads)] + (0.1 if (block, threads, persistent) == (8, 256, 0) else 0.0)
 
     monkeypatch.setattr(autotune, "time_candidate", fake_time)
     c = autotune.tune(precision=1, use_cache=True)
-    assert (c["block"], c["threads"]) == (8, 256)
+    assert (c["block"], c["threads"], c["persistent"]) == (8, 256, 0)
     assert c["chunk"] == 96 and c["chunk"] / 2 <= 0.05 * autotune.SHORTEST_RUN_STEPS
-    assert len(calls) == len(scores)
+    assert len(calls) == 2 * len(scores)
     stored = json.load(open(cache))
     assert list(stored.values())[0]["block"] == 8
     # cached: no new timing runs
     c2 = autotune.tune(precision=1, use_cache=True)
-    assert len(calls) == len(scores) and (c2["block"], c2["threads"]) == (8, 256)
+    assert len(calls) == 2 * len(scores) and (c2["block"], c2["threads"]) == (8, 256)
     # other precision: a separate entry
     autotune.tune(precision=0, use_cache=True)
-    assert len(calls) == 2 * len(scores) and len(json.load(open(cache))) == 2
+    assert len(calls) == 4 * len(scores) and len(json.load(open(cache))) == 2
 
 
 def test_cache_key_follows_the_current_device(tmp_path, monkeypatch):
@@ -65,7 +66,7 @@ def test_cache_key_follows_the_current_device(tmp_path, monkeypatch):
     dev = _fake_torch(monkeypatch)
     calls = []
 
-    def fake_time(block, threads=256, precision=1, **kw):
+    def fake_time(block, threads=256, precision=1, persistent=1, **kw):
         calls.append(dev.cur)
         return float(block * threads) if dev.cur == 0 else float(1000 - block * threads)
 
@@ -85,7 +86,8 @@ def test_tune_without_cache_leaves_no_file(tmp_path, monkeypatch):
     cache = tmp_path / "none.json"
     monkeypatch.setenv("DBA_AUTOTUNE_CACHE", str(cache))
     _fake_torch(monkeypatch)
-    monkeypatch.setattr(autotune, "time_candidate", lambda block, threads=256, precision=1, **kw: block * threads)
+    monkeypatch.setattr(autotune, "time_candidate",
+                        lambda block, threads=256, precision=1, persistent=1, **kw: block * threads + persistent)
     c = autotune.tune(precision=1, use_cache=False)
     assert (c["block"], c["threads"]) == (16, 512)
     assert not cache.exists()

@@ -247,3 +247,27 @@ def test_field_into_caller_buffer():
         s.field("x", out=np.empty(10))
     with pytest.raises(ValueError):
         s.field("x", out=np.empty(64 * 64, np.float32))
+
+
+@pytest.mark.parametrize("model", ["dendrite", "modelb", "kh"])
+def test_fp32_init_and_readback(model):
+    """dba_init_f32 gives the same run as dba_init with the same values in FP64, and
+    dba_read_field_f32 returns dba_read_field's values rounded to float."""
+    if model == "dendrite":
+        cfg = dendrite_cfg(DENDRITE_REF, 64, 64, 1, 8, precision=1)
+    elif model == "modelb":
+        cfg = modelb_cfg(dict(MODELB_REF, metric_eps=1e-3), 64, 64, 1, 16, precision=1, conserved=1)
+    else:
+        cfg = kh_cfg(dict(KH_REF, metric_eps=10.0), 64, 64, 8, precision=1)
+    a = dba_b200.Simulation(cfg).init()
+    nic = {"dendrite": 2, "modelb": 3, "kh": 4}[model]
+    names = a.fields[:nic] if model != "kh" else ["rho", "p", "vx", "vy"]
+    ic = np.concatenate([a.field_f32(f).ravel() for f in names]).astype(np.float32)
+    b = dba_b200.Simulation(cfg).init_f32(ic)
+    c = dba_b200.Simulation(cfg).init([ic[k * a.n:(k + 1) * a.n].astype(np.float64) for k in range(nic)])
+    for s in (b, c):
+        s.step(30, 1)
+    for f in b.fields[:nic]:
+        assert np.array_equal(b.field(f), c.field(f)), f
+        assert np.array_equal(b.field_f32(f), c.field(f).astype(np.float32)), f
+    b.sync()

@@ -71,3 +71,36 @@ def test_union_retry_limit_reports_timeout():
     with pytest.raises(dba_b200.DBAError) as e:
         s.sync()
     assert e.value.code == 6
+
+
+def _ref_post():
+    import os
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    import make_post_golden as mpg
+    return mpg, np.load(os.path.join(here, "golden", "ref_post.npz"))
+
+
+def test_tip_profile_matches_reference_tool():
+    """dba_tip_profile on a resident 64^3 field against Tip_Profile.dat of the reference's
+    own Extract_Tip on the same field (tests/golden/make_post_golden.py)."""
+    mpg, g = _ref_post()
+    f = mpg.tip_field()
+    s = dba_b200.Simulation(dendrite_cfg(DENDRITE_REF, 64, 64, 64, 8)).init([f, np.zeros_like(f)])
+    tip, m = s.tip_profile(40)
+    assert np.array_equal(np.stack([np.arange(41), m - tip], axis=1), g["tip_profile"])
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_size_distribution_matches_reference_tool(prec):
+    """dba_size_distribution on a resident 256^3 Model B z field against size_dist.txt and
+    avg_radius.txt of the reference's own coarsening_analysis on the same field."""
+    mpg, g = _ref_post()
+    z = mpg.sphere_field(g["spheres"])
+    s = dba_b200.Simulation(modelb_cfg(MB, 256, 256, 256, 8, precision=prec)).init(
+        [np.full_like(z, 0.03125), np.full_like(z, 0.03125), z])
+    avg, vol, sizes = s.size_distribution("z")
+    assert np.array_equal(sizes, g["sizes"])
+    assert float(f"{np.cbrt(vol * 0.75 / np.pi / len(sizes)):.6g}") == float(g["avg_radius"])
+    s.sync()

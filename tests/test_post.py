@@ -1,5 +1,7 @@
-"""CPU restatement of the reference's post-processing tools, pinned to hand-made
-fields with known answers (Extract_Tip.cpp:68-87, coarsening_analysis.cpp:46-165)."""
+"""CPU restatement of the reference's post-processing tools (Extract_Tip.cpp:68-87,
+coarsening_analysis.cpp:46-165), pinned two ways: hand-made fields with known
+answers, and the outputs of the reference's own tools, built from their sources,
+on seeded fields (tests/golden/ref_post.npz, tests/golden/make_post_golden.py)."""
 import numpy as np
 
 import oracle_lib as ol
@@ -34,3 +36,31 @@ def test_tip_profile_known_answer():
     g[2, 0, :] = 1.0                          # below the window (z < Nz/2): ignored
     tip, m = ol.tip_profile(g, dz=4)
     assert tip.tolist() == [6, 2, 10, 0, 0] and m == 10
+
+
+def _ref_post():
+    import os
+    import sys
+    here = os.path.dirname(os.path.abspath(__file__))
+    sys.path.insert(0, os.path.join(here, "golden"))
+    import make_post_golden as mpg
+    return mpg, np.load(os.path.join(here, "golden", "ref_post.npz"))
+
+
+def test_tip_profile_restatement_matches_reference_tool():
+    """The restatement against Tip_Profile.dat written by the reference's own Extract_Tip
+    (example_Dendritic_growth/Extract_Tip.cpp:68-108) on the same 64^3 field."""
+    mpg, g = _ref_post()
+    tip, m = ol.tip_profile(mpg.tip_field())
+    assert np.array_equal(np.stack([np.arange(41), m - tip], axis=1), g["tip_profile"])
+
+
+def test_size_distribution_restatement_matches_reference_tool():
+    """The restatement against size_dist.txt / avg_radius.txt written by the reference's own
+    coarsening_analysis (example_Reactive_ModelB/coarsening_analysis.cpp:46-199) on the same
+    256^3 field (its grid size is fixed at 256^3)."""
+    mpg, g = _ref_post()
+    avg, vol, sizes = ol.size_distribution(mpg.sphere_field(g["spheres"]))
+    assert np.array_equal(sizes, g["sizes"])
+    r = np.cbrt(vol * 0.75 / np.pi / len(sizes))
+    assert float(f"{r:.6g}") == float(g["avg_radius"])
