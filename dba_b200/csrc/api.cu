@@ -492,6 +492,55 @@ int gather(dba_ctx* c, const void* b0, const void* b1, const uint8_t* par, size_
     return cuda_status(cudaStreamSynchronize(c->st));
 }
 
+// rows [row0, row0 + nrows) of the two dendrite fields (p, T), current values (each
+// field's channel parity per block), packed field after field into out; or unpacked from
+// in into both buffers of those rows (the slab exchange's ghost rows)
+struct RowsP {
+    void* f[2][2];   // [field][buffer]
+    const uint8_t* par;
+    int nb, nx, B, nbx, row0, nrows;
+};
+
+template <typename R>
+__global__ void rows_pack_kernel(RowsP P, R* out)
+{
+    const size_t per = (size_t)P.nrows * P.nx, n = 2 * per;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int q = i < per ? 0 : 1;
+        const size_t k = i - (size_t)q * per;
+        const int y = P.row0 + (int)(k / P.nx), x = (int)(k % P.nx);
+        const int b = x / P.B + P.nbx * (y / P.B);
+        out[i] = ((const R*)P.f[q][P.par[(size_t)q * P.nb + b] ? 1 : 0])[(size_t)y * P.nx + x];
+    }
+}
+
+template <typename R>
+__global__ void rows_unpack_kernel(RowsP P, const R* in)
+{
+    const size_t per = (size_t)P.nrows * P.nx, n = 2 * per;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int q = i < per ? 0 : 1;
+        const size_t gi = (size_t)P.row0 * P.nx + (i - (size_t)q * per);
+        ((R*)P.f[q][0])[gi] = in[i];
+        ((R*)P.f[q][1])[gi] = in[i];
+    }
+}
+
+// next-step wake flags of block rows [brow0, brow0 + nbrows) of every channel: read into
+// out ([channel][nbrows * nbx]), OR-ed in from in, or cleared
+__global__ void flag_rows_kernel(uint8_t* wake, int nch, int nb, int nbx, int brow0, int nbrows, uint8_t* out,
+                                 const uint8_t* in, int op)
+{
+    const int per = nbrows * nbx, n = per * nch;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int ch = i / per, k = i - ch * per;
+        uint8_t* w = wake + (size_t)ch * nb + (size_t)brow0 * nbx + k;
+        if (op == 0) out[i] = *w ? 1 : 0;
+        else if (op == 1) *w = (*w || in[i]) ? 1 : 0;
+        else *w = 0;
+    }
+}
+
 __global__ void to_float_kernel(const double* src, float* dst, size_t n)
 {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -932,6 +981,65 @@ int dba_read_field_f32(dba_ctx* c, int field, float* host)
     DBA_TRY(cudaGetLastError());
     DBA_TRY(cudaMemcpyAsync(host, c->fstaging, c->n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
     DBA_TRY(cudaStreamSynchronize(c->st));
+    return DBA_OK;
+}
+
+namespace {
+int slab_check(dba_ctx* c, int row0, int nrows)
+{
+    if (!c) return DBA_ERR_ARG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    const dba_config& k = c->cfg;
+    if (k.model != DBA_MODEL_DENDRITE || k.nz != 1) return DBA_ERR_CONFIG;   // 2-D dendrite slabs only
+    if (row0 < 0 || nrows < 1 || row0 + nrows > k.ny) return DBA_ERR_ARG;
+    return DBA_OK;
+}
+}  // namespace
+
+namespace {
+RowsP rows_params(dba_ctx* c, int row0, int nrows)
+{
+    RowsP P;
+    for (int q = 0; q < 2; ++q)
+        for (int k = 0; k < 2; ++k) P.f[q][k] = c->state[q][k];
+    P.par = cur_par(c);
+    P.nb = c->g.nb; P.nx = c->cfg.nx; P.B = c->B; P.nbx = c->g.nbx; P.row0 = row0; P.nrows = nrows;
+    return P;
+}
+}  // namespace
+
+int dba_rows_pack(dba_ctx* c, int row0, int nrows, void* dev_out)
+{
+    int st = slab_check(c, row0, nrows);
+    if (st) return st;
+    if (!dev_out) return DBA_ERR_ARG;
+    const RowsP P = rows_params(c, row0, nrows);
+    if (c->esz == 8) rows_pack_kernel<double><<<4 * c->sms, 256, 0, c->st>>>(P, (double*)dev_out);
+    else rows_pack_kernel<float><<<4 * c->sms, 256, 0, c->st>>>(P, (float*)dev_out);
+    return cuda_status(cudaGetLastError());
+}
+
+int dba_rows_unpack(dba_ctx* c, int row0, int nrows, const void* dev_in)
+{
+    int st = slab_check(c, row0, nrows);
+    if (st) return st;
+    if (!dev_in) return DBA_ERR_ARG;
+    const RowsP P = rows_params(c, row0, nrows);
+    if (c->esz == 8) rows_unpack_kernel<double><<<4 * c->sms, 256, 0, c->st>>>(P, (const double*)dev_in);
+    else rows_unpack_kernel<float><<<4 * c->sms, 256, 0, c->st>>>(P, (const float*)dev_in);
+    return cuda_status(cudaGetLastError());
+}
+
+int dba_flag_rows(dba_ctx* c, int op, int brow0, int nbrows, void* dev_buf)
+{
+    if (!c) return DBA_ERR_ARG;
+    int st = slab_check(c, brow0 * c->B, nbrows * c->B);
+    if (st) return st;
+    if (op < 0 || op > 2 || (op < 2 && !dev_buf)) return DBA_ERR_ARG;
+    uint8_t* w = c->wake + ((c->step + 1) % 3) * (size_t)c->nch * c->g.nb;   // what the next step reads
+    flag_rows_kernel<<<c->sms, 256, 0, c->st>>>(w, c->nch, c->g.nb, c->g.nbx, brow0, nbrows, (uint8_t*)dev_buf,
+                                                 (const uint8_t*)dev_buf, op);
+    DBA_TRY(cudaGetLastError());
     return DBA_OK;
 }
 

@@ -20,14 +20,21 @@ bool modelb_tiles_ok(int D, int B, int nx, int ny)
     return D == 2 && (B == 8 || B == 16) && nx % MBTile<16>::T == 0 && ny % MBTile<16>::T == 0;
 }
 
+// staging of the tile kernel: bulk copies (1) or 16-byte cp.async pieces (0)
+#ifndef MB_TILE_BULK
+#define MB_TILE_BULK 1
+#endif
+constexpr bool kMBTileBulk = MB_TILE_BULK != 0;
+
 template <int B>
 static int tile_grid_b(int sms, int ntiles)
 {
     const size_t sm = MBTile<B>::smem;
-    cudaFuncSetAttribute(modelb_tile_step<B, kMBTileRows, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaFuncSetAttribute(modelb_tile_step<B, kMBTileRows, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(modelb_tile_step<B, kMBTileRows, true, kMBTileBulk>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(modelb_tile_step<B, kMBTileRows, false, kMBTileBulk>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, modelb_tile_step<B, kMBTileRows, true>, MBTile<B>::NT, sm) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, modelb_tile_step<B, kMBTileRows, true, kMBTileBulk>, MBTile<B>::NT,
+                                                      sm) != cudaSuccess ||
         occ < 1)
         occ = 1;
     const int g = occ * sms;
@@ -67,8 +74,8 @@ cudaError_t launch_modelb_tiles(int B, bool dba_mode, int grid, cudaStream_t st,
 #define XT(b)                                                                                         \
     if (B == b) {                                                                                     \
         const size_t sm = MBTile<b>::smem;                                                            \
-        if (dba_mode) modelb_tile_step<b, kMBTileRows, true><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, K, Q, L);   \
-        else modelb_tile_step<b, kMBTileRows, false><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, K, Q, L);           \
+        if (dba_mode) modelb_tile_step<b, kMBTileRows, true, kMBTileBulk><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, K, Q, L);   \
+        else modelb_tile_step<b, kMBTileRows, false, kMBTileBulk><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, K, Q, L);           \
         return cudaGetLastError();                                                                    \
     }
     XT(8) XT(16)

@@ -109,18 +109,12 @@ struct QA {
     }
 };
 
-#ifndef KH_TILE_MINB_DBA_F32
-#define KH_TILE_MINB_DBA_F32 3   // resident CTAs per SM of the FP32 DBA variant
-#endif
-
 template <typename R, int B> struct KHTile {
     // 13 warps: every staging phase below is one item per thread (400 primitive
     // cells, 320 gradient cells, 288 face pairs, 256 updates), so no warp runs a
     // second round while the others wait at the phase's barrier
     static constexpr int NT = 416;
     static constexpr int MINB = sizeof(R) == 4 ? 3 : 2;   // resident CTAs per SM
-    // the DBA variant (wake-up metric, persistence) under its own occupancy target
-    static constexpr int MINB_DBA = sizeof(R) == 4 ? KH_TILE_MINB_DBA_F32 : 2;
     static constexpr int T = 16;               // tile edge in cells
     static constexpr int TB = T / B;           // blocks per tile edge
     static constexpr int NBT = TB * TB;
@@ -147,8 +141,7 @@ template <int B, int RB>
 __device__ __forceinline__ int kh_region(int lx, int ly) { return (lx + B) / B + RB * ((ly + B) / B); }
 
 template <typename R, int B, bool DBA>
-__global__ void __launch_bounds__(KHTile<R, B>::NT, DBA ? KHTile<R, B>::MINB_DBA : KHTile<R, B>::MINB)
-    kh_tile_step(GridP g, FlagP f, KHTileP<R> P)
+__global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_step(GridP g, FlagP f, KHTileP<R> P)
 {
     using S = KHTile<R, B>;
     constexpr int NT = S::NT, T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, TPP = S::TPP;

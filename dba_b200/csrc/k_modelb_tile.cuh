@@ -8,9 +8,13 @@
 //     and only active blocks' cells are updated; inactive blocks inside a
 //     listed tile contribute their persisted potentials, exactly as inactive
 //     neighbour blocks do (stale-read rule, kernel.cu:594-654);
-//   * the tile plus a 2-cell halo of x, y, z is staged with 16-byte cp.async
-//     copies, double-buffered: tile i+1 is in flight while tile i computes.
-//     Each 16-byte piece lies inside one block, whose parity picks the buffer;
+//   * the tile plus a 2-cell halo of x, y, z is staged double-buffered (tile
+//     i+1 in flight while tile i computes) by the TMA engine: one thread per
+//     staged row and field issues one bulk copy (cp.async.bulk) per block
+//     segment of the row -- the 4-cell halo on each side and one B-wide
+//     segment per block -- from the buffer that block's parity picks; the
+//     copies complete on the stage's mbarrier (bounded wait).  The alternative
+//     form (BULK = false) spreads 16-byte cp.async pieces over the CTA;
 //   * each thread owns a 4-column x R-row patch (R = kMBTileRows; 256 / R
 //     threads per CTA).  A staged row of the patch is one 16-byte shared load,
 //     its left and right neighbours taken from the adjacent lanes;
@@ -146,7 +150,48 @@ __device__ __forceinline__ f2 ring_lap_v(const MBPairP& K, const float* s, int i
 
 __device__ __forceinline__ float4 f4_of(f2 a, f2 b) { return make_float4(f2_lo(a), f2_hi(a), f2_lo(b), f2_hi(b)); }
 
-template <int B, int R, bool DBA>
+// ---- bulk-copy staging (the TMA engine's non-tensor copies, completion on an mbarrier)
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* m, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// this phase's single arrival, announcing `bytes` of copies that complete on it
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* m, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(m)), "r"(bytes) : "memory");
+}
+// global -> shared copy of `bytes` (16-byte aligned addresses, a multiple of 16 bytes), counted on m
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* m)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(m)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned long long* m, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(m)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// Wait for the phase of m with the given parity.  Bounded: after 2^22 polls the
+// status word gets DBA_ERR_TIMEOUT (6); the wait then goes on, again bounded, for
+// the copies still in flight into this CTA's shared memory before the caller
+// continues (their results are then flagged as unusable by the status).
+__device__ __forceinline__ void mbar_wait(unsigned long long* m, unsigned parity, int* status)
+{
+    for (int it = 0; it < (1 << 22); ++it)
+        if (mbar_test(m, parity)) return;
+    raise_status(status, 6);
+    for (int it = 0; it < (1 << 22); ++it)
+        if (mbar_test(m, parity)) return;
+}
+
+// BULK: stage each tile row as one bulk copy per block segment (cp.async.bulk, completion
+// on a per-stage mbarrier), issued by one thread per staged row and field; otherwise
+// 16-byte cp.async pieces spread over the CTA
+template <int B, int R, bool DBA, bool BULK>
 __global__ void __launch_bounds__(256 / R, 4)
     modelb_tile_step(GridP g, FlagP f, MBFastP P, MBPairP K, MBFastBuf Q, LazyP L)
 {
@@ -164,6 +209,8 @@ __global__ void __launch_bounds__(256 / R, 4)
     __shared__ int s_nx[2][NBT];         // wake tests of the blocks of tiles with parity 0 / 1
     __shared__ float s_Cf[3];
     __shared__ unsigned long long s_fix[3];
+    __shared__ __align__(8) unsigned long long s_mbar[2];   // BULK: completion of stage 0 / 1
+    unsigned mb_phase = 0;                                   // BULK: parity of each stage's next phase (bits 0, 1)
 
     const int tid = threadIdx.x;
     const int G = gridDim.x;
@@ -172,6 +219,11 @@ __global__ void __launch_bounds__(256 / R, 4)
     if (tid < 3) {
         s_Cf[tid] = lazy_offset(L, tid);
         s_fix[tid] = 0ull;
+    }
+    if (BULK && tid == 0) {
+        mbar_init(&s_mbar[0], 1);
+        mbar_init(&s_mbar[1], 1);
+        mbar_init_fence();
     }
 
     // per-thread constants: staging column and rows (thread q_c + QC q_r takes
@@ -212,7 +264,38 @@ __global__ void __launch_bounds__(256 / R, 4)
             s_nact[st][tid] = (uint8_t)nb_act;
         }
     };
+    // BULK staging of a tile: thread f * SR + r copies staged row r of field f as one bulk
+    // copy per block segment of the row (columns -4 .. -1, then B-wide segments, then
+    // T .. T+3), each from the buffer its block's parity picks; 3 * SR * (T + 8) * 4 bytes
+    // complete on the stage's mbarrier, whose arrival thread 0 posts before the copies
+    constexpr int NSEG = T / B + 2;
+    constexpr unsigned STAGE_BYTES = 3u * S::SR * (T + 8) * sizeof(float);
+    auto issue_bulk = [&](int tbx, int tby, int st) {
+        if (tid < 3 * S::SR) {
+            // the stage's previous contents were read through the generic proxy (ordered by the
+            // barrier before this call); order those reads before the async-proxy writes
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            const int fq = tid / S::SR, r = tid - fq * S::SR;
+            const int X0 = tbx * T, Y0 = tby * T;
+            const int ry = (r - 2 + B) / B;
+            const float* b0 = fq == 0 ? Q.x[0] : (fq == 1 ? Q.y[0] : Q.z[0]);
+            const float* b1 = fq == 0 ? Q.x[1] : (fq == 1 ? Q.y[1] : Q.z[1]);
+            float* drow = stage + st * 3 * SV + fq * SV + r * SP + 4;   // column c at drow[c]
+            const size_t grow = (size_t)wrap_p(Y0 + r - 2, g.ny) * nx;
+#pragma unroll
+            for (int k = 0; k < NSEG; ++k) {
+                const int c0 = k == 0 ? -4 : (k - 1) * B, c1 = k == NSEG - 1 ? T + 4 : k * B;
+                const int par = s_npar[st][(c0 + B) / B + RB * ry];
+                bulk_g2s(drow + c0, (par ? b1 : b0) + grow + wrap_p(X0 + c0, g.nx), (unsigned)(c1 - c0) * 4u,
+                         &s_mbar[st]);
+            }
+        }
+    };
     auto issue = [&](int tbx, int tby, int st) {
+        if (BULK) {
+            issue_bulk(tbx, tby, st);
+            return;
+        }
         if (q_on) {
             const int X0 = tbx * T, Y0 = tby * T;
             float* dst = stage + st * 3 * SV + q_soff;
@@ -273,6 +356,7 @@ __global__ void __launch_bounds__(256 / R, 4)
             nbr_load(tbx, tby);
             nbr_store(0);
             if (tid < NBT) s_nx[0][tid] = 0;
+            if (BULK && tid == 0) mbar_expect_tx(&s_mbar[0], STAGE_BYTES);
             __syncthreads();
             issue(tbx, tby, 0);
             if (cnt > 1) {
@@ -284,7 +368,14 @@ __global__ void __launch_bounds__(256 / R, 4)
         for (int i = 0; i < cnt; ++i) {
             const int st = i & 1;
             if (i + 1 < cnt) nbr_store(st ^ 1);  // table of tile i + 1, loaded one tile ago
-            cp_async_wait0();
+            if (BULK) {
+                mbar_wait(&s_mbar[st], (mb_phase >> st) & 1u, f.status);
+                mb_phase ^= 1u << st;
+                // the next phase of the other stage (its last phase completed for tile i - 1)
+                if (i + 1 < cnt && tid == 0) mbar_expect_tx(&s_mbar[st ^ 1], STAGE_BYTES);
+            } else {
+                cp_async_wait0();
+            }
             __syncthreads();                     // tile i staged, table i + 1 stored; tile i - 1 done
             // tile i - 1 has been read by every thread, so its stage buffer, the
             // potentials and the wake tests of parity st ^ 1 are free: stage tile i + 1

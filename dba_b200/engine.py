@@ -142,6 +142,9 @@ def load_library():
             "dba_batch_destroy": (None, [V]),
             "dba_batch_set_option": (_i, [V, _i, ctypes.c_longlong]),
             "dba_set_option": (_i, [V, _i, ctypes.c_longlong]),
+            "dba_rows_pack": (_i, [V, _i, _i, V]),
+            "dba_rows_unpack": (_i, [V, _i, _i, V]),
+            "dba_flag_rows": (_i, [V, _i, _i, _i, V]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -309,6 +312,16 @@ class Simulation:
             return self.size_distribution(field, int(nis.value))
         _check(st, "dba_size_distribution")
         return avg.value, vol.value, sizes[:nis.value].copy()
+
+    def rows_pack(self, row0, nrows, dev_ptr):
+        _check(self._L.dba_rows_pack(self._h, int(row0), int(nrows), ctypes.c_void_p(dev_ptr)), "dba_rows_pack")
+
+    def rows_unpack(self, row0, nrows, dev_ptr):
+        _check(self._L.dba_rows_unpack(self._h, int(row0), int(nrows), ctypes.c_void_p(dev_ptr)), "dba_rows_unpack")
+
+    def flag_rows(self, op, brow0, nbrows, dev_ptr=0):
+        _check(self._L.dba_flag_rows(self._h, int(op), int(brow0), int(nbrows), ctypes.c_void_p(dev_ptr)),
+               "dba_flag_rows")
 
     def set_option(self, option, value):
         """dba_set_option: OPT_WAIT_LIMIT bounds the device retry loops (post-processing)."""

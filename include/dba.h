@@ -334,6 +334,22 @@ int dba_tip_profile(dba_ctx* ctx, int field, int dz, int* tip_x, int* tip_x_max)
 int dba_size_distribution(dba_ctx* ctx, int field, double* avg, long* volume, long* islands, long* sizes,
                           long max_sizes);
 
+/* ---- one 2-D dendrite domain split into y-slabs across contexts (one per GPU) ----
+   The reference's CUDA-MPI programs (example_Dendritic_growth/CUDA-MPI/dendrite.cpp:387-397,
+   459-644) split the domain across ranks and exchange halo layers and wake flags each step.
+   Here each rank's context holds its slab plus one ghost block row on each side
+   (dba_b200/slabs.py drives the exchange over torch.distributed).  All three calls are
+   asynchronous on the context's stream, take device pointers and work between steps.
+     dba_rows_pack   current values of p then T of rows [row0, row0 + nrows) -> dev_out
+                     (2 * nrows * nx values of the context's precision)
+     dba_rows_unpack the same layout from dev_in into both buffers of those rows
+     dba_flag_rows   the next step's wake flags of block rows [brow0, brow0 + nbrows), both
+                     channels (p then T, nbrows * nbx bytes each): op 0 copies them to dev_buf,
+                     op 1 ORs dev_buf into them, op 2 clears them (dev_buf unused). */
+int dba_rows_pack(dba_ctx* ctx, int row0, int nrows, void* dev_out);
+int dba_rows_unpack(dba_ctx* ctx, int row0, int nrows, const void* dev_in);
+int dba_flag_rows(dba_ctx* ctx, int op, int brow0, int nbrows, void* dev_buf);
+
 /* Context options (no counterpart in the reference).
  *   DBA_OPT_WAIT_LIMIT  attempts a bounded device retry loop makes before it gives up
  *                       (default 1 << 20): the union step of dba_size_distribution, whose

@@ -772,6 +772,13 @@ void oracle_dendrite_get(void* h, double* p, double* T, int* wake_p, int* wake_T
     if (next_p) std::memcpy(next_p, d->next_p.data(), nb);
     if (next_T) std::memcpy(next_T, d->next_T.data(), nb);
 }
+void oracle_dendrite_set_flags(void* h, const int* wake_p, const int* wake_T)
+{
+    auto* d = (Dendrite*)h;
+    size_t nb = d->g.nb() * sizeof(int);
+    std::memcpy(d->wake_p.data(), wake_p, nb);
+    std::memcpy(d->wake_T.data(), wake_T, nb);
+}
 double oracle_dendrite_tip(void* h) { return ((Dendrite*)h)->tip(); }
 void oracle_dendrite_free(void* h) { delete (Dendrite*)h; }
 

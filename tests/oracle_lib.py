@@ -32,6 +32,7 @@ def lib():
             "oracle_dendrite_step": (None, [vp, ctypes.c_int, ctypes.c_int]),
             "oracle_dendrite_get": (None, [vp, _D, _D, _I, _I, _I, _I]),
             "oracle_dendrite_tip": (ctypes.c_double, [vp]),
+            "oracle_dendrite_set_flags": (None, [vp, _I, _I]),
             "oracle_tip_profile": (None, [_D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _I,
                                           ctypes.POINTER(ctypes.c_int)]),
             "oracle_size_distribution": (ctypes.c_long, [_D, ctypes.c_int, ctypes.c_int, ctypes.c_int, _D,
@@ -94,6 +95,11 @@ class OracleDendrite:
         p = np.ascontiguousarray(p, dtype=np.float64)
         T = np.ascontiguousarray(T, dtype=np.float64)
         lib().oracle_dendrite_set(self.h, dptr(p), dptr(T))
+
+    def set_flags(self, wake_p, wake_T):
+        a = np.ascontiguousarray(wake_p, dtype=np.int32)
+        b = np.ascontiguousarray(wake_T, dtype=np.int32)
+        lib().oracle_dendrite_set_flags(self.h, iptr(a), iptr(b))
 
     def step(self, n=1, mode=1):
         lib().oracle_dendrite_step(self.h, n, mode)
