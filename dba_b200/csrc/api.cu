@@ -62,7 +62,7 @@ struct dba_ctx {
     // FP32 2-D Model B conserved: lazy correction state (k_modelb_fast.cuh)
     bool lazy = false;
     long long wait_limit = 1LL << 20;  // attempts of a bounded device retry loop (DBA_OPT_WAIT_LIMIT)
-    bool tiles = false;               // FP32 2-D Model B on 32x32-cell tiles (k_modelb_tile.cuh)
+    int tiles = 0;                    // FP32 2-D Model B on 32x32-cell tiles (k_modelb_tile.cuh): 1 cp.async, 2 bulk staging
     float* fstaging = nullptr;        // dba_read_field_f32: a field as floats (allocated on first use)
     bool kh_tiles = false;            // KH one-kernel step on 16x16-cell tiles (k_kh_tile.cuh)
     bool den_tiles = false;           // FP32 3-D dendrite on 32x8x8-cell tiles (k_dendrite_tile.cuh)
@@ -718,7 +718,7 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
         c->grid = c->esz == 8 ? kh_tile_grid<double>(c->B, c->sms, nt) : kh_tile_grid<float>(c->B, c->sms, nt);
     }
     if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->tiles && modelb_tiles_ok(c->D, c->B, cfg->nx, cfg->ny)) {
-        c->tiles = true;
+        c->tiles = cfg->tiles == 2 ? 2 : 1;
         c->grid = modelb_tile_grid(c->B, c->sms, (cfg->nx / 32) * (cfg->ny / 32));
     }
     if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->conserved && modelb_uses_fast<float>(c->D, c->B)) {

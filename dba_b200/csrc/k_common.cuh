@@ -117,6 +117,26 @@ __device__ __forceinline__ void wake_faces_2d(uint8_t* w, int bx, int by, int nb
     w[bx + (by == nby - 1 ? 0 : by + 1) * nbx] = 1;
 }
 
+// Neighbour k of block (bx, by, bz) for the wake-up scatter, from block coordinates
+// (no division), one neighbour per calling thread: k = 0 the block itself, 1..6 the
+// faces -x, +x, -y, +y, -z, +z, 7..10 the in-plane diagonals (-1,-1), (-1,+1),
+// (+1,-1), (+1,+1).  Periodic wrap, or -1 off a zero-flux edge, as block_nb.
+__device__ __forceinline__ int block_nb_k(const GridP& g, int bx, int by, int bz, int k)
+{
+    const int dx = (k == 1 || k == 7 || k == 8) ? -1 : ((k == 2 || k == 9 || k == 10) ? 1 : 0);
+    const int dy = (k == 3 || k == 7 || k == 9) ? -1 : ((k == 4 || k == 8 || k == 10) ? 1 : 0);
+    const int dz = k == 5 ? -1 : (k == 6 ? 1 : 0);
+    bx += dx; by += dy; bz += dz;
+    if (g.bc) {
+        if (bx < 0 || bx >= g.nbx || by < 0 || by >= g.nby || bz < 0 || bz >= g.nbz) return -1;
+    } else {
+        bx = bx < 0 ? g.nbx - 1 : (bx >= g.nbx ? 0 : bx);
+        by = by < 0 ? g.nby - 1 : (by >= g.nby ? 0 : by);
+        bz = bz < 0 ? g.nbz - 1 : (bz >= g.nbz ? 0 : bz);
+    }
+    return bx + g.nbx * (by + g.nby * bz);
+}
+
 // self + faces + 4 in-plane diagonals (example_Kelvin_Helmholtz/KH_DBA.cu:1026-1039)
 __device__ __forceinline__ void wake_faces_diag(const GridP& g, uint8_t* w, int b)
 {

@@ -231,13 +231,18 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
                 int X0, Y0, Z0;
                 tile_xyz(s_tile[i], X0, Y0, Z0);
                 const int b = (X0 / B + tid) + g.nbx * (Y0 / B + g.nby * (Z0 / B));
-                if ((tm >> tid) & 1u) {
-                    f.next[b] = (uint8_t)s_np[tid];
-                    if (s_np[tid]) wake_faces(g, f.wake_nxt, b);
-                }
-                if ((tm >> (4 + tid)) & 1u) {
-                    f.next[nb + b] = (uint8_t)s_nT[tid];
-                    if (s_nT[tid]) wake_faces(g, f.wake_nxt + nb, b);
+                if ((tm >> tid) & 1u) f.next[b] = (uint8_t)s_np[tid];
+                if ((tm >> (4 + tid)) & 1u) f.next[nb + b] = (uint8_t)s_nT[tid];
+            }
+            // wake-up scatter, self + 6 faces per channel (kernel.cu:577-634), one
+            // neighbour per thread: thread (ch * TBX + blk) * 7 + k
+            if (DBA && tid < 2 * TBX * 7) {
+                const int k = tid % 7, cb = tid / 7, ch = cb / TBX, kt = cb - ch * TBX;
+                if (((tm >> (4 * ch + kt)) & 1u) && (ch ? s_nT[kt] : s_np[kt])) {
+                    int X0, Y0, Z0;
+                    tile_xyz(s_tile[i], X0, Y0, Z0);
+                    const int nbk = block_nb_k(g, X0 / B + kt, Y0 / B, Z0 / B, k);
+                    if (nbk >= 0) f.wake_nxt[(size_t)ch * nb + nbk] = 1;
                 }
             }
         }

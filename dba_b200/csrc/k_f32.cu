@@ -20,20 +20,16 @@ bool modelb_tiles_ok(int D, int B, int nx, int ny)
     return D == 2 && (B == 8 || B == 16) && nx % MBTile<16>::T == 0 && ny % MBTile<16>::T == 0;
 }
 
-// staging of the tile kernel: bulk copies (1) or 16-byte cp.async pieces (0)
-#ifndef MB_TILE_BULK
-#define MB_TILE_BULK 1
-#endif
-constexpr bool kMBTileBulk = MB_TILE_BULK != 0;
-
 template <int B>
 static int tile_grid_b(int sms, int ntiles)
 {
     const size_t sm = MBTile<B>::smem;
-    cudaFuncSetAttribute(modelb_tile_step<B, kMBTileRows, true, kMBTileBulk>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaFuncSetAttribute(modelb_tile_step<B, kMBTileRows, false, kMBTileBulk>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(modelb_tile_step<B, kMBTileRows, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(modelb_tile_step<B, kMBTileRows, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(modelb_tile_step<B, kMBTileRows, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaFuncSetAttribute(modelb_tile_step<B, kMBTileRows, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, modelb_tile_step<B, kMBTileRows, true, kMBTileBulk>, MBTile<B>::NT,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, modelb_tile_step<B, kMBTileRows, true, false>, MBTile<B>::NT,
                                                       sm) != cudaSuccess ||
         occ < 1)
         occ = 1;
@@ -68,15 +64,21 @@ int modelb_tile_grid(int B, int sms, int ntiles)
 }
 
 cudaError_t launch_modelb_tiles(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
-                                const MBFastP& P, const MBFastBuf& Q, const LazyP& L)
+                                const MBFastP& P, const MBFastBuf& Q, const LazyP& L, bool bulk)
 {
     const MBPairP K = make_pair_params(P);
-#define XT(b)                                                                                         \
-    if (B == b) {                                                                                     \
-        const size_t sm = MBTile<b>::smem;                                                            \
-        if (dba_mode) modelb_tile_step<b, kMBTileRows, true, kMBTileBulk><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, K, Q, L);   \
-        else modelb_tile_step<b, kMBTileRows, false, kMBTileBulk><<<grid, MBTile<b>::NT, sm, st>>>(g, f, P, K, Q, L);           \
-        return cudaGetLastError();                                                                    \
+#define XT(b)                                                                                                     \
+    if (B == b) {                                                                                                 \
+        const size_t sm = MBTile<b>::smem;                                                                        \
+        const int nt = MBTile<b>::NT;                                                                             \
+        if (bulk) {                                                                                               \
+            if (dba_mode) modelb_tile_step<b, kMBTileRows, true, true><<<grid, nt, sm, st>>>(g, f, P, K, Q, L);   \
+            else modelb_tile_step<b, kMBTileRows, false, true><<<grid, nt, sm, st>>>(g, f, P, K, Q, L);           \
+        } else {                                                                                                  \
+            if (dba_mode) modelb_tile_step<b, kMBTileRows, true, false><<<grid, nt, sm, st>>>(g, f, P, K, Q, L);  \
+            else modelb_tile_step<b, kMBTileRows, false, false><<<grid, nt, sm, st>>>(g, f, P, K, Q, L);          \
+        }                                                                                                         \
+        return cudaGetLastError();                                                                                \
     }
     XT(8) XT(16)
 #undef XT

@@ -84,7 +84,7 @@ bool modelb_uses_fast(int D, int B)
 
 template <typename R>
 cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
-                          const MBP<R>& P, const LazyP* lz, bool tiles)
+                          const MBP<R>& P, const LazyP* lz, int tiles)
 {
     if constexpr (sizeof(R) == 4) {
         if (modelb_uses_fast<R>(D, B)) {
@@ -92,7 +92,7 @@ cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st
             if (lz) L = *lz;
             const MBFastP FP = make_fast_params(P);
             const MBFastBuf FB = make_fast_buf(P);
-            if (tiles) return launch_modelb_tiles(B, dba_mode, grid, st, g, f, FP, FB, L);
+            if (tiles) return launch_modelb_tiles(B, dba_mode, grid, st, g, f, FP, FB, L, tiles == 2);
 #define XF(b)                                                                                   \
     if (B == b) {                                                                               \
         const size_t sm = MBFastShape<b>::smem;                                                 \
@@ -354,7 +354,7 @@ template cudaError_t launch_batch_tips<REAL_T>(cudaStream_t, const BatchP&, cons
 template bool shape_supported<REAL_T>(int, int, int);
 template int step_grid<REAL_T>(int, int, int, int);
 template cudaError_t launch_dendrite<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const DenP<REAL_T>&);
-template cudaError_t launch_modelb<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const MBP<REAL_T>&, const LazyP*, bool);
+template cudaError_t launch_modelb<REAL_T>(int, int, bool, int, cudaStream_t, const GridP&, const FlagP&, const MBP<REAL_T>&, const LazyP*, int);
 template bool modelb_uses_fast<REAL_T>(int, int);
 template cudaError_t launch_kh<REAL_T>(int, bool, int, cudaStream_t, const GridP&, const FlagP&, const KHP<REAL_T>&);
 template cudaError_t launch_correct<REAL_T>(int, cudaStream_t, const GridP&, const CorrP<REAL_T>&);

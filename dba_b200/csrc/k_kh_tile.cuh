@@ -468,9 +468,15 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                 }
                 if (P.conserved)
                     for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = s_bsum[q][tid];
-                if (DBA) {
-                    f.next[b] = (uint8_t)s_nx[tid];
-                    if (s_nx[tid]) wake_faces_diag(g, f.wake_nxt, b);
+                if (DBA) f.next[b] = (uint8_t)s_nx[tid];
+            }
+            // wake-up scatter: self, the faces (the z faces wrap onto the block itself) and
+            // the in-plane diagonals (KH_DBA.cu:988-1044), one neighbour per thread
+            if (DBA && tid < 11 * NBT) {
+                const int kt = tid / 11, k = tid - kt * 11;
+                if (((tm >> kt) & 1u) && s_nx[kt]) {
+                    const int nbk = block_nb_k(g, tbx * TB + kt % TB, tby * TB + kt / TB, 0, k);
+                    if (nbk >= 0) f.wake_nxt[nbk] = 1;
                 }
             }
             __syncthreads();                      // shared tiles and tables reused by the next tile

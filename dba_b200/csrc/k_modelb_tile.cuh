@@ -9,12 +9,14 @@
 //     listed tile contribute their persisted potentials, exactly as inactive
 //     neighbour blocks do (stale-read rule, kernel.cu:594-654);
 //   * the tile plus a 2-cell halo of x, y, z is staged double-buffered (tile
-//     i+1 in flight while tile i computes) by the TMA engine: one thread per
-//     staged row and field issues one bulk copy (cp.async.bulk) per block
-//     segment of the row -- the 4-cell halo on each side and one B-wide
-//     segment per block -- from the buffer that block's parity picks; the
-//     copies complete on the stage's mbarrier (bounded wait).  The alternative
-//     form (BULK = false) spreads 16-byte cp.async pieces over the CTA;
+//     i+1 in flight while tile i computes) with 16-byte cp.async pieces spread
+//     over the CTA, each inside one block, whose parity picks the buffer; or
+//     (BULK, `tiles = 2`) by the TMA engine: one thread per staged row and field
+//     issues one bulk copy (cp.async.bulk) per block segment of the row -- the
+//     4-cell halo on each side and one B-wide segment per block -- completing on
+//     the stage's mbarrier (bounded wait).  The bulk form is measured slower on
+//     the 2048^2 workload (58 against 42 us per step: 432 copies of 16 to 64
+//     bytes per tile through the copy engine), so cp.async is the default;
 //   * each thread owns a 4-column x R-row patch (R = kMBTileRows; 256 / R
 //     threads per CTA).  A staged row of the patch is one 16-byte shared load,
 //     its left and right neighbours taken from the adjacent lanes;

@@ -34,15 +34,17 @@ cudaError_t launch_dendrite3_tiles(bool dba_mode, int grid, cudaStream_t st, con
 // FP32 2-D uses the fast kernels (lazy conserved correction, reduction fused):
 // the 32x32-cell tile kernel when `tiles` (see modelb_tiles_ok), else one block
 // at a time.  `lz` may be null for FP64.
+// tiles: 0 the one-block kernel, 1 the tile kernel with 16-byte cp.async staging, 2 the
+// tile kernel with bulk-copy (TMA engine) staging
 template <typename R>
 cudaError_t launch_modelb(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
-                          const MBP<R>& P, const LazyP* lz, bool tiles);
+                          const MBP<R>& P, const LazyP* lz, int tiles);
 template <typename R> bool modelb_uses_fast(int D, int B);
 bool modelb_tiles_ok(int D, int B, int nx, int ny);
 // persistent grid of the tile kernel (also sets its shared-memory limit on the current device)
 int modelb_tile_grid(int B, int sms, int ntiles);
 cudaError_t launch_modelb_tiles(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
-                                const MBFastP& P, const MBFastBuf& Q, const LazyP& L);
+                                const MBFastP& P, const MBFastBuf& Q, const LazyP& L, bool bulk);
 cudaError_t launch_gather_lazy(cudaStream_t st, const GridP& g, int B, const float* b0, const float* b1,
                                const uint8_t* par, const long long* tot_q, const long long* chg_q, size_t count,
                                double* out);

@@ -90,7 +90,10 @@ typedef struct dba_config {
     int tiles;                 /* 1 (default): tile kernels where the shape allows -- FP32 2-D Model B on 32x32
                                   cells (nx, ny multiples of 32, block 8 or 16), KH on 16x16 cells (nx, ny
                                   multiples of 16, block 8 or 16), FP32 3-D dendrite on 32x8x8 cells (block 8,
-                                  nx a multiple of 32); 0: the one-block kernels and the four-stage KH kernels */
+                                  nx a multiple of 32); 2: as 1, with the FP32 2-D Model B tiles staged by
+                                  bulk copies of the TMA engine (one per block segment of a staged row)
+                                  instead of 16-byte cp.async pieces; 0: the one-block kernels and the
+                                  four-stage KH kernels */
     double cfl;                /* KH: > 0 picks each step's dt = cfl * min(dx, dy) / max(c + |v|) on the device
                                   (tile kernel only); 0 (default): the fixed dt */
 } dba_config;

@@ -1,4 +1,5 @@
-"""FP32 2-D Model B: the 32x32-cell tile kernel against the one-block-at-a-time kernel.
+"""FP32 2-D Model B: the 32x32-cell tile kernel (both staging forms: `tiles = 1`
+16-byte cp.async pieces, `tiles = 2` bulk copies) against the one-block-at-a-time kernel.
 
 Both kernels evaluate every point formula with the same explicitly rounded
 operations, so with the same DBA flags they must produce bit-identical fields,
@@ -28,11 +29,11 @@ def patch_ic(nx, ny, cx, cy, radius, seed=7):
     return [a[None] for a in (x, y, z)]
 
 
-def _pair(B, conserved, nx=128, ny=96):
+def _pair(B, conserved, nx=128, ny=96, form=1):
     prm = dict(MODELB_REF, metric_eps=3e-4, k_0=0.3)
     ic = patch_ic(nx, ny, cx=8, cy=40, radius=22)
     sims = []
-    for tiles in (1, 0):
+    for tiles in (form, 0):
         cfg = modelb_cfg(prm, nx, ny, 1, B, precision=1, conserved=conserved, tiles=tiles)
         sims.append(dba_b200.Simulation(cfg).init(ic))
     return sims
@@ -46,10 +47,11 @@ def _same(a, b):
     assert np.array_equal(a.flags(0), b.flags(0))
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("B", [8, 16])
 @pytest.mark.parametrize("conserved", [0, 1])
-def test_tiles_bitexact_vs_block_kernel_dba(B, conserved):
-    t, k = _pair(B, conserved)
+def test_tiles_bitexact_vs_block_kernel_dba(B, conserved, form):
+    t, k = _pair(B, conserved, form=form)
     assert t.info.grid_ctas <= (128 // 32) * (96 // 32)      # tile grid: at most one CTA per tile
     seen = set()
     for _ in range(12):          # single steps through the first wake-up transients
@@ -67,9 +69,10 @@ def test_tiles_bitexact_vs_block_kernel_dba(B, conserved):
     k.sync()
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("B", [8, 16])
-def test_tiles_bitexact_vs_block_kernel_regular_then_dba(B):
-    t, k = _pair(B, 1)
+def test_tiles_bitexact_vs_block_kernel_regular_then_dba(B, form):
+    t, k = _pair(B, 1, form=form)
     t.step(30, 0)
     k.step(30, 0)
     _same(t, k)
@@ -88,8 +91,9 @@ def test_tiles_conserved_mass_exact():
         assert abs(b - a) / abs(a) <= 1e-10, (a, b)
 
 
+@pytest.mark.parametrize("form", [1, 2])
 @pytest.mark.parametrize("B", [8, 16])
-def test_tiles_many_tiles_per_cta(B):
+def test_tiles_many_tiles_per_cta(B, form):
     """2048x1024 has 2048 tiles, several per CTA, so each CTA stages the next listed
     tile while it computes the current one (and loads the neighbour table of the one
     after); the results must still equal the block kernel's bit for bit, in regular
@@ -98,7 +102,7 @@ def test_tiles_many_tiles_per_cta(B):
     prm = dict(MODELB_REF, metric_eps=3e-4, k_0=0.3)
     ic = patch_ic(nx, ny, cx=700, cy=500, radius=380, seed=11)
     t, k = (dba_b200.Simulation(modelb_cfg(prm, nx, ny, 1, B, precision=1, conserved=1, tiles=tl)).init(ic)
-            for tl in (1, 0))
+            for tl in (form, 0))
     assert t.info.grid_ctas < (nx // 32) * (ny // 32)
     t.step(5, 0)
     k.step(5, 0)
