@@ -147,6 +147,15 @@ __device__ __forceinline__ void wake_faces_diag(const GridP& g, uint8_t* w, int 
     wake_one(g, w, b, 1, 1, 0);
 }
 
+// threadIdx.x read afresh where it is used: values derived from it inside a loop are
+// then computed there, not hoisted out of the loop and kept live in registers
+__device__ __forceinline__ int tid_fresh()
+{
+    int t;
+    asm volatile("mov.u32 %0, %%tid.x;" : "=r"(t));
+    return t;
+}
+
 __device__ __forceinline__ void raise_status(int* status, int code)
 {
     atomicCAS(status, 0, code);

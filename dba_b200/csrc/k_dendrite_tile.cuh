@@ -41,7 +41,9 @@ struct DenTile {
     static constexpr int NR = RX * 3 * 3;        // neighbourhood blocks
     static constexpr int TPP = NT / TBX;         // tiles per scan pass
     static constexpr size_t smem = sizeof(float) * 2 * 2 * SV;   // [stage][p, T]
+    static constexpr int WS0 = 64, WN0 = 128;    // first thread of the wake-up scatter / tests
     static_assert(TX * B == NT, "one column per thread");
+    static_assert(NR <= WS0 && WS0 + 2 * TBX * 7 <= WN0 && WN0 + TBX <= NT, "bookkeeping beside the table");
 };
 
 template <bool DBA>
@@ -49,7 +51,7 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
 {
     using S = DenTile;
     constexpr int NT = S::NT, B = S::B, TX = S::TX, TBX = S::TBX, SW = S::SW, SP = S::SP, SR = S::SR, PL = S::PL,
-                  SV = S::SV, NQ = S::NQ, RX = S::RX, NR = S::NR, TPP = S::TPP;
+                  SV = S::SV, NQ = S::NQ, RX = S::RX, NR = S::NR, TPP = S::TPP, WS0 = S::WS0, WN0 = S::WN0;
     extern __shared__ __align__(128) float smem_f[];   // [stage][p|T][z][y][x]
     __shared__ int s_tile[TPP];
     __shared__ unsigned s_tmeta[TPP];   // bits 0-3 p-active blocks, 4-7 T-active, 8-11 p parity, 12-15 T parity
@@ -227,17 +229,21 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
                 if (DBA && wT) s_nT[kb] = 1;
             }
             __syncthreads();
-            if (DBA && tid < TBX) {
+            // The wake-up bookkeeping runs on warps 2-4, beside the next tile's neighbour
+            // table (threads below NR) and before the barrier that follows it.  Tests:
+            if (DBA && tid >= WN0 && tid < WN0 + TBX) {
+                const int kt = tid_fresh() - WN0;
                 int X0, Y0, Z0;
                 tile_xyz(s_tile[i], X0, Y0, Z0);
-                const int b = (X0 / B + tid) + g.nbx * (Y0 / B + g.nby * (Z0 / B));
-                if ((tm >> tid) & 1u) f.next[b] = (uint8_t)s_np[tid];
-                if ((tm >> (4 + tid)) & 1u) f.next[nb + b] = (uint8_t)s_nT[tid];
+                const int b = (X0 / B + kt) + g.nbx * (Y0 / B + g.nby * (Z0 / B));
+                if ((tm >> kt) & 1u) f.next[b] = (uint8_t)s_np[kt];
+                if ((tm >> (4 + kt)) & 1u) f.next[nb + b] = (uint8_t)s_nT[kt];
             }
-            // wake-up scatter, self + 6 faces per channel (kernel.cu:577-634), one
-            // neighbour per thread: thread (ch * TBX + blk) * 7 + k
-            if (DBA && tid < 2 * TBX * 7) {
-                const int k = tid % 7, cb = tid / 7, ch = cb / TBX, kt = cb - ch * TBX;
+            // scatter, self + 6 faces per channel (kernel.cu:577-634), one neighbour per
+            // thread: thread WS0 + (ch * TBX + blk) * 7 + k
+            if (DBA && tid >= WS0 && tid < WS0 + 2 * TBX * 7) {
+                const int t = tid_fresh() - WS0;
+                const int k = t % 7, cb = t / 7, ch = cb / TBX, kt = cb - ch * TBX;
                 if (((tm >> (4 * ch + kt)) & 1u) && (ch ? s_nT[kt] : s_np[kt])) {
                     int X0, Y0, Z0;
                     tile_xyz(s_tile[i], X0, Y0, Z0);

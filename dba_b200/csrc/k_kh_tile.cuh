@@ -31,7 +31,11 @@
 //
 // Launch shape: 416 threads (13 warps), so that each phase is one item per
 // thread (400, 320, 288 and 256 items) and no warp runs a second round while
-// the others wait at the phase's barrier.  Each thread's tile-local cells are
+// the others wait at the phase's barrier.  The DBA bookkeeping runs on the
+// warps a phase leaves idle, off the path the barriers wait on: the wake-up
+// scatter (the tests are final after phase 2) on warps 9-12 during phase 3,
+// the ring persistence (copied from the shared tiles) on warps 8-12 during
+// phase 4.  Each thread's tile-local cells are
 // fixed for the whole launch; the list entries carry the tiles' coordinates.
 // Cells are staged as 16-byte vectors (Q4 / QA), and the next listed tile's
 // phase-1 inputs are copied with cp.async while the current tile computes.
@@ -132,8 +136,15 @@ template <typename R, int B> struct KHTile {
     static constexpr int TPP = NT / NBT;       // tiles per scan pass
     static constexpr int NS = 4 * N1;                 // staged next-tile inputs, R elements
     static constexpr size_t smem = sizeof(R) * ((size_t)4 * (NW + NP + NG + NFX + NFY + NU) + NS);
+    // DBA bookkeeping on the warps phases 3 and 4 leave idle: the wake-up scatter
+    // (11 neighbours per block) from thread SC0, the ring persistence (4 (B - 1)
+    // cells per block) from thread PR0
+    static constexpr int SC0 = (N3 + 31) / 32 * 32;
+    static constexpr int PR0 = (T * T + 31) / 32 * 32;
+    static constexpr int NRING = 4 * (B - 1);
     static_assert(T % B == 0 && B >= 2 && NBT <= 16, "tile shape");
     static_assert(N1 <= NT && N2 <= NT && N3 <= NT && T * T <= NT, "one item per thread and phase");
+    static_assert(SC0 + 11 * NBT <= NT && PR0 + NBT * NRING <= NT, "bookkeeping on idle warps");
 };
 
 // region (block of the 3x3 neighbourhood of blocks around the tile) of tile-local cell (lx, ly)
@@ -386,10 +397,21 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                     if (xf3) sFx.put(y3 * FXW + x3 + 1, Q{P.Fl[0][gi], P.Fl[1][gi], P.Fl[2][gi], P.Fl[3][gi]});
                     if (yf3) sFy.put((y3 + 1) * T + x3, Q{P.Fl[4][gi], P.Fl[5][gi], P.Fl[6][gi], P.Fl[7][gi]});
                 }
+            } else if (DBA && tid >= S::SC0 && tid < S::SC0 + 11 * NBT) {
+                // wake-up tests and scatter on the idle warps: self, the faces (the z faces wrap
+                // onto the block itself) and the in-plane diagonals (KH_DBA.cu:988-1044), one
+                // neighbour per thread; the self thread also records the block's test
+                const int t = tid_fresh() - S::SC0;
+                const int kt = t / 11, k = t - kt * 11;
+                if ((tm >> kt) & 1u) {
+                    const int nbk = block_nb_k(g, tbx * TB + kt % TB, tby * TB + kt / TB, 0, k);
+                    if (k == 0) f.next[nbk] = (uint8_t)s_nx[kt];
+                    if (s_nx[kt] && nbk >= 0) f.wake_nxt[nbk] = 1;
+                }
             }
             __syncthreads();
 
-            // 4. update of own active cells; persistence for blocks that may sleep
+            // 4. update of own active cells; ring persistence for blocks that may sleep
             const bool own = h4 && ((tm >> ukb) & 1u);
             double ch[4] = {0.0, 0.0, 0.0, 0.0};
             if (own) {
@@ -417,31 +439,39 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                     kh_prim_of<R>(un.a, un.b, un.c, un.d, K, r, pp, uu, vv);
                     atomicMax(&s_vblk[ukb], __float_as_uint(kh_speed<R>(r, pp, uu, vv, K.gam)));
                 }
-                if (DBA && !s_nx[ukb]) {
-                    const int pi = (uy + 1) * P1 + ux + 1;
-                    const int bxl = ux % B, byl = uy % B;
-                    if (bxl == 0 || bxl == B - 1 || byl == 0 || byl == B - 1) {
-                        const Q hp = sP(pi), gx = sGx(pi), gy = sGy(pi);
-                        P.Wp[0][gi] = hp.a;
-                        P.Wp[1][gi] = hp.b;
-                        P.Wp[2][gi] = hp.c;
-                        P.Wp[3][gi] = hp.d;
-                        P.Gd[0][gi] = gx.a;
-                        P.Gd[1][gi] = gy.a;
-                        P.Gd[2][gi] = gx.b;
-                        P.Gd[3][gi] = gy.b;
-                        P.Gd[4][gi] = gx.c;
-                        P.Gd[5][gi] = gy.c;
-                        P.Gd[6][gi] = gx.d;
-                        P.Gd[7][gi] = gy.d;
-                    }
+            } else if (DBA && tid >= S::PR0 && tid < S::PR0 + NBT * S::NRING) {
+                // ring persistence on the idle warps, from the shared tiles: ring cell e of
+                // tile block kt (bottom row, top row, left column, right column)
+                const int t = tid_fresh() - S::PR0;
+                const int kt = t / S::NRING, e = t - kt * S::NRING;
+                if (((tm >> kt) & 1u) && !s_nx[kt]) {
+                    const int bxl = e < B ? e : (e < 2 * B ? e - B : (e < 3 * B - 2 ? 0 : B - 1));
+                    const int byl = e < B ? 0 : (e < 2 * B ? B - 1 : (e < 3 * B - 2 ? e - 2 * B + 1 : e - 3 * B + 3));
+                    const int px = (kt % TB) * B + bxl, py = (kt / TB) * B + byl;
+                    const size_t gi = (size_t)(base + px + g.nx * py);
+                    const int pi = (py + 1) * P1 + px + 1;
+                    const Q hp = sP(pi), gx = sGx(pi), gy = sGy(pi);
+                    P.Wp[0][gi] = hp.a;
+                    P.Wp[1][gi] = hp.b;
+                    P.Wp[2][gi] = hp.c;
+                    P.Wp[3][gi] = hp.d;
+                    P.Gd[0][gi] = gx.a;
+                    P.Gd[1][gi] = gy.a;
+                    P.Gd[2][gi] = gx.b;
+                    P.Gd[3][gi] = gy.b;
+                    P.Gd[4][gi] = gx.c;
+                    P.Gd[5][gi] = gy.c;
+                    P.Gd[6][gi] = gx.d;
+                    P.Gd[7][gi] = gy.d;
                     if (bxl == B - 1) {
+                        const Q fr = sFx(py * FXW + px + 1);
                         P.Fl[0][gi] = fr.a;
                         P.Fl[1][gi] = fr.b;
                         P.Fl[2][gi] = fr.c;
                         P.Fl[3][gi] = fr.d;
                     }
                     if (byl == B - 1) {
+                        const Q fu = sFy((py + 1) * T + px);
                         P.Fl[4][gi] = fu.a;
                         P.Fl[5][gi] = fu.b;
                         P.Fl[6][gi] = fu.c;
@@ -468,16 +498,6 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                 }
                 if (P.conserved)
                     for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = s_bsum[q][tid];
-                if (DBA) f.next[b] = (uint8_t)s_nx[tid];
-            }
-            // wake-up scatter: self, the faces (the z faces wrap onto the block itself) and
-            // the in-plane diagonals (KH_DBA.cu:988-1044), one neighbour per thread
-            if (DBA && tid < 11 * NBT) {
-                const int kt = tid / 11, k = tid - kt * 11;
-                if (((tm >> kt) & 1u) && s_nx[kt]) {
-                    const int nbk = block_nb_k(g, tbx * TB + kt % TB, tby * TB + kt / TB, 0, k);
-                    if (nbk >= 0) f.wake_nxt[nbk] = 1;
-                }
             }
             __syncthreads();                      // shared tiles and tables reused by the next tile
         }
