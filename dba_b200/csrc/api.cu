@@ -66,6 +66,8 @@ struct dba_ctx {
     float* fstaging = nullptr;        // dba_read_field_f32: a field as floats (allocated on first use)
     bool kh_tiles = false;            // KH one-kernel step on 16x16-cell tiles (k_kh_tile.cuh)
     bool den_tiles = false;           // FP32 3-D dendrite on 32x8x8-cell tiles (k_dendrite_tile.cuh)
+    int* tlist = nullptr;             // tile queue of the tile kernels that take tiles dynamically
+    unsigned* tctr = nullptr;         //   (2 ints per tile; counters, zeroed by each step's last CTA)
     float* kvmax = nullptr;           // KH tiles: per-block largest signal speed (CFL)
     unsigned* kgmax = nullptr;        // KH tiles: rotating maxima of the CFL speed, float bits [3]
     double* ktime = nullptr;          // KH tiles: simulated time accumulated on the device (CFL)
@@ -124,6 +126,8 @@ FlagP flags_for(dba_ctx* c, long s)
     f.bsum = c->bsum;
     f.status = c->status;
     f.stats = c->stats;
+    f.tlist = c->tlist;
+    f.tctr = c->tctr;
     return f;
 }
 
@@ -710,8 +714,15 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
     c->grid = c->esz == 8 ? step_grid<double>(cfg->model, c->D, c->B, c->sms) : step_grid<float>(cfg->model, c->D, c->B, c->sms);
     if (c->grid < 1) c->grid = c->sms;
     if (cfg->model == DBA_MODEL_DENDRITE && c->esz == 4 && cfg->tiles && dendrite_tiles_ok(c->D, c->B, cfg->nx)) {
+        const size_t nt = (size_t)(cfg->nx / 32) * (cfg->ny / 8) * (cfg->nz / 8);
         c->den_tiles = true;
-        c->grid = dendrite3_tile_grid(c->sms, (cfg->nx / 32) * (cfg->ny / 8) * (cfg->nz / 8));
+        c->grid = dendrite3_tile_grid(c->sms, (int)nt);
+        c->tlist = (int*)dev_alloc(c, 2 * nt * sizeof(int), &err);
+        if (!err) c->tctr = (unsigned*)dev_alloc(c, 4 * sizeof(unsigned), &err);
+        if (err) {
+            dba_destroy(c);
+            return err;
+        }
     }
     if (c->kh_tiles) {
         const int nt = (cfg->nx / 16) * (cfg->ny / 16);

@@ -42,6 +42,10 @@ struct FlagP {
     double* bsum;
     int* status;
     unsigned long long* stats;  // kStatWords striped activity counters (count_stats)
+    // listed tiles of the step, for the tile kernels that hand tiles out dynamically
+    // (tile_list_append / tile_queue_done); null elsewhere
+    int* tlist = nullptr;       // (tile, meta) pairs
+    unsigned* tctr = nullptr;   // [0] entries listed, [1] entries taken, [2] CTAs done
 };
 
 __device__ __forceinline__ int wrapc(int v, int n, int bc)
@@ -145,6 +149,39 @@ __device__ __forceinline__ void wake_faces_diag(const GridP& g, uint8_t* w, int 
     wake_one(g, w, b, -1, 1, 0);
     wake_one(g, w, b, 1, -1, 0);
     wake_one(g, w, b, 1, 1, 0);
+}
+
+// Tile queue of one step.  A scan kernel appends the step's listed tiles as (tile, meta)
+// pairs to f.tlist, counting in f.tctr[0] (one atomic per warp); the tile kernel's CTAs
+// take entries in any order through the counter f.tctr[1], so a CTA whose tiles are
+// cheap takes more of them; the last CTA to finish (ticket f.tctr[2]) zeroes the three
+// counters for the next step.  Every tile's result is independent of which CTA
+// computes it and when.
+__device__ __forceinline__ void tile_list_append(const FlagP& f, bool take, int tile, unsigned meta, unsigned cap)
+{
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (m == 0) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(f.tctr, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (take) {
+        const unsigned k = base + (unsigned)__popc(m & ((1u << lane) - 1u));
+        if (k < cap) {                 // cap: the list's capacity (tiles of the grid)
+            f.tlist[2 * (size_t)k] = tile;
+            f.tlist[2 * (size_t)k + 1] = (int)meta;
+        }
+    }
+}
+// one thread per CTA, after the CTA's last take
+__device__ __forceinline__ void tile_queue_done(const FlagP& f)
+{
+    __threadfence();
+    if (atomicAdd(f.tctr + 2, 1u) == gridDim.x - 1) {
+        f.tctr[0] = 0u;
+        f.tctr[1] = 0u;
+        f.tctr[2] = 0u;
+    }
 }
 
 // threadIdx.x read afresh where it is used: values derived from it inside a loop are

@@ -5,7 +5,11 @@
 // reorganised so that a CTA works on four x-adjacent blocks at a time:
 //
 //   * a tile is listed when any channel (p or T) of any of its blocks is
-//     active; only active channels of active blocks are updated;
+//     active; only active channels of active blocks are updated.  A scan
+//     kernel lists the step's tiles in a device queue and the CTAs take them
+//     one at a time (tile_list_append / tile_queue_done): active tiles cluster
+//     around the growing front, and with a fixed share of the domain per CTA
+//     the busiest CTA held about 1.25 times the mean work;
 //   * p and T of the tile plus a 1-cell halo are staged in shared memory as
 //     40-float rows (x from X0-4 to X0+35): each row is five whole 32-byte
 //     sectors, where one 8-cell block row with its x halo touches three sectors
@@ -39,31 +43,72 @@ struct DenTile {
     static constexpr int NQ = SR * SR * (SW / 4);// 16-byte pieces per field
     static constexpr int RX = TBX + 2;           // neighbourhood extent in blocks: x
     static constexpr int NR = RX * 3 * 3;        // neighbourhood blocks
-    static constexpr int TPP = NT / TBX;         // tiles per scan pass
     static constexpr size_t smem = sizeof(float) * 2 * 2 * SV;   // [stage][p, T]
     static constexpr int WS0 = 64, WN0 = 128;    // first thread of the wake-up scatter / tests
+    static constexpr int GT = 192;               // the thread that takes tiles from the queue
     static_assert(TX * B == NT, "one column per thread");
-    static_assert(NR <= WS0 && WS0 + 2 * TBX * 7 <= WN0 && WN0 + TBX <= NT, "bookkeeping beside the table");
+    static_assert(NR <= WS0 && WS0 + 2 * TBX * 7 <= WN0 && WN0 + TBX <= GT && GT < NT, "bookkeeping beside the table");
 };
+
+// Scan of one step for dendrite3_tile_step: per-block bookkeeping of both channels
+// (parity flip of active blocks, clearing of the flag array two steps ahead, activity
+// counts) and one tile-queue entry per tile with an active channel.  One thread per
+// block, the TBX blocks of a tile on adjacent lanes.
+template <bool DBA>
+__global__ void __launch_bounds__(256) dendrite3_tile_scan(GridP g, FlagP f)
+{
+    constexpr int B = DenTile::B, TX = DenTile::TX, TBX = DenTile::TBX;
+    const int nb = g.nb;
+    const int ntx = g.nx / TX, nty = g.ny / B, ntz = g.nz / B;
+    const long long nitems = (long long)ntx * nty * ntz * TBX;
+    for (long long t0 = (long long)blockIdx.x * blockDim.x; t0 < nitems; t0 += (long long)gridDim.x * blockDim.x) {
+        const long long it = t0 + threadIdx.x;
+        const bool valid = it < nitems;
+        const int tile = (int)(it / TBX), kq = (int)(it % TBX);
+        int act = 0, pp = 0, pT = 0;
+        if (valid) {
+            const int X0 = (tile % ntx) * TX, Y0 = ((tile / ntx) % nty) * B, Z0 = (tile / (ntx * nty)) * B;
+            const int b = (X0 / B + kq) + g.nbx * (Y0 / B + g.nby * (Z0 / B));
+            pp = f.par_cur[b];
+            pT = f.par_cur[nb + b];
+            act = DBA ? ((f.wake_cur[b] ? 1 : 0) | (f.wake_cur[nb + b] ? 2 : 0)) : 3;
+            f.wake_clr[b] = 0;
+            f.wake_clr[nb + b] = 0;
+            if (!DBA) {
+                f.wake_nxt[b] = 1;
+                f.wake_nxt[nb + b] = 1;
+            }
+            f.par_nxt[b] = (uint8_t)(pp ^ (act & 1));
+            f.par_nxt[nb + b] = (uint8_t)(pT ^ ((act >> 1) & 1));
+        }
+        count_stats(f.stats, act, valid);
+        const unsigned m0 = __ballot_sync(0xffffffffu, valid && (act & 1));
+        const unsigned m1 = __ballot_sync(0xffffffffu, valid && (act & 2));
+        const unsigned m2 = __ballot_sync(0xffffffffu, valid && pp);
+        const unsigned m3 = __ballot_sync(0xffffffffu, valid && pT);
+        const int g0 = (threadIdx.x & 31) & ~(TBX - 1);
+        const unsigned gm = (1u << TBX) - 1u;
+        const unsigned meta = ((m0 >> g0) & gm) | (((m1 >> g0) & gm) << 4) | (((m2 >> g0) & gm) << 8) |
+                              (((m3 >> g0) & gm) << 12);
+        tile_list_append(f, valid && kq == 0 && (meta & 0xffu) != 0, tile, meta, (unsigned)(nitems / TBX));
+    }
+}
 
 template <bool DBA>
 __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, DenP<float> P)
 {
     using S = DenTile;
     constexpr int NT = S::NT, B = S::B, TX = S::TX, TBX = S::TBX, SW = S::SW, SP = S::SP, SR = S::SR, PL = S::PL,
-                  SV = S::SV, NQ = S::NQ, RX = S::RX, NR = S::NR, TPP = S::TPP, WS0 = S::WS0, WN0 = S::WN0;
+                  SV = S::SV, NQ = S::NQ, RX = S::RX, NR = S::NR, WS0 = S::WS0, WN0 = S::WN0, GT = S::GT;
     extern __shared__ __align__(128) float smem_f[];   // [stage][p|T][z][y][x]
-    __shared__ int s_tile[TPP];
-    __shared__ unsigned s_tmeta[TPP];   // bits 0-3 p-active blocks, 4-7 T-active, 8-11 p parity, 12-15 T parity
-    __shared__ int s_cnt;
+    __shared__ int s_tile[4];           // tiles i .. i + 3 (slot i % 4), -1 past the end of the queue
+    __shared__ unsigned s_tmeta[4];     // bits 0-3 p-active blocks, 4-7 T-active, 8-11 p parity, 12-15 T parity
     __shared__ uint8_t s_par[2][2][NR];  // [stage][channel][neighbour block]
     __shared__ int s_np[TBX], s_nT[TBX];
 
     const int tid = threadIdx.x;
-    const int G = gridDim.x;
     const int nb = g.nb;
-    const int ntx = g.nx / TX, nty = g.ny / B, ntz = g.nz / B;
-    const int ntiles = ntx * nty * ntz;
+    const int ntx = g.nx / TX, nty = g.ny / B;
     const size_t nx = (size_t)g.nx, nxy = (size_t)g.nx * g.ny;
     const float f0 = (float)P.f0, f1 = (float)P.f1, f2 = (float)P.f2, f3 = (float)P.f3;
     const float dt = (float)P.dt, delta = (float)P.delta, eps2 = (float)P.eps2, gam = (float)P.gamma;
@@ -132,68 +177,56 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
         cp_async_commit();
     };
 
-    for (long long j0 = 0; blockIdx.x + (long long)G * j0 < ntiles; j0 += TPP) {
-        // ---- scan: per-block bookkeeping of both channels, one list entry per tile
-        {
-            const long long tl = blockIdx.x + (long long)G * (j0 + tid / TBX);
-            const int kq = tid % TBX;
-            const bool valid = tl < ntiles;
-            const int tile = (int)tl;
-            int act = 0, pp = 0, pT = 0;
-            if (valid) {
-                int X0, Y0, Z0;
-                tile_xyz(tile, X0, Y0, Z0);
-                const int b = (X0 / B + kq) + g.nbx * (Y0 / B + g.nby * (Z0 / B));
-                pp = f.par_cur[b];
-                pT = f.par_cur[nb + b];
-                act = DBA ? ((f.wake_cur[b] ? 1 : 0) | (f.wake_cur[nb + b] ? 2 : 0)) : 3;
-                f.wake_clr[b] = 0;
-                f.wake_clr[nb + b] = 0;
-                if (!DBA) {
-                    f.wake_nxt[b] = 1;
-                    f.wake_nxt[nb + b] = 1;
-                }
-                f.par_nxt[b] = (uint8_t)(pp ^ (act & 1));
-                f.par_nxt[nb + b] = (uint8_t)(pT ^ ((act >> 1) & 1));
-            }
-            count_stats(f.stats, act, valid);
-            const unsigned m0 = __ballot_sync(0xffffffffu, valid && (act & 1));
-            const unsigned m1 = __ballot_sync(0xffffffffu, valid && (act & 2));
-            const unsigned m2 = __ballot_sync(0xffffffffu, valid && pp);
-            const unsigned m3 = __ballot_sync(0xffffffffu, valid && pT);
-            const int g0 = (tid & 31) & ~(TBX - 1);
-            const unsigned gm = (1u << TBX) - 1u;
-            const unsigned meta = ((m0 >> g0) & gm) | (((m1 >> g0) & gm) << 4) | (((m2 >> g0) & gm) << 8) |
-                                  (((m3 >> g0) & gm) << 12);
-            if (tid == 0) s_cnt = 0;
-            __syncthreads();
-            list_append(valid && kq == 0 && (meta & 0xffu) != 0, tile, (int)meta, s_tile,
-                        reinterpret_cast<int*>(s_tmeta), &s_cnt);
-            __syncthreads();
+    // The step's listed tiles (dendrite3_tile_scan) are taken from the tile queue by
+    // thread GT, two tiles ahead: during tile i it reads the list entry of tile i + 2
+    // (taken during tile i - 1) into slot (i + 2) % 4 and takes the entry for tile i + 3,
+    // so neither the counter's atomic nor the list load is waited for on a barrier's
+    // path.  Slot (i + 2) % 4 held tile i - 2; tile i - 1's slot is still read by the
+    // wake-up bookkeeping meanwhile.
+    const int cnt = (int)min(__ldcg(f.tctr), (unsigned)(ntx * nty * (g.nz / B)));
+    int k_pend = 0;
+    auto entry = [&](int k, int slot) {
+        if (k < cnt) {
+            s_tile[slot] = __ldcg(f.tlist + 2 * (size_t)k);
+            s_tmeta[slot] = (unsigned)__ldcg(f.tlist + 2 * (size_t)k + 1);
+        } else {
+            s_tile[slot] = -1;
         }
-        const int cnt = s_cnt;
-        if (cnt > 0) {
+    };
+    if (tid == GT) {
+        const int k = (int)atomicAdd(f.tctr + 1, 2u);
+        entry(k, 0);
+        entry(k + 1, 1);
+        k_pend = (int)atomicAdd(f.tctr + 1, 1u);
+    }
+    __syncthreads();
+        if (s_tile[0] >= 0) {
             build_nbr(0, 0);
             __syncthreads();
             issue(0, 0);
         }
-        for (int i = 0; i < cnt; ++i) {
-            const int st = i & 1;
-            if (i + 1 < cnt) build_nbr(i + 1, st ^ 1);
+        for (int i = 0; s_tile[i & 3] >= 0; ++i) {
+            const int st = i & 1, cs = i & 3, ns = (i + 1) & 3;
+            const bool more = s_tile[ns] >= 0;
+            if (more) build_nbr(ns, st ^ 1);
+            if (tid == GT) {
+                entry(k_pend, (i + 2) & 3);
+                k_pend = (int)atomicAdd(f.tctr + 1, 1u);
+            }
             __syncthreads();                     // next table ready; stage st^1 free
             if (tid < TBX) {
                 s_np[tid] = 0;
                 s_nT[tid] = 0;
             }
-            if (i + 1 < cnt) issue(i + 1, st ^ 1);
+            if (more) issue(ns, st ^ 1);
             else cp_async_commit();
             cp_async_wait1();
             __syncthreads();                     // tile i staged (plain stores of wall pieces included)
-            const unsigned tm = s_tmeta[i];
+            const unsigned tm = s_tmeta[cs];
             const bool pa = (tm >> kb) & 1u, Ta = (tm >> (4 + kb)) & 1u;
             if (pa || Ta) {
                 int X0, Y0, Z0;
-                tile_xyz(s_tile[i], X0, Y0, Z0);
+                tile_xyz(s_tile[cs], X0, Y0, Z0);
                 const float* sp = smem_f + st * 2 * SV;
                 const float* sT = sp + SV;
                 float* pout = ((tm >> (8 + kb)) & 1u) ? P.p[0] : P.p[1];
@@ -234,7 +267,7 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
             if (DBA && tid >= WN0 && tid < WN0 + TBX) {
                 const int kt = tid_fresh() - WN0;
                 int X0, Y0, Z0;
-                tile_xyz(s_tile[i], X0, Y0, Z0);
+                tile_xyz(s_tile[cs], X0, Y0, Z0);
                 const int b = (X0 / B + kt) + g.nbx * (Y0 / B + g.nby * (Z0 / B));
                 if ((tm >> kt) & 1u) f.next[b] = (uint8_t)s_np[kt];
                 if ((tm >> (4 + kt)) & 1u) f.next[nb + b] = (uint8_t)s_nT[kt];
@@ -246,14 +279,13 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
                 const int k = t % 7, cb = t / 7, ch = cb / TBX, kt = cb - ch * TBX;
                 if (((tm >> (4 * ch + kt)) & 1u) && (ch ? s_nT[kt] : s_np[kt])) {
                     int X0, Y0, Z0;
-                    tile_xyz(s_tile[i], X0, Y0, Z0);
+                    tile_xyz(s_tile[cs], X0, Y0, Z0);
                     const int nbk = block_nb_k(g, X0 / B + kt, Y0 / B, Z0 / B, k);
                     if (nbk >= 0) f.wake_nxt[(size_t)ch * nb + nbk] = 1;
                 }
             }
         }
-        __syncthreads();                         // list and buffers reused by the next scan pass
-    }
+    if (tid == GT) tile_queue_done(f);
 }
 
 }  // namespace dba

@@ -1,6 +1,8 @@
 // FP32 instantiations of the step kernels (stencil arithmetic in float, FMA
 // contraction allowed; conserved-change sums stay FP64).
 #define REAL_T float
+#include <algorithm>
+
 #include "k_inst.cuh"
 
 namespace dba {
@@ -53,8 +55,16 @@ int dendrite3_tile_grid(int sms, int ntiles)
 cudaError_t launch_dendrite3_tiles(bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
                                    const DenP<float>& P)
 {
-    if (dba_mode) dendrite3_tile_step<true><<<grid, DenTile::NT, DenTile::smem, st>>>(g, f, P);
-    else dendrite3_tile_step<false><<<grid, DenTile::NT, DenTile::smem, st>>>(g, f, P);
+    if (!f.tlist || !f.tctr) return cudaErrorInvalidValue;
+    // the scan lists the step's tiles (one thread per block), the tile kernel takes them
+    const int sg = (int)std::min<long long>(((long long)g.nb + 255) / 256, 65535);
+    if (dba_mode) {
+        dendrite3_tile_scan<true><<<sg, 256, 0, st>>>(g, f);
+        dendrite3_tile_step<true><<<grid, DenTile::NT, DenTile::smem, st>>>(g, f, P);
+    } else {
+        dendrite3_tile_scan<false><<<sg, 256, 0, st>>>(g, f);
+        dendrite3_tile_step<false><<<grid, DenTile::NT, DenTile::smem, st>>>(g, f, P);
+    }
     return cudaGetLastError();
 }
 
