@@ -727,6 +727,12 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
     if (c->kh_tiles) {
         const int nt = (cfg->nx / 16) * (cfg->ny / 16);
         c->grid = c->esz == 8 ? kh_tile_grid<double>(c->B, c->sms, nt) : kh_tile_grid<float>(c->B, c->sms, nt);
+        c->tlist = (int*)dev_alloc(c, 2 * (size_t)nt * sizeof(int), &err);
+        if (!err) c->tctr = (unsigned*)dev_alloc(c, 4 * sizeof(unsigned), &err);
+        if (err) {
+            dba_destroy(c);
+            return err;
+        }
     }
     if (cfg->model == DBA_MODEL_MODELB && c->esz == 4 && cfg->tiles && modelb_tiles_ok(c->D, c->B, cfg->nx, cfg->ny)) {
         c->tiles = cfg->tiles == 2 ? 2 : 1;

@@ -163,11 +163,19 @@ template <typename R>
 cudaError_t launch_kh_tile(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
                            const KHTileP<R>& P)
 {
+    if (!f.tlist || !f.tctr) return cudaErrorInvalidValue;
+    // the scan lists the step's tiles (one thread per block), the tile kernel takes them
+    const int sg = (int)(((long long)g.nb + 255) / 256 < 65535 ? ((long long)g.nb + 255) / 256 : 65535);
 #define XT(b)                                                                                          \
     if (B == b) {                                                                                      \
         const size_t sm = KHTile<R, b>::smem;                                                          \
-        if (dba_mode) kh_tile_step<R, b, true><<<grid, KHTile<R, b>::NT, sm, st>>>(g, f, P);           \
-        else kh_tile_step<R, b, false><<<grid, KHTile<R, b>::NT, sm, st>>>(g, f, P);                   \
+        if (dba_mode) {                                                                                \
+            kh_tile_scan<R, b, true><<<sg, 256, 0, st>>>(g, f, P);                                     \
+            kh_tile_step<R, b, true><<<grid, KHTile<R, b>::NT, sm, st>>>(g, f, P);                     \
+        } else {                                                                                       \
+            kh_tile_scan<R, b, false><<<sg, 256, 0, st>>>(g, f, P);                                    \
+            kh_tile_step<R, b, false><<<grid, KHTile<R, b>::NT, sm, st>>>(g, f, P);                    \
+        }                                                                                              \
         return cudaGetLastError();                                                                     \
     }
     XT(8) XT(16)

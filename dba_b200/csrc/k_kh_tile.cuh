@@ -133,7 +133,7 @@ template <typename R, int B> struct KHTile {
     // x and y gradients, x and y face fluxes, own conserved fields
     static constexpr int NW = E2 * P2, NP = E1 * P1, NG = 2 * E1 * P1;
     static constexpr int NFX = T * FXW, NFY = (T + 1) * T, NU = T * T;
-    static constexpr int TPP = NT / NBT;       // tiles per scan pass
+    static constexpr int GT = NT - 1;          // the thread that takes tiles from the queue (no phase-2 item)
     static constexpr int NS = 4 * N1;                 // staged next-tile inputs, R elements
     static constexpr size_t smem = sizeof(R) * ((size_t)4 * (NW + NP + NG + NFX + NFY + NU) + NS);
     // DBA bookkeeping on the warps phases 3 and 4 leave idle: the wake-up scatter
@@ -145,17 +145,67 @@ template <typename R, int B> struct KHTile {
     static_assert(T % B == 0 && B >= 2 && NBT <= 16, "tile shape");
     static_assert(N1 <= NT && N2 <= NT && N3 <= NT && T * T <= NT, "one item per thread and phase");
     static_assert(SC0 + 11 * NBT <= NT && PR0 + NBT * NRING <= NT, "bookkeeping on idle warps");
+    static_assert(GT >= N2 && GT >= SC0 + 11 * NBT && GT >= PR0 + NBT * NRING, "queue thread without phase items");
 };
 
 // region (block of the 3x3 neighbourhood of blocks around the tile) of tile-local cell (lx, ly)
 template <int B, int RB>
 __device__ __forceinline__ int kh_region(int lx, int ly) { return (lx + B) / B + RB * ((ly + B) / B); }
 
+// Scan of one step for kh_tile_step: per-block bookkeeping (parity flip of active
+// blocks, clearing of the flag array two steps ahead, activity counts; inactive
+// blocks' conserved change sums zeroed and their signal speeds folded into the
+// step's maximum) and one tile-queue entry per tile with an active block.  One
+// thread per block, the NBT blocks of a tile on adjacent lanes.
+template <typename R, int B, bool DBA>
+__global__ void __launch_bounds__(256) kh_tile_scan(GridP g, FlagP f, KHTileP<R> P)
+{
+    using S = KHTile<R, B>;
+    constexpr int T = S::T, TB = S::TB, NBT = S::NBT;
+    const int ntx = g.nx / T, nty = g.ny / T, ntiles = ntx * nty;
+    const long long nitems = (long long)ntiles * NBT;
+    const bool cfl = P.cfl > 0.0;
+    for (long long t0 = (long long)blockIdx.x * blockDim.x; t0 < nitems; t0 += (long long)gridDim.x * blockDim.x) {
+        const long long it = t0 + threadIdx.x;
+        const bool valid = it < nitems;
+        const int tile = (int)(it / NBT), kq = (int)(it % NBT);
+        int act = 0, pp = 0, entry = 0;
+        unsigned vm = 0u;
+        if (valid) {
+            const int tby = tile / ntx, tbx = tile - tby * ntx;
+            const int b = (tbx * TB + kq % TB) + g.nbx * (tby * TB + kq / TB);
+            const int X0 = tbx * T, Y0 = tby * T;
+            const bool inner = X0 >= 2 && X0 + T + 2 <= g.nx && Y0 >= 2 && Y0 + T + 2 <= g.ny;
+            entry = tbx | (tby << 15) | ((int)inner << 30);
+            pp = f.par_cur[b];
+            act = DBA ? (f.wake_cur[b] ? 1 : 0) : 1;
+            f.wake_clr[b] = 0;
+            if (!DBA) f.wake_nxt[b] = 1;
+            f.par_nxt[b] = (uint8_t)(pp ^ act);
+            if (P.conserved && !act)
+                for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = 0.0;
+            if (cfl && !act) vm = __float_as_uint(P.vmax[b]);
+        }
+        count_stats(f.stats, act, valid);
+        const unsigned ma = __ballot_sync(0xffffffffu, valid && act);
+        const unsigned mp = __ballot_sync(0xffffffffu, valid && pp);
+        const int g0 = (threadIdx.x & 31) & ~(NBT - 1);
+        const unsigned gm = NBT >= 32 ? 0xffffffffu : ((1u << NBT) - 1u);
+        const unsigned abits = (ma >> g0) & gm, pbits = (mp >> g0) & gm;
+        tile_list_append(f, valid && kq == 0 && abits != 0, entry, abits | (pbits << 16), (unsigned)ntiles);
+        if (cfl) {
+            // speeds are non-negative floats: their bits order as unsigned integers
+            for (int o = 16; o > 0; o >>= 1) vm = max(vm, __shfl_xor_sync(0xffffffffu, vm, o));
+            if ((threadIdx.x & 31) == 0 && vm) atomicMax(P.gmax_cur, vm);
+        }
+    }
+}
+
 template <typename R, int B, bool DBA>
 __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_step(GridP g, FlagP f, KHTileP<R> P)
 {
     using S = KHTile<R, B>;
-    constexpr int NT = S::NT, T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, TPP = S::TPP;
+    constexpr int NT = S::NT, T = S::T, TB = S::TB, NBT = S::NBT, RB = S::RB, GT = S::GT;
     constexpr int E2 = S::E2, P2 = S::P2, E1 = S::E1, P1 = S::P1, FXW = S::FXW;
     constexpr int V = B * B;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -169,9 +219,9 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
     const QA<R> sFy{sFx.base + 4 * S::NFX, S::NFY};              // [T+1][T]  flux through the face above (x, y) at (y + 1) * T + x
     const QA<R> sU{sFy.base + 4 * S::NFY, S::NU};                // [T][T]    own cells' conserved fields
     R* sStage = sU.base + 4 * S::NU;            // [4][N1] phase-1 conserved inputs of the next tile, copied ahead
-    __shared__ int s_tile[TPP];                 // listed tiles: tbx | tby << 15 | halo-inside-domain << 30
-    __shared__ unsigned s_tmeta[TPP];           // bits 0..15 active blocks, 16..31 their parity
-    __shared__ int s_cnt;
+    __shared__ int s_tile[4];                   // tiles i .. i + 3 (slot i % 4): tbx | tby << 15 | halo-inside-domain << 30,
+                                                //   -1 past the end of the queue
+    __shared__ unsigned s_tmeta[4];             // bits 0..15 active blocks, 16..31 their parity
     __shared__ uint8_t s_npar[2][RB * RB], s_nact[2][RB * RB];   // neighbourhood of this tile and the next
     __shared__ int s_nx[NBT];
     __shared__ double s_run[4][NT / 32];
@@ -181,7 +231,6 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
     __shared__ double s_dt;
 
     const int tid = threadIdx.x;
-    const int G = gridDim.x;
     const int ntx = g.nx / T, nty = g.ny / T, ntiles = ntx * nty;
     const size_t nx = (size_t)g.nx;
     const bool cfl = P.cfl > 0.0;
@@ -236,274 +285,264 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
     const int ux = (ukb % TB) * B + uv % B, uy = (ukb / TB) * B + uv / B;
     const int o4 = ux + g.nx * uy;
 
-    for (long long j0 = 0; blockIdx.x + (long long)G * j0 < ntiles; j0 += TPP) {
-        // ---- scan: per-block bookkeeping, one list entry per tile with an active block
-        {
-            const long long tl = blockIdx.x + (long long)G * (j0 + tid / NBT);
-            const int kq = tid % NBT;
-            const bool valid = tl < ntiles;
-            const int tile = (int)tl;
-            int act = 0, pp = 0, entry = 0;
-            if (valid) {
-                const int tby = tile / ntx, tbx = tile - tby * ntx;
-                const int b = (tbx * TB + kq % TB) + g.nbx * (tby * TB + kq / TB);
-                const int X0 = tbx * T, Y0 = tby * T;
-                const bool inner = X0 >= 2 && X0 + T + 2 <= g.nx && Y0 >= 2 && Y0 + T + 2 <= g.ny;
-                entry = tbx | (tby << 15) | ((int)inner << 30);
-                pp = f.par_cur[b];
-                act = DBA ? (f.wake_cur[b] ? 1 : 0) : 1;
-                f.wake_clr[b] = 0;
-                if (!DBA) f.wake_nxt[b] = 1;
-                f.par_nxt[b] = (uint8_t)(pp ^ act);
-                if (P.conserved && !act)
-                    for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = 0.0;
-                if (cfl && !act) atomicMax(&s_vcta, __float_as_uint(P.vmax[b]));
-            }
-            count_stats(f.stats, act, valid);
-            const unsigned ma = __ballot_sync(0xffffffffu, valid && act);
-            const unsigned mp = __ballot_sync(0xffffffffu, valid && pp);
-            const int g0 = (tid & 31) & ~(NBT - 1);
-            const unsigned gm = NBT >= 32 ? 0xffffffffu : ((1u << NBT) - 1u);
-            const unsigned abits = (ma >> g0) & gm, pbits = (mp >> g0) & gm;
-            if (tid == 0) s_cnt = 0;
-            __syncthreads();
-            list_append(valid && kq == 0 && abits != 0, entry, (int)(abits | (pbits << 16)), s_tile,
-                        reinterpret_cast<int*>(s_tmeta), &s_cnt);
-            __syncthreads();
-        }
-        const int cnt = s_cnt;
-        // Tile i's phase-1 inputs (the conserved fields of the owning block's current
-        // buffer where it is active, of its other buffer where it is not) are copied
-        // into sStage while tile i-1 computes; each thread copies and later reads only
-        // its own phase-1 cell.  Within a step nothing writes what is copied: active
-        // blocks write their other buffer, which no neighbour reads this step (a
-        // neighbour reads an active block's current buffer).
-        auto neighbourhood = [&](int entry, int buf) {
-            if (tid < RB * RB) {
-                const int tbx = entry & 0x7fff, tby = (entry >> 15) & 0x7fff;
-                const int bx = wrap_p(tbx * TB + tid % RB - 1, g.nbx), by = wrap_p(tby * TB + tid / RB - 1, g.nby);
-                const int ob = bx + g.nbx * by;
-                s_npar[buf][tid] = f.par_cur[ob];
-                s_nact[buf][tid] = DBA ? (f.wake_cur[ob] ? 1 : 0) : 1;
-            }
-        };
-        struct TileAt {
-            int X0, Y0;
-            bool inner;       // the 2-cell halo stays inside the domain: no periodic wrap
-            long long base;   // index of the tile's first cell
-        };
-        auto tile_at = [&](int entry) -> TileAt {
-            const int X0 = (entry & 0x7fff) * T, Y0 = ((entry >> 15) & 0x7fff) * T;
-            return TileAt{X0, Y0, ((entry >> 30) & 1) != 0, (long long)X0 + (long long)nx * Y0};
-        };
-        auto cell_index = [&](const TileAt& t, int lx, int ly, int off) -> size_t {
-            return t.inner ? (size_t)(t.base + off)
-                           : (size_t)wrap_p(t.X0 + lx, g.nx) + nx * (size_t)wrap_p(t.Y0 + ly, g.ny);
-        };
-        auto prefetch = [&](const TileAt& t, int buf) {
-            if (h1) {
-                const size_t gi = cell_index(t, x1, y1, o1);
-                const bool act = s_nact[buf][r1];
-                const int par = s_npar[buf][r1];
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    cp_async_elem<sizeof(R)>(sStage + q * S::N1 + tid, P.U[q][act ? par : par ^ 1] + gi);
-            }
-            cp_async_commit();
-        };
-        if (cnt > 0) {
-            neighbourhood(s_tile[0], 0);
-            __syncthreads();
-            prefetch(tile_at(s_tile[0]), 0);
-        }
-        for (int i = 0; i < cnt; ++i) {
-            const int entry = s_tile[i];
-            const unsigned tm = s_tmeta[i];
-            const int nb = i & 1;                 // this tile's neighbourhood tables
-            const TileAt cur = tile_at(entry);
+    // Tile i's phase-1 inputs (the conserved fields of the owning block's current
+    // buffer where it is active, of its other buffer where it is not) are copied
+    // into sStage while tile i-1 computes; each thread copies and later reads only
+    // its own phase-1 cell.  Within a step nothing writes what is copied: active
+    // blocks write their other buffer, which no neighbour reads this step (a
+    // neighbour reads an active block's current buffer).
+    auto neighbourhood = [&](int entry, int buf) {
+        if (tid < RB * RB) {
             const int tbx = entry & 0x7fff, tby = (entry >> 15) & 0x7fff;
-            const long long base = cur.base;
-            if (tid < NBT) {
-                s_nx[tid] = 0;
-                s_vblk[tid] = 0u;
-            }
-            if (i + 1 < cnt) neighbourhood(s_tile[i + 1], nb ^ 1);
-
-            // 1. primitives on tile + 2, from the staged inputs
-            cp_async_wait0();
-            if (h1) {
-                const R v0 = sStage[tid], v1 = sStage[S::N1 + tid], v2 = sStage[2 * S::N1 + tid],
-                        v3 = sStage[3 * S::N1 + tid];
-                R r, pp, u, v;
-                kh_prim_of<R>(v0, v1, v2, v3, K, r, pp, u, v);
-                if (in1 && s_nact[nb][r1]) sU.put(y1 * T + x1, Q{v0, v1, v2, v3});
-                sW.put(s1, Q{r, pp, u, v});
-            }
-            __syncthreads();
-            if (i + 1 < cnt) prefetch(tile_at(s_tile[i + 1]), nb ^ 1);
-
-            // 2. gradients and half-step states on tile + 1; wake-up metric of own cells
-            if (h2) {
-                if (s_nact[nb][r2]) {
-                    const Q c = sW(s2), xp = sW(s2 + 1), xm = sW(s2 - 1), yp = sW(s2 + P2), ym = sW(s2 - P2);
-                    // rho_dx rho_dy p_dx p_dy vx_dx vx_dy vy_dx vy_dy
-                    R gr[8] = {kh_grad<R>(xp.a, xm.a, K.hx), kh_grad<R>(yp.a, ym.a, K.hy),
-                               kh_grad<R>(xp.b, xm.b, K.hx), kh_grad<R>(yp.b, ym.b, K.hy),
-                               kh_grad<R>(xp.c, xm.c, K.hx), kh_grad<R>(yp.c, ym.c, K.hy),
-                               kh_grad<R>(xp.d, xm.d, K.hx), kh_grad<R>(yp.d, ym.d, K.hy)};
-                    R rp, ppp, up, vp;
-                    kh_prime_of<R>(c.a, c.b, c.c, c.d, gr, K, rp, ppp, up, vp);
-                    sP.put(p2, Q{rp, ppp, up, vp});
-                    sGx.put(p2, Q{gr[0], gr[2], gr[4], gr[6]});
-                    sGy.put(p2, Q{gr[1], gr[3], gr[5], gr[7]});
-                    if (DBA && in2 && kh_metric<R>(gr) > (R)P.thr) s_nx[x2 / B + TB * (y2 / B)] = 1;
-                } else {
-                    const size_t gi = cell_index(cur, x2, y2, o2);
-                    sP.put(p2, Q{P.Wp[0][gi], P.Wp[1][gi], P.Wp[2][gi], P.Wp[3][gi]});
-                    sGx.put(p2, Q{P.Gd[0][gi], P.Gd[2][gi], P.Gd[4][gi], P.Gd[6][gi]});
-                    sGy.put(p2, Q{P.Gd[1][gi], P.Gd[3][gi], P.Gd[5][gi], P.Gd[7][gi]});
-                }
-            }
-            __syncthreads();
-
-            // 3. face fluxes.  Cell (x3, y3) owns the x face on its right (needed for rows
-            //    0 .. T-1) and the y face above it (columns 0 .. T-1); both are computed where
-            //    the cell's block is active and read back where it is not.
-            if (h3) {
-                if (s_nact[nb][r3]) {
-                    // face states from the +side cell (m) and this cell (p); getflux takes
-                    // rho, p, normal velocity, tangential velocity of both sides
-                    const Q w0 = sP(p3);
-                    if (xf3) {
-                        const Q w1 = sP(p3 + 1), g0 = sGx(p3), g1 = sGx(p3 + 1);
-                        R fM, fE, fX, fY;
-                        kh_getflux<R>(K, kh_face_m<R>(w1.a, g1.a, K.ex), kh_face_p<R>(w0.a, g0.a, K.ex),
-                                      kh_face_m<R>(w1.b, g1.b, K.ex), kh_face_p<R>(w0.b, g0.b, K.ex),
-                                      kh_face_m<R>(w1.c, g1.c, K.ex), kh_face_p<R>(w0.c, g0.c, K.ex),
-                                      kh_face_m<R>(w1.d, g1.d, K.ex), kh_face_p<R>(w0.d, g0.d, K.ex), fM, fE, fX, fY);
-                        sFx.put(y3 * FXW + x3 + 1, Q{fM, fE, fX, fY});
-                    }
-                    if (yf3) {
-                        const Q w1 = sP(p3 + P1), g0 = sGy(p3), g1 = sGy(p3 + P1);
-                        R fM, fE, fX, fY;
-                        kh_getflux<R>(K, kh_face_m<R>(w1.a, g1.a, K.ey), kh_face_p<R>(w0.a, g0.a, K.ey),
-                                      kh_face_m<R>(w1.b, g1.b, K.ey), kh_face_p<R>(w0.b, g0.b, K.ey),
-                                      kh_face_m<R>(w1.d, g1.d, K.ey), kh_face_p<R>(w0.d, g0.d, K.ey),
-                                      kh_face_m<R>(w1.c, g1.c, K.ey), kh_face_p<R>(w0.c, g0.c, K.ey), fM, fE, fX, fY);
-                        sFy.put((y3 + 1) * T + x3, Q{fM, fE, fY, fX});   // normal momentum is Momy here
-                    }
-                } else {
-                    const size_t gi = cell_index(cur, x3, y3, o3);
-                    if (xf3) sFx.put(y3 * FXW + x3 + 1, Q{P.Fl[0][gi], P.Fl[1][gi], P.Fl[2][gi], P.Fl[3][gi]});
-                    if (yf3) sFy.put((y3 + 1) * T + x3, Q{P.Fl[4][gi], P.Fl[5][gi], P.Fl[6][gi], P.Fl[7][gi]});
-                }
-            } else if (DBA && tid >= S::SC0 && tid < S::SC0 + 11 * NBT) {
-                // wake-up tests and scatter on the idle warps: self, the faces (the z faces wrap
-                // onto the block itself) and the in-plane diagonals (KH_DBA.cu:988-1044), one
-                // neighbour per thread; the self thread also records the block's test
-                const int t = tid_fresh() - S::SC0;
-                const int kt = t / 11, k = t - kt * 11;
-                if ((tm >> kt) & 1u) {
-                    const int nbk = block_nb_k(g, tbx * TB + kt % TB, tby * TB + kt / TB, 0, k);
-                    if (k == 0) f.next[nbk] = (uint8_t)s_nx[kt];
-                    if (s_nx[kt] && nbk >= 0) f.wake_nxt[nbk] = 1;
-                }
-            }
-            __syncthreads();
-
-            // 4. update of own active cells; ring persistence for blocks that may sleep
-            const bool own = h4 && ((tm >> ukb) & 1u);
-            double ch[4] = {0.0, 0.0, 0.0, 0.0};
-            if (own) {
-                const int dst = (int)((tm >> (16 + ukb)) & 1u) ^ 1;
-                const size_t gi = (size_t)(base + o4);
-                const int ui = uy * T + ux;
-                // fluxes (Mass, Energy, Momx, Momy) through the right, left, upper and lower faces
-                const Q fr = sFx(uy * FXW + ux + 1), fl = sFx(uy * FXW + ux);
-                const Q fu = sFy((uy + 1) * T + ux), fd = sFy(uy * T + ux);
-                const Q u0 = sU(ui);
-                const R c[4] = {kh_change<R>(K.dtdx, fr.a, fl.a, fu.a, fd.a), kh_change<R>(K.dtdx, fr.c, fl.c, fu.c, fd.c),
-                                kh_change<R>(K.dtdx, fr.d, fl.d, fu.d, fd.d), kh_change<R>(K.dtdx, fr.b, fl.b, fu.b, fd.b)};
-                const Q un{ka(u0.a, c[0]), ka(u0.b, c[1]), ka(u0.c, c[2]), ka(u0.d, c[3])};   // Mass Momx Momy Energy
-                P.U[0][dst][gi] = un.a;
-                P.U[1][dst][gi] = un.b;
-                P.U[2][dst][gi] = un.c;
-                P.U[3][dst][gi] = un.d;
-                if (P.conserved) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) ch[q] = (double)c[q];
-                }
-                if (!(isfinite(un.a) && isfinite(un.b) && isfinite(un.c) && isfinite(un.d))) raise_status(f.status, 5);
-                if (cfl) {
-                    R r, pp, uu, vv;
-                    kh_prim_of<R>(un.a, un.b, un.c, un.d, K, r, pp, uu, vv);
-                    atomicMax(&s_vblk[ukb], __float_as_uint(kh_speed<R>(r, pp, uu, vv, K.gam)));
-                }
-            } else if (DBA && tid >= S::PR0 && tid < S::PR0 + NBT * S::NRING) {
-                // ring persistence on the idle warps, from the shared tiles: ring cell e of
-                // tile block kt (bottom row, top row, left column, right column)
-                const int t = tid_fresh() - S::PR0;
-                const int kt = t / S::NRING, e = t - kt * S::NRING;
-                if (((tm >> kt) & 1u) && !s_nx[kt]) {
-                    const int bxl = e < B ? e : (e < 2 * B ? e - B : (e < 3 * B - 2 ? 0 : B - 1));
-                    const int byl = e < B ? 0 : (e < 2 * B ? B - 1 : (e < 3 * B - 2 ? e - 2 * B + 1 : e - 3 * B + 3));
-                    const int px = (kt % TB) * B + bxl, py = (kt / TB) * B + byl;
-                    const size_t gi = (size_t)(base + px + g.nx * py);
-                    const int pi = (py + 1) * P1 + px + 1;
-                    const Q hp = sP(pi), gx = sGx(pi), gy = sGy(pi);
-                    P.Wp[0][gi] = hp.a;
-                    P.Wp[1][gi] = hp.b;
-                    P.Wp[2][gi] = hp.c;
-                    P.Wp[3][gi] = hp.d;
-                    P.Gd[0][gi] = gx.a;
-                    P.Gd[1][gi] = gy.a;
-                    P.Gd[2][gi] = gx.b;
-                    P.Gd[3][gi] = gy.b;
-                    P.Gd[4][gi] = gx.c;
-                    P.Gd[5][gi] = gy.c;
-                    P.Gd[6][gi] = gx.d;
-                    P.Gd[7][gi] = gy.d;
-                    if (bxl == B - 1) {
-                        const Q fr = sFx(py * FXW + px + 1);
-                        P.Fl[0][gi] = fr.a;
-                        P.Fl[1][gi] = fr.b;
-                        P.Fl[2][gi] = fr.c;
-                        P.Fl[3][gi] = fr.d;
-                    }
-                    if (byl == B - 1) {
-                        const Q fu = sFy((py + 1) * T + px);
-                        P.Fl[4][gi] = fu.a;
-                        P.Fl[5][gi] = fu.b;
-                        P.Fl[6][gi] = fu.c;
-                        P.Fl[7][gi] = fu.d;
-                    }
-                }
-            }
-            if (P.conserved) {
-                // Mass, Energy, Momx, Momy order for the sums (Conserved/KH_DBA.cu:1561-1564)
-                double cm[1] = {ch[0]}, ce[1] = {ch[3]}, cx[1] = {ch[1]}, cy[1] = {ch[2]};
-                block_tree_sums<V, 1>(cm, s_run[0], s_bsum[0], 0);
-                block_tree_sums<V, 1>(ce, s_run[1], s_bsum[1], 0);
-                block_tree_sums<V, 1>(cx, s_run[2], s_bsum[2], 0);
-                block_tree_sums<V, 1>(cy, s_run[3], s_bsum[3], 0);
-                __syncthreads();
-            }
-            if (cfl) __syncthreads();
-            if (tid < NBT && ((tm >> tid) & 1u)) {
-                const int bx = tbx * TB + tid % TB, by = tby * TB + tid / TB;
-                const int b = bx + g.nbx * by;
-                if (cfl) {
-                    P.vmax[b] = __uint_as_float(s_vblk[tid]);
-                    atomicMax(&s_vcta, s_vblk[tid]);
-                }
-                if (P.conserved)
-                    for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = s_bsum[q][tid];
-            }
-            __syncthreads();                      // shared tiles and tables reused by the next tile
+            const int bx = wrap_p(tbx * TB + tid % RB - 1, g.nbx), by = wrap_p(tby * TB + tid / RB - 1, g.nby);
+            const int ob = bx + g.nbx * by;
+            s_npar[buf][tid] = f.par_cur[ob];
+            s_nact[buf][tid] = DBA ? (f.wake_cur[ob] ? 1 : 0) : 1;
         }
-        __syncthreads();                          // list reused by the next scan pass
+    };
+    struct TileAt {
+        int X0, Y0;
+        bool inner;       // the 2-cell halo stays inside the domain: no periodic wrap
+        long long base;   // index of the tile's first cell
+    };
+    auto tile_at = [&](int entry) -> TileAt {
+        const int X0 = (entry & 0x7fff) * T, Y0 = ((entry >> 15) & 0x7fff) * T;
+        return TileAt{X0, Y0, ((entry >> 30) & 1) != 0, (long long)X0 + (long long)nx * Y0};
+    };
+    auto cell_index = [&](const TileAt& t, int lx, int ly, int off) -> size_t {
+        return t.inner ? (size_t)(t.base + off)
+                       : (size_t)wrap_p(t.X0 + lx, g.nx) + nx * (size_t)wrap_p(t.Y0 + ly, g.ny);
+    };
+    auto prefetch = [&](const TileAt& t, int buf) {
+        if (h1) {
+            const size_t gi = cell_index(t, x1, y1, o1);
+            const bool act = s_nact[buf][r1];
+            const int par = s_npar[buf][r1];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                cp_async_elem<sizeof(R)>(sStage + q * S::N1 + tid, P.U[q][act ? par : par ^ 1] + gi);
+        }
+        cp_async_commit();
+    };
+    // The step's listed tiles (kh_tile_scan) are taken from the tile queue by thread GT,
+    // two tiles ahead: during phase 2 of tile i (GT has no phase-2 item) it reads the
+    // list entry of tile i + 2, taken during tile i - 1, into slot (i + 2) % 4 and takes
+    // the entry for tile i + 3, so the counter's atomic and the list load are never
+    // waited for on a barrier's path.
+    const int cnt = (int)min(__ldcg(f.tctr), (unsigned)ntiles);
+    int k_pend = 0;
+    auto take = [&](int k, int slot) {
+        if (k < cnt) {
+            s_tile[slot] = __ldcg(f.tlist + 2 * (size_t)k);
+            s_tmeta[slot] = (unsigned)__ldcg(f.tlist + 2 * (size_t)k + 1);
+        } else {
+            s_tile[slot] = -1;
+        }
+    };
+    if (tid == GT) {
+        const int k = (int)atomicAdd(f.tctr + 1, 2u);
+        take(k, 0);
+        take(k + 1, 1);
+        k_pend = (int)atomicAdd(f.tctr + 1, 1u);
+    }
+    __syncthreads();
+    if (s_tile[0] >= 0) {
+        neighbourhood(s_tile[0], 0);
+        __syncthreads();
+        prefetch(tile_at(s_tile[0]), 0);
+    }
+    for (int i = 0; s_tile[i & 3] >= 0; ++i) {
+        const int cs = i & 3;
+        const bool more = s_tile[(i + 1) & 3] >= 0;
+        const int entry = s_tile[cs];
+        const unsigned tm = s_tmeta[cs];
+        const int nb = i & 1;                 // this tile's neighbourhood tables
+        const TileAt cur = tile_at(entry);
+        const int tbx = entry & 0x7fff, tby = (entry >> 15) & 0x7fff;
+        const long long base = cur.base;
+        if (tid < NBT) {
+            s_nx[tid] = 0;
+            s_vblk[tid] = 0u;
+        }
+        if (more) neighbourhood(s_tile[(i + 1) & 3], nb ^ 1);
+
+        // 1. primitives on tile + 2, from the staged inputs
+        cp_async_wait0();
+        if (h1) {
+            const R v0 = sStage[tid], v1 = sStage[S::N1 + tid], v2 = sStage[2 * S::N1 + tid],
+                    v3 = sStage[3 * S::N1 + tid];
+            R r, pp, u, v;
+            kh_prim_of<R>(v0, v1, v2, v3, K, r, pp, u, v);
+            if (in1 && s_nact[nb][r1]) sU.put(y1 * T + x1, Q{v0, v1, v2, v3});
+            sW.put(s1, Q{r, pp, u, v});
+        }
+        __syncthreads();
+        if (more) prefetch(tile_at(s_tile[(i + 1) & 3]), nb ^ 1);
+
+        // 2. gradients and half-step states on tile + 1; wake-up metric of own cells
+        if (h2) {
+            if (s_nact[nb][r2]) {
+                const Q c = sW(s2), xp = sW(s2 + 1), xm = sW(s2 - 1), yp = sW(s2 + P2), ym = sW(s2 - P2);
+                // rho_dx rho_dy p_dx p_dy vx_dx vx_dy vy_dx vy_dy
+                R gr[8] = {kh_grad<R>(xp.a, xm.a, K.hx), kh_grad<R>(yp.a, ym.a, K.hy),
+                           kh_grad<R>(xp.b, xm.b, K.hx), kh_grad<R>(yp.b, ym.b, K.hy),
+                           kh_grad<R>(xp.c, xm.c, K.hx), kh_grad<R>(yp.c, ym.c, K.hy),
+                           kh_grad<R>(xp.d, xm.d, K.hx), kh_grad<R>(yp.d, ym.d, K.hy)};
+                R rp, ppp, up, vp;
+                kh_prime_of<R>(c.a, c.b, c.c, c.d, gr, K, rp, ppp, up, vp);
+                sP.put(p2, Q{rp, ppp, up, vp});
+                sGx.put(p2, Q{gr[0], gr[2], gr[4], gr[6]});
+                sGy.put(p2, Q{gr[1], gr[3], gr[5], gr[7]});
+                if (DBA && in2 && kh_metric<R>(gr) > (R)P.thr) s_nx[x2 / B + TB * (y2 / B)] = 1;
+            } else {
+                const size_t gi = cell_index(cur, x2, y2, o2);
+                sP.put(p2, Q{P.Wp[0][gi], P.Wp[1][gi], P.Wp[2][gi], P.Wp[3][gi]});
+                sGx.put(p2, Q{P.Gd[0][gi], P.Gd[2][gi], P.Gd[4][gi], P.Gd[6][gi]});
+                sGy.put(p2, Q{P.Gd[1][gi], P.Gd[3][gi], P.Gd[5][gi], P.Gd[7][gi]});
+            }
+        } else if (tid == GT) {
+            take(k_pend, (i + 2) & 3);           // slot (i + 2) % 4 held tile i - 2
+            k_pend = (int)atomicAdd(f.tctr + 1, 1u);
+        }
+        __syncthreads();
+
+        // 3. face fluxes.  Cell (x3, y3) owns the x face on its right (needed for rows
+        //    0 .. T-1) and the y face above it (columns 0 .. T-1); both are computed where
+        //    the cell's block is active and read back where it is not.
+        if (h3) {
+            if (s_nact[nb][r3]) {
+                // face states from the +side cell (m) and this cell (p); getflux takes
+                // rho, p, normal velocity, tangential velocity of both sides
+                const Q w0 = sP(p3);
+                if (xf3) {
+                    const Q w1 = sP(p3 + 1), g0 = sGx(p3), g1 = sGx(p3 + 1);
+                    R fM, fE, fX, fY;
+                    kh_getflux<R>(K, kh_face_m<R>(w1.a, g1.a, K.ex), kh_face_p<R>(w0.a, g0.a, K.ex),
+                                  kh_face_m<R>(w1.b, g1.b, K.ex), kh_face_p<R>(w0.b, g0.b, K.ex),
+                                  kh_face_m<R>(w1.c, g1.c, K.ex), kh_face_p<R>(w0.c, g0.c, K.ex),
+                                  kh_face_m<R>(w1.d, g1.d, K.ex), kh_face_p<R>(w0.d, g0.d, K.ex), fM, fE, fX, fY);
+                    sFx.put(y3 * FXW + x3 + 1, Q{fM, fE, fX, fY});
+                }
+                if (yf3) {
+                    const Q w1 = sP(p3 + P1), g0 = sGy(p3), g1 = sGy(p3 + P1);
+                    R fM, fE, fX, fY;
+                    kh_getflux<R>(K, kh_face_m<R>(w1.a, g1.a, K.ey), kh_face_p<R>(w0.a, g0.a, K.ey),
+                                  kh_face_m<R>(w1.b, g1.b, K.ey), kh_face_p<R>(w0.b, g0.b, K.ey),
+                                  kh_face_m<R>(w1.d, g1.d, K.ey), kh_face_p<R>(w0.d, g0.d, K.ey),
+                                  kh_face_m<R>(w1.c, g1.c, K.ey), kh_face_p<R>(w0.c, g0.c, K.ey), fM, fE, fX, fY);
+                    sFy.put((y3 + 1) * T + x3, Q{fM, fE, fY, fX});   // normal momentum is Momy here
+                }
+            } else {
+                const size_t gi = cell_index(cur, x3, y3, o3);
+                if (xf3) sFx.put(y3 * FXW + x3 + 1, Q{P.Fl[0][gi], P.Fl[1][gi], P.Fl[2][gi], P.Fl[3][gi]});
+                if (yf3) sFy.put((y3 + 1) * T + x3, Q{P.Fl[4][gi], P.Fl[5][gi], P.Fl[6][gi], P.Fl[7][gi]});
+            }
+        } else if (DBA && tid >= S::SC0 && tid < S::SC0 + 11 * NBT) {
+            // wake-up tests and scatter on the idle warps: self, the faces (the z faces wrap
+            // onto the block itself) and the in-plane diagonals (KH_DBA.cu:988-1044), one
+            // neighbour per thread; the self thread also records the block's test
+            const int t = tid_fresh() - S::SC0;
+            const int kt = t / 11, k = t - kt * 11;
+            if ((tm >> kt) & 1u) {
+                const int nbk = block_nb_k(g, tbx * TB + kt % TB, tby * TB + kt / TB, 0, k);
+                if (k == 0) f.next[nbk] = (uint8_t)s_nx[kt];
+                if (s_nx[kt] && nbk >= 0) f.wake_nxt[nbk] = 1;
+            }
+        }
+        __syncthreads();
+
+        // 4. update of own active cells; ring persistence for blocks that may sleep
+        const bool own = h4 && ((tm >> ukb) & 1u);
+        double ch[4] = {0.0, 0.0, 0.0, 0.0};
+        if (own) {
+            const int dst = (int)((tm >> (16 + ukb)) & 1u) ^ 1;
+            const size_t gi = (size_t)(base + o4);
+            const int ui = uy * T + ux;
+            // fluxes (Mass, Energy, Momx, Momy) through the right, left, upper and lower faces
+            const Q fr = sFx(uy * FXW + ux + 1), fl = sFx(uy * FXW + ux);
+            const Q fu = sFy((uy + 1) * T + ux), fd = sFy(uy * T + ux);
+            const Q u0 = sU(ui);
+            const R c[4] = {kh_change<R>(K.dtdx, fr.a, fl.a, fu.a, fd.a), kh_change<R>(K.dtdx, fr.c, fl.c, fu.c, fd.c),
+                            kh_change<R>(K.dtdx, fr.d, fl.d, fu.d, fd.d), kh_change<R>(K.dtdx, fr.b, fl.b, fu.b, fd.b)};
+            const Q un{ka(u0.a, c[0]), ka(u0.b, c[1]), ka(u0.c, c[2]), ka(u0.d, c[3])};   // Mass Momx Momy Energy
+            P.U[0][dst][gi] = un.a;
+            P.U[1][dst][gi] = un.b;
+            P.U[2][dst][gi] = un.c;
+            P.U[3][dst][gi] = un.d;
+            if (P.conserved) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) ch[q] = (double)c[q];
+            }
+            if (!(isfinite(un.a) && isfinite(un.b) && isfinite(un.c) && isfinite(un.d))) raise_status(f.status, 5);
+            if (cfl) {
+                R r, pp, uu, vv;
+                kh_prim_of<R>(un.a, un.b, un.c, un.d, K, r, pp, uu, vv);
+                atomicMax(&s_vblk[ukb], __float_as_uint(kh_speed<R>(r, pp, uu, vv, K.gam)));
+            }
+        } else if (DBA && tid >= S::PR0 && tid < S::PR0 + NBT * S::NRING) {
+            // ring persistence on the idle warps, from the shared tiles: ring cell e of
+            // tile block kt (bottom row, top row, left column, right column)
+            const int t = tid_fresh() - S::PR0;
+            const int kt = t / S::NRING, e = t - kt * S::NRING;
+            if (((tm >> kt) & 1u) && !s_nx[kt]) {
+                const int bxl = e < B ? e : (e < 2 * B ? e - B : (e < 3 * B - 2 ? 0 : B - 1));
+                const int byl = e < B ? 0 : (e < 2 * B ? B - 1 : (e < 3 * B - 2 ? e - 2 * B + 1 : e - 3 * B + 3));
+                const int px = (kt % TB) * B + bxl, py = (kt / TB) * B + byl;
+                const size_t gi = (size_t)(base + px + g.nx * py);
+                const int pi = (py + 1) * P1 + px + 1;
+                const Q hp = sP(pi), gx = sGx(pi), gy = sGy(pi);
+                P.Wp[0][gi] = hp.a;
+                P.Wp[1][gi] = hp.b;
+                P.Wp[2][gi] = hp.c;
+                P.Wp[3][gi] = hp.d;
+                P.Gd[0][gi] = gx.a;
+                P.Gd[1][gi] = gy.a;
+                P.Gd[2][gi] = gx.b;
+                P.Gd[3][gi] = gy.b;
+                P.Gd[4][gi] = gx.c;
+                P.Gd[5][gi] = gy.c;
+                P.Gd[6][gi] = gx.d;
+                P.Gd[7][gi] = gy.d;
+                if (bxl == B - 1) {
+                    const Q fr = sFx(py * FXW + px + 1);
+                    P.Fl[0][gi] = fr.a;
+                    P.Fl[1][gi] = fr.b;
+                    P.Fl[2][gi] = fr.c;
+                    P.Fl[3][gi] = fr.d;
+                }
+                if (byl == B - 1) {
+                    const Q fu = sFy((py + 1) * T + px);
+                    P.Fl[4][gi] = fu.a;
+                    P.Fl[5][gi] = fu.b;
+                    P.Fl[6][gi] = fu.c;
+                    P.Fl[7][gi] = fu.d;
+                }
+            }
+        }
+        if (P.conserved) {
+            // Mass, Energy, Momx, Momy order for the sums (Conserved/KH_DBA.cu:1561-1564)
+            double cm[1] = {ch[0]}, ce[1] = {ch[3]}, cx[1] = {ch[1]}, cy[1] = {ch[2]};
+            block_tree_sums<V, 1>(cm, s_run[0], s_bsum[0], 0);
+            block_tree_sums<V, 1>(ce, s_run[1], s_bsum[1], 0);
+            block_tree_sums<V, 1>(cx, s_run[2], s_bsum[2], 0);
+            block_tree_sums<V, 1>(cy, s_run[3], s_bsum[3], 0);
+            __syncthreads();
+        }
+        if (cfl) __syncthreads();
+        if (tid < NBT && ((tm >> tid) & 1u)) {
+            const int bx = tbx * TB + tid % TB, by = tby * TB + tid / TB;
+            const int b = bx + g.nbx * by;
+            if (cfl) {
+                P.vmax[b] = __uint_as_float(s_vblk[tid]);
+                atomicMax(&s_vcta, s_vblk[tid]);
+            }
+            if (P.conserved)
+                for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = s_bsum[q][tid];
+        }
+        __syncthreads();                      // shared tiles and tables reused by the next tile
     }
     if (cfl && tid == 0) atomicMax(P.gmax_cur, s_vcta);
+    if (tid == GT) tile_queue_done(f);
 }
 
 }  // namespace dba
