@@ -271,7 +271,8 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
         y2 = T;
     }
     const int r2 = kh_region<B, RB>(x2, y2), p2 = (y2 + 1) * P1 + x2 + 1, s2 = (y2 + 2) * P2 + x2 + 2;
-    const bool in2 = x2 >= 0 && x2 < T && y2 >= 0 && y2 < T;
+    // tile block of an own gradient cell (its wake-up test), -1 for the ring
+    const int nx2 = (x2 >= 0 && x2 < T && y2 >= 0 && y2 < T) ? x2 / B + TB * (y2 / B) : -1;
     const int o2 = x2 + g.nx * y2;
     // phase 3: face-owning cell (x3, y3) of columns and rows -1 .. T-1, skipping (-1, -1)
     const bool h3 = tid < S::N3;
@@ -393,7 +394,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                 sP.put(p2, Q{rp, ppp, up, vp});
                 sGx.put(p2, Q{gr[0], gr[2], gr[4], gr[6]});
                 sGy.put(p2, Q{gr[1], gr[3], gr[5], gr[7]});
-                if (DBA && in2 && kh_metric<R>(gr) > (R)P.thr) s_nx[x2 / B + TB * (y2 / B)] = 1;
+                if (DBA && nx2 >= 0 && kh_metric<R>(gr) > (R)P.thr) s_nx[nx2] = 1;
             } else {
                 const size_t gi = cell_index(cur, x2, y2, o2);
                 sP.put(p2, Q{P.Wp[0][gi], P.Wp[1][gi], P.Wp[2][gi], P.Wp[3][gi]});
@@ -441,10 +442,12 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
             // wake-up tests and scatter on the idle warps: self, the faces (the z faces wrap
             // onto the block itself) and the in-plane diagonals (KH_DBA.cu:988-1044), one
             // neighbour per thread; the self thread also records the block's test
+            // (the tile's entry is read again from shared memory: nothing is kept live for this)
             const int t = tid_fresh() - S::SC0;
             const int kt = t / 11, k = t - kt * 11;
-            if ((tm >> kt) & 1u) {
-                const int nbk = block_nb_k(g, tbx * TB + kt % TB, tby * TB + kt / TB, 0, k);
+            const int te = s_tile[i & 3];
+            if ((s_tmeta[i & 3] >> kt) & 1u) {
+                const int nbk = block_nb_k(g, (te & 0x7fff) * TB + kt % TB, ((te >> 15) & 0x7fff) * TB + kt / TB, 0, k);
                 if (k == 0) f.next[nbk] = (uint8_t)s_nx[kt];
                 if (s_nx[kt] && nbk >= 0) f.wake_nxt[nbk] = 1;
             }
@@ -484,11 +487,12 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
             // tile block kt (bottom row, top row, left column, right column)
             const int t = tid_fresh() - S::PR0;
             const int kt = t / S::NRING, e = t - kt * S::NRING;
-            if (((tm >> kt) & 1u) && !s_nx[kt]) {
+            const int te = s_tile[i & 3];
+            if (((s_tmeta[i & 3] >> kt) & 1u) && !s_nx[kt]) {
                 const int bxl = e < B ? e : (e < 2 * B ? e - B : (e < 3 * B - 2 ? 0 : B - 1));
                 const int byl = e < B ? 0 : (e < 2 * B ? B - 1 : (e < 3 * B - 2 ? e - 2 * B + 1 : e - 3 * B + 3));
                 const int px = (kt % TB) * B + bxl, py = (kt / TB) * B + byl;
-                const size_t gi = (size_t)(base + px + g.nx * py);
+                const size_t gi = (size_t)((te & 0x7fff) * T + px) + (size_t)g.nx * (size_t)(((te >> 15) & 0x7fff) * T + py);
                 const int pi = (py + 1) * P1 + px + 1;
                 const Q hp = sP(pi), gx = sGx(pi), gy = sGy(pi);
                 P.Wp[0][gi] = hp.a;
