@@ -326,6 +326,7 @@ def measure(args, name, w, steps, warmup, preroll, world=1, rank=0, local=0, cpu
             "ms_per_step": t_max / steps, "dtype": "f32" if w["precision"] else "f64",
             "config": {"workload": name, "model": w["model"], "grid": [cfg.nx, cfg.ny, cfg.nz],
                        "block": cfg.block, "conserved": bool(cfg.conserved), "mode": "DBA" if w["mode"] else "regular",
+                       "metric_eps": w["params"].get("metric_eps"),
                        "preroll_steps": preroll,
                        "active_fraction": cells / max(1, steps) / (total_blocks * prof["cells_per_block"]),
                        "l2": ("state larger than L2 (%.0f MB resident), no flush" if sim.info.device_bytes > 126e6
@@ -658,10 +659,18 @@ def main():
     ap.add_argument("--sweep-requests", type=int, default=256)
     ap.add_argument("--sweep-rate", type=float, default=200.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--sweep-seed", type=int, default=0)
+    ap.add_argument("--metric-eps", type=float, default=None,
+                    help="override the workload's wake-up threshold (Model B, KH), e.g. 0 to keep every block "
+                         "active for a profile of the all-active DBA step")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     w = WORKLOADS[args.workload]
+    if args.metric_eps is not None:
+        if w["model"] == "dendrite":
+            ap.error("--metric-eps applies to Model B and KH workloads")
+        w = dict(w, params=dict(w["params"], metric_eps=args.metric_eps))
+        WORKLOADS[args.workload] = w
     if args.impl == "reference":
         if args.steps > 40:
             args.steps = 40   # each reference step is a full dense CPU step; keep the run to minutes
