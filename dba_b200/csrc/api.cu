@@ -713,7 +713,7 @@ int dba_create(const dba_config* cfg, dba_ctx** out)
     }
     c->grid = c->esz == 8 ? step_grid<double>(cfg->model, c->D, c->B, c->sms) : step_grid<float>(cfg->model, c->D, c->B, c->sms);
     if (c->grid < 1) c->grid = c->sms;
-    if (cfg->model == DBA_MODEL_DENDRITE && c->esz == 4 && cfg->tiles && dendrite_tiles_ok(c->D, c->B, cfg->nx)) {
+    if (cfg->model == DBA_MODEL_DENDRITE && c->esz == 4 && cfg->tiles && dendrite_tiles_ok(c->D, c->B, cfg->nx, cfg->ny, cfg->nz)) {
         const size_t nt = (size_t)(cfg->nx / 32) * (cfg->ny / 8) * (cfg->nz / 8);
         c->den_tiles = true;
         c->grid = dendrite3_tile_grid(c->sms, (int)nt);

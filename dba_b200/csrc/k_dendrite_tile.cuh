@@ -65,10 +65,11 @@ __global__ void __launch_bounds__(256) dendrite3_tile_scan(GridP g, FlagP f)
         const long long it = t0 + threadIdx.x;
         const bool valid = it < nitems;
         const int tile = (int)(it / TBX), kq = (int)(it % TBX);
-        int act = 0, pp = 0, pT = 0;
+        int act = 0, pp = 0, pT = 0, entry = 0;
         if (valid) {
-            const int X0 = (tile % ntx) * TX, Y0 = ((tile / ntx) % nty) * B, Z0 = (tile / (ntx * nty)) * B;
-            const int b = (X0 / B + kq) + g.nbx * (Y0 / B + g.nby * (Z0 / B));
+            const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
+            entry = tx | (ty << 10) | (tz << 20);
+            const int b = (tx * TBX + kq) + g.nbx * (ty + g.nby * tz);
             pp = f.par_cur[b];
             pT = f.par_cur[nb + b];
             act = DBA ? ((f.wake_cur[b] ? 1 : 0) | (f.wake_cur[nb + b] ? 2 : 0)) : 3;
@@ -90,7 +91,7 @@ __global__ void __launch_bounds__(256) dendrite3_tile_scan(GridP g, FlagP f)
         const unsigned gm = (1u << TBX) - 1u;
         const unsigned meta = ((m0 >> g0) & gm) | (((m1 >> g0) & gm) << 4) | (((m2 >> g0) & gm) << 8) |
                               (((m3 >> g0) & gm) << 12);
-        tile_list_append(f, valid && kq == 0 && (meta & 0xffu) != 0, tile, meta, (unsigned)(nitems / TBX));
+        tile_list_append(f, valid && kq == 0 && (meta & 0xffu) != 0, entry, meta, (unsigned)(nitems / TBX));
     }
 }
 
@@ -116,10 +117,11 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
     const int kb = tid / (B * B);                 // this thread's block within the tile
     const int cx = kb * B + tid % B, cy = (tid / B) % B;   // and its column
 
-    auto tile_xyz = [&](int tile, int& X0, int& Y0, int& Z0) {
-        X0 = (tile % ntx) * TX;
-        Y0 = ((tile / ntx) % nty) * B;
-        Z0 = (tile / (ntx * nty)) * B;
+    // queue entries carry the tile's coordinates (tx | y << 10 | z << 20, in tiles)
+    auto tile_xyz = [&](int e, int& X0, int& Y0, int& Z0) {
+        X0 = (e & 1023) * TX;
+        Y0 = ((e >> 10) & 1023) * B;
+        Z0 = (e >> 20) * B;
     };
     auto build_nbr = [&](int idx, int st) {
         for (int r = tid; r < NR; r += NT) {

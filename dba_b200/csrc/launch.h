@@ -27,7 +27,11 @@ template <typename R>
 cudaError_t launch_dendrite(int D, int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
                             const DenP<R>& P);
 // FP32 3-D dendrite on 32x8x8-cell tiles (k_dendrite_tile.cuh)
-inline bool dendrite_tiles_ok(int D, int B, int nx) { return D == 3 && B == 8 && nx % 32 == 0; }
+// (tile coordinates are packed into 10-bit fields of the tile-queue entry)
+inline bool dendrite_tiles_ok(int D, int B, int nx, int ny, int nz)
+{
+    return D == 3 && B == 8 && nx % 32 == 0 && nx / 32 <= 1024 && ny / 8 <= 1024 && nz / 8 <= 1024;
+}
 int dendrite3_tile_grid(int sms, int ntiles);
 cudaError_t launch_dendrite3_tiles(bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
                                    const DenP<float>& P);
