@@ -257,26 +257,38 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
     const int r1 = kh_region<B, RB>(x1, y1), s1 = (y1 + 2) * P2 + x1 + 2;
     const bool in1 = x1 >= 0 && x1 < T && y1 >= 0 && y1 < T;
     const int o1 = x1 + g.nx * y1;
-    // phase 2: gradient cell (x2, y2): row -1 (columns 0 .. T-1), rows 0 .. T-1 (columns -1 .. T), row T
+    // Phases 2 and 3 take the tile's own cells on threads 0 .. T*T-1 (warps 0-7) and
+    // its 1-cell ring after them (warps 8-9): with one block per tile the own cells
+    // belong to the tile's active block, so warps 0-7 never take the branch that
+    // reads an inactive neighbour's persisted values.
+    // phase 2: gradient cell (x2, y2): own cells, then ring row -1, row T, column -1,
+    // column T (the ring's corners feed no face)
     const bool h2 = tid < S::N2;
     int x2, y2;
-    if (tid < T) {
-        x2 = tid;
-        y2 = -1;
-    } else if (tid < T + T * E1) {
-        x2 = (tid - T) % E1 - 1;
-        y2 = (tid - T) / E1;
+    if (tid < T * T) {
+        x2 = tid % T;
+        y2 = tid / T;
     } else {
-        x2 = tid - T - T * E1;
-        y2 = T;
+        const int k = tid - T * T, side = k / T, j = k - side * T;
+        x2 = side == 0 || side == 1 ? j : (side == 2 ? -1 : T);
+        y2 = side == 0 ? -1 : (side == 1 ? T : j);
     }
     const int r2 = kh_region<B, RB>(x2, y2), p2 = (y2 + 1) * P1 + x2 + 1, s2 = (y2 + 2) * P2 + x2 + 2;
     // tile block of an own gradient cell (its wake-up test), -1 for the ring
     const int nx2 = (x2 >= 0 && x2 < T && y2 >= 0 && y2 < T) ? x2 / B + TB * (y2 / B) : -1;
     const int o2 = x2 + g.nx * y2;
-    // phase 3: face-owning cell (x3, y3) of columns and rows -1 .. T-1, skipping (-1, -1)
+    // phase 3: face-owning cell (x3, y3) of columns and rows -1 .. T-1, skipping (-1, -1):
+    // own cells, then row -1 (its y faces), then column -1 (its x faces)
     const bool h3 = tid < S::N3;
-    const int x3 = (tid + 1) % (T + 1) - 1, y3 = (tid + 1) / (T + 1) - 1;
+    int x3, y3;
+    if (tid < T * T) {
+        x3 = tid % T;
+        y3 = tid / T;
+    } else {
+        const int k = tid - T * T;
+        x3 = k < T ? k : -1;
+        y3 = k < T ? -1 : k - T;
+    }
     const int r3 = kh_region<B, RB>(x3, y3), p3 = (y3 + 1) * P1 + x3 + 1;
     const bool xf3 = y3 >= 0, yf3 = x3 >= 0;
     const int o3 = x3 + g.nx * y3;
@@ -382,7 +394,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
 
         // 2. gradients and half-step states on tile + 1; wake-up metric of own cells
         if (h2) {
-            if (s_nact[nb][r2]) {
+            if ((NBT == 1 && tid < T * T) || s_nact[nb][r2]) {
                 const Q c = sW(s2), xp = sW(s2 + 1), xm = sW(s2 - 1), yp = sW(s2 + P2), ym = sW(s2 - P2);
                 // rho_dx rho_dy p_dx p_dy vx_dx vx_dy vy_dx vy_dy
                 R gr[8] = {kh_grad<R>(xp.a, xm.a, K.hx), kh_grad<R>(yp.a, ym.a, K.hy),
@@ -411,7 +423,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
         //    0 .. T-1) and the y face above it (columns 0 .. T-1); both are computed where
         //    the cell's block is active and read back where it is not.
         if (h3) {
-            if (s_nact[nb][r3]) {
+            if ((NBT == 1 && tid < T * T) || s_nact[nb][r3]) {
                 // face states from the +side cell (m) and this cell (p); getflux takes
                 // rho, p, normal velocity, tangential velocity of both sides
                 const Q w0 = sP(p3);
