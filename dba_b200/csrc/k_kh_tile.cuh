@@ -23,11 +23,13 @@
 //      the old values), FP64 per-block change sums for conserved DBA.
 //
 // A block persists what neighbours could later read as stale and cannot be
-// recomputed from its buffers -- the gradients and half-step states of its
-// 1-cell ring (they depend on neighbours' primitives as of that step) and the
-// fluxes of its right column and top row -- only when its own wake-up test is
-// negative: a block whose test is positive is active next step (it wakes
-// itself), so nothing it computes now is read stale.
+// recomputed from its buffers -- the half-step states with the x gradients of
+// its left column and with the y gradients of its bottom row (they depend on
+// neighbours' primitives as of that step; a face's flux is computed by the cell
+// left of or below it, so these are all an active neighbour reads of a sleeping
+// block's cells) and the fluxes of its right column and top row -- only when its
+// own wake-up test is negative: a block whose test is positive is active next
+// step (it wakes itself), so nothing it computes now is read stale.
 //
 // Launch shape: 416 threads (13 warps), so that each phase is one item per
 // thread (400, 320, 288 and 256 items) and no warp runs a second round while
@@ -408,10 +410,19 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                 sGy.put(p2, Q{gr[1], gr[3], gr[5], gr[7]});
                 if (DBA && nx2 >= 0 && kh_metric<R>(gr) > (R)P.thr) s_nx[nx2] = 1;
             } else {
-                const size_t gi = cell_index(cur, x2, y2, o2);
-                sP.put(p2, Q{P.Wp[0][gi], P.Wp[1][gi], P.Wp[2][gi], P.Wp[3][gi]});
-                sGx.put(p2, Q{P.Gd[0][gi], P.Gd[2][gi], P.Gd[4][gi], P.Gd[6][gi]});
-                sGy.put(p2, Q{P.Gd[1][gi], P.Gd[3][gi], P.Gd[5][gi], P.Gd[7][gi]});
+                // A face's flux is computed by its owner (the cell left of an x face, below a
+                // y face) when that owner is active; an inactive cell is therefore read only
+                // as the right cell of an x face (its block's left column: half-step state and
+                // x gradient) or the upper cell of a y face (bottom row: half-step state and
+                // y gradient), and only those persisted values are loaded
+                const bool rx = x2 >= 0 && x2 % B == 0 && y2 >= 0 && y2 < T;
+                const bool ry = y2 >= 0 && y2 % B == 0 && x2 >= 0 && x2 < T;
+                if (rx || ry) {
+                    const size_t gi = cell_index(cur, x2, y2, o2);
+                    sP.put(p2, Q{P.Wp[0][gi], P.Wp[1][gi], P.Wp[2][gi], P.Wp[3][gi]});
+                    if (rx) sGx.put(p2, Q{P.Gd[0][gi], P.Gd[2][gi], P.Gd[4][gi], P.Gd[6][gi]});
+                    if (ry) sGy.put(p2, Q{P.Gd[1][gi], P.Gd[3][gi], P.Gd[5][gi], P.Gd[7][gi]});
+                }
             }
         } else if (tid == GT) {
             take(k_pend, (i + 2) & 3);           // slot (i + 2) % 4 held tile i - 2
@@ -446,9 +457,14 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                     sFy.put((y3 + 1) * T + x3, Q{fM, fE, fY, fX});   // normal momentum is Momy here
                 }
             } else {
-                const size_t gi = cell_index(cur, x3, y3, o3);
-                if (xf3) sFx.put(y3 * FXW + x3 + 1, Q{P.Fl[0][gi], P.Fl[1][gi], P.Fl[2][gi], P.Fl[3][gi]});
-                if (yf3) sFy.put((y3 + 1) * T + x3, Q{P.Fl[4][gi], P.Fl[5][gi], P.Fl[6][gi], P.Fl[7][gi]});
+                // an inactive owner's face flux is read only across its block's edge: the
+                // x face of its right column, the y face of its top row
+                const bool lx = xf3 && (x3 < 0 || x3 % B == B - 1), ly = yf3 && (y3 < 0 || y3 % B == B - 1);
+                if (lx || ly) {
+                    const size_t gi = cell_index(cur, x3, y3, o3);
+                    if (lx) sFx.put(y3 * FXW + x3 + 1, Q{P.Fl[0][gi], P.Fl[1][gi], P.Fl[2][gi], P.Fl[3][gi]});
+                    if (ly) sFy.put((y3 + 1) * T + x3, Q{P.Fl[4][gi], P.Fl[5][gi], P.Fl[6][gi], P.Fl[7][gi]});
+                }
             }
         } else if (DBA && tid >= S::SC0 && tid < S::SC0 + 11 * NBT) {
             // wake-up tests and scatter on the idle warps: self, the faces (the z faces wrap
@@ -496,7 +512,11 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
             }
         } else if (DBA && tid >= S::PR0 && tid < S::PR0 + NBT * S::NRING) {
             // ring persistence on the idle warps, from the shared tiles: ring cell e of
-            // tile block kt (bottom row, top row, left column, right column)
+            // tile block kt (bottom row, top row, left column, right column).  Persisted is
+            // what a neighbour can read of the block while it sleeps (phase 2's rule): the
+            // half-step state and x gradient of the left column, the half-step state and
+            // y gradient of the bottom row, the x-face fluxes of the right column and the
+            // y-face fluxes of the top row
             const int t = tid_fresh() - S::PR0;
             const int kt = t / S::NRING, e = t - kt * S::NRING;
             const int te = s_tile[i & 3];
@@ -506,19 +526,27 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                 const int px = (kt % TB) * B + bxl, py = (kt / TB) * B + byl;
                 const size_t gi = (size_t)((te & 0x7fff) * T + px) + (size_t)g.nx * (size_t)(((te >> 15) & 0x7fff) * T + py);
                 const int pi = (py + 1) * P1 + px + 1;
-                const Q hp = sP(pi), gx = sGx(pi), gy = sGy(pi);
-                P.Wp[0][gi] = hp.a;
-                P.Wp[1][gi] = hp.b;
-                P.Wp[2][gi] = hp.c;
-                P.Wp[3][gi] = hp.d;
-                P.Gd[0][gi] = gx.a;
-                P.Gd[1][gi] = gy.a;
-                P.Gd[2][gi] = gx.b;
-                P.Gd[3][gi] = gy.b;
-                P.Gd[4][gi] = gx.c;
-                P.Gd[5][gi] = gy.c;
-                P.Gd[6][gi] = gx.d;
-                P.Gd[7][gi] = gy.d;
+                if (bxl == 0 || byl == 0) {
+                    const Q hp = sP(pi);
+                    P.Wp[0][gi] = hp.a;
+                    P.Wp[1][gi] = hp.b;
+                    P.Wp[2][gi] = hp.c;
+                    P.Wp[3][gi] = hp.d;
+                }
+                if (bxl == 0) {
+                    const Q gx = sGx(pi);
+                    P.Gd[0][gi] = gx.a;
+                    P.Gd[2][gi] = gx.b;
+                    P.Gd[4][gi] = gx.c;
+                    P.Gd[6][gi] = gx.d;
+                }
+                if (byl == 0) {
+                    const Q gy = sGy(pi);
+                    P.Gd[1][gi] = gy.a;
+                    P.Gd[3][gi] = gy.b;
+                    P.Gd[5][gi] = gy.c;
+                    P.Gd[7][gi] = gy.d;
+                }
                 if (bxl == B - 1) {
                     const Q fr = sFx(py * FXW + px + 1);
                     P.Fl[0][gi] = fr.a;
