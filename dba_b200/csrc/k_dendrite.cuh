@@ -101,6 +101,8 @@ __global__ void __launch_bounds__(kThreads) dendrite_step(GridP g, FlagP f, DenP
     __shared__ int s_list[NT], s_lmeta[NT];
     __shared__ int s_cnt;
     __shared__ int s_blk[K], s_meta[K], s_np[K], s_nT[K];
+    __shared__ int s_bx[K], s_by[K], s_bz[K];   // block coordinates of the round's blocks
+    static_assert(K * 14 <= NT, "one wake-up scatter thread per block, channel and neighbour");
 
     const int tid = threadIdx.x;
     const int G = gridDim.x;
@@ -137,27 +139,41 @@ __global__ void __launch_bounds__(kThreads) dendrite_step(GridP g, FlagP f, DenP
         for (int q0 = 0; q0 < cnt; q0 += K) {
             if (tid < K) {
                 int q = q0 + tid;
-                s_blk[tid] = q < cnt ? s_list[q] : -1;
+                const int blk = q < cnt ? s_list[q] : -1;
+                s_blk[tid] = blk;
                 s_meta[tid] = q < cnt ? s_lmeta[q] : 0;
+                if (blk >= 0) {
+                    s_bx[tid] = blk % g.nbx;
+                    s_by[tid] = (blk / g.nbx) % g.nby;
+                    s_bz[tid] = blk / (g.nbx * g.nby);
+                }
                 s_np[tid] = 0;
                 s_nT[tid] = 0;
             }
             __syncthreads();
-            // stage p and T of each block plus a 1-cell halo (owner's current buffer)
+            // stage p and T of each block plus a 1-cell halo (owner's current buffer).  2-D
+            // grids (small, L2-resident at the workloads' sizes) load both buffers beside the
+            // owner's parity and select afterwards, so the staging waits for one memory
+            // round trip instead of two; 3-D grids load the parity first
             for (int i = tid; i < K * TV; i += NT) {
                 const int k = i / TV;
-                const int blk = s_blk[k];
-                if (blk < 0) continue;
+                if (s_blk[k] < 0) continue;
                 const int j = i - k * TV;
                 const int lx = j % E, ly = (j / E) % E, lz = (D == 3) ? j / (E * E) : 0;
-                const int bx = blk % g.nbx, by = (blk / g.nbx) % g.nby, bz = blk / (g.nbx * g.nby);
-                const int gx = wrapc(bx * B + lx - 1, g.nx, g.bc);
-                const int gy = wrapc(by * B + ly - 1, g.ny, g.bc);
-                const int gz = (D == 3) ? wrapc(bz * B + lz - 1, g.nz, g.bc) : 0;
+                const int gx = wrapc(s_bx[k] * B + lx - 1, g.nx, g.bc);
+                const int gy = wrapc(s_by[k] * B + ly - 1, g.ny, g.bc);
+                const int gz = (D == 3) ? wrapc(s_bz[k] * B + lz - 1, g.nz, g.bc) : 0;
                 const int ob = gx / B + g.nbx * (gy / B + g.nby * ((D == 3) ? gz / B : 0));
                 const size_t gi = (size_t)gx + (size_t)g.nx * ((size_t)gy + (size_t)g.ny * gz);
-                sp[i] = (f.par_cur[ob] ? P.p[1] : P.p[0])[gi];
-                sT[i] = (f.par_cur[nb + ob] ? P.T[1] : P.T[0])[gi];
+                if constexpr (D == 2) {
+                    const uint8_t pp = f.par_cur[ob], pT = f.par_cur[nb + ob];
+                    const R p0 = P.p[0][gi], p1 = P.p[1][gi], T0 = P.T[0][gi], T1 = P.T[1][gi];
+                    sp[i] = pp ? p1 : p0;
+                    sT[i] = pT ? T1 : T0;
+                } else {
+                    sp[i] = (f.par_cur[ob] ? P.p[1] : P.p[0])[gi];
+                    sT[i] = (f.par_cur[nb + ob] ? P.T[1] : P.T[0])[gi];
+                }
             }
             __syncthreads();
 #pragma unroll
@@ -169,7 +185,7 @@ __global__ void __launch_bounds__(kThreads) dendrite_step(GridP g, FlagP f, DenP
                 const int m = s_meta[k];
                 const int lx = v % B, ly = (v / B) % B, lz = (D == 3) ? v / (B * B) : 0;
                 const int ti = k * TV + (lx + 1) + SY * (ly + 1) + SZ * (lz + 1);
-                const int bx = blk % g.nbx, by = (blk / g.nbx) % g.nby, bz = blk / (g.nbx * g.nby);
+                const int bx = s_bx[k], by = s_by[k], bz = s_bz[k];
                 const size_t gi = (size_t)(bx * B + lx) +
                                   (size_t)g.nx * ((size_t)(by * B + ly) + (size_t)g.ny * (size_t)((D == 3) ? bz * B + lz : 0));
                 const R pc = sp[ti], Tc = sT[ti];
@@ -190,17 +206,17 @@ __global__ void __launch_bounds__(kThreads) dendrite_step(GridP g, FlagP f, DenP
                 }
             }
             __syncthreads();
-            if (DBA && tid < K) {
-                const int blk = s_blk[tid];
-                if (blk >= 0) {
-                    const int m = s_meta[tid];
-                    if (m & 1) {
-                        f.next[blk] = (uint8_t)s_np[tid];
-                        if (s_np[tid]) wake_faces(g, f.wake_nxt, blk);
-                    }
-                    if (m & 2) {
-                        f.next[nb + blk] = (uint8_t)s_nT[tid];
-                        if (s_nT[tid]) wake_faces(g, f.wake_nxt + nb, blk);
+            // wake-up tests and scatter: self + 6 faces per channel (kernel.cu:577-634), one
+            // neighbour per thread (thread (2 k + ch) * 7 + n), from the block coordinates
+            if (DBA && tid < K * 14) {
+                const int k = tid / 14, r = tid - k * 14, ch = r / 7, n = r - ch * 7;
+                const int blk = s_blk[k];
+                if (blk >= 0 && ((s_meta[k] >> ch) & 1)) {
+                    const int t = ch ? s_nT[k] : s_np[k];
+                    if (n == 0) f.next[(size_t)ch * nb + blk] = (uint8_t)t;
+                    if (t) {
+                        const int nbk = block_nb_k(g, s_bx[k], s_by[k], s_bz[k], n);
+                        if (nbk >= 0) f.wake_nxt[(size_t)ch * nb + nbk] = 1;
                     }
                 }
             }
