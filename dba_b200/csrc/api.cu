@@ -66,6 +66,8 @@ struct dba_ctx {
     float* fstaging = nullptr;        // dba_read_field_f32: a field as floats (allocated on first use)
     bool kh_tiles = false;            // KH one-kernel step on 16x16-cell tiles (k_kh_tile.cuh)
     bool den_tiles = false;           // FP32 3-D dendrite on 32x8x8-cell tiles (k_dendrite_tile.cuh)
+    double lazy_ncells = 0;           // divisor of the FP32 conserved offset when the context is a slab of a
+                                      //   larger domain (dba_slab_rows); 0: this context's cells
     int* tlist = nullptr;             // tile queue of the tile kernels that take tiles dynamically
     unsigned* tctr = nullptr;         //   (2 ints per tile; counters, zeroed by each step's last CTA)
     float* kvmax = nullptr;           // KH tiles: per-block largest signal speed (CFL)
@@ -271,7 +273,7 @@ LazyP lazy_params(dba_ctx* c, long s, bool conserved_step)
     L.chg_prev = chg + 3 * ((s + 2) % 3);
     L.chg_clear = chg + 3 * ((s + 1) % 3);
     L.chg_cur = reinterpret_cast<unsigned long long*>(chg + 3 * (s % 3));
-    L.ncells = (double)c->n;
+    L.ncells = c->lazy_ncells > 0 ? c->lazy_ncells : (double)c->n;
     L.lazy = 1;
     L.accumulate = conserved_step ? 1 : 0;
     return L;
@@ -496,34 +498,38 @@ int gather(dba_ctx* c, const void* b0, const void* b1, const uint8_t* par, size_
     return cuda_status(cudaStreamSynchronize(c->st));
 }
 
-// rows [row0, row0 + nrows) of the two dendrite fields (p, T), current values (each
-// field's channel parity per block), packed field after field into out; or unpacked from
-// in into both buffers of those rows (the slab exchange's ghost rows)
+// rows [row0, row0 + nrows) of a slab's exchanged fields, packed field after field into
+// out (current values: each field's channel parity per block, or the one buffer of a
+// persisted field); or unpacked from in into both buffers of those rows (the slab
+// exchange's ghost rows).  Dendrite: p, T.  Model B: x, y, z and the persisted
+// potentials of x, y, z.
 struct RowsP {
-    void* f[2][2];   // [field][buffer]
+    void* f[6][2];   // [field][buffer] (a persisted field: the same array twice)
+    int ch[6];       // the field's flag channel (parity), -1 for a persisted field
     const uint8_t* par;
-    int nb, nx, B, nbx, row0, nrows;
+    int nf, nb, nx, B, nbx, row0, nrows;
 };
 
 template <typename R>
 __global__ void rows_pack_kernel(RowsP P, R* out)
 {
-    const size_t per = (size_t)P.nrows * P.nx, n = 2 * per;
+    const size_t per = (size_t)P.nrows * P.nx, n = (size_t)P.nf * per;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int q = i < per ? 0 : 1;
+        const int q = (int)(i / per);
         const size_t k = i - (size_t)q * per;
         const int y = P.row0 + (int)(k / P.nx), x = (int)(k % P.nx);
         const int b = x / P.B + P.nbx * (y / P.B);
-        out[i] = ((const R*)P.f[q][P.par[(size_t)q * P.nb + b] ? 1 : 0])[(size_t)y * P.nx + x];
+        const int buf = P.ch[q] < 0 ? 0 : (P.par[(size_t)P.ch[q] * P.nb + b] ? 1 : 0);
+        out[i] = ((const R*)P.f[q][buf])[(size_t)y * P.nx + x];
     }
 }
 
 template <typename R>
 __global__ void rows_unpack_kernel(RowsP P, const R* in)
 {
-    const size_t per = (size_t)P.nrows * P.nx, n = 2 * per;
+    const size_t per = (size_t)P.nrows * P.nx, n = (size_t)P.nf * per;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const int q = i < per ? 0 : 1;
+        const int q = (int)(i / per);
         const size_t gi = (size_t)P.row0 * P.nx + (i - (size_t)q * per);
         ((R*)P.f[q][0])[gi] = in[i];
         ((R*)P.f[q][1])[gi] = in[i];
@@ -531,7 +537,7 @@ __global__ void rows_unpack_kernel(RowsP P, const R* in)
 }
 
 // next-step wake flags of block rows [brow0, brow0 + nbrows) of every channel: read into
-// out ([channel][nbrows * nbx]), OR-ed in from in, or cleared
+// out ([channel][nbrows * nbx]), OR-ed in from in, cleared, or set from in
 __global__ void flag_rows_kernel(uint8_t* wake, int nch, int nb, int nbx, int brow0, int nbrows, uint8_t* out,
                                  const uint8_t* in, int op)
 {
@@ -541,7 +547,8 @@ __global__ void flag_rows_kernel(uint8_t* wake, int nch, int nb, int nbx, int br
         uint8_t* w = wake + (size_t)ch * nb + (size_t)brow0 * nbx + k;
         if (op == 0) out[i] = *w ? 1 : 0;
         else if (op == 1) *w = (*w || in[i]) ? 1 : 0;
-        else *w = 0;
+        else if (op == 2) *w = 0;
+        else *w = in[i] ? 1 : 0;
     }
 }
 
@@ -564,7 +571,7 @@ int field_on_device(dba_ctx* c, int field)
         return cuda_status(launch_gather_lazy(c->st, c->g, c->B, (const float*)c->state[field][0],
                                               (const float*)c->state[field][1], cur_par(c),
                                               c->lz + 3 * ((sn + 1) % 2) + field, c->lz + 6 + 3 * ((sn + 2) % 3) + field,
-                                              c->n, c->staging));
+                                              c->n, c->lazy_ncells > 0 ? c->lazy_ncells : (double)c->n, c->staging));
     }
     if (model == DBA_MODEL_KH && field < 4)
         return c->kh_tiles ? gather(c, c->state[field][0], c->state[field][1], cur_par(c), 0, 1, c->n, nullptr)
@@ -942,7 +949,7 @@ int dba_read_field(dba_ctx* c, int field, double* host)
                 cudaError_t e = launch_gather_lazy(c->st, c->g, c->B, (const float*)c->state[q][0],
                                                    (const float*)c->state[q][1], cur_par(c),
                                                    c->lz + 3 * ((sn + 1) % 2) + q, c->lz + 6 + 3 * ((sn + 2) % 3) + q, c->n,
-                                                   c->staging);
+                                                   c->lazy_ncells > 0 ? c->lazy_ncells : (double)c->n, c->staging);
                 if (e == cudaSuccess) e = cudaMemcpyAsync(dst, c->staging, c->n * sizeof(double), cudaMemcpyDeviceToHost, c->st);
                 if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
                 if (e != cudaSuccess) return cuda_status(e);
@@ -1007,7 +1014,8 @@ int slab_check(dba_ctx* c, int row0, int nrows)
     if (!c) return DBA_ERR_ARG;
     if (!c->initialized) return DBA_ERR_STATE;
     const dba_config& k = c->cfg;
-    if (k.model != DBA_MODEL_DENDRITE || k.nz != 1) return DBA_ERR_CONFIG;   // 2-D dendrite slabs only
+    if ((k.model != DBA_MODEL_DENDRITE && k.model != DBA_MODEL_MODELB) || k.nz != 1)
+        return DBA_ERR_CONFIG;   // 2-D dendrite and Model B slabs
     if (row0 < 0 || nrows < 1 || row0 + nrows > k.ny) return DBA_ERR_ARG;
     return DBA_OK;
 }
@@ -1016,9 +1024,22 @@ int slab_check(dba_ctx* c, int row0, int nrows)
 namespace {
 RowsP rows_params(dba_ctx* c, int row0, int nrows)
 {
-    RowsP P;
-    for (int q = 0; q < 2; ++q)
-        for (int k = 0; k < 2; ++k) P.f[q][k] = c->state[q][k];
+    RowsP P{};
+    if (c->cfg.model == DBA_MODEL_DENDRITE) {
+        P.nf = 2;
+        for (int q = 0; q < 2; ++q) {
+            for (int k = 0; k < 2; ++k) P.f[q][k] = c->state[q][k];
+            P.ch[q] = q;
+        }
+    } else {
+        P.nf = 6;
+        for (int q = 0; q < 3; ++q) {
+            for (int k = 0; k < 2; ++k) P.f[q][k] = c->state[q][k];
+            P.ch[q] = 0;
+            P.f[3 + q][0] = P.f[3 + q][1] = c->aux[q];
+            P.ch[3 + q] = -1;
+        }
+    }
     P.par = cur_par(c);
     P.nb = c->g.nb; P.nx = c->cfg.nx; P.B = c->B; P.nbx = c->g.nbx; P.row0 = row0; P.nrows = nrows;
     return P;
@@ -1052,11 +1073,47 @@ int dba_flag_rows(dba_ctx* c, int op, int brow0, int nbrows, void* dev_buf)
     if (!c) return DBA_ERR_ARG;
     int st = slab_check(c, brow0 * c->B, nbrows * c->B);
     if (st) return st;
-    if (op < 0 || op > 2 || (op < 2 && !dev_buf)) return DBA_ERR_ARG;
+    if (op < 0 || op > 3 || (op != 2 && !dev_buf)) return DBA_ERR_ARG;
     uint8_t* w = c->wake + ((c->step + 1) % 3) * (size_t)c->nch * c->g.nb;   // what the next step reads
     flag_rows_kernel<<<c->sms, 256, 0, c->st>>>(w, c->nch, c->g.nb, c->g.nbx, brow0, nbrows, (uint8_t*)dev_buf,
                                                  (const uint8_t*)dev_buf, op);
     DBA_TRY(cudaGetLastError());
+    return DBA_OK;
+}
+
+int dba_slab_rows(dba_ctx* c, int first_block_row, int block_rows, long long domain_cells)
+{
+    int st = slab_check(c, 0, 1);
+    if (st) return st;
+    if (c->cfg.model != DBA_MODEL_MODELB) return DBA_ERR_CONFIG;
+    // the FP64 conserved correction sums per-block values in a fixed tree over the
+    // context's blocks, which a slab cannot reproduce; the FP32 fixed-point totals can
+    if (c->cfg.conserved && !c->lazy) return DBA_ERR_CONFIG;
+    if (first_block_row < 0 || block_rows < 1 || first_block_row + block_rows > c->g.nby || domain_cells < 1)
+        return DBA_ERR_ARG;
+    DBA_TRY(cudaStreamSynchronize(c->st));
+    c->g.ob0 = first_block_row;
+    c->g.ob1 = first_block_row + block_rows;
+    c->lazy_ncells = (double)domain_cells;
+    // captured graphs hold the old grid parameters
+    for (auto& tier : c->graphs)
+        for (auto& row : tier)
+            for (auto& gexec : row)
+                if (gexec) {
+                    cudaGraphExecDestroy(gexec);
+                    gexec = nullptr;
+                }
+    return DBA_OK;
+}
+
+int dba_lazy_change(dba_ctx* c, int op, void* buf)
+{
+    if (!c || !buf || op < 0 || op > 1) return DBA_ERR_ARG;
+    if (!c->initialized) return DBA_ERR_STATE;
+    if (!c->lazy) return DBA_ERR_CONFIG;
+    long long* slot = c->lz + 6 + 3 * (c->step % 3);   // chg[s % 3] of the last step s
+    if (op == 0) DBA_TRY(cudaMemcpyAsync(buf, slot, 3 * sizeof(long long), cudaMemcpyDefault, c->st));
+    else DBA_TRY(cudaMemcpyAsync(slot, buf, 3 * sizeof(long long), cudaMemcpyDefault, c->st));
     return DBA_OK;
 }
 

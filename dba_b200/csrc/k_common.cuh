@@ -22,6 +22,11 @@ struct GridP {
     int nx, ny, nz;        // cells
     int nbx, nby, nbz, nb; // blocks
     int bc;                // 0 periodic, 1 zero-flux (clamp)
+    // Block rows [ob0, ob1) are this context's own; the others are ghost rows of a slab
+    // (a copy of a neighbouring rank's blocks): the Model B kernels never update, test or
+    // wake from a ghost block, while its flag still says whether its potentials are
+    // recomputed or read persisted.  Default: every row owned.
+    int ob0 = 0, ob1 = 1 << 30;
 };
 
 // Per-step flag pointers.  Arrays are [channel][nb].

@@ -9,11 +9,11 @@ namespace dba {
 
 cudaError_t launch_gather_lazy(cudaStream_t st, const GridP& g, int B, const float* b0, const float* b1,
                                const uint8_t* par, const long long* tot_q, const long long* chg_q, size_t count,
-                               double* out)
+                               double ncells, double* out)
 {
     size_t blocks = (count + kThreads - 1) / kThreads;
     int grid = (int)(blocks < 4096 ? blocks : 4096);
-    gather_lazy_kernel<<<grid, kThreads, 0, st>>>(g, B, b0, b1, par, tot_q, chg_q, count, out);
+    gather_lazy_kernel<<<grid, kThreads, 0, st>>>(g, B, b0, b1, par, tot_q, chg_q, count, ncells, out);
     return cudaGetLastError();
 }
 

@@ -115,7 +115,8 @@ __global__ void __launch_bounds__(kThreads) modelb_step(GridP g, FlagP f, MBP<R>
         int act = 0, meta = 0;
         if (valid) {
             int pp = f.par_cur[b];
-            act = DBA ? (f.wake_cur[b] ? 1 : 0) : 1;
+            const int by = (b / g.nbx) % g.nby;
+            act = (by >= g.ob0 && by < g.ob1) ? (DBA ? (f.wake_cur[b] ? 1 : 0) : 1) : 0;
             f.wake_clr[b] = 0;
             if (!DBA) f.wake_nxt[b] = 1;
             f.par_nxt[b] = (uint8_t)(pp ^ act);

@@ -340,7 +340,8 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
         int act = 0, meta = 0;
         if (valid) {
             int pp = f.par_cur[b];
-            act = DBA ? (f.wake_cur[b] ? 1 : 0) : 1;
+            const int by = (b / g.nbx) % g.nby;
+            act = (by >= g.ob0 && by < g.ob1) ? (DBA ? (f.wake_cur[b] ? 1 : 0) : 1) : 0;
             f.wake_clr[b] = 0;
             if (!DBA) f.wake_nxt[b] = 1;
             f.par_nxt[b] = (uint8_t)(pp ^ act);
@@ -498,9 +499,9 @@ __global__ void __launch_bounds__(kThreads) modelb_fast_step(GridP g, FlagP f, M
 static __global__ void __launch_bounds__(kThreads) gather_lazy_kernel(GridP g, int B, const float* b0, const float* b1,
                                                                       const uint8_t* par, const long long* tot_q,
                                                                       const long long* chg_q, size_t count,
-                                                                      double* out)
+                                                                      double ncells, double* out)
 {
-    const double C = (double)(*tot_q + *chg_q) * kFixUnit / (double)count;
+    const double C = (double)(*tot_q + *chg_q) * kFixUnit / ncells;
     for (size_t i = (size_t)blockIdx.x * kThreads + threadIdx.x; i < count; i += (size_t)gridDim.x * kThreads) {
         const int x = (int)(i % g.nx), y = (int)(i / g.nx);
         const int ob = x / B + g.nbx * (y / B);

@@ -331,7 +331,8 @@ __global__ void __launch_bounds__(256 / R, 4)
                 const int b = (tbx * TB + kq % TB) + g.nbx * (tby * TB + kq / TB);
                 entry = tbx | (tby << 16);
                 pp = f.par_cur[b];
-                act = DBA ? (f.wake_cur[b] ? 1 : 0) : 1;
+                const int by = tby * TB + kq / TB;
+                act = (by >= g.ob0 && by < g.ob1) ? (DBA ? (f.wake_cur[b] ? 1 : 0) : 1) : 0;
                 f.wake_clr[b] = 0;
                 if (!DBA) f.wake_nxt[b] = 1;
                 f.par_nxt[b] = (uint8_t)(pp ^ act);
@@ -395,6 +396,9 @@ __global__ void __launch_bounds__(256 / R, 4)
             const float* sy = sx + SV;
             const float* sz = sy + SV;
             const bool own = (tm >> kb) & 1u;
+            // potentials of this patch are recomputed where its block is active this step --
+            // listed here, or (a slab's ghost block, never listed) flagged by its owner
+            const bool fresh = own || s_nact[st][kb % TB + 1 + RB * (kb / TB + 1)];
 
             // ---- potentials of this patch (Calc_mu, kernel.cu:371-388)
             // Laplacians of the patch: every lane of the warp takes part (the row
@@ -405,7 +409,7 @@ __global__ void __launch_bounds__(256 / R, 4)
             quad_laps<SP, R>(K, sx, s0, lx_, cx_);
             quad_laps<SP, R>(K, sy, s0, ly_, cy_);
             quad_laps<SP, R>(K, sz, s0, lz_, cz_);
-            if (own) {
+            if (fresh) {
                 float wmax = -INFINITY;                      // largest |lap z| of the patch (wake test)
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
@@ -421,7 +425,7 @@ __global__ void __launch_bounds__(256 / R, 4)
                     *reinterpret_cast<float4*>(mu + MV + mi) = f4_of(uy[0], uy[1]);
                     *reinterpret_cast<float4*>(mu + 2 * MV + mi) = f4_of(uz[0], uz[1]);
                 }
-                if (DBA && wmax > P.thr) s_nx[st][kb] = 1;
+                if (DBA && own && wmax > P.thr) s_nx[st][kb] = 1;
             } else {
                 // inactive block inside the tile: its persisted ring (stale potentials)
 #pragma unroll

@@ -49,9 +49,11 @@ bool modelb_tiles_ok(int D, int B, int nx, int ny);
 int modelb_tile_grid(int B, int sms, int ntiles);
 cudaError_t launch_modelb_tiles(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f,
                                 const MBFastP& P, const MBFastBuf& Q, const LazyP& L, bool bulk);
+// ncells: the divisor of the conserved offset (the whole domain's cells; a slab's context
+// holds only part of it)
 cudaError_t launch_gather_lazy(cudaStream_t st, const GridP& g, int B, const float* b0, const float* b1,
                                const uint8_t* par, const long long* tot_q, const long long* chg_q, size_t count,
-                               double* out);
+                               double ncells, double* out);
 template <typename R>
 cudaError_t launch_kh(int B, bool dba_mode, int grid, cudaStream_t st, const GridP& g, const FlagP& f, const KHP<R>& P);
 template <typename R> cudaError_t launch_correct(int grid, cudaStream_t st, const GridP& g, const CorrP<R>& P);

@@ -145,6 +145,8 @@ def load_library():
             "dba_rows_pack": (_i, [V, _i, _i, V]),
             "dba_rows_unpack": (_i, [V, _i, _i, V]),
             "dba_flag_rows": (_i, [V, _i, _i, _i, V]),
+            "dba_slab_rows": (_i, [V, _i, _i, ctypes.c_longlong]),
+            "dba_lazy_change": (_i, [V, _i, V]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -322,6 +324,16 @@ class Simulation:
     def flag_rows(self, op, brow0, nbrows, dev_ptr=0):
         _check(self._L.dba_flag_rows(self._h, int(op), int(brow0), int(nbrows), ctypes.c_void_p(dev_ptr)),
                "dba_flag_rows")
+
+    def slab_rows(self, first_block_row, block_rows, domain_cells):
+        """dba_slab_rows: the context is a slab of a larger Model B domain; block rows
+        [first, first + count) are its own, the others ghosts."""
+        _check(self._L.dba_slab_rows(self._h, int(first_block_row), int(block_rows), int(domain_cells)),
+               "dba_slab_rows")
+
+    def lazy_change(self, op, ptr):
+        """dba_lazy_change: the last step's fixed-point change totals to (op 0) or from (op 1) ptr."""
+        _check(self._L.dba_lazy_change(self._h, int(op), ctypes.c_void_p(ptr)), "dba_lazy_change")
 
     def set_option(self, option, value):
         """dba_set_option: OPT_WAIT_LIMIT bounds the device retry loops (post-processing)."""

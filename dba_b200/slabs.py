@@ -1,8 +1,9 @@
-"""One 2-D dendrite domain split into y-slabs across ranks (one GPU each).
+"""One 2-D domain split into y-slabs across ranks (one GPU each): dendrite and Model B.
 
 The reference's CUDA-MPI programs decompose the domain across ranks and exchange,
 every step, the halo layers of the fields and the wake-up flags of the boundary
-blocks (example_Dendritic_growth/CUDA-MPI/dendrite.cpp:387-397, 459-644).  Here:
+blocks (example_Dendritic_growth/CUDA-MPI/dendrite.cpp:387-397, 459-644;
+example_Reactive_ModelB/CUDA-MPI/reaction.cpp:416-438, 529-552).  Here:
 
 * the global grid (nx, ny), DBA block edge B, is split into `world` slabs of
   H = ny / world rows (H a multiple of B); rank r owns global rows [r H, (r+1) H);
@@ -26,6 +27,24 @@ stale intermediates, so with the flags exchanged the slab run advances exactly
 the cells, with exactly the arithmetic, of the single-domain run: it equals it
 bit for bit (tests/test_slabs_gloo.py, two gloo ranks on CPU with the CPU
 restatement as the stepper; tests/test_gpu_slabs.py, engine contexts).
+
+Model B (ModelBSlabRun) reads, across a block edge, the chemical potentials of
+the neighbouring block -- recomputed where that block is active this step, its
+persisted values where it is not (the reference's stale reads) -- so its ghost
+blocks carry their owner's flags instead of being kept inactive:
+  1. halo: the first and last owned block rows go to the neighbours -- x, y, z, the
+     persisted potentials and the next step's flags of those blocks -- which write
+     them into their ghost rows (the flags set, not OR-ed);
+  2. the step; the context knows which block rows are its own (dba_slab_rows) and
+     never updates, tests or wakes from a ghost block, whose flag only says whether
+     its potentials are recomputed (from the ghost copy of x, y, z: the rows an own
+     cell reads lie within the ghost row) or read persisted;
+  3. wake-ups scattered into the ghost rows go to their owners and are OR-ed in;
+  4. FP32 conserved contexts: the step's fixed-point change totals are summed over
+     the ranks (exact integer sums), so every rank applies the whole domain's
+     conservation offset.
+The slab run again advances the cells of the single-domain run with the same
+arithmetic and equals it bit for bit.
 
 Communication: DistComm uses torch.distributed point-to-point operations (NCCL
 between GPUs, gloo on CPU) on the buffers the stepper hands out (CUDA tensors
@@ -51,8 +70,8 @@ class SlabLayout:
         return [(rank * self.H - self.B + k) % self.ny for k in range(self.local_ny)]
 
     def local_config(self, cfg):
-        """A copy of the global dendrite config for one slab (periodic in y: the ghost
-        rows stand between the slab and its wrap)."""
+        """A copy of the global config for one slab (periodic in y: the ghost rows stand
+        between the slab and its wrap)."""
         c = engine.Config()
         for k, _ in engine.Config._fields_:
             setattr(c, k, getattr(cfg, k))
@@ -69,8 +88,11 @@ class EngineStepper:
         self.torch = torch
         self.stream = torch.cuda.ExternalStream(sim.stream)
         dt = torch.float64 if sim.cfg.precision == 0 else torch.float32
-        self.rows = lambda: torch.empty(2 * layout.B * layout.nx, dtype=dt, device="cuda")
-        self.flags = lambda: torch.empty(2 * (layout.nx // layout.B), dtype=torch.uint8, device="cuda")
+        modelb = sim.cfg.model == engine.MODELS["modelb"]
+        nf, nch = (6, 1) if modelb else (2, 2)     # exchanged fields (dba_rows_pack), flag channels
+        self.rows = lambda: torch.empty(nf * layout.B * layout.nx, dtype=dt, device="cuda")
+        self.flags = lambda: torch.empty(nch * (layout.nx // layout.B), dtype=torch.uint8, device="cuda")
+        self.totals = lambda: torch.empty(3, dtype=torch.int64, device="cuda")
 
     def pack_rows(self, row0):
         t = self.rows()
@@ -90,6 +112,24 @@ class EngineStepper:
 
     def clear_flags(self, brow):
         self.sim.flag_rows(2, brow, 1)
+
+    def set_flags(self, brow, t):
+        self.sim.flag_rows(3, brow, 1, t.data_ptr())
+
+    def own_rows(self, first, count, domain_cells):
+        self.sim.slab_rows(first, count, domain_cells)
+
+    def conserved_totals(self):
+        """An FP32 conserved context keeps fixed-point totals that the ranks must share."""
+        return bool(self.sim.cfg.conserved) and self.sim.cfg.precision == 1
+
+    def get_totals(self):
+        t = self.totals()
+        self.sim.lazy_change(0, t.data_ptr())
+        return t
+
+    def put_totals(self, t):
+        self.sim.lazy_change(1, t.data_ptr())
 
     def step(self, n=1, mode=1):
         self.sim.step(n, mode)
@@ -119,6 +159,14 @@ class LocalComm:
         down, up = (rank - 1) % self.world, (rank + 1) % self.world
         return self.box[down][1], self.box[up][0]
 
+    def sum_posted(self):
+        """The sum over the ranks of what each posted as its first item."""
+        total = None
+        for r in range(self.world):
+            t = self.box[r][0]
+            total = t.clone() if total is None else total + t
+        return total
+
 
 class DistComm:
     """torch.distributed point-to-point exchange with the ring neighbours (NCCL or gloo).
@@ -137,6 +185,10 @@ class DistComm:
         for r in d.batch_isend_irecv(ops):
             r.wait()
 
+    def sum(self, t):
+        """In place: the sum over the ranks (exact for integer tensors)."""
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM, group=self.group)
+
 
 class SlabRun:
     """Drives one rank's slab (stepper) through the exchange protocol above.
@@ -144,8 +196,9 @@ class SlabRun:
     `step(n)` advances n DBA steps.  With DistComm every rank calls it; with LocalComm,
     `SlabRun.step_all(runs, n)` advances all slabs of the process together."""
 
-    def __init__(self, stepper, layout, rank, comm):
+    def __init__(self, stepper, layout, rank, comm, mode=1):
         self.s, self.L, self.rank, self.comm = stepper, layout, rank, comm
+        self.mode = mode                            # 1 DBA steps, 0 regular steps
         self.top_ghost = layout.H + layout.B        # first local row of the upper ghost block row
         self.top_gbrow = layout.nbr + 1
 
@@ -206,6 +259,89 @@ class SlabRun:
                 with r.s.ordered():
                     r.s.step(1, 1)
             phase(lambda r: r._flags_send(), lambda r, a, b: r._flags_recv(a, b))
+        for r in runs:
+            r.s.barrier()
+
+
+class ModelBSlabRun(SlabRun):
+    """Model B's slab protocol (module docstring): ghost blocks carry their owner's flags,
+    persisted potentials travel with the halo, conserved totals are summed over the ranks."""
+
+    def start(self):
+        L = self.L
+        self.s.own_rows(1, L.nbr, L.nx * L.ny)
+
+    def _halo_send(self):
+        L = self.L
+        return (self.s.pack_rows(L.B), self.s.pack_rows(L.H), self.s.get_flags(1), self.s.get_flags(L.nbr))
+
+    def _halo_recv(self, from_down, from_up, flags_from_down, flags_from_up):
+        self.s.unpack_rows(0, from_down)
+        self.s.unpack_rows(self.top_ghost, from_up)
+        self.s.set_flags(0, flags_from_down)
+        self.s.set_flags(self.top_gbrow, flags_from_up)
+
+    def _flags_recv(self, from_down, from_up):
+        # wake-ups the neighbours' steps scattered into their ghost rows, for my boundary rows
+        self.s.or_flags(1, from_down)
+        self.s.or_flags(self.L.nbr, from_up)
+
+    def step(self, n=1):
+        c = self.comm
+        with self.s.ordered():
+            for _ in range(n):
+                down, up, f_down, f_up = self._halo_send()
+                rd, ru, fd, fu = self.s.rows(), self.s.rows(), self.s.flags(), self.s.flags()
+                c.sendrecv(down, up, rd, ru)
+                c.sendrecv(f_down, f_up, fd, fu)
+                self._halo_recv(rd, ru, fd, fu)
+                self.s.step(1, 1 if self.mode else 0)
+                down, up = self._flags_send()
+                fd, fu = self.s.flags(), self.s.flags()
+                c.sendrecv(down, up, fd, fu)
+                self._flags_recv(fd, fu)
+                if self.s.conserved_totals():
+                    t = self.s.get_totals()
+                    c.sum(t)
+                    self.s.put_totals(t)
+
+    @staticmethod
+    def step_all(runs, n=1):
+        comm = runs[0].comm
+
+        def phase(send, recv):
+            for r in runs:
+                with r.s.ordered():
+                    comm.post(r.rank, *send(r))
+            for r in runs:
+                r.s.barrier()
+            for r in runs:
+                with r.s.ordered():
+                    recv(r, *comm.collect(r.rank))
+
+        def halo_send(r):
+            d, u, fd, fu = r._halo_send()
+            return (d, fd), (u, fu)
+
+        def halo_recv(r, from_down, from_up):
+            r._halo_recv(from_down[0], from_up[0], from_down[1], from_up[1])
+
+        for _ in range(n):
+            phase(halo_send, halo_recv)
+            for r in runs:
+                with r.s.ordered():
+                    r.s.step(1, 1 if r.mode else 0)
+            phase(lambda r: r._flags_send(), lambda r, a, b: r._flags_recv(a, b))
+            if runs[0].s.conserved_totals():
+                for r in runs:
+                    with r.s.ordered():
+                        comm.post(r.rank, r.s.get_totals(), None)
+                for r in runs:
+                    r.s.barrier()
+                total = comm.sum_posted()
+                for r in runs:
+                    with r.s.ordered():
+                        r.s.put_totals(total)
         for r in runs:
             r.s.barrier()
 

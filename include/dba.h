@@ -337,21 +337,37 @@ int dba_tip_profile(dba_ctx* ctx, int field, int dz, int* tip_x, int* tip_x_max)
 int dba_size_distribution(dba_ctx* ctx, int field, double* avg, long* volume, long* islands, long* sizes,
                           long max_sizes);
 
-/* ---- one 2-D dendrite domain split into y-slabs across contexts (one per GPU) ----
+/* ---- one 2-D domain split into y-slabs across contexts (one per GPU) ----
    The reference's CUDA-MPI programs (example_Dendritic_growth/CUDA-MPI/dendrite.cpp:387-397,
-   459-644) split the domain across ranks and exchange halo layers and wake flags each step.
-   Here each rank's context holds its slab plus one ghost block row on each side
-   (dba_b200/slabs.py drives the exchange over torch.distributed).  All three calls are
+   459-644; example_Reactive_ModelB/CUDA-MPI/reaction.cpp:416-438, 529-552) split the domain
+   across ranks and exchange halo layers and wake flags each step.  Here each rank's context
+   holds its slab plus one ghost block row on each side (dba_b200/slabs.py drives the
+   exchange over torch.distributed).  Dendrite and Model B (2-D).  The calls are
    asynchronous on the context's stream, take device pointers and work between steps.
-     dba_rows_pack   current values of p then T of rows [row0, row0 + nrows) -> dev_out
-                     (2 * nrows * nx values of the context's precision)
+     dba_rows_pack   current values of rows [row0, row0 + nrows) -> dev_out, field after
+                     field (nrows * nx values of the context's precision each): dendrite p, T;
+                     Model B x, y, z, then the persisted potentials of x, y, z
      dba_rows_unpack the same layout from dev_in into both buffers of those rows
-     dba_flag_rows   the next step's wake flags of block rows [brow0, brow0 + nbrows), both
-                     channels (p then T, nbrows * nbx bytes each): op 0 copies them to dev_buf,
-                     op 1 ORs dev_buf into them, op 2 clears them (dev_buf unused). */
+     dba_flag_rows   the next step's wake flags of block rows [brow0, brow0 + nbrows), every
+                     channel (dendrite p then T; nbrows * nbx bytes each): op 0 copies them to
+                     dev_buf, op 1 ORs dev_buf into them, op 2 clears them (dev_buf unused),
+                     op 3 sets them from dev_buf
+     dba_slab_rows   Model B: block rows [first_block_row, first_block_row + block_rows) are
+                     this context's own, the others ghosts (never updated, tested or woken
+                     from; their flags only say whether their potentials are recomputed or
+                     read persisted); domain_cells is the whole domain's cell count, the
+                     divisor of the FP32 conserved offset.  Not for FP64 conserved contexts
+                     (DBA_ERR_CONFIG: their correction sums per-block values in a fixed tree
+                     over one context's blocks).
+     dba_lazy_change FP32 conserved Model B: the fixed-point change totals (3 int64, 2^-40
+                     units) the last step added, copied to buf (op 0) or replaced from buf
+                     (op 1), host or device memory; the slab run sums them over the ranks
+                     before the next step. */
 int dba_rows_pack(dba_ctx* ctx, int row0, int nrows, void* dev_out);
 int dba_rows_unpack(dba_ctx* ctx, int row0, int nrows, const void* dev_in);
 int dba_flag_rows(dba_ctx* ctx, int op, int brow0, int nbrows, void* dev_buf);
+int dba_slab_rows(dba_ctx* ctx, int first_block_row, int block_rows, long long domain_cells);
+int dba_lazy_change(dba_ctx* ctx, int op, void* buf);
 
 /* Context options (no counterpart in the reference).
  *   DBA_OPT_WAIT_LIMIT  attempts a bounded device retry loop makes before it gives up

@@ -363,6 +363,17 @@ struct ModelB {
     std::vector<double> ch_x, ch_y, ch_z;
     std::vector<int> wake, next;
     double last_avg[3] = {0, 0, 0};
+    // Block rows [ob0, ob1) are this domain's own; the others are ghost rows of a slab
+    // (copies of a neighbouring rank's blocks): never updated, tested or woken from, while
+    // a ghost's flag still says whether its potentials are recomputed this step.  Default:
+    // every row owned.
+    int ob0 = 0, ob1 = 1 << 30;
+    bool owned(int bb) const
+    {
+        const int r = (bb / g.nbx) % g.nby;
+        return r >= ob0 && r < ob1;
+    }
+    bool owned_cell(int Y) const { return Y / g.by >= ob0 && Y / g.by < ob1; }
 
     // prm: dt dx chi_xy chi_xz chi_yz chi_xb chi_yb chi_zb vx vy vz rx ry rz n m
     //      ex ey ez ephi Mx My Mz Mphi x0 y0 z0 K z_crit p_gel k_0 Metric_eps
@@ -448,8 +459,16 @@ struct ModelB {
     void step_regular()                                        // kernel.cu:1060-1090
     {
         all_cells([&](int X, int Y, int Z, size_t i) { calc_mu_cell(X, Y, Z, i); });
-        all_cells([&](int X, int Y, int Z, size_t i) { update_cell(X, Y, Z, i); });
-        x = x_new; y = y_new; z = z_new;
+        all_cells([&](int X, int Y, int Z, size_t i) {
+            if (owned_cell(Y)) update_cell(X, Y, Z, i);
+        });
+        all_cells([&](int, int Y, int, size_t i) {
+            if (owned_cell(Y)) {
+                x[i] = x_new[i];
+                y[i] = y_new[i];
+                z[i] = z_new[i];
+            }
+        });
     }
     // per-block sum of one change array in TREE order over the block's cells
     double block_sum(const std::vector<double>& c, int bb) const
@@ -467,7 +486,7 @@ struct ModelB {
             if (wake[bb]) g.for_block(bb, [&](int X, int Y, int Z, size_t i) { calc_mu_cell(X, Y, Z, i); });
         });
         par_for(nb, g.n(), [&](int bb) {                       // Update_wakeup
-            if (wake[bb])
+            if (wake[bb] && owned(bb))
                 g.for_block(bb, [&](int X, int Y, int Z, size_t i) { update_cell(X, Y, Z, i); });
             else if (conserved)
                 g.for_block(bb, [&](int, int, int, size_t i) { ch_x[i] = 0; ch_y[i] = 0; ch_z[i] = 0; });
@@ -493,14 +512,14 @@ struct ModelB {
             x = x_new; y = y_new; z = z_new;                   // Swap_regular
         } else {
             par_for(nb, g.n(), [&](int bb) {                   // Swap_wakeup :469-517
-                if (wake[bb])
+                if (wake[bb] && owned(bb))
                     g.for_block(bb, [&](int, int, int, size_t i) { x[i] = x_new[i]; y[i] = y_new[i]; z[i] = z_new[i]; });
             });
         }
         for (int bb = 0; bb < nb; ++bb) {                      // Wakeup_Next :657-713
             int s = wake[bb];
             wake[bb] = 0;
-            if (s) {
+            if (s && owned(bb)) {
                 int nxt = 0;
                 g.for_block(bb, [&](int, int, int, size_t i) { if (metric[i] > eps_thr) nxt = 1; });
                 next[bb] = nxt;
@@ -837,6 +856,26 @@ void oracle_modelb_get_flags(void* h, int* wake, int* next)
     if (next) std::memcpy(next, m->next.data(), m->g.nb() * sizeof(int));
 }
 void oracle_modelb_last_avg(void* h, double* avg3) { std::memcpy(avg3, ((ModelB*)h)->last_avg, 24); }
+// slab runs: own block rows, and setting fields (0 x 1 y 2 z 4 dfdx 5 dfdy 6 dfdz) and flags
+void oracle_modelb_set_owned(void* h, int ob0, int ob1)
+{
+    auto* m = (ModelB*)h;
+    m->ob0 = ob0;
+    m->ob1 = ob1;
+}
+void oracle_modelb_set_field(void* h, int which, const double* in)
+{
+    auto* m = (ModelB*)h;
+    std::vector<double>* a[] = {&m->x, &m->y, &m->z, &m->b, &m->dfdx, &m->dfdy, &m->dfdz, &m->metric};
+    std::memcpy(a[which]->data(), in, m->g.n() * 8);
+    if (which < 3)
+        for (size_t i = 0; i < m->g.n(); ++i) m->b[i] = 1.0 - m->x[i] - m->y[i] - m->z[i];
+}
+void oracle_modelb_set_flags(void* h, const int* wake)
+{
+    auto* m = (ModelB*)h;
+    std::memcpy(m->wake.data(), wake, m->g.nb() * sizeof(int));
+}
 void oracle_modelb_free(void* h) { delete (ModelB*)h; }
 
 // ---- KH ----

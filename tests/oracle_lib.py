@@ -48,6 +48,9 @@ def lib():
             "oracle_modelb_get_flags": (None, [vp, _I, _I]),
             "oracle_modelb_last_avg": (None, [vp, _D]),
             "oracle_modelb_free": (None, [vp]),
+            "oracle_modelb_set_owned": (None, [vp, ctypes.c_int, ctypes.c_int]),
+            "oracle_modelb_set_field": (None, [vp, ctypes.c_int, _D]),
+            "oracle_modelb_set_flags": (None, [vp, _I]),
             "oracle_kh_new": (vp, [ctypes.c_int] * 4 + [_D, ctypes.c_int]),
             "oracle_kh_init_smooth": (None, [vp]),
             "oracle_kh_set_primitive": (None, [vp, _D, _D, _D, _D]),
@@ -154,6 +157,18 @@ class OracleModelB:
         a = np.empty(3)
         lib().oracle_modelb_last_avg(self.h, dptr(a))
         return a
+
+    def set_owned(self, ob0, ob1):
+        """Slab runs: block rows [ob0, ob1) are own, the others ghosts."""
+        lib().oracle_modelb_set_owned(self.h, int(ob0), int(ob1))
+
+    def set_field(self, name, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        lib().oracle_modelb_set_field(self.h, self.FIELDS.index(name), dptr(a))
+
+    def set_flags(self, wake):
+        a = np.ascontiguousarray(wake, dtype=np.int32)
+        lib().oracle_modelb_set_flags(self.h, iptr(a))
 
     def __del__(self):
         if getattr(self, "h", None):
