@@ -235,7 +235,11 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
                 float* Tout = ((tm >> (12 + kb)) & 1u) ? P.T[0] : P.T[1];
                 int si = PL + (cy + 1) * SP + cx + 4;        // plane z = 0 of this column
                 float pm = sp[si - PL], pc = sp[si], Tm = sT[si - PL], Tc = sT[si];
-                bool wp = false, wT = false, bad = false;
+                bool wp = false, wT = false;
+                // NaN once any stored value is not finite (x * 0 is 0 only for finite x);
+                // the zero comes from a kernel parameter, so it cannot be folded away
+                const float zero = __fmul_rn(dt, 0.f);
+                float chk = zero;
                 const size_t gcol = (size_t)(X0 + cx) + nx * (size_t)(Y0 + cy);
 #pragma unroll 2
                 for (int z = 0; z < B; ++z) {
@@ -247,19 +251,19 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
                                               f2, f3, dt, delta, eps2, gam);
                         pout[gi] = pn;
                         wp |= pn >= thr_p && pn <= thr_p_hi;
-                        bad |= !isfinite(pn);
+                        chk = __fmaf_rn(pn, zero, chk);
                     }
                     if (Ta) {
                         const float Tn = den_T_new<float, DBA>(Tc, sT[si + 1], sT[si - 1], sT[si + SP], sT[si - SP],
                                                                Tq, Tm, pa, pn, pc, f1, dt);
                         Tout[gi] = Tn;
                         wT |= fabsf(Tn - Tc) >= thr_T;
-                        bad |= !isfinite(Tn);
+                        chk = __fmaf_rn(Tn, zero, chk);
                     }
                     pm = pc; pc = pq; Tm = Tc; Tc = Tq;
                     si += PL;
                 }
-                if (bad) raise_status(f.status, 5);
+                if (!(chk == 0.f)) raise_status(f.status, 5);
                 if (DBA && wp) s_np[kb] = 1;
                 if (DBA && wT) s_nT[kb] = 1;
             }

@@ -63,6 +63,10 @@ __device__ __forceinline__ float kq(float a)
 }
 __device__ __forceinline__ double kq(double a) { return __dsqrt_rn(a); }
 
+// fused multiply-add with a single rounding (non-finite checks only: no result depends on it)
+__device__ __forceinline__ float kfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double kfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 __device__ __forceinline__ float krcp(float a)
 {
     float r;

@@ -504,7 +504,11 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
 #pragma unroll
                 for (int q = 0; q < 4; ++q) ch[q] = (double)c[q];
             }
-            if (!(isfinite(un.a) && isfinite(un.b) && isfinite(un.c) && isfinite(un.d))) raise_status(f.status, 5);
+            // NaN once any stored value is not finite (x * 0 is 0 only for finite x; the
+            // zero is computed from a kernel parameter, so it cannot be folded away)
+            const R zero = km(K.hdt, (R)0);
+            const R chk = kfma(un.a, zero, kfma(un.b, zero, kfma(un.c, zero, km(un.d, zero))));
+            if (!(chk == (R)0)) raise_status(f.status, 5);
             if (cfl) {
                 R r, pp, uu, vv;
                 kh_prim_of<R>(un.a, un.b, un.c, un.d, K, r, pp, uu, vv);
