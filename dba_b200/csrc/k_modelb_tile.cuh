@@ -218,6 +218,7 @@ __global__ void __launch_bounds__(256 / R, 4)
     const int G = gridDim.x;
     const int ntx = g.nx / T, nty = g.ny / T, ntiles = ntx * nty;
     const size_t nx = (size_t)g.nx;
+    const bool ghosts = g.ob0 > 0 || g.ob1 < g.nby;     // a slab with ghost block rows
     if (tid < 3) {
         s_Cf[tid] = lazy_offset(L, tid);
         s_fix[tid] = 0ull;
@@ -398,7 +399,7 @@ __global__ void __launch_bounds__(256 / R, 4)
             const bool own = (tm >> kb) & 1u;
             // potentials of this patch are recomputed where its block is active this step --
             // listed here, or (a slab's ghost block, never listed) flagged by its owner
-            const bool fresh = own || s_nact[st][kb % TB + 1 + RB * (kb / TB + 1)];
+            const bool fresh = own || (ghosts && s_nact[st][kb % TB + 1 + RB * (kb / TB + 1)]);
 
             // ---- potentials of this patch (Calc_mu, kernel.cu:371-388)
             // Laplacians of the patch: every lane of the warp takes part (the row
