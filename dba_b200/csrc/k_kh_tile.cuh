@@ -147,6 +147,7 @@ template <typename R, int B> struct KHTile {
     static_assert(T % B == 0 && B >= 2 && NBT <= 16, "tile shape");
     static_assert(N1 <= NT && N2 <= NT && N3 <= NT && T * T <= NT, "one item per thread and phase");
     static_assert(SC0 + 11 * NBT <= NT && PR0 + NBT * NRING <= NT, "bookkeeping on idle warps");
+    static_assert(B * B % 32 == 0 && T * T % 32 == 0, "a warp's update cells lie in one block");
     static_assert(GT >= N2 && GT >= SC0 + 11 * NBT && GT >= PR0 + NBT * NRING, "queue thread without phase items");
 };
 
@@ -510,9 +511,15 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
             const R chk = kfma(un.a, zero, kfma(un.b, zero, kfma(un.c, zero, km(un.d, zero))));
             if (!(chk == (R)0)) raise_status(f.status, 5);
             if (cfl) {
+                // the block's largest signal speed: a warp maximum, then one shared atomic per
+                // warp (a warp's update cells lie in one block, and own is the same on all its
+                // lanes); speeds are non-negative, so their bits order as unsigned integers
                 R r, pp, uu, vv;
                 kh_prim_of<R>(un.a, un.b, un.c, un.d, K, r, pp, uu, vv);
-                atomicMax(&s_vblk[ukb], __float_as_uint(kh_speed<R>(r, pp, uu, vv, K.gam)));
+                unsigned v = __float_as_uint(kh_speed<R>(r, pp, uu, vv, K.gam));
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+                if ((tid & 31) == 0) atomicMax(&s_vblk[ukb], v);
             }
         } else if (DBA && tid >= S::PR0 && tid < S::PR0 + NBT * S::NRING) {
             // ring persistence on the idle warps, from the shared tiles: ring cell e of
