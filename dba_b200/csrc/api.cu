@@ -228,6 +228,7 @@ KHTileP<R> kh_tile_params(dba_ctx* c, bool dba_mode, long s)
     P.gmax_cur = c->kgmax + s % 3;
     P.gmax_clear = c->kgmax + (s + 1) % 3;
     P.time = c->ktime;
+    P.Kc = kh_consts<R>(k.dt, P.dx, P.dy, P.vol, P.gamma);
     return P;
 }
 

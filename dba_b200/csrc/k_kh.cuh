@@ -87,7 +87,7 @@ struct KHK {
 };
 
 template <typename R>
-__device__ __forceinline__ KHK<R> kh_consts(double dt, double dx, double dy, double vol, double gamma)
+__host__ __device__ __forceinline__ KHK<R> kh_consts(double dt, double dx, double dy, double vol, double gamma)
 {
     KHK<R> K;
     K.vol = (R)vol;

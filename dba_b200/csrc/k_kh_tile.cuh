@@ -69,6 +69,9 @@ struct KHTileP {
     unsigned* gmax_cur;           // this step's maximum (atomicMax)
     unsigned* gmax_clear;         // the slot the next step fills
     double* time;                 // simulated time
+    // the formula constants (kh_consts) computed on the host, read by the kernel from the
+    // parameter space; hdt and dtdx are replaced in the kernel by those of the step's dt
+    KHK<R> Kc;
 };
 
 // largest signal speed of a cell: sound speed + flow speed
@@ -231,7 +234,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
     __shared__ double s_bsum[4][NBT];
     __shared__ unsigned s_vblk[NBT];            // this tile's blocks' largest speed (float bits)
     __shared__ unsigned s_vcta;                 // this CTA's largest speed over its blocks
-    __shared__ double s_dt;
+    __shared__ R s_hdt, s_dtdx;                 // the step's dt-dependent constants
 
     const int tid = threadIdx.x;
     const int ntx = g.nx / T, nty = g.ny / T, ntiles = ntx * nty;
@@ -246,12 +249,15 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                 *P.time += dt;
             }
         }
-        s_dt = dt;
+        const KHK<R> Kd = kh_consts<R>(dt, P.dx, P.dy, P.vol, P.gamma);
+        s_hdt = Kd.hdt;
+        s_dtdx = Kd.dtdx;
         s_vcta = 0u;
     }
     __syncthreads();
-    const double dtc = s_dt;
-    const KHK<R> K = kh_consts<R>(dtc, P.dx, P.dy, P.vol, P.gamma);
+    KHK<R> K = P.Kc;
+    K.hdt = s_hdt;
+    K.dtdx = s_dtdx;
 
     // This thread's item in each phase; the same tile-local cells for every tile.
     // phase 1: primitive cell (x1, y1) of the tile + 2
