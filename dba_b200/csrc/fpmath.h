@@ -18,6 +18,8 @@
  *   atan : |x| <= tan(pi/8): t = x; below tan(3pi/8): t = (x-1)/(x+1) and pi/4
  *          added; above: t = 1/x and the result reflected about pi/2;
  *          atan(t) = t + t z P(z) (z = t^2).
+ * dba_atanf is the FP32 arctangent of the FP32 dendrite kernels (same form
+ * without the middle interval).
  * Only +, -, *, /, fma() and exponent-bit manipulation are used.  fma() is
  * correctly rounded on both sides, so the results are bit-identical as long as
  * neither compiler contracts the plain expressions (host: -ffp-contract=off;
@@ -130,6 +132,31 @@ static DBA_FM_HD double dba_atan(double x)
         r = DBA_FM_PIO2_HI - (at - DBA_FM_PIO2_LO);
     }
     return x < 0.0 ? -r : r;
+}
+
+/* FP32 arctangent of the FP32 dendrite kernels (throughput precision; the FP64
+   kernels and the checker use dba_atan): |x| > 1 is reflected through t = 1/|x|,
+   atan x = pi/2 - atan t, and atan(t) = t + t z Q(z) with z = t^2 in [0, 1] and Q
+   the 9-term fit of gen_fpmath.py.  With a correctly rounded reciprocal (the host
+   build) the error is within 1.5 ulp (tested against mpmath); the device takes the
+   reciprocal from rcp.approx (within 1 ulp of 1/|x|, which moves atan t by at most
+   about one more ulp of the result).  NaN propagates; +-inf gives +-pi/2.  No
+   product below feeds an addition, so no compiler contraction can change it. */
+static DBA_FM_HD float dba_atanf(float x)
+{
+    const float a = fabsf(x);
+#ifdef __CUDA_ARCH__
+    float ra;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(ra) : "f"(a));
+#else
+    const float ra = 1.0f / a;
+#endif
+    const bool big = a > 1.0f;
+    const float t = big ? ra : a;
+    const float z = t * t;
+    float r = fmaf(t * z, dba_fm_atanf_poly(z), t);
+    if (big) r = (DBA_FM_PIO2F_HI - r) + DBA_FM_PIO2F_LO;
+    return copysignf(r, x);
 }
 
 /* tanh from the shared exponential, sign(x) (1 - e^(-2|x|)) / (1 + e^(-2|x|)):

@@ -1,6 +1,6 @@
 /* Generated by gen_fpmath.py -- do not edit by hand. */
 #pragma once
-/* fit errors (absolute, on the remainder functions): exp 3.404e-18, log 3.741e-17, atan 2.098e-17 */
+/* fit errors (absolute, on the remainder functions): exp 3.404e-18, log 3.741e-17, atan 2.098e-17, FP32 atan 1.560e-08 (before rounding its coefficients to float) */
 #define DBA_FM_DEG_EXP 11
 #define DBA_FM_DEG_LOG 8
 #define DBA_FM_DEG_ATAN 12
@@ -14,6 +14,8 @@
 #define DBA_FM_TAN_PI8 (0.41421356237309503)
 #define DBA_FM_TAN_3PI8 (2.414213562373095)
 #define DBA_FM_SQRT2 (1.4142135623730951)
+#define DBA_FM_PIO2F_HI (1.5707963705062866f)
+#define DBA_FM_PIO2F_LO (-4.371138828673793e-08f)
 #ifndef DBA_FM_HD
 #ifdef __CUDACC__
 #define DBA_FM_HD __host__ __device__ __forceinline__
@@ -65,5 +67,18 @@ static DBA_FM_HD double dba_fm_atan_poly(double x)
     p = fma(p, x, -0.1428571428571149);
     p = fma(p, x, 0.19999999999999993);
     p = fma(p, x, -0.3333333333333333);
+    return p;
+}
+static DBA_FM_HD float dba_fm_atanf_poly(float x)
+{
+    float p = -0.002386418404057622f;
+    p = fmaf(p, x, 0.01350557804107666f);
+    p = fmaf(p, x, -0.035868171602487564f);
+    p = fmaf(p, x, 0.06249900907278061f);
+    p = fmaf(p, x, -0.08656762540340424f);
+    p = fmaf(p, x, 0.11033736169338226f);
+    p = fmaf(p, x, -0.14278565347194672f);
+    p = fmaf(p, x, 0.19999739527702332f);
+    p = fmaf(p, x, -0.3333333134651184f);
     return p;
 }

@@ -35,7 +35,7 @@ struct DenP {
 
 template <typename R> __device__ __forceinline__ R atan_r(R v);
 template <> __device__ __forceinline__ double atan_r<double>(double v) { return dba_atan(v); }
-template <> __device__ __forceinline__ float atan_r<float>(float v) { return atanf(v); }
+template <> __device__ __forceinline__ float atan_r<float>(float v) { return dba_atanf(v); }
 
 // explicitly rounded operations, so every kernel that advances dendrite cells
 // through den_p_new / den_T_new produces the same bits (in FP64 they equal the
@@ -46,7 +46,14 @@ __device__ __forceinline__ float ds(float a, float b) { return __fsub_rn(a, b); 
 __device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float dm(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ float dd(float a, float b) { return __fdiv_rn(a, b); }
+// FP32 divides with div.approx (a times the approximate reciprocal of b, within
+// 2 ulp), as the FP32 KH kernels do; FP64 keeps IEEE rounding
+__device__ __forceinline__ float dd(float a, float b)
+{
+    float r;
+    asm("div.approx.ftz.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
 __device__ __forceinline__ double dd(double a, double b) { return __ddiv_rn(a, b); }
 
 // Evolve_p (example_Dendritic_growth/kernel.cu:220-241) for one cell from its

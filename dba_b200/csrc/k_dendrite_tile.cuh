@@ -149,6 +149,32 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
 #pragma unroll
         for (int k = 0; k < TBX; ++k)
             if ((am >> k) & 1u) need |= 0xfu << (2 * k);
+        if (X0 > 0 && X0 + TX < g.nx && Y0 > 0 && Y0 + B < g.ny && Z0 > 0 && Z0 + B < g.nz) {
+            // No staged cell wraps or meets a wall: thread t < 200 copies piece column
+            // c4 = t % 10 of staged row y = (t / 10) % 10 in planes z = t / 100 + 2j,
+            // j = 0..4, so its shared offsets are 4t + 800j and its source offsets step
+            // by two planes; the lanes of a warp cover consecutive pieces of 3.2 rows.
+            static_assert(SP == SW && PL == SR * SP && SR % 2 == 0 && 2 * SR * (SW / 4) <= NT,
+                          "piece (c4, y, z) at shared offset 4 (c4 + 10 y + 100 z)");
+            if (tid < 2 * SR * (SW / 4)) {
+                const int c4 = tid % (SW / 4), ry = (tid / (SW / 4)) % SR, rzb = tid / (SR * (SW / 4));
+                if ((need >> c4) & 1u) {
+                    const int rxy = (4 * c4 - 4 + B) / B + RX * ((ry - 1 + B) / B);
+                    const long long o0 = (long long)(X0 + 4 * c4 - 4) +
+                                         (long long)nx * ((long long)(Y0 + ry - 1) + (long long)g.ny * (Z0 + rzb - 1));
+#pragma unroll
+                    for (int j = 0; j < SR / 2; ++j) {
+                        const int reg = rxy + RX * 3 * (j == 0 ? rzb : (j == SR / 2 - 1 ? 1 + rzb : 1));
+                        const long long o = o0 + (long long)(2 * j) * (long long)nxy;
+                        float* d = dst + 4 * tid + 2 * PL * j;
+                        cp_async16(d, (s_par[st][0][reg] ? P.p[1] : P.p[0]) + o);
+                        cp_async16(d + SV, (s_par[st][1][reg] ? P.T[1] : P.T[0]) + o);
+                    }
+                }
+            }
+            cp_async_commit();
+            return;
+        }
         for (int q = tid; q < NQ; q += NT) {
             const int c4 = q % (SW / 4), ry = (q / (SW / 4)) % SR, rz = q / ((SW / 4) * SR);
             if (!((need >> c4) & 1u)) continue;

@@ -756,8 +756,9 @@ double oracle_tree_sum(const double* v, long n)
 {
     return dba_tree_sum(std::vector<double>(v, v + n));
 }
-double oracle_fm(int which, double x)   // 0 exp, 1 log, 2 atan (the shared fpmath functions)
+double oracle_fm(int which, double x)   // 0 exp, 1 log, 2 atan, 3 FP32 atan (the shared fpmath functions)
 {
+    if (which == 3) return (double)dba_atanf((float)x);
     return which == 0 ? dba_exp(x) : which == 1 ? dba_log(x) : dba_atan(x);
 }
 

@@ -1,5 +1,6 @@
 """The shared FP64 atan/log/exp (dba_b200/csrc/fpmath.h) against mpmath: <= 2.5 ulp,
-C99 special values.  Run through the CPU build of the same header."""
+C99 special values; the FP32 atan of the FP32 dendrite kernels: <= 1.5 ulp with a
+correctly rounded reciprocal.  Run through the CPU build of the same header."""
 import math
 import random
 
@@ -51,6 +52,30 @@ def test_special_values():
     assert L.oracle_fm(2, math.inf) == pytest.approx(math.pi / 2, rel=0, abs=1e-16)
     assert L.oracle_fm(2, -math.inf) == pytest.approx(-math.pi / 2, rel=0, abs=1e-16)
     assert L.oracle_fm(2, 1.0) == pytest.approx(math.pi / 4, rel=2e-16)
+
+
+def test_fp32_atan_ulp_error():
+    """dba_atanf on every float of a dense sample of [0, 1] and of (1, 1e7], and on
+    random floats over the whole range, in float ulps of the exact value."""
+    rng = np.random.default_rng(7)
+    xs = np.concatenate([np.linspace(0.0, 1.0, 20001), np.geomspace(1.0, 1e7, 20001),
+                         rng.uniform(-40.0, 40.0, 4000),
+                         rng.integers(0, 0x7f800000, 4000, dtype=np.uint32).view(np.float32).astype(np.float64)])
+    xs = xs.astype(np.float32).astype(np.float64)
+    L = lib()
+    worst = 0.0
+    for x in xs:
+        y = L.oracle_fm(3, float(x))
+        assert y == float(np.float32(y))
+        t = mp.atan(mp.mpf(float(x)))
+        tf = np.float32(float(t))
+        u = float(np.spacing(np.abs(tf))) if tf != 0 else 1e-45
+        worst = max(worst, float(abs(mp.mpf(y) - t)) / u)
+    assert worst <= 1.5, worst
+    assert L.oracle_fm(3, 0.0) == 0.0
+    assert L.oracle_fm(3, math.inf) == float(np.float32(math.pi / 2))
+    assert L.oracle_fm(3, -math.inf) == -float(np.float32(math.pi / 2))
+    assert math.isnan(L.oracle_fm(3, math.nan))
 
 
 def test_halving_by_multiplication_rounds_like_division():

@@ -15,7 +15,7 @@ from cases import DENDRITE_REF, dendrite_cfg
 pytestmark = pytest.mark.gpu
 
 
-def _pair(bc, corner, shape=(64, 32, 40)):
+def _pair(bc, corner, shape=(96, 32, 40)):
     prm = dict(DENDRITE_REF, Delta=1.15, delta=0.2, metric_p=1e-3, metric_T=1e-5)
     sims = []
     for t in (1, 0):
