@@ -155,6 +155,7 @@ DenP<R> den_params(dba_ctx* c)
     P.f3 = 1. / k.tau;
     P.dt = k.dt; P.delta = k.delta; P.eps2 = k.epsilon * k.epsilon; P.gamma = k.gamma;
     P.thr_p = k.metric_p; P.thr_p_hi = 1.0 - k.metric_p; P.thr_T = k.metric_T;
+    P.c32 = den_c32(P.f0, P.f1, P.f2, P.f3, P.dt, P.delta, P.eps2, P.gamma);
     return P;
 }
 

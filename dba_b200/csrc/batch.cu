@@ -343,6 +343,7 @@ int dba_batch_add(dba_batch* b, const dba_config* k, const double* ic, int* slot
     r.f0 = 1. / (2 * k->dx); r.f1 = 1. / k->dx / k->dx; r.f2 = -k->alpha / Pi; r.f3 = 1. / k->tau;
     r.dt = k->dt; r.delta = k->delta; r.eps2 = k->epsilon * k->epsilon; r.gamma = k->gamma;
     r.thr_p = k->metric_p; r.thr_p_hi = 1.0 - k->metric_p; r.thr_T = k->metric_T;
+    r.c32 = den_c32(r.f0, r.f1, r.f2, r.f3, r.dt, r.delta, r.eps2, r.gamma);
     // initial condition into buffer 0 (parity 0): from the caller's FP64 arrays, or
     // generated on the device by the single-domain engine's dba_init rules
     if (ic) {

@@ -27,6 +27,7 @@ struct SlotRec {
     void* p[2];
     void* T[2];
     double f0, f1, f2, f3, dt, delta, eps2, gamma, thr_p, thr_p_hi, thr_T;
+    DenC32 c32;   // FP32 slots: the folded constants of den_p_f32 / den_T_f32
 };
 
 struct BatchP {
@@ -214,15 +215,23 @@ __device__ __forceinline__ void batch_step_body(const BatchP& bp, const FlagP& f
                 const R pc = sp[ti], Tc = sT[ti];
                 R pn = pc;
                 if (m & 1) {
-                    pn = den_p_new<R>(pc, Tc, sp[ti + 1], sp[ti - 1], sp[ti + E], sp[ti - E], pc, pc, f0, f1, f2, f3,
-                                      dt, (R)d.r.delta, (R)d.r.eps2, (R)d.r.gamma);
+                    if constexpr (std::is_same<R, float>::value)
+                        pn = den_p_f32<2>(pc, Tc, sp[ti + 1], sp[ti - 1], sp[ti + E], sp[ti - E], pc, pc, d.r.c32);
+                    else
+                        pn = den_p_new<R>(pc, Tc, sp[ti + 1], sp[ti - 1], sp[ti + E], sp[ti - E], pc, pc, f0, f1, f2,
+                                          f3, dt, (R)d.r.delta, (R)d.r.eps2, (R)d.r.gamma);
                     ((m & 4) ? (R*)d.r.p[0] : (R*)d.r.p[1])[gi] = pn;
                     if (pn >= (R)d.r.thr_p && pn <= (R)d.r.thr_p_hi) s_np[k] = 1;
                     if (!isfinite(pn)) raise_status(f.status, 5);
                 }
                 if (m & 2) {
-                    const R Tn = den_T_new<R, DBA>(Tc, sT[ti + 1], sT[ti - 1], sT[ti + E], sT[ti - E], Tc, Tc,
-                                                   (m & 1) != 0, pn, pc, f1, dt);
+                    R Tn;
+                    if constexpr (std::is_same<R, float>::value)
+                        Tn = den_T_f32<2, DBA>(Tc, sT[ti + 1], sT[ti - 1], sT[ti + E], sT[ti - E], Tc, Tc, (m & 1) != 0,
+                                               pn, pc, d.r.c32);
+                    else
+                        Tn = den_T_new<R, DBA>(Tc, sT[ti + 1], sT[ti - 1], sT[ti + E], sT[ti - E], Tc, Tc,
+                                               (m & 1) != 0, pn, pc, f1, dt);
                     ((m & 8) ? (R*)d.r.T[0] : (R*)d.r.T[1])[gi] = Tn;
                     if (fabs(Tn - Tc) >= (R)d.r.thr_T) s_nT[k] = 1;
                     if (!isfinite(Tn)) raise_status(f.status, 5);

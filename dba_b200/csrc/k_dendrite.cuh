@@ -19,10 +19,23 @@
 // (T + dt lapT + p_new - p, kernel.cu:289).
 #pragma once
 
+#include <type_traits>
+
 #include "fpmath.h"
 #include "k_common.cuh"
 
 namespace dba {
+
+// FP32 constants of the dendrite point formulas, folded on the host from the FP64
+// parameters (one rounding each; den_p_f32 / den_T_f32)
+struct DenC32 {
+    float ce;        // eps^2 / dx^2: weight of the raw p Laplacian (neighbour sum - 2D p)
+    float cn;        // dt / tau
+    float cT;        // dt / dx^2: weight of the raw T Laplacian
+    float g, g1, gd; // gamma; gamma (1 - delta) and gamma delta: gamma sigma = g1 + gd |n|^4_4
+    float gmin;      // the isotropy cut |grad p|^2 <= 1e-6 on raw central differences: 1e-6 (2 dx)^2
+    float f2;        // -alpha / Pi
+};
 
 template <typename R>
 struct DenP {
@@ -31,7 +44,22 @@ struct DenP {
     double f0, f1, f2, f3;   // 1/(2dx), 1/dx/dx, -alpha/Pi, 1/tau  (kernel.cu:98-101)
     double dt, delta, eps2, gamma;
     double thr_p, thr_p_hi, thr_T;   // metric_p, 1.0 - metric_p, metric_T
+    DenC32 c32;              // FP32 kernels: the folded constants
 };
+
+inline DenC32 den_c32(double f0, double f1, double f2, double f3, double dt, double delta, double eps2, double gamma)
+{
+    DenC32 c;
+    c.ce = (float)(eps2 * f1);
+    c.cn = (float)(dt * f3);
+    c.cT = (float)(dt * f1);
+    c.g = (float)gamma;
+    c.g1 = (float)(gamma * (1.0 - delta));
+    c.gd = (float)(gamma * delta);
+    c.gmin = (float)(1e-6 / (f0 * f0));
+    c.f2 = (float)f2;
+    return c;
+}
 
 template <typename R> __device__ __forceinline__ R atan_r(R v);
 template <> __device__ __forceinline__ double atan_r<double>(double v) { return dba_atan(v); }
@@ -76,6 +104,51 @@ __device__ __forceinline__ R den_p_new(R pc, R Tc, R pxp, R pxm, R pyp, R pym, R
     const R mm = dm(f2, atan_r<R>(dm(dm(gam, sigma), Tc)));
     const R pchg = dm(f3, da(dm(eps2, lapP), dm(dm(pc, ds((R)1, pc)), da(ds(pc, (R)0.5), mm))));
     return da(pc, dm(dt, pchg));
+}
+
+// FP32 form of Evolve_p (the throughput precision; errors against FP64 are stated per
+// test): the same quantities with the constants folded (DenC32) and products feeding
+// sums fused.  The central differences stay raw -- the anisotropy |n|^4_4 =
+// sum g^4 / (sum g^2)^2 is scale-free and the isotropy cut is scaled instead -- and
+// the Laplacians are raw neighbour sums minus 2D times the centre, weighted once.
+// D = 2 reads no z neighbours.  Every FP32 kernel advancing dendrite cells calls
+// these two, so they agree bit for bit.
+template <int D>
+__device__ __forceinline__ float den_p_f32(float pc, float Tc, float pxp, float pxm, float pyp, float pym, float pzp,
+                                           float pzm, const DenC32& c)
+{
+    const float gx = __fsub_rn(pxp, pxm), gy = __fsub_rn(pyp, pym);
+    const float gx2 = __fmul_rn(gx, gx), gy2 = __fmul_rn(gy, gy);
+    float lap, g2, g4;
+    if constexpr (D == 3) {
+        const float gz = __fsub_rn(pzp, pzm), gz2 = __fmul_rn(gz, gz);
+        lap = __fadd_rn(__fadd_rn(__fadd_rn(pxp, pxm), __fadd_rn(pyp, pym)), __fadd_rn(pzp, pzm));
+        lap = __fmaf_rn(-6.f, pc, lap);
+        g2 = __fadd_rn(__fadd_rn(gx2, gy2), gz2);
+        g4 = __fmaf_rn(gx2, gx2, __fmaf_rn(gy2, gy2, __fmul_rn(gz2, gz2)));
+    } else {
+        lap = __fmaf_rn(-4.f, pc, __fadd_rn(__fadd_rn(pxp, pxm), __fadd_rn(pyp, pym)));
+        g2 = __fadd_rn(gx2, gy2);
+        g4 = __fmaf_rn(gx2, gx2, __fmul_rn(gy2, gy2));
+    }
+    const float gs = g2 <= c.gmin ? c.g : __fmaf_rn(c.gd, dd(g4, __fmul_rn(g2, g2)), c.g1);
+    const float w = __fmaf_rn(c.f2, dba_atanf(__fmul_rn(gs, Tc)), __fsub_rn(pc, 0.5f));
+    const float nl = __fmul_rn(__fmul_rn(pc, __fsub_rn(1.f, pc)), w);
+    return __fmaf_rn(c.cn, __fmaf_rn(c.ce, lap, nl), pc);
+}
+
+// FP32 form of Evolve_T (below): T + dt/dx^2 (raw Laplacian), then the p change in the
+// reference's order for the mode
+template <int D, bool DBA>
+__device__ __forceinline__ float den_T_f32(float Tc, float Txp, float Txm, float Typ, float Tym, float Tzp, float Tzm,
+                                           bool p_active, float pn, float pc, const DenC32& c)
+{
+    float s = __fadd_rn(__fadd_rn(Txp, Txm), __fadd_rn(Typ, Tym));
+    if constexpr (D == 3) s = __fmaf_rn(-6.f, Tc, __fadd_rn(s, __fadd_rn(Tzp, Tzm)));
+    else s = __fmaf_rn(-4.f, Tc, s);
+    const float Tn = __fmaf_rn(c.cT, s, Tc);
+    if (DBA) return p_active ? __fadd_rn(Tn, __fsub_rn(pn, pc)) : Tn;
+    return __fsub_rn(__fadd_rn(Tn, pn), pc);
 }
 
 // Evolve_T (kernel.cu:286-289 regular, :468-489 DBA): T + dt lapT, plus the p
@@ -198,15 +271,24 @@ __global__ void __launch_bounds__(kThreads) dendrite_step(GridP g, FlagP f, DenP
                 const R pc = sp[ti], Tc = sT[ti];
                 R pn = pc;
                 if (m & 1) {   // Evolve_p (kernel.cu:220-241)
-                    pn = den_p_new<R>(pc, Tc, sp[ti + 1], sp[ti - 1], sp[ti + SY], sp[ti - SY], sp[ti + SZ], sp[ti - SZ],
-                                      f0, f1, f2, f3, dt, delta, eps2, gam);
+                    if constexpr (std::is_same<R, float>::value)
+                        pn = den_p_f32<D>(pc, Tc, sp[ti + 1], sp[ti - 1], sp[ti + SY], sp[ti - SY], sp[ti + SZ],
+                                          sp[ti - SZ], P.c32);
+                    else
+                        pn = den_p_new<R>(pc, Tc, sp[ti + 1], sp[ti - 1], sp[ti + SY], sp[ti - SY], sp[ti + SZ],
+                                          sp[ti - SZ], f0, f1, f2, f3, dt, delta, eps2, gam);
                     ((m & 4) ? P.p[0] : P.p[1])[gi] = pn;
                     if (pn >= thr_p && pn <= thr_p_hi) s_np[k] = 1;
                     if (!isfinite(pn)) raise_status(f.status, 5);
                 }
                 if (m & 2) {   // Evolve_T (kernel.cu:286-289, :468-489)
-                    const R Tn = den_T_new<R, DBA>(Tc, sT[ti + 1], sT[ti - 1], sT[ti + SY], sT[ti - SY], sT[ti + SZ],
-                                                   sT[ti - SZ], (m & 1) != 0, pn, pc, f1, dt);
+                    R Tn;
+                    if constexpr (std::is_same<R, float>::value)
+                        Tn = den_T_f32<D, DBA>(Tc, sT[ti + 1], sT[ti - 1], sT[ti + SY], sT[ti - SY], sT[ti + SZ],
+                                               sT[ti - SZ], (m & 1) != 0, pn, pc, P.c32);
+                    else
+                        Tn = den_T_new<R, DBA>(Tc, sT[ti + 1], sT[ti - 1], sT[ti + SY], sT[ti - SY], sT[ti + SZ],
+                                               sT[ti - SZ], (m & 1) != 0, pn, pc, f1, dt);
                     ((m & 8) ? P.T[0] : P.T[1])[gi] = Tn;
                     if (fabs(Tn - Tc) >= thr_T) s_nT[k] = 1;
                     if (!isfinite(Tn)) raise_status(f.status, 5);

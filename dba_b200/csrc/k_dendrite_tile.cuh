@@ -1,7 +1,7 @@
 // k_dendrite_tile.cuh -- FP32 3-D dendrite step over 32x8x8-cell tiles.
 //
 // Same DBA semantics and the same point arithmetic as dendrite_step
-// (k_dendrite.cuh; den_p_new / den_T_new fix every rounding) for 8^3 blocks,
+// (k_dendrite.cuh; den_p_f32 / den_T_f32 fix every rounding) for 8^3 blocks,
 // reorganised so that a CTA works on four x-adjacent blocks at a time:
 //
 //   * a tile is listed when any channel (p or T) of any of its blocks is
@@ -111,8 +111,8 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
     const int nb = g.nb;
     const int ntx = g.nx / TX, nty = g.ny / B;
     const size_t nx = (size_t)g.nx, nxy = (size_t)g.nx * g.ny;
-    const float f0 = (float)P.f0, f1 = (float)P.f1, f2 = (float)P.f2, f3 = (float)P.f3;
-    const float dt = (float)P.dt, delta = (float)P.delta, eps2 = (float)P.eps2, gam = (float)P.gamma;
+    const DenC32 C = P.c32;
+    const float dt = (float)P.dt;
     const float thr_p = (float)P.thr_p, thr_p_hi = (float)P.thr_p_hi, thr_T = (float)P.thr_T;
     const int kb = tid / (B * B);                 // this thread's block within the tile
     const int cx = kb * B + tid % B, cy = (tid / B) % B;   // and its column
@@ -273,15 +273,14 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
                     const size_t gi = gcol + nxy * (size_t)(Z0 + z);
                     float pn = pc;
                     if (pa) {
-                        pn = den_p_new<float>(pc, Tc, sp[si + 1], sp[si - 1], sp[si + SP], sp[si - SP], pq, pm, f0, f1,
-                                              f2, f3, dt, delta, eps2, gam);
+                        pn = den_p_f32<3>(pc, Tc, sp[si + 1], sp[si - 1], sp[si + SP], sp[si - SP], pq, pm, C);
                         pout[gi] = pn;
                         wp |= pn >= thr_p && pn <= thr_p_hi;
                         chk = __fmaf_rn(pn, zero, chk);
                     }
                     if (Ta) {
-                        const float Tn = den_T_new<float, DBA>(Tc, sT[si + 1], sT[si - 1], sT[si + SP], sT[si - SP],
-                                                               Tq, Tm, pa, pn, pc, f1, dt);
+                        const float Tn = den_T_f32<3, DBA>(Tc, sT[si + 1], sT[si - 1], sT[si + SP], sT[si - SP], Tq, Tm,
+                                                           pa, pn, pc, C);
                         Tout[gi] = Tn;
                         wT |= fabsf(Tn - Tc) >= thr_T;
                         chk = __fmaf_rn(Tn, zero, chk);
