@@ -139,7 +139,14 @@ template <typename R, int B> struct KHTile {
     static constexpr int NW = E2 * P2, NP = E1 * P1, NG = 2 * E1 * P1;
     static constexpr int NFX = T * FXW, NFY = (T + 1) * T, NU = T * T;
     static constexpr int GT = NT - 1;          // the thread that takes tiles from the queue (no phase-2 item)
-    static constexpr int NS = 4 * N1;                 // staged next-tile inputs, R elements
+    // the next tile's phase-1 inputs, staged as 16-byte pieces of PC cells: rows of the
+    // tile + 2 halo widened to whole pieces (x from -HL to T + HL - 1), each piece inside
+    // one block (B and T are multiples of PC), NPC pieces per field
+    static constexpr int PC = 16 / (int)sizeof(R);
+    static constexpr int HL = (2 + PC - 1) / PC * PC;
+    static constexpr int SW1 = T + 2 * HL;            // staged row width in cells
+    static constexpr int NPR = SW1 / PC, NPC = E2 * NPR;
+    static constexpr int NS = 4 * E2 * SW1;           // staged next-tile inputs, R elements
     static constexpr size_t smem = sizeof(R) * ((size_t)4 * (NW + NP + NG + NFX + NFY + NU) + NS);
     // DBA bookkeeping on the warps phases 3 and 4 leave idle: the wake-up scatter
     // (11 neighbours per block) from thread SC0, the ring persistence (4 (B - 1)
@@ -152,6 +159,7 @@ template <typename R, int B> struct KHTile {
     static_assert(SC0 + 11 * NBT <= NT && PR0 + NBT * NRING <= NT, "bookkeeping on idle warps");
     static_assert(B * B % 32 == 0 && T * T % 32 == 0, "a warp's update cells lie in one block");
     static_assert(GT >= N2 && GT >= SC0 + 11 * NBT && GT >= PR0 + NBT * NRING, "queue thread without phase items");
+    static_assert(B % PC == 0 && NPC <= NT && (SW1 * sizeof(R)) % 16 == 0, "one staged piece per thread, in one block");
 };
 
 // region (block of the 3x3 neighbourhood of blocks around the tile) of tile-local cell (lx, ly)
@@ -224,7 +232,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
     const QA<R> sFx{sGx.base + 4 * S::NG, S::NFX};               // [T][FXW]  flux through the face right of (x, y) at y * FXW + x + 1
     const QA<R> sFy{sFx.base + 4 * S::NFX, S::NFY};              // [T+1][T]  flux through the face above (x, y) at (y + 1) * T + x
     const QA<R> sU{sFy.base + 4 * S::NFY, S::NU};                // [T][T]    own cells' conserved fields
-    R* sStage = sU.base + 4 * S::NU;            // [4][N1] phase-1 conserved inputs of the next tile, copied ahead
+    R* sStage = sU.base + 4 * S::NU;            // [4][E2][SW1] phase-1 conserved inputs of the next tile, copied ahead
     __shared__ int s_tile[4];                   // tiles i .. i + 3 (slot i % 4): tbx | tby << 15 | halo-inside-domain << 30,
                                                 //   -1 past the end of the queue
     __shared__ unsigned s_tmeta[4];             // bits 0..15 active blocks, 16..31 their parity
@@ -265,7 +273,6 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
     const int x1 = tid % E2 - 2, y1 = tid / E2 - 2;
     const int r1 = kh_region<B, RB>(x1, y1), s1 = (y1 + 2) * P2 + x1 + 2;
     const bool in1 = x1 >= 0 && x1 < T && y1 >= 0 && y1 < T;
-    const int o1 = x1 + g.nx * y1;
     // Phases 2 and 3 take the tile's own cells on threads 0 .. T*T-1 (warps 0-7) and
     // its 1-cell ring after them (warps 8-9): with one block per tile the own cells
     // belong to the tile's active block, so warps 0-7 never take the branch that
@@ -309,9 +316,10 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
 
     // Tile i's phase-1 inputs (the conserved fields of the owning block's current
     // buffer where it is active, of its other buffer where it is not) are copied
-    // into sStage while tile i-1 computes; each thread copies and later reads only
-    // its own phase-1 cell.  Within a step nothing writes what is copied: active
-    // blocks write their other buffer, which no neighbour reads this step (a
+    // into sStage while tile i-1 computes, one 16-byte piece of each field per thread
+    // (thread t < NPC: piece t % NPR of staged row t / NPR); the copies complete before
+    // the barrier that ends tile i-1.  Within a step nothing writes what is copied:
+    // active blocks write their other buffer, which no neighbour reads this step (a
     // neighbour reads an active block's current buffer).
     auto neighbourhood = [&](int entry, int buf) {
         if (tid < RB * RB) {
@@ -336,13 +344,19 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                        : (size_t)wrap_p(t.X0 + lx, g.nx) + nx * (size_t)wrap_p(t.Y0 + ly, g.ny);
     };
     auto prefetch = [&](const TileAt& t, int buf) {
-        if (h1) {
-            const size_t gi = cell_index(t, x1, y1, o1);
-            const bool act = s_nact[buf][r1];
-            const int par = s_npar[buf][r1];
+        if (tid < S::NPC) {
+            const int ry = tid / S::NPR, c = tid - ry * S::NPR;
+            const int lx = c * S::PC - S::HL, ly = ry - 2;
+            const int r = kh_region<B, RB>(lx, ly);
+            // pieces start on multiples of PC and nx is a multiple of T, so a wrapped
+            // piece stays whole
+            const size_t gi = t.inner ? (size_t)(t.base + lx + (long long)nx * ly)
+                                      : (size_t)wrap_p(t.X0 + lx, g.nx) + nx * (size_t)wrap_p(t.Y0 + ly, g.ny);
+            const int par = s_npar[buf][r];
+            const int b = s_nact[buf][r] ? par : par ^ 1;
+            R* d = sStage + ry * S::SW1 + c * S::PC;
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                cp_async_elem<sizeof(R)>(sStage + q * S::N1 + tid, P.U[q][act ? par : par ^ 1] + gi);
+            for (int q = 0; q < 4; ++q) cp_async16(d + q * E2 * S::SW1, P.U[q][b] + gi);
         }
         cp_async_commit();
     };
@@ -372,6 +386,8 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
         neighbourhood(s_tile[0], 0);
         __syncthreads();
         prefetch(tile_at(s_tile[0]), 0);
+        cp_async_wait0();
+        __syncthreads();
     }
     for (int i = 0; s_tile[i & 3] >= 0; ++i) {
         const int cs = i & 3;
@@ -389,10 +405,10 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
         if (more) neighbourhood(s_tile[(i + 1) & 3], nb ^ 1);
 
         // 1. primitives on tile + 2, from the staged inputs
-        cp_async_wait0();
         if (h1) {
-            const R v0 = sStage[tid], v1 = sStage[S::N1 + tid], v2 = sStage[2 * S::N1 + tid],
-                    v3 = sStage[3 * S::N1 + tid];
+            const int si = (y1 + 2) * S::SW1 + x1 + S::HL;
+            const R v0 = sStage[si], v1 = sStage[E2 * S::SW1 + si], v2 = sStage[2 * E2 * S::SW1 + si],
+                    v3 = sStage[3 * E2 * S::SW1 + si];
             R r, pp, u, v;
             kh_prim_of<R>(v0, v1, v2, v3, K, r, pp, u, v);
             if (in1 && s_nact[nb][r1]) sU.put(y1 * T + x1, Q{v0, v1, v2, v3});
@@ -600,7 +616,8 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
             if (P.conserved)
                 for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = s_bsum[q][tid];
         }
-        __syncthreads();                      // shared tiles and tables reused by the next tile
+        cp_async_wait0();                     // tile i + 1's inputs (copied since phase 1)
+        __syncthreads();                      // shared tiles and tables reused by the next tile; inputs staged
     }
     if (cfl && tid == 0) atomicMax(P.gmax_cur, s_vcta);
     if (tid == GT) tile_queue_done(f);
