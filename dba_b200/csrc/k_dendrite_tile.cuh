@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
     __shared__ int s_tile[4];           // tiles i .. i + 3 (slot i % 4), -1 past the end of the queue
     __shared__ unsigned s_tmeta[4];     // bits 0-3 p-active blocks, 4-7 T-active, 8-11 p parity, 12-15 T parity
     __shared__ uint8_t s_par[2][2][NR];  // [stage][channel][neighbour block]
-    __shared__ int s_np[TBX], s_nT[TBX];
+    __shared__ int s_np[2][TBX], s_nT[2][TBX];   // wake tests of tiles with parity 0 / 1
 
     const int tid = threadIdx.x;
     const int nb = g.nb;
@@ -205,12 +205,43 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
         cp_async_commit();
     };
 
+    // Wake-up bookkeeping of tile j (tests final once its update is done), on warps 2-4
+    // after the barrier that opens tile j + 1, beside the staging of tile j + 2.  Tests:
+    auto bookkeep = [&](int j) {
+        if (!DBA) return;
+        const int js = j & 3, jp = j & 1;
+        const unsigned tm = s_tmeta[js];
+        if (tid >= WN0 && tid < WN0 + TBX) {
+            const int kt = tid_fresh() - WN0;
+            int X0, Y0, Z0;
+            tile_xyz(s_tile[js], X0, Y0, Z0);
+            const int b = (X0 / B + kt) + g.nbx * (Y0 / B + g.nby * (Z0 / B));
+            if ((tm >> kt) & 1u) f.next[b] = (uint8_t)s_np[jp][kt];
+            if ((tm >> (4 + kt)) & 1u) f.next[nb + b] = (uint8_t)s_nT[jp][kt];
+        }
+        // scatter, self + 6 faces per channel (kernel.cu:577-634), one neighbour per
+        // thread: thread WS0 + (ch * TBX + blk) * 7 + k
+        if (tid >= WS0 && tid < WS0 + 2 * TBX * 7) {
+            const int t = tid_fresh() - WS0;
+            const int k = t % 7, cb = t / 7, ch = cb / TBX, kt = cb - ch * TBX;
+            if (((tm >> (4 * ch + kt)) & 1u) && (ch ? s_nT[jp][kt] : s_np[jp][kt])) {
+                int X0, Y0, Z0;
+                tile_xyz(s_tile[js], X0, Y0, Z0);
+                const int nbk = block_nb_k(g, X0 / B + kt, Y0 / B, Z0 / B, k);
+                if (nbk >= 0) f.wake_nxt[(size_t)ch * nb + nbk] = 1;
+            }
+        }
+    };
+
     // The step's listed tiles (dendrite3_tile_scan) are taken from the tile queue by
     // thread GT, two tiles ahead: during tile i it reads the list entry of tile i + 2
     // (taken during tile i - 1) into slot (i + 2) % 4 and takes the entry for tile i + 3,
     // so neither the counter's atomic nor the list load is waited for on a barrier's
-    // path.  Slot (i + 2) % 4 held tile i - 2; tile i - 1's slot is still read by the
-    // wake-up bookkeeping meanwhile.
+    // path.  Slot (i + 2) % 4 held tile i - 2, whose bookkeeping ended before the
+    // barrier that closed tile i - 1's staging; tile i - 1's slot is read by its
+    // bookkeeping after the next barrier.  Two barriers per tile: tile i - 1's update
+    // has ended at the one that opens tile i, where its bookkeeping runs (wake tests
+    // double-buffered by tile parity), and the stage tile i + 1 refills is free there.
     const int cnt = (int)min(__ldcg(f.tctr), (unsigned)(ntx * nty * (g.nz / B)));
     int k_pend = 0;
     auto entry = [&](int k, int slot) {
@@ -233,7 +264,8 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
             __syncthreads();
             issue(0, 0);
         }
-        for (int i = 0; s_tile[i & 3] >= 0; ++i) {
+        int i = 0;
+        for (; s_tile[i & 3] >= 0; ++i) {
             const int st = i & 1, cs = i & 3, ns = (i + 1) & 3;
             const bool more = s_tile[ns] >= 0;
             if (more) build_nbr(ns, st ^ 1);
@@ -241,10 +273,11 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
                 entry(k_pend, (i + 2) & 3);
                 k_pend = (int)atomicAdd(f.tctr + 1, 1u);
             }
-            __syncthreads();                     // next table ready; stage st^1 free
+            __syncthreads();                     // next table ready; stage st^1 free; tile i - 1 done
+            if (i > 0) bookkeep(i - 1);
             if (tid < TBX) {
-                s_np[tid] = 0;
-                s_nT[tid] = 0;
+                s_np[i & 1][tid] = 0;
+                s_nT[i & 1][tid] = 0;
             }
             if (more) issue(ns, st ^ 1);
             else cp_async_commit();
@@ -266,56 +299,38 @@ __global__ void __launch_bounds__(256, 3) dendrite3_tile_step(GridP g, FlagP f, 
                 // the zero comes from a kernel parameter, so it cannot be folded away
                 const float zero = __fmul_rn(dt, 0.f);
                 float chk = zero;
-                const size_t gcol = (size_t)(X0 + cx) + nx * (size_t)(Y0 + cy);
+                const size_t g0 = (size_t)(X0 + cx) + nx * ((size_t)(Y0 + cy) + (size_t)g.ny * Z0);
+                float* po = pout + g0;
+                float* to = Tout + g0;
 #pragma unroll 2
                 for (int z = 0; z < B; ++z) {
                     const float pq = sp[si + PL], Tq = sT[si + PL];
-                    const size_t gi = gcol + nxy * (size_t)(Z0 + z);
                     float pn = pc;
                     if (pa) {
                         pn = den_p_f32<3>(pc, Tc, sp[si + 1], sp[si - 1], sp[si + SP], sp[si - SP], pq, pm, C);
-                        pout[gi] = pn;
+                        *po = pn;
                         wp |= pn >= thr_p && pn <= thr_p_hi;
                         chk = __fmaf_rn(pn, zero, chk);
                     }
                     if (Ta) {
                         const float Tn = den_T_f32<3, DBA>(Tc, sT[si + 1], sT[si - 1], sT[si + SP], sT[si - SP], Tq, Tm,
                                                            pa, pn, pc, C);
-                        Tout[gi] = Tn;
+                        *to = Tn;
                         wT |= fabsf(Tn - Tc) >= thr_T;
                         chk = __fmaf_rn(Tn, zero, chk);
                     }
                     pm = pc; pc = pq; Tm = Tc; Tc = Tq;
                     si += PL;
+                    po += nxy;
+                    to += nxy;
                 }
                 if (!(chk == 0.f)) raise_status(f.status, 5);
-                if (DBA && wp) s_np[kb] = 1;
-                if (DBA && wT) s_nT[kb] = 1;
-            }
-            __syncthreads();
-            // The wake-up bookkeeping runs on warps 2-4, beside the next tile's neighbour
-            // table (threads below NR) and before the barrier that follows it.  Tests:
-            if (DBA && tid >= WN0 && tid < WN0 + TBX) {
-                const int kt = tid_fresh() - WN0;
-                int X0, Y0, Z0;
-                tile_xyz(s_tile[cs], X0, Y0, Z0);
-                const int b = (X0 / B + kt) + g.nbx * (Y0 / B + g.nby * (Z0 / B));
-                if ((tm >> kt) & 1u) f.next[b] = (uint8_t)s_np[kt];
-                if ((tm >> (4 + kt)) & 1u) f.next[nb + b] = (uint8_t)s_nT[kt];
-            }
-            // scatter, self + 6 faces per channel (kernel.cu:577-634), one neighbour per
-            // thread: thread WS0 + (ch * TBX + blk) * 7 + k
-            if (DBA && tid >= WS0 && tid < WS0 + 2 * TBX * 7) {
-                const int t = tid_fresh() - WS0;
-                const int k = t % 7, cb = t / 7, ch = cb / TBX, kt = cb - ch * TBX;
-                if (((tm >> (4 * ch + kt)) & 1u) && (ch ? s_nT[kt] : s_np[kt])) {
-                    int X0, Y0, Z0;
-                    tile_xyz(s_tile[cs], X0, Y0, Z0);
-                    const int nbk = block_nb_k(g, X0 / B + kt, Y0 / B, Z0 / B, k);
-                    if (nbk >= 0) f.wake_nxt[(size_t)ch * nb + nbk] = 1;
-                }
+                if (DBA && wp) s_np[i & 1][kb] = 1;
+                if (DBA && wT) s_nT[i & 1][kb] = 1;
             }
         }
+        __syncthreads();                         // the last tile's wake tests complete
+        if (i > 0) bookkeep(i - 1);
     if (tid == GT) tile_queue_done(f);
 }
 
