@@ -147,7 +147,7 @@ template <typename R, int B> struct KHTile {
     static constexpr int SW1 = T + 2 * HL;            // staged row width in cells
     static constexpr int NPR = SW1 / PC, NPC = E2 * NPR;
     static constexpr int NS = 4 * E2 * SW1;           // staged next-tile inputs, R elements
-    static constexpr size_t smem = sizeof(R) * ((size_t)4 * (NW + NP + NG + NFX + NFY + NU) + NS);
+    static constexpr size_t smem = sizeof(R) * ((size_t)4 * (NW + NP + NG + NFX + NFY + 2 * NU) + NS);
     // DBA bookkeeping on the warps phases 3 and 4 leave idle: the wake-up scatter
     // (11 neighbours per block) from thread SC0, the ring persistence (4 (B - 1)
     // cells per block) from thread PR0
@@ -231,16 +231,18 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
     const QA<R> sGy{sGx.base + 4 * E1 * P1, E1 * P1};            // [E1][P1]  y gradients
     const QA<R> sFx{sGx.base + 4 * S::NG, S::NFX};               // [T][FXW]  flux through the face right of (x, y) at y * FXW + x + 1
     const QA<R> sFy{sFx.base + 4 * S::NFX, S::NFY};              // [T+1][T]  flux through the face above (x, y) at (y + 1) * T + x
-    const QA<R> sU{sFy.base + 4 * S::NFY, S::NU};                // [T][T]    own cells' conserved fields
-    R* sStage = sU.base + 4 * S::NU;            // [4][E2][SW1] phase-1 conserved inputs of the next tile, copied ahead
+    // [2][T][T] own cells' conserved fields, by tile parity (tile i + 1's phase 1 may run
+    // while tile i's update still reads its own): cell u of parity p at p * NU + u
+    const QA<R> sU{sFy.base + 4 * S::NFY, 2 * S::NU};
+    R* sStage = sU.base + 8 * S::NU;            // [4][E2][SW1] phase-1 conserved inputs of the next tile, copied ahead
     __shared__ int s_tile[4];                   // tiles i .. i + 3 (slot i % 4): tbx | tby << 15 | halo-inside-domain << 30,
                                                 //   -1 past the end of the queue
     __shared__ unsigned s_tmeta[4];             // bits 0..15 active blocks, 16..31 their parity
     __shared__ uint8_t s_npar[2][RB * RB], s_nact[2][RB * RB];   // neighbourhood of this tile and the next
-    __shared__ int s_nx[NBT];
+    __shared__ int s_nx[2][NBT];                // wake tests of the tiles with parity 0 / 1
     __shared__ double s_run[4][NT / 32];
     __shared__ double s_bsum[4][NBT];
-    __shared__ unsigned s_vblk[NBT];            // this tile's blocks' largest speed (float bits)
+    __shared__ unsigned s_vblk[2][NBT];         // the blocks' largest speed (float bits), by tile parity
     __shared__ unsigned s_vcta;                 // this CTA's largest speed over its blocks
     __shared__ R s_hdt, s_dtdx;                 // the step's dt-dependent constants
 
@@ -360,6 +362,24 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
         }
         cp_async_commit();
     };
+    // Per-block results of tile j once its update has ended (after the barrier that
+    // follows the next tile's phase 1, or after the loop): the blocks' largest signal
+    // speeds and the conserved change sums, written by one thread per block.  Two
+    // barriers fewer per tile than writing them at the end of tile j.
+    auto tile_end = [&](int j) {
+        const unsigned tmj = s_tmeta[j & 3];
+        if (tid < NBT && ((tmj >> tid) & 1u)) {
+            const int te = s_tile[j & 3];
+            const int bx = (te & 0x7fff) * TB + tid % TB, by = ((te >> 15) & 0x7fff) * TB + tid / TB;
+            const int b = bx + g.nbx * by;
+            if (cfl) {
+                P.vmax[b] = __uint_as_float(s_vblk[j & 1][tid]);
+                atomicMax(&s_vcta, s_vblk[j & 1][tid]);
+            }
+            if (P.conserved)
+                for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = s_bsum[q][tid];
+        }
+    };
     // The step's listed tiles (kh_tile_scan) are taken from the tile queue by thread GT,
     // two tiles ahead: during phase 2 of tile i (GT has no phase-2 item) it reads the
     // list entry of tile i + 2, taken during tile i - 1, into slot (i + 2) % 4 and takes
@@ -389,18 +409,19 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
         cp_async_wait0();
         __syncthreads();
     }
-    for (int i = 0; s_tile[i & 3] >= 0; ++i) {
+    int i = 0;
+    for (; s_tile[i & 3] >= 0; ++i) {
         const int cs = i & 3;
         const bool more = s_tile[(i + 1) & 3] >= 0;
         const int entry = s_tile[cs];
         const unsigned tm = s_tmeta[cs];
         const int nb = i & 1;                 // this tile's neighbourhood tables
         const TileAt cur = tile_at(entry);
-        const int tbx = entry & 0x7fff, tby = (entry >> 15) & 0x7fff;
         const long long base = cur.base;
+        const int tp = i & 1;                 // this tile's wake tests, speeds and own fields
         if (tid < NBT) {
-            s_nx[tid] = 0;
-            s_vblk[tid] = 0u;
+            s_nx[tp][tid] = 0;
+            s_vblk[tp][tid] = 0u;
         }
         if (more) neighbourhood(s_tile[(i + 1) & 3], nb ^ 1);
 
@@ -411,10 +432,11 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                     v3 = sStage[3 * E2 * S::SW1 + si];
             R r, pp, u, v;
             kh_prim_of<R>(v0, v1, v2, v3, K, r, pp, u, v);
-            if (in1 && s_nact[nb][r1]) sU.put(y1 * T + x1, Q{v0, v1, v2, v3});
+            if (in1 && s_nact[nb][r1]) sU.put(tp * S::NU + y1 * T + x1, Q{v0, v1, v2, v3});
             sW.put(s1, Q{r, pp, u, v});
         }
-        __syncthreads();
+        __syncthreads();                      // primitives staged; tile i - 1 updated
+        if (i > 0) tile_end(i - 1);
         if (more) prefetch(tile_at(s_tile[(i + 1) & 3]), nb ^ 1);
 
         // 2. gradients and half-step states on tile + 1; wake-up metric of own cells
@@ -431,7 +453,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                 sP.put(p2, Q{rp, ppp, up, vp});
                 sGx.put(p2, Q{gr[0], gr[2], gr[4], gr[6]});
                 sGy.put(p2, Q{gr[1], gr[3], gr[5], gr[7]});
-                if (DBA && nx2 >= 0 && kh_metric<R>(gr) > (R)P.thr) s_nx[nx2] = 1;
+                if (DBA && nx2 >= 0 && kh_metric<R>(gr) > (R)P.thr) s_nx[tp][nx2] = 1;
             } else {
                 // A face's flux is computed by its owner (the cell left of an x face, below a
                 // y face) when that owner is active; an inactive cell is therefore read only
@@ -499,11 +521,12 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
             const int te = s_tile[i & 3];
             if ((s_tmeta[i & 3] >> kt) & 1u) {
                 const int nbk = block_nb_k(g, (te & 0x7fff) * TB + kt % TB, ((te >> 15) & 0x7fff) * TB + kt / TB, 0, k);
-                if (k == 0) f.next[nbk] = (uint8_t)s_nx[kt];
-                if (s_nx[kt] && nbk >= 0) f.wake_nxt[nbk] = 1;
+                if (k == 0) f.next[nbk] = (uint8_t)s_nx[tp][kt];
+                if (s_nx[tp][kt] && nbk >= 0) f.wake_nxt[nbk] = 1;
             }
         }
-        __syncthreads();
+        cp_async_wait0();                     // tile i + 1's inputs (copied since phase 1)
+        __syncthreads();                      // fluxes complete; tile i + 1's inputs staged
 
         // 4. update of own active cells; ring persistence for blocks that may sleep
         const bool own = h4 && ((tm >> ukb) & 1u);
@@ -515,7 +538,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
             // fluxes (Mass, Energy, Momx, Momy) through the right, left, upper and lower faces
             const Q fr = sFx(uy * FXW + ux + 1), fl = sFx(uy * FXW + ux);
             const Q fu = sFy((uy + 1) * T + ux), fd = sFy(uy * T + ux);
-            const Q u0 = sU(ui);
+            const Q u0 = sU(tp * S::NU + ui);
             const R c[4] = {kh_change<R>(K.dtdx, fr.a, fl.a, fu.a, fd.a), kh_change<R>(K.dtdx, fr.c, fl.c, fu.c, fd.c),
                             kh_change<R>(K.dtdx, fr.d, fl.d, fu.d, fd.d), kh_change<R>(K.dtdx, fr.b, fl.b, fu.b, fd.b)};
             const Q un{ka(u0.a, c[0]), ka(u0.b, c[1]), ka(u0.c, c[2]), ka(u0.d, c[3])};   // Mass Momx Momy Energy
@@ -541,7 +564,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
                 unsigned v = __float_as_uint(kh_speed<R>(r, pp, uu, vv, K.gam));
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
-                if ((tid & 31) == 0) atomicMax(&s_vblk[ukb], v);
+                if ((tid & 31) == 0) atomicMax(&s_vblk[tp][ukb], v);
             }
         } else if (DBA && tid >= S::PR0 && tid < S::PR0 + NBT * S::NRING) {
             // ring persistence on the idle warps, from the shared tiles: ring cell e of
@@ -553,7 +576,7 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
             const int t = tid_fresh() - S::PR0;
             const int kt = t / S::NRING, e = t - kt * S::NRING;
             const int te = s_tile[i & 3];
-            if (((s_tmeta[i & 3] >> kt) & 1u) && !s_nx[kt]) {
+            if (((s_tmeta[i & 3] >> kt) & 1u) && !s_nx[tp][kt]) {
                 const int bxl = e < B ? e : (e < 2 * B ? e - B : (e < 3 * B - 2 ? 0 : B - 1));
                 const int byl = e < B ? 0 : (e < 2 * B ? B - 1 : (e < 3 * B - 2 ? e - 2 * B + 1 : e - 3 * B + 3));
                 const int px = (kt % TB) * B + bxl, py = (kt / TB) * B + byl;
@@ -603,22 +626,11 @@ __global__ void __launch_bounds__(KHTile<R, B>::NT, KHTile<R, B>::MINB) kh_tile_
             block_tree_sums<V, 1>(ce, s_run[1], s_bsum[1], 0);
             block_tree_sums<V, 1>(cx, s_run[2], s_bsum[2], 0);
             block_tree_sums<V, 1>(cy, s_run[3], s_bsum[3], 0);
-            __syncthreads();
         }
-        if (cfl) __syncthreads();
-        if (tid < NBT && ((tm >> tid) & 1u)) {
-            const int bx = tbx * TB + tid % TB, by = tby * TB + tid / TB;
-            const int b = bx + g.nbx * by;
-            if (cfl) {
-                P.vmax[b] = __uint_as_float(s_vblk[tid]);
-                atomicMax(&s_vcta, s_vblk[tid]);
-            }
-            if (P.conserved)
-                for (int q = 0; q < 4; ++q) f.bsum[(size_t)q * g.nb + b] = s_bsum[q][tid];
-        }
-        cp_async_wait0();                     // tile i + 1's inputs (copied since phase 1)
-        __syncthreads();                      // shared tiles and tables reused by the next tile; inputs staged
     }
+    __syncthreads();                          // the last tile updated
+    if (i > 0) tile_end(i - 1);
+    __syncthreads();
     if (cfl && tid == 0) atomicMax(P.gmax_cur, s_vcta);
     if (tid == GT) tile_queue_done(f);
 }
