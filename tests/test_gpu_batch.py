@@ -33,6 +33,25 @@ def test_batch_slot_fp64_bitexact_vs_oracle(B, bc):
     b.sync()
 
 
+@pytest.mark.parametrize("bc", [0, 1])
+def test_batch_slot_fp32_equals_single_simulation(bc):
+    """The FP32 batch kernel and the single-simulation FP32 kernel evaluate the same
+    explicitly rounded point formulas (den_p_f32 / den_T_f32), so a slot of an FP32
+    batch holds the same bits as the same simulation advanced on its own, step after
+    step, periodic and zero-flux (several slots share the batch)."""
+    b = dba_b200.Batch(precision=1, block=8, max_slots=4, block_capacity=4096, cell_capacity=1 << 16)
+    b.add(dendrite_cfg(dict(DENDRITE_REF, Delta=0.6), 32, 48, 1, 8, precision=1, bc=1))
+    s = b.add(dendrite_cfg(DENDRITE_REF, 64, 64, 1, 8, precision=1, bc=bc))
+    sim = dba_b200.Simulation(dendrite_cfg(DENDRITE_REF, 64, 64, 1, 8, precision=1, bc=bc)).init()
+    for n in (1, 19, 20, 120):
+        b.step(n)
+        sim.step(n, 1)
+        assert np.array_equal(b.field(s, "p"), sim.field("p")), n
+        assert np.array_equal(b.field(s, "T"), sim.field("T")), n
+    b.sync()
+    sim.sync()
+
+
 def _req(edge, u, eps4, i=0):
     return dict(id=i, t_arrive=0.0, edge=edge, u=u, eps4=eps4, delta_offset=0.6)
 
